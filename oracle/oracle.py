@@ -1,0 +1,282 @@
+"""ORACLE — test infrastructure only.
+
+CPU restatement of the reference (JeffreyEarly/spectral-kernel-benchmarks)
+arithmetic on the spectral hot path.  Only tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline / reference legs import this module, and only as the
+checker or the timed CPU baseline: the CUDA provider never calls it.
+
+Small exact pieces (retained modes, K^2 groups, FNV order hashes, fixtures with
+the mt19937_64 + normal_distribution generator, the O(N^4) direct DFTs) live in
+oracle/skb_oracle.cpp (liboracle.so).  Full-size transforms use numpy's
+pocketfft in float64, mapped to the reference's WVM frequency-major layout;
+they are pinned to the direct DFT by tests/test_oracle_pins.py.
+
+Layouts (all follow include/skbench/skbench.hpp and src/model.cpp:219-244):
+  real        [field][z][y][x]                      (x fastest)
+  wvm         [ky][kx][field][z]                    (plane = z + nz*field fastest)
+  retained    [mode][field][z]                      (z fastest)
+  modal       [mode][field][j]                      (j fastest)
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def library():
+    """Load liboracle.so, building it with the oracle Makefile when absent."""
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+        lib = ctypes.CDLL(path)
+        lib.oracle_last_error.restype = ctypes.c_char_p
+        _LIB = lib
+    return _LIB
+
+
+def _p(array):
+    return array.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError(library().oracle_last_error().decode())
+
+
+U64 = ctypes.c_uint64
+
+
+@dataclass(frozen=True)
+class Workload:
+    """skbench.hpp:23-39 Workload; lx = ly = 1 and antialias on, as every profile."""
+    nx: int
+    ny: int
+    nz: int
+    fields: int
+
+    @property
+    def planes(self):
+        return self.nz * self.fields
+
+    @property
+    def nx_half(self):
+        return self.nx // 2 + 1
+
+    @property
+    def nj(self):
+        """model.cpp:124-127: floor(2*(Nz-1)/3)."""
+        return 0 if self.nz < 2 else 2 * (self.nz - 1) // 3
+
+
+@dataclass
+class Modes:
+    k: np.ndarray
+    l: np.ndarray
+    kx: np.ndarray
+    ky: np.ndarray
+    conj: np.ndarray
+    radial: np.ndarray
+
+    def __len__(self):
+        return len(self.k)
+
+
+def retained_modes(nx, ny):
+    """model.cpp:129-167 radial 2/3 retained modes (see skb_oracle.cpp)."""
+    cap = nx * (nx // 2 + 1) + ny
+    k = np.zeros(cap, np.int64)
+    l = np.zeros(cap, np.int64)
+    kx = np.zeros(cap, np.uint64)
+    ky = np.zeros(cap, np.uint64)
+    conj = np.zeros(cap, np.uint8)
+    radial = np.zeros(cap)
+    count = U64()
+    _check(library().oracle_retained_modes(U64(nx), U64(ny), ctypes.c_double(1.0), ctypes.c_double(1.0),
+                                           ctypes.c_int(1), _p(k), _p(l), _p(kx), _p(ky), _p(conj), _p(radial),
+                                           U64(cap), ctypes.byref(count)))
+    n = count.value
+    return Modes(k[:n].copy(), l[:n].copy(), kx[:n].astype(np.int64), ky[:n].astype(np.int64),
+                 conj[:n].astype(bool), radial[:n].copy())
+
+
+def k2_groups(nx, ny):
+    """model.cpp:169-207: (keys, first, counts) of the contiguous K^2 groups."""
+    cap = nx * (nx // 2 + 1) + ny
+    keys = np.zeros(cap, np.uint64)
+    first = np.zeros(cap, np.uint64)
+    counts = np.zeros(cap, np.uint64)
+    count = U64()
+    _check(library().oracle_groups(U64(nx), U64(ny), _p(keys), _p(first), _p(counts), U64(cap), ctypes.byref(count)))
+    n = count.value
+    return keys[:n].copy(), first[:n].astype(np.int64), counts[:n].astype(np.int64)
+
+
+def hashes(w: Workload):
+    """(retained mode order, K^2 group order, WVM full-spectrum order) FNV-1a hashes."""
+    bufs = [ctypes.create_string_buffer(64) for _ in range(3)]
+    _check(library().oracle_hashes(U64(w.nx), U64(w.ny), U64(w.nz), U64(w.fields), *bufs))
+    return tuple(b.value.decode() for b in bufs)
+
+
+FIXTURES = ("impulse", "sinusoid", "random", "dc", "nyquist")
+
+
+def make_fixture(w: Workload, kind, seed):
+    """model.cpp:618-661 makeFixture -> real[field][z][y][x]."""
+    kind_index = FIXTURES.index(kind) if isinstance(kind, str) else int(kind)
+    out = np.zeros(w.nx * w.ny * w.planes)
+    _check(library().oracle_make_fixture(U64(w.nx), U64(w.ny), U64(w.nz), U64(w.fields), ctypes.c_int(kind_index),
+                                         U64(seed), _p(out)))
+    return out
+
+
+def flux_inputs(modes: Modes, fields, nj, seed):
+    """benchmark.cpp:4045-4058 modal inputs [mode][field][j] (complex128)."""
+    out = np.zeros(2 * len(modes) * fields * nj)
+    k = np.ascontiguousarray(modes.k)
+    l = np.ascontiguousarray(modes.l)
+    _check(library().oracle_flux_inputs(_p(k), _p(l), U64(len(modes)), U64(fields), U64(nj), U64(seed), _p(out)))
+    return out.view(np.complex128)
+
+
+def direct_r2c(w: Workload, real):
+    """model.cpp:663-684 direct DFT -> WVM spectrum (complex128, flat)."""
+    out = np.zeros(2 * w.ny * w.nx_half * w.planes)
+    real = np.ascontiguousarray(real, dtype=np.float64)
+    _check(library().oracle_direct_r2c(U64(w.nx), U64(w.ny), U64(w.planes), _p(real), _p(out)))
+    return out.view(np.complex128)
+
+
+def direct_c2r(w: Workload, wvm):
+    """model.cpp:686-716 direct inverse DFT (unnormalised) -> real."""
+    out = np.zeros(w.nx * w.ny * w.planes)
+    spec = np.ascontiguousarray(wvm, dtype=np.complex128).view(np.float64)
+    _check(library().oracle_direct_c2r(U64(w.nx), U64(w.ny), U64(w.planes), _p(spec), _p(out)))
+    return out
+
+
+def fft_r2c(w: Workload, real):
+    """FFTWProvider::forward (fftw_provider.cpp:537-572) restated with pocketfft:
+    unnormalised 2-D r2c of every plane, written frequency-major (WVM)."""
+    planes = np.asarray(real, dtype=np.float64).reshape(w.planes, w.ny, w.nx)
+    spec = np.fft.rfft2(planes, axes=(1, 2))  # [plane][ky][kx]
+    return np.ascontiguousarray(spec.transpose(1, 2, 0)).reshape(-1)
+
+
+def fft_c2r(w: Workload, wvm):
+    """FFTWProvider::inverse (fftw_provider.cpp:574-610): unnormalised c2r with
+    FFTW's half-spectrum semantics (columns c2c, then rows c2r; the imaginary
+    parts of the kx = 0 and kx = Nx/2 bins of each row are ignored)."""
+    spec = np.asarray(wvm, dtype=np.complex128).reshape(w.ny, w.nx_half, w.planes).transpose(2, 0, 1)
+    real = np.fft.irfft2(spec, s=(w.ny, w.nx), axes=(1, 2), norm="forward")
+    return np.ascontiguousarray(real).reshape(-1)
+
+
+def gather_retained(w: Workload, modes: Modes, wvm, scale=1.0):
+    """model.cpp:310-321 gatherRetained -> retained [mode][plane]."""
+    spec = np.asarray(wvm).reshape(w.ny, w.nx_half, w.planes)
+    vals = spec[modes.ky, modes.kx, :]
+    vals = np.where(modes.conj[:, None], np.conj(vals), vals)
+    return (scale * vals).reshape(-1)
+
+
+def embed_retained(w: Workload, modes: Modes, retained):
+    """model.cpp:323-339 embedRetained: zero-fill, scatter, kx = 0 Hermitian partner."""
+    comp = np.asarray(retained).reshape(len(modes), w.planes)
+    stored = np.where(modes.conj[:, None], np.conj(comp), comp)
+    spec = np.zeros((w.ny, w.nx_half, w.planes), np.complex128)
+    spec[modes.ky, modes.kx, :] = stored
+    rep = (modes.kx == 0) & (modes.ky != 0) & (2 * modes.ky != w.ny)
+    spec[(w.ny - modes.ky[rep]) % w.ny, 0, :] = np.conj(stored[rep])
+    return spec.reshape(-1)
+
+
+def k2_family(w: Workload):
+    """model.cpp:523-565 squaredWavenumberVerticalFixture: (forward[g][j][z], inverse[g][z][j])."""
+    keys, _, _ = k2_groups(w.nx, w.ny)
+    nj, nz = w.nj, w.nz
+    fwd = np.zeros(len(keys) * nj * nz)
+    inv = np.zeros(len(keys) * nj * nz)
+    keys = np.ascontiguousarray(keys)
+    _check(library().oracle_k2_vertical_family(U64(nz), U64(nj), _p(keys), U64(len(keys)), _p(fwd), _p(inv)))
+    return fwd.reshape(len(keys), nj, nz), inv.reshape(len(keys), nz, nj)
+
+
+def grouped_vertical(w: Workload, family, direction, data):
+    """Per-group vertical projection (model.cpp:567-605 applied per K^2 group, as
+    VerticalGemmProvider does, vertical_gemm.cpp:534-596).  forward: retained
+    [mode][field][z] -> modal [mode][field][j]; inverse the reverse."""
+    fwd, inv = family
+    _, first, counts = k2_groups(w.nx, w.ny)
+    rows_in, rows_out, mats = (w.nz, w.nj, fwd) if direction == "forward" else (w.nj, w.nz, inv)
+    H = int(first[-1] + counts[-1])
+    x = np.asarray(data, dtype=np.complex128).reshape(H * w.fields, rows_in)
+    out = np.empty((H * w.fields, rows_out), np.complex128)
+    for g, (f0, c) in enumerate(zip(first, counts)):
+        a, b = f0 * w.fields, (f0 + c) * w.fields
+        out[a:b] = x[a:b] @ mats[g].T
+    return out.reshape(-1)
+
+
+def pointwise(volume, scale, shared, derivative, workers=1):
+    """pointwise_advection.cpp:143-147: -scale*(u*qx + v*qy + w*qz)."""
+    shared = np.ascontiguousarray(shared, dtype=np.float64)
+    derivative = np.ascontiguousarray(derivative, dtype=np.float64)
+    out = np.empty(volume)
+    _check(library().oracle_pointwise(U64(volume), ctypes.c_double(scale), _p(shared), _p(derivative), _p(out),
+                                      U64(workers)))
+    return out
+
+
+def flux(n, nz, modal_in, targets=4, family=None, modes=None):
+    """The 15 -> 4 streamed flux of runProductionLifetimeFluxBenchmark
+    (benchmark.cpp:4182-4241 oracle order, 4405-4424 executeAll): inverse
+    vertical GEMM of all input fields, inverse horizontal of [U,V,W] once, then per
+    target the inverse of its derivative triple, pointwise advection with
+    scale 1/(Nx*Ny)^2, forward horizontal + retention, and finally the forward
+    vertical GEMM of the targets.  ``targets`` = 3 gives the 12 -> 3 variant.
+    Returns modal [mode][target][j]."""
+    fields_in = 3 + 3 * targets
+    w_in = Workload(n, n, nz, fields_in)
+    w_out = Workload(n, n, nz, targets)
+    w3 = Workload(n, n, nz, 3)
+    w1 = Workload(n, n, nz, 1)
+    modes = modes or retained_modes(n, n)
+    family = family or k2_family(w_out)
+    H = len(modes)
+    phys = grouped_vertical(w_in, family, "inverse", modal_in).reshape(H, fields_in, nz)
+    scale = 1.0 / float((n * n) ** 2)
+    shared = fft_c2r(w3, embed_retained(w3, modes, phys[:, 0:3, :].reshape(-1)))
+    phys_out = np.empty((H, targets, nz), np.complex128)
+    for t in range(targets):
+        trip = phys[:, 3 + 3 * t:6 + 3 * t, :].reshape(-1)
+        deriv = fft_c2r(w3, embed_retained(w3, modes, trip))
+        target = pointwise(n * n * nz, scale, shared, deriv)
+        phys_out[:, t, :] = gather_retained(w1, modes, fft_r2c(w1, target)).reshape(H, nz)
+    return grouped_vertical(w_out, family, "forward", phys_out.reshape(-1))
+
+
+def max_rel_error(actual, expected):
+    """model.cpp:718-726: max |a-b| / max(1, max |b|)."""
+    a = np.asarray(actual).reshape(-1)
+    b = np.asarray(expected).reshape(-1)
+    return float(np.max(np.abs(a - b), initial=0.0) / max(1.0, float(np.max(np.abs(b), initial=0.0))))
+
+
+def rel_l2_error(actual, expected):
+    """model.cpp:738-751: ||a-b||_2 / ||b||_2 (absolute when ||b|| = 0)."""
+    a = np.asarray(actual, dtype=np.complex128).reshape(-1)
+    b = np.asarray(expected, dtype=np.complex128).reshape(-1)
+    num = float(np.sum(np.abs(a - b) ** 2))
+    den = float(np.sum(np.abs(b) ** 2))
+    return float(np.sqrt(num if den == 0.0 else num / den))

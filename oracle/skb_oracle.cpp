@@ -1,0 +1,400 @@
+// ORACLE — test infrastructure only.  A CPU restatement of the reference
+// (JeffreyEarly/spectral-kernel-benchmarks) arithmetic for the spectral hot
+// path, used by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
+// leg as the checker.  The CUDA provider never links, loads or calls it.
+//
+// Parity pinning: tests/test_oracle_pins.py checks every function here against
+// the reference's known answers (mode counts, group counts, FNV order hashes)
+// and against golden vectors produced by the reference's own compiled sources
+// (tests/golden/make_golden.py, oracle/_ref).
+//
+// All entry points are extern "C" with plain pointers; complex arrays are
+// interleaved (re, im) doubles.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <random>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+struct Mode {
+    std::int64_t k, l;
+    std::uint64_t kx, ky;
+    bool conj;
+    double radial;
+};
+
+// model.cpp:34-45: DFT index order 0, 1, ..., ceil(n/2)-1, -floor(n/2), ..., -1.
+std::vector<std::int64_t> signedModes(std::uint64_t n) {
+    std::vector<std::int64_t> out;
+    for (std::uint64_t v = 0; v < (n + 1) / 2; ++v) out.push_back(static_cast<std::int64_t>(v));
+    for (std::uint64_t v = n / 2; v > 0; --v) out.push_back(-static_cast<std::int64_t>(v));
+    return out;
+}
+
+// model.cpp:52-65: self-conjugate, primary and Nyquist predicates.
+bool selfConj(std::int64_t m, std::uint64_t n) {
+    return m == 0 || (n % 2 == 0 && m == -static_cast<std::int64_t>(n / 2));
+}
+
+// model.cpp:129-167: radial 2/3 retention over primary members, Nyquist axes
+// excluded, stable-sorted by (radius, k, l).  The squares are stored through
+// volatile so no fused multiply-add changes the radius bits.
+std::vector<Mode> modesOf(std::uint64_t nx, std::uint64_t ny, double lx, double ly, bool antialias) {
+    const auto ks = signedModes(nx);
+    const auto ls = signedModes(ny);
+    const double maxK = 2.0 * kPi * (static_cast<double>(nx / 2) / lx);
+    std::vector<Mode> modes;
+    for (const auto l : ls) {
+        for (const auto k : ks) {
+            const bool primary = l > 0 || (selfConj(l, ny) && (k > 0 || selfConj(k, nx)));
+            const bool nyq = (nx % 2 == 0 && k == -static_cast<std::int64_t>(nx / 2)) ||
+                             (ny % 2 == 0 && l == -static_cast<std::int64_t>(ny / 2));
+            if (!primary || nyq) continue;
+            const double pk = 2.0 * kPi * static_cast<double>(k) / lx;
+            const double pl = 2.0 * kPi * static_cast<double>(l) / ly;
+            volatile double a = pk * pk;
+            volatile double b = pl * pl;
+            const double radial = std::sqrt(a + b);
+            if (antialias && radial > 2.0 * maxK / 3.0) continue;
+            Mode m{k, l, 0, 0, false, radial};
+            if (k >= 0) {
+                m.kx = static_cast<std::uint64_t>(k);
+                m.ky = static_cast<std::uint64_t>(l >= 0 ? l : static_cast<std::int64_t>(ny) + l);
+            } else {
+                m.kx = static_cast<std::uint64_t>(-k);
+                m.ky = static_cast<std::uint64_t>(-l >= 0 ? -l : static_cast<std::int64_t>(ny) - l);
+                m.conj = true;
+            }
+            modes.push_back(m);
+        }
+    }
+    std::stable_sort(modes.begin(), modes.end(), [](const Mode& a, const Mode& b) {
+        if (a.radial != b.radial) return a.radial < b.radial;
+        if (a.k != b.k) return a.k < b.k;
+        return a.l < b.l;
+    });
+    return modes;
+}
+
+std::uint64_t absKey(std::int64_t v) {
+    return v < 0 ? static_cast<std::uint64_t>(-(v + 1)) + 1 : static_cast<std::uint64_t>(v);
+}
+
+struct Group {
+    std::uint64_t key, first, count;
+};
+
+// model.cpp:169-207: contiguous runs of the integer key k^2 + l^2.
+std::vector<Group> groupsOf(const std::vector<Mode>& modes) {
+    std::vector<Group> groups;
+    std::set<std::uint64_t> done;
+    for (std::uint64_t i = 0; i < modes.size(); ++i) {
+        const auto k = absKey(modes[i].k), l = absKey(modes[i].l);
+        const auto key = k * k + l * l;
+        if (groups.empty() || groups.back().key != key) {
+            if (done.count(key)) throw std::invalid_argument("non-contiguous K^2 group");
+            if (!groups.empty()) done.insert(groups.back().key);
+            groups.push_back({key, i, 1});
+        } else {
+            ++groups.back().count;
+        }
+    }
+    return groups;
+}
+
+// model.cpp:86-104: FNV-1a over little-endian integer bytes.
+struct Fnv {
+    std::uint64_t h = UINT64_C(14695981039346656037);
+    template <typename T>
+    void add(T value) {
+        using U = std::make_unsigned_t<T>;
+        const auto bits = static_cast<U>(value);
+        for (std::size_t b = 0; b < sizeof(T); ++b) {
+            h ^= static_cast<std::uint8_t>((bits >> (8 * b)) & 0xff);
+            h *= UINT64_C(1099511628211);
+        }
+    }
+    void text(char* out) const { std::snprintf(out, 64, "fnv1a64:%016llx", static_cast<unsigned long long>(h)); }
+};
+
+thread_local std::string lastError;
+
+template <typename Body>
+int guarded(Body body) {
+    try {
+        body();
+        return 0;
+    } catch (const std::exception& e) {
+        lastError = e.what();
+        return -1;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* oracle_last_error() { return lastError.c_str(); }
+
+int oracle_retained_modes(std::uint64_t nx, std::uint64_t ny, double lx, double ly, int antialias,
+                          std::int64_t* k, std::int64_t* l, std::uint64_t* kx, std::uint64_t* ky,
+                          std::uint8_t* conj, double* radial, std::uint64_t capacity, std::uint64_t* count) {
+    return guarded([&] {
+        const auto modes = modesOf(nx, ny, lx, ly, antialias != 0);
+        *count = modes.size();
+        if (modes.size() > capacity) throw std::invalid_argument("capacity");
+        for (std::size_t i = 0; i < modes.size(); ++i) {
+            k[i] = modes[i].k;
+            l[i] = modes[i].l;
+            kx[i] = modes[i].kx;
+            ky[i] = modes[i].ky;
+            conj[i] = modes[i].conj;
+            radial[i] = modes[i].radial;
+        }
+    });
+}
+
+int oracle_groups(std::uint64_t nx, std::uint64_t ny, std::uint64_t* keys, std::uint64_t* first,
+                  std::uint64_t* counts, std::uint64_t capacity, std::uint64_t* count) {
+    return guarded([&] {
+        const auto groups = groupsOf(modesOf(nx, ny, 1.0, 1.0, true));
+        *count = groups.size();
+        if (groups.size() > capacity) throw std::invalid_argument("capacity");
+        for (std::size_t g = 0; g < groups.size(); ++g) {
+            keys[g] = groups[g].key;
+            first[g] = groups[g].first;
+            counts[g] = groups[g].count;
+        }
+    });
+}
+
+// model.cpp:462-469, 209-217, 471-487.
+int oracle_hashes(std::uint64_t nx, std::uint64_t ny, std::uint64_t nz, std::uint64_t fields, char* modeHash,
+                  char* groupHash, char* wvmHash) {
+    return guarded([&] {
+        const auto modes = modesOf(nx, ny, 1.0, 1.0, true);
+        Fnv mh;
+        for (const auto& m : modes) {
+            mh.add(m.k);
+            mh.add(m.l);
+        }
+        mh.text(modeHash);
+        Fnv gh;
+        for (const auto& g : groupsOf(modes)) {
+            gh.add(g.key);
+            gh.add(g.first);
+            gh.add(g.count);
+        }
+        gh.text(groupHash);
+        Fnv wh;
+        const auto nxHalf = nx / 2 + 1;
+        for (std::uint64_t ky = 0; ky < ny; ++ky) {
+            const std::int64_t sky = ky <= ny / 2 ? static_cast<std::int64_t>(ky)
+                                                  : static_cast<std::int64_t>(ky) - static_cast<std::int64_t>(ny);
+            for (std::uint64_t kx = 0; kx < nxHalf; ++kx)
+                for (std::uint64_t f = 0; f < fields; ++f)
+                    for (std::uint64_t z = 0; z < nz; ++z) {
+                        wh.add(static_cast<std::int64_t>(kx));
+                        wh.add(sky);
+                        wh.add(z);
+                        wh.add(f);
+                    }
+        }
+        wh.text(wvmHash);
+    });
+}
+
+// model.cpp:618-661.  kind: 0 impulse, 1 sinusoid, 2 random (standard normal
+// from mt19937_64(seed) in x-fastest order), 3 dc, 4 nyquist.
+int oracle_make_fixture(std::uint64_t nx, std::uint64_t ny, std::uint64_t nz, std::uint64_t fields, int kind,
+                        std::uint64_t seed, double* out) {
+    return guarded([&] {
+        std::mt19937_64 gen(seed);
+        std::normal_distribution<double> normal;
+        std::fill_n(out, nx * ny * nz * fields, 0.0);
+        for (std::uint64_t f = 0; f < fields; ++f)
+            for (std::uint64_t z = 0; z < nz; ++z) {
+                const auto plane = z + nz * f;
+                const double amp = 1.0 + 0.125 * static_cast<double>(plane);
+                double* p = out + plane * nx * ny;
+                if (kind == 0) {
+                    p[(1 + plane) % nx + nx * ((2 + 3 * plane) % ny)] = amp;
+                    continue;
+                }
+                for (std::uint64_t y = 0; y < ny; ++y)
+                    for (std::uint64_t x = 0; x < nx; ++x) {
+                        double v = 0.0;
+                        if (kind == 1) {
+                            const double phase = 0.17 * static_cast<double>(plane);
+                            v = amp * std::cos(2.0 * kPi *
+                                                   (static_cast<double>(x) / static_cast<double>(nx) +
+                                                    2.0 * static_cast<double>(y) / static_cast<double>(ny)) +
+                                               phase);
+                        } else if (kind == 2) {
+                            v = normal(gen);
+                        } else if (kind == 3) {
+                            v = amp;
+                        } else if (kind == 4) {
+                            v = amp * (((x + y) % 2 == 0) ? 1.0 : -1.0);
+                        }
+                        p[x + nx * y] = v;
+                    }
+            }
+    });
+}
+
+// benchmark.cpp:4045-4058: modal inputs uniform[-0.125, 0.125] from
+// mt19937_64(seed), j fastest, then field, then mode; zero imaginary part at DC.
+int oracle_flux_inputs(const std::int64_t* k, const std::int64_t* l, std::uint64_t modes, std::uint64_t fields,
+                       std::uint64_t nj, std::uint64_t seed, double* out) {
+    return guarded([&] {
+        std::mt19937_64 gen(seed);
+        std::uniform_real_distribution<double> u(-0.125, 0.125);
+        for (std::uint64_t m = 0; m < modes; ++m) {
+            const bool dc = k[m] == 0 && l[m] == 0;
+            for (std::uint64_t f = 0; f < fields; ++f)
+                for (std::uint64_t j = 0; j < nj; ++j) {
+                    double* v = out + 2 * (j + nj * (f + fields * m));
+                    v[0] = u(gen);
+                    v[1] = dc ? 0.0 : u(gen);
+                }
+        }
+    });
+}
+
+// model.cpp:663-684: unnormalised direct 2-D r2c of `planes` x-fastest planes
+// into the WVM frequency-major half spectrum (index plane + planes*(kx + nxHalf*ky)).
+int oracle_direct_r2c(std::uint64_t nx, std::uint64_t ny, std::uint64_t planes, const double* in, double* out) {
+    return guarded([&] {
+        const auto nxHalf = nx / 2 + 1;
+        for (std::uint64_t p = 0; p < planes; ++p)
+            for (std::uint64_t ky = 0; ky < ny; ++ky)
+                for (std::uint64_t kx = 0; kx < nxHalf; ++kx) {
+                    double re = 0.0, im = 0.0;
+                    for (std::uint64_t y = 0; y < ny; ++y)
+                        for (std::uint64_t x = 0; x < nx; ++x) {
+                            const double angle = -2.0 * kPi *
+                                                 (static_cast<double>(kx * x) / static_cast<double>(nx) +
+                                                  static_cast<double>(ky * y) / static_cast<double>(ny));
+                            const double v = in[x + nx * (y + ny * p)];
+                            re += v * std::cos(angle);
+                            im += v * std::sin(angle);
+                        }
+                    double* o = out + 2 * (p + planes * (kx + nxHalf * ky));
+                    o[0] = re;
+                    o[1] = im;
+                }
+    });
+}
+
+// model.cpp:686-716: unnormalised direct c2r; the full spectrum is recovered from
+// the stored half by conjugate symmetry for kx > nx/2, and the real part is kept.
+int oracle_direct_c2r(std::uint64_t nx, std::uint64_t ny, std::uint64_t planes, const double* in, double* out) {
+    return guarded([&] {
+        const auto nxHalf = nx / 2 + 1;
+        for (std::uint64_t p = 0; p < planes; ++p)
+            for (std::uint64_t y = 0; y < ny; ++y)
+                for (std::uint64_t x = 0; x < nx; ++x) {
+                    double re = 0.0;
+                    for (std::uint64_t ky = 0; ky < ny; ++ky)
+                        for (std::uint64_t kx = 0; kx < nx; ++kx) {
+                            std::uint64_t skx = kx, sky = ky;
+                            double sign = 1.0;
+                            if (kx > nx / 2) {
+                                skx = nx - kx;
+                                sky = (ny - ky) % ny;
+                                sign = -1.0;
+                            }
+                            const double* c = in + 2 * (p + planes * (skx + nxHalf * sky));
+                            const double angle = 2.0 * kPi *
+                                                 (static_cast<double>(kx * x) / static_cast<double>(nx) +
+                                                  static_cast<double>(ky * y) / static_cast<double>(ny));
+                            re += c[0] * std::cos(angle) - sign * c[1] * std::sin(angle);
+                        }
+                    out[x + nx * (y + ny * p)] = re;
+                }
+    });
+}
+
+// pointwise_advection.cpp:143-147: target = -scale*(u*qx + v*qy + w*qz) with
+// shared = [u, v, w] and derivative = [qx, qy, qz] volume-strided; split
+// across `workers` host threads as contiguous ranges (spatial-static policy).
+int oracle_pointwise(std::uint64_t volume, double scale, const double* shared, const double* derivative,
+                     double* target, std::uint64_t workers) {
+    return guarded([&] {
+        auto range = [&](std::uint64_t begin, std::uint64_t end) {
+            const double* u = shared;
+            const double* v = shared + volume;
+            const double* w = shared + 2 * volume;
+            const double* qx = derivative;
+            const double* qy = derivative + volume;
+            const double* qz = derivative + 2 * volume;
+            for (std::uint64_t i = begin; i < end; ++i)
+                target[i] = -scale * (u[i] * qx[i] + v[i] * qy[i] + w[i] * qz[i]);
+        };
+        if (workers <= 1) {
+            range(0, volume);
+            return;
+        }
+        std::vector<std::thread> threads;
+        for (std::uint64_t t = 0; t < workers; ++t)
+            threads.emplace_back(range, volume * t / workers, volume * (t + 1) / workers);
+        for (auto& t : threads) t.join();
+    });
+}
+
+// model.cpp:489-565: truncated orthonormal DCT-II base, then per K^2 group a
+// rotation of row pairs (j, j+1) by 0.5*pi*((key mod 4093)+1)/4094 and a sign
+// flip of an unpaired last row when the key is odd.  forward[g][j][z],
+// inverse[g][z][j].
+int oracle_k2_vertical_family(std::uint64_t nz, std::uint64_t nj, const std::uint64_t* keys, std::uint64_t groups,
+                              double* forward, double* inverse) {
+    return guarded([&] {
+        std::vector<double> base(nj * nz);
+        for (std::uint64_t j = 0; j < nj; ++j) {
+            const double norm = j == 0 ? std::sqrt(1.0 / static_cast<double>(nz)) : std::sqrt(2.0 / static_cast<double>(nz));
+            for (std::uint64_t z = 0; z < nz; ++z)
+                base[j * nz + z] = norm * std::cos(kPi * (static_cast<double>(z) + 0.5) * static_cast<double>(j) /
+                                                   static_cast<double>(nz));
+        }
+        const auto elems = nj * nz;
+        for (std::uint64_t g = 0; g < groups; ++g) {
+            const auto key = keys[g];
+            const double phase = static_cast<double>((key % UINT64_C(4093)) + 1) / 4094.0;
+            const double c = std::cos(0.5 * kPi * phase);
+            const double s = std::sin(0.5 * kPi * phase);
+            double* F = forward + g * elems;
+            double* I = inverse + g * elems;
+            for (std::uint64_t j = 0; j < nj; j += 2)
+                for (std::uint64_t z = 0; z < nz; ++z) {
+                    const double a = base[j * nz + z];
+                    double ar = a;
+                    if (j + 1 < nj) {
+                        const double b = base[(j + 1) * nz + z];
+                        ar = c * a + s * b;
+                        const double br = -s * a + c * b;
+                        F[(j + 1) * nz + z] = br;
+                        I[z * nj + j + 1] = br;
+                    } else if ((key & 1U) != 0) {
+                        ar = -a;
+                    }
+                    F[j * nz + z] = ar;
+                    I[z * nj + j] = ar;
+                }
+        }
+    });
+}
+
+}  // extern "C"
