@@ -1,0 +1,333 @@
+/*
+ * skb_cuda.h — C ABI of the B200 `cuda` provider for the skbench spectral path.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns
+ * an int status (SKB_OK = 0).  On failure skb_last_error() returns the message
+ * of the calling thread's most recent error.  The status classes mirror the
+ * exception types the reference's providers throw, so a C++ wrapper can
+ * rethrow the same type and keep the CLI's exit codes
+ * (include/skbench/skbench.hpp, src/main.cpp:242-245):
+ *   SKB_ERR_INVALID_ARGUMENT  std::invalid_argument (bad shape, null pointer)
+ *   SKB_ERR_RUNTIME           std::runtime_error    (CUDA failure, unsupported)
+ *   SKB_ERR_LOGIC             std::logic_error      (wrong layout / direction)
+ *   SKB_ERR_OUT_OF_MEMORY     std::bad_alloc
+ *
+ * Pointer families.  Functions without a suffix take HOST arrays and block
+ * until the result is back in host memory (the reference's providers are
+ * host-array APIs).  `_device` functions take DEVICE pointers, enqueue on the
+ * given CUDA stream (NULL = the handle's own stream) and return without
+ * synchronising.  Device arrays use the handle's precision: double for
+ * SKB_PRECISION_FP64 handles, float for SKB_PRECISION_FP32; complex values are
+ * interleaved (re, im) pairs unless a split view is given.
+ *
+ * Layouts are the reference's (src/model.cpp:219-244):
+ *   real      [field][z][y][x]            x fastest
+ *   wvm       [ky][kx][field][z]          WVM frequency-major half spectrum,
+ *                                         index z + Nz*field + planes*(kx + (Nx/2+1)*ky)
+ *   retained  [mode][field][z]            index z + Nz*field + planes*mode
+ *   modal     [mode][field][j]            index j + Nj*field + Nj*fields*mode
+ * Transforms are unnormalised in both directions like FFTW's.
+ *
+ * Handles own their device scratch; steady-state calls allocate nothing.
+ * A handle is single-owner: calls on one handle must not overlap.
+ */
+#ifndef SKB_CUDA_H
+#define SKB_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SKB_API __attribute__((visibility("default")))
+#else
+#define SKB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SKB_OK 0
+#define SKB_ERR_INVALID_ARGUMENT (-1)
+#define SKB_ERR_RUNTIME (-2)
+#define SKB_ERR_LOGIC (-3)
+#define SKB_ERR_OUT_OF_MEMORY (-4)
+
+#define SKB_PRECISION_FP64 0
+#define SKB_PRECISION_FP32 1
+
+#define SKB_GEMM_FP64 0
+#define SKB_GEMM_FP32 1
+#define SKB_GEMM_TF32X3 2
+#define SKB_GEMM_BF16X3 3
+
+#define SKB_LAYOUT_INTERLEAVED 0
+#define SKB_LAYOUT_SPLIT 1
+
+/* VerticalGemmBufferPolicy (skbench.hpp:132-136). */
+#define SKB_BUFFERS_BIDIRECTIONAL 0
+#define SKB_BUFFERS_FORWARD_ONLY 1
+#define SKB_BUFFERS_INVERSE_ONLY 2
+
+/* Vertical operator families (src/model.cpp:489-565, plus the build's seeded
+ * Sturm-Liouville family). */
+#define SKB_FAMILY_COMMON_DCT2 0
+#define SKB_FAMILY_K2_ROTATION 1
+#define SKB_FAMILY_STURM_LIOUVILLE 2
+
+/* Workload (skbench.hpp:23-39). */
+typedef struct skb_workload {
+    uint64_t nx, ny, nz, fields;
+    double lx, ly;
+    int32_t antialias;
+} skb_workload;
+
+/* Complex (skbench.hpp:15-18). */
+typedef struct skb_complex {
+    double real, imag;
+} skb_complex;
+
+/* RetainedMode (skbench.hpp:41-48). */
+typedef struct skb_retained_mode {
+    int64_t k, l;
+    uint64_t stored_kx, stored_ky;
+    int32_t conjugates_stored_value;
+    double radial_mode;
+} skb_retained_mode;
+
+/* VerticalModeGroup (skbench.hpp:50-56). */
+typedef struct skb_mode_group {
+    uint64_t squared_mode_key, first_mode, mode_count;
+} skb_mode_group;
+
+/* FieldView / ConstFieldView of FFTWStreamingPrunedSplitProvider
+ * (skbench.hpp:536-546): element (mode, z) at z + mode_stride*mode.  A split
+ * view has both pointers; an interleaved view sets imag = NULL and real points
+ * at complex (re, im) pairs. */
+typedef struct skb_field_view {
+    void* real;
+    void* imag;
+    uint64_t mode_stride;
+} skb_field_view;
+
+/* Accounting getters shared by every handle (skbench.hpp:401-416, 495-515,
+ * 169-187).  planning_seconds = table and launch-configuration set-up. */
+typedef struct skb_provider_info {
+    double allocation_seconds;
+    double planning_seconds;
+    double other_setup_seconds;
+    uint64_t persistent_bytes;
+    uint64_t scratch_bytes;
+    uint64_t planning_bytes;
+    uint64_t active_kx;
+    uint64_t full_kx;
+    uint64_t row_transforms_per_direction;
+    uint64_t column_transforms_per_direction;
+    uint64_t omitted_column_transforms_per_direction;
+    uint64_t launches_per_execution;
+    int32_t precision;
+    int32_t destroys_native_input;
+    char library_identity[128];
+    char version[64];
+} skb_provider_info;
+
+/* ---------------------------------------------------------------- library */
+SKB_API const char* skb_last_error(void);
+SKB_API const char* skb_version(void);
+SKB_API int skb_device_count(int* count);
+/* Synchronise the current device (host-side barrier for timing). */
+SKB_API int skb_device_synchronize(void);
+
+/* ------------------------------------------------- model (host, no GPU)  */
+/* retainedHorizontalModes, src/model.cpp:129-167. */
+SKB_API int skb_retained_modes(const skb_workload* w, skb_retained_mode* out, uint64_t capacity, uint64_t* count);
+/* squaredWavenumberGroups, src/model.cpp:169-207. */
+SKB_API int skb_squared_wavenumber_groups(const skb_workload* w, skb_mode_group* out, uint64_t capacity, uint64_t* count);
+/* modeOrderHash / verticalModeGroupHash / wvmSpectrumOrderHash,
+ * src/model.cpp:209-217, 462-487; each buffer holds at least 32 chars. */
+SKB_API int skb_order_hashes(const skb_workload* w, char* mode_hash, char* group_hash, char* wvm_hash);
+/* makeFixture, src/model.cpp:618-661; kind 0 impulse, 1 sinusoid, 2 random,
+ * 3 dc, 4 nyquist; out holds nx*ny*nz*fields doubles. */
+SKB_API int skb_make_fixture(const skb_workload* w, int kind, uint64_t seed, double* out);
+/* Vertical operator family: forward[g][j][z], inverse[g][z][j] for
+ * groups*nj*nz doubles each (groups = 1 for SKB_FAMILY_COMMON_DCT2);
+ * orthonormalVerticalFixture / squaredWavenumberVerticalFixture,
+ * src/model.cpp:489-565.  id holds at least 96 chars. */
+SKB_API int skb_vertical_family(const skb_workload* w, int family, uint64_t seed, double* forward, double* inverse,
+                        uint64_t capacity, uint64_t* groups, char* id);
+
+/* ---------------------------------------------- full 2-D r2c/c2r provider */
+/* Replaces FFTWProvider (skbench.hpp:364-421; src/fftw_provider.cpp:206-917). */
+typedef struct skb_fft_provider skb_fft_provider;
+SKB_API int skb_fft_create(const skb_workload* w, int precision, skb_fft_provider** out);
+SKB_API int skb_fft_destroy(skb_fft_provider* p);
+SKB_API int skb_fft_info(const skb_fft_provider* p, skb_provider_info* info);
+/* forward(const double*, Complex*), fftw_provider.cpp:304-309. */
+SKB_API int skb_fft_forward(skb_fft_provider* p, const double* input, skb_complex* wvm_spectrum);
+/* inverse(Complex*, double*), fftw_provider.cpp:311-316; the input is preserved. */
+SKB_API int skb_fft_inverse(skb_fft_provider* p, skb_complex* wvm_spectrum, double* output);
+/* forwardSplit / inverseSplit, skbench.hpp:390-391. */
+SKB_API int skb_fft_forward_split(skb_fft_provider* p, const double* input, double* spectrum_real, double* spectrum_imag);
+SKB_API int skb_fft_inverse_split(skb_fft_provider* p, double* spectrum_real, double* spectrum_imag, double* output);
+/* gatherRetainedOuter / embedRetainedOuter and the split/scale variants,
+ * fftw_provider.cpp:318-395. */
+SKB_API int skb_fft_gather_retained(skb_fft_provider* p, const skb_complex* wvm_spectrum, skb_complex* retained);
+SKB_API int skb_fft_embed_retained(skb_fft_provider* p, const skb_complex* retained, skb_complex* wvm_spectrum);
+SKB_API int skb_fft_gather_retained_to_split(skb_fft_provider* p, const skb_complex* wvm_spectrum, double* retained_real,
+                                     double* retained_imag, double scale);
+SKB_API int skb_fft_embed_retained_from_split(skb_fft_provider* p, const double* retained_real, const double* retained_imag,
+                                      skb_complex* wvm_spectrum);
+/* Device forms. */
+SKB_API int skb_fft_forward_device(skb_fft_provider* p, const void* real, void* wvm_spectrum, void* stream);
+SKB_API int skb_fft_inverse_device(skb_fft_provider* p, const void* wvm_spectrum, void* real, void* stream);
+SKB_API int skb_fft_gather_retained_device(skb_fft_provider* p, const void* wvm_spectrum, const skb_field_view* views,
+                                   uint64_t view_count, double scale, void* stream);
+SKB_API int skb_fft_embed_retained_device(skb_fft_provider* p, const skb_field_view* views, uint64_t view_count,
+                                  void* wvm_spectrum, void* stream);
+
+/* ------------------------------------------- pruned horizontal provider */
+/* Replaces FFTWPrunedProvider (skbench.hpp:467-520) and
+ * FFTWStreamingPrunedSplitProvider (skbench.hpp:534-624): row r2c/c2r on all
+ * rows, column c2c only on the active kx band, retention / embedding with the
+ * kx = 0 Hermitian repair fused into the column kernels. */
+typedef struct skb_pruned_provider skb_pruned_provider;
+SKB_API int skb_pruned_create(const skb_workload* w, int precision, skb_pruned_provider** out);
+SKB_API int skb_pruned_destroy(skb_pruned_provider* p);
+SKB_API int skb_pruned_info(const skb_pruned_provider* p, skb_provider_info* info);
+/* forward / forwardSplit / inverse / inverseSplit, pruned_fftw_provider.cpp:230-269. */
+SKB_API int skb_pruned_forward(skb_pruned_provider* p, const double* input, skb_complex* retained);
+SKB_API int skb_pruned_forward_split(skb_pruned_provider* p, const double* input, double* retained_real,
+                             double* retained_imag, double scale);
+SKB_API int skb_pruned_inverse(skb_pruned_provider* p, const skb_complex* retained, double* output);
+SKB_API int skb_pruned_inverse_split(skb_pruned_provider* p, const double* retained_real, const double* retained_imag,
+                             double* output);
+/* forwardSplitFields / inverseSplitFields, pruned_fftw_provider.cpp:787-805;
+ * one host view per field, split layout. */
+SKB_API int skb_pruned_forward_split_fields(skb_pruned_provider* p, const double* input, const skb_field_view* fields,
+                                    uint64_t field_count, double scale);
+SKB_API int skb_pruned_inverse_split_fields(skb_pruned_provider* p, const skb_field_view* fields, uint64_t field_count,
+                                    double* output);
+/* Device forms over field views (views may be split or interleaved). */
+SKB_API int skb_pruned_forward_device(skb_pruned_provider* p, const void* real, const skb_field_view* fields,
+                              uint64_t field_count, double scale, void* stream);
+SKB_API int skb_pruned_inverse_device(skb_pruned_provider* p, const skb_field_view* fields, uint64_t field_count,
+                              void* real, void* stream);
+/* Component stages for diagnostic timings (executeForwardRows /
+ * executeForwardColumns+gather / embed+executeInverseColumns /
+ * executeInverseRows, skbench.hpp:478-492); they use the handle's scratch. */
+SKB_API int skb_pruned_forward_rows_device(skb_pruned_provider* p, const void* real, void* stream);
+SKB_API int skb_pruned_forward_columns_device(skb_pruned_provider* p, const skb_field_view* fields, uint64_t field_count,
+                                      double scale, void* stream);
+SKB_API int skb_pruned_inverse_columns_device(skb_pruned_provider* p, const skb_field_view* fields, uint64_t field_count,
+                                      void* stream);
+SKB_API int skb_pruned_inverse_rows_device(skb_pruned_provider* p, void* real, void* stream);
+
+/* ----------------------------------------------- vertical GEMM provider */
+/* Replaces VerticalGemmProvider (skbench.hpp:152-218,
+ * src/vertical_gemm.cpp:270-634).  forward/inverse matrices are the family in
+ * reference layout (forward[g][j][z], inverse[g][z][j]); groups are the K^2
+ * groups (one group covering every mode for the common family). */
+typedef struct skb_vertical_provider skb_vertical_provider;
+SKB_API int skb_vertical_create(const skb_workload* w, const skb_mode_group* groups, uint64_t group_count,
+                        const double* forward, const double* inverse, int layout, int buffer_policy,
+                        int gemm_precision, skb_vertical_provider** out);
+SKB_API int skb_vertical_destroy(skb_vertical_provider* p);
+SKB_API int skb_vertical_info(const skb_vertical_provider* p, skb_provider_info* info);
+/* loadPhysicalInput / loadModalInput / executeForward / executeInverse /
+ * copyForwardOutput / copyInverseOutput, vertical_gemm.cpp:731-770 (host
+ * arrays; interleaved layout). */
+SKB_API int skb_vertical_load_physical_input(skb_vertical_provider* p, const skb_complex* input);
+SKB_API int skb_vertical_load_modal_input(skb_vertical_provider* p, const skb_complex* input);
+SKB_API int skb_vertical_execute_forward(skb_vertical_provider* p);
+SKB_API int skb_vertical_execute_inverse(skb_vertical_provider* p);
+SKB_API int skb_vertical_copy_forward_output(skb_vertical_provider* p, skb_complex* output);
+SKB_API int skb_vertical_copy_inverse_output(skb_vertical_provider* p, skb_complex* output);
+/* Split-layout host loads and copies (split*Data accessors, skbench.hpp:203-210). */
+SKB_API int skb_vertical_load_physical_input_split(skb_vertical_provider* p, const double* real, const double* imag);
+SKB_API int skb_vertical_load_modal_input_split(skb_vertical_provider* p, const double* real, const double* imag);
+SKB_API int skb_vertical_copy_forward_output_split(skb_vertical_provider* p, double* real, double* imag);
+SKB_API int skb_vertical_copy_inverse_output_split(skb_vertical_provider* p, double* real, double* imag);
+/* Device forms: imag = NULL means interleaved complex in `real`. */
+SKB_API int skb_vertical_forward_device(skb_vertical_provider* p, const void* in_real, const void* in_imag, void* out_real,
+                                void* out_imag, void* stream);
+SKB_API int skb_vertical_inverse_device(skb_vertical_provider* p, const void* in_real, const void* in_imag, void* out_real,
+                                void* out_imag, void* stream);
+
+/* ------------------------------------------------- pointwise advection */
+/* Replaces PointwiseAdvectionExecutor (src/pointwise_advection.hpp:18-43). */
+typedef struct skb_pointwise_executor skb_pointwise_executor;
+SKB_API int skb_pointwise_create(uint64_t volume_elements, double scale, int precision, skb_pointwise_executor** out);
+SKB_API int skb_pointwise_destroy(skb_pointwise_executor* p);
+/* execute(shared, derivative, target), pointwise_advection.cpp:178-195. */
+SKB_API int skb_pointwise_execute(skb_pointwise_executor* p, const double* shared, const double* derivative, double* target);
+SKB_API int skb_pointwise_execute_device(skb_pointwise_executor* p, const void* shared, const void* derivative, void* target,
+                                 void* stream);
+
+/* ------------------------------------------------- 15 -> 4 flux pipeline */
+/* The composed streamed flux of runProductionLifetimeFluxBenchmark's
+ * executeAll (src/benchmark.cpp:4405-4424): inverse vertical GEMM of the
+ * 3+3T modal inputs, inverse pruned horizontal of [U,V,W], then per target the
+ * inverse of its derivative triple, pointwise advection with scale
+ * 1/(Nx*Ny)^2, forward pruned horizontal + retention, and the forward vertical
+ * GEMM of the T targets.  T = 4 is the reference's 15 -> 4 boundary; T = 3 is
+ * the 12 -> 3 serving variant.  `members` independent ensemble members are
+ * evaluated per call, member-major: input [member][mode][field][j]. */
+#define SKB_FLUX_FP64_PLAIN 0
+#define SKB_FLUX_FP32 1
+#define SKB_FLUX_SPLIT_TF32X3 2
+#define SKB_FLUX_SPLIT_BF16X3 3
+
+typedef struct skb_flux_options {
+    uint64_t n;        /* Nx = Ny */
+    uint64_t nz;
+    uint64_t targets;  /* 4 (15 -> 4) or 3 (12 -> 3) */
+    uint64_t members;  /* ensemble members per call */
+    int32_t mode;      /* SKB_FLUX_* */
+    int32_t family;    /* SKB_FAMILY_K2_ROTATION or SKB_FAMILY_STURM_LIOUVILLE */
+    uint64_t family_seed;
+} skb_flux_options;
+
+typedef struct skb_flux skb_flux;
+SKB_API int skb_flux_create(const skb_flux_options* options, skb_flux** out);
+SKB_API int skb_flux_destroy(skb_flux* p);
+SKB_API int skb_flux_info(const skb_flux* p, skb_provider_info* info);
+/* Sizes in complex elements for all members. */
+SKB_API int skb_flux_sizes(const skb_flux* p, uint64_t* modes, uint64_t* nj, uint64_t* input_elements,
+                   uint64_t* output_elements);
+/* Host arrays (double complex), blocking. */
+SKB_API int skb_flux_execute(skb_flux* p, const skb_complex* modal_input, skb_complex* modal_output);
+/* Device arrays: FP64 complex for SKB_FLUX_FP64_PLAIN, FP32 complex otherwise. */
+SKB_API int skb_flux_execute_device(skb_flux* p, const void* modal_input, void* modal_output, void* stream);
+/* Capture execute_device on these buffers into a CUDA graph and replay it. */
+SKB_API int skb_flux_capture_graph(skb_flux* p, const void* modal_input, void* modal_output);
+SKB_API int skb_flux_replay_graph(skb_flux* p, void* stream);
+
+/* --------------------------------------------------------------- timing */
+/* Events on a handle's stream, for benchmark harnesses. */
+typedef struct skb_timer skb_timer;
+SKB_API int skb_timer_create(skb_timer** out);
+SKB_API int skb_timer_destroy(skb_timer* t);
+SKB_API int skb_timer_start(skb_timer* t, void* stream);
+SKB_API int skb_timer_stop(skb_timer* t, void* stream);
+SKB_API int skb_timer_elapsed_ms(skb_timer* t, double* ms);
+/* The stream a handle enqueues on (for callers that time around it). */
+SKB_API void* skb_fft_stream(skb_fft_provider* p);
+SKB_API void* skb_pruned_stream(skb_pruned_provider* p);
+SKB_API void* skb_vertical_stream(skb_vertical_provider* p);
+SKB_API void* skb_pointwise_stream(skb_pointwise_executor* p);
+SKB_API void* skb_flux_stream(skb_flux* p);
+
+/* Device buffers for callers without their own allocator (tests, bindings). */
+SKB_API int skb_device_alloc(uint64_t bytes, void** ptr);
+SKB_API int skb_device_free(void* ptr);
+SKB_API int skb_host_alloc_pinned(uint64_t bytes, void** ptr);
+SKB_API int skb_host_free_pinned(void* ptr);
+SKB_API int skb_copy_to_device(void* dst, const void* src, uint64_t bytes, void* stream);
+SKB_API int skb_copy_to_host(void* dst, const void* src, uint64_t bytes, void* stream);
+SKB_API int skb_stream_synchronize(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SKB_CUDA_H */

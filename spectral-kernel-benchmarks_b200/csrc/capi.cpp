@@ -1,0 +1,1226 @@
+// extern "C" entry points of include/skb_cuda.h.
+
+#include "skb_cuda.h"
+
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "flux.hpp"
+#include "pointwise.hpp"
+#include "runtime.hpp"
+#include "util.hpp"
+
+using namespace skb;
+
+namespace {
+
+thread_local std::string g_lastError;
+
+template <typename F>
+int guard(F&& body) {
+    try {
+        body();
+        return SKB_OK;
+    } catch (const Error& e) {
+        g_lastError = e.what();
+        return e.code();
+    } catch (const std::invalid_argument& e) {
+        g_lastError = e.what();
+        return SKB_ERR_INVALID_ARGUMENT;
+    } catch (const std::bad_alloc& e) {
+        g_lastError = e.what();
+        return SKB_ERR_OUT_OF_MEMORY;
+    } catch (const std::logic_error& e) {
+        g_lastError = e.what();
+        return SKB_ERR_LOGIC;
+    } catch (const std::exception& e) {
+        g_lastError = e.what();
+        return SKB_ERR_RUNTIME;
+    }
+}
+
+void require(bool ok, const char* what) {
+    if (!ok) throw Error(SKB_ERR_INVALID_ARGUMENT, what);
+}
+
+Workload to_workload(const skb_workload* w) {
+    require(w != nullptr, "workload must be non-null");
+    Workload out{w->nx, w->ny, w->nz, w->fields, w->lx, w->ly, w->antialias != 0};
+    validate_workload(out);
+    return out;
+}
+
+Precision to_precision(int p) {
+    if (p == SKB_PRECISION_FP64) return Precision::f64;
+    if (p == SKB_PRECISION_FP32) return Precision::f32;
+    throw Error(SKB_ERR_INVALID_ARGUMENT, "precision must be SKB_PRECISION_FP64 or SKB_PRECISION_FP32");
+}
+
+cudaStream_t make_stream() {
+    cudaStream_t s = nullptr;
+    check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+    return s;
+}
+
+void copy_in(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync H2D");
+}
+
+void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync D2H");
+}
+
+void sync(cudaStream_t s) { check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize"); }
+
+ViewSet to_views(const skb_field_view* views, uint64_t count, uint64_t nz) {
+    require(views != nullptr || count == 0, "field views must be non-null");
+    require(count <= static_cast<uint64_t>(kMaxViews), "too many field views");
+    ViewSet v{};
+    v.count = static_cast<int>(count);
+    for (uint64_t i = 0; i < count; ++i) {
+        require(views[i].real != nullptr, "field view pointers must be non-null");
+        require(views[i].mode_stride >= nz, "field view mode stride must be at least Nz");
+        v.v[i] = {views[i].real, views[i].imag, static_cast<long long>(views[i].mode_stride)};
+    }
+    return v;
+}
+
+// Default retained layout [mode][field][z] as one interleaved view per field.
+ViewSet retained_views(void* base, const Workload& w, size_t complexBytes) {
+    ViewSet v{};
+    v.count = static_cast<int>(w.fields);
+    for (uint64_t f = 0; f < w.fields; ++f)
+        v.v[f] = {static_cast<unsigned char*>(base) + complexBytes * f * w.nz, nullptr,
+                  static_cast<long long>(w.planes())};
+    return v;
+}
+
+ViewSet retained_split_views(void* re, void* im, const Workload& w, size_t realBytes) {
+    ViewSet v{};
+    v.count = static_cast<int>(w.fields);
+    for (uint64_t f = 0; f < w.fields; ++f)
+        v.v[f] = {static_cast<unsigned char*>(re) + realBytes * f * w.nz,
+                  static_cast<unsigned char*>(im) + realBytes * f * w.nz, static_cast<long long>(w.planes())};
+    return v;
+}
+
+void fill_identity(skb_provider_info* info, const char* identity) {
+    std::strncpy(info->library_identity, identity, sizeof(info->library_identity) - 1);
+    std::strncpy(info->version, skb_version(), sizeof(info->version) - 1);
+}
+
+// Host doubles <-> device values of precision p through a staging buffer.
+struct HostAdapter {
+    Precision p;
+    DeviceBuffer staging;  // doubles, used only for f32 handles
+    void ensure(size_t doubles) {
+        if (p == Precision::f32 && staging.bytes() < doubles * sizeof(double)) staging.allocate(doubles * sizeof(double));
+    }
+    void upload(void* dst, const double* src, size_t n, cudaStream_t s) {
+        if (p == Precision::f64) {
+            copy_in(dst, src, n * sizeof(double), s);
+            return;
+        }
+        ensure(n);
+        copy_in(staging.get(), src, n * sizeof(double), s);
+        check_cuda(launch_convert_f64_to_f32(staging.get<double>(), static_cast<float*>(dst), (long long)n, s),
+                   "convert kernel");
+    }
+    void download(double* dst, const void* src, size_t n, cudaStream_t s) {
+        if (p == Precision::f64) {
+            copy_out(dst, src, n * sizeof(double), s);
+            return;
+        }
+        ensure(n);
+        check_cuda(launch_convert_f32_to_f64(static_cast<const float*>(src), staging.get<double>(), (long long)n, s),
+                   "convert kernel");
+        copy_out(dst, staging.get(), n * sizeof(double), s);
+    }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------ handles
+
+struct skb_fft_provider {
+    Workload w;
+    Precision p;
+    cudaStream_t stream = nullptr;
+    std::unique_ptr<HorizontalPlan> plan;
+    DeviceBuffer real, spectrum, retained, splitRe, splitIm;
+    HostAdapter host{Precision::f64, {}};
+    double otherSetup = 0.0, allocation = 0.0;
+    ~skb_fft_provider() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct skb_pruned_provider {
+    Workload w;
+    Precision p;
+    cudaStream_t stream = nullptr;
+    std::unique_ptr<HorizontalPlan> plan;
+    DeviceBuffer real, retained, retainedIm;
+    HostAdapter host{Precision::f64, {}};
+    double otherSetup = 0.0, allocation = 0.0;
+    ~skb_pruned_provider() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct skb_vertical_provider {
+    Workload w;
+    int layout = SKB_LAYOUT_INTERLEAVED;
+    int policy = SKB_BUFFERS_BIDIRECTIONAL;
+    GemmPrecision gp = GemmPrecision::f64;
+    Precision p = Precision::f64;
+    cudaStream_t stream = nullptr;
+    std::unique_ptr<VerticalPlan> forward, inverse;
+    uint64_t columns = 0, groups = 0;
+    DeviceBuffer physIn, physInIm, modalOut, modalOutIm, modalIn, modalInIm, physOut, physOutIm;
+    HostAdapter host{Precision::f64, {}};
+    double allocation = 0.0, preparation = 0.0;
+    ~skb_vertical_provider() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct skb_pointwise_executor {
+    uint64_t volume = 0;
+    double scale = 0.0;
+    Precision p = Precision::f64;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer shared, derivative, target;
+    HostAdapter host{Precision::f64, {}};
+    ~skb_pointwise_executor() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct skb_flux {
+    std::unique_ptr<FluxPipeline> pipeline;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer in, out;
+    HostAdapter host{Precision::f64, {}};
+    ~skb_flux() {
+        pipeline.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct skb_timer {
+    cudaEvent_t start = nullptr, stop = nullptr;
+    ~skb_timer() {
+        if (start) cudaEventDestroy(start);
+        if (stop) cudaEventDestroy(stop);
+    }
+};
+
+extern "C" {
+
+const char* skb_last_error(void) { return g_lastError.c_str(); }
+
+const char* skb_version(void) { return "skb-cuda 0.1.0 (sm_100a)"; }
+
+int skb_device_count(int* count) {
+    return guard([&] {
+        require(count != nullptr, "count must be non-null");
+        check_cuda(cudaGetDeviceCount(count), "cudaGetDeviceCount");
+    });
+}
+
+int skb_device_synchronize(void) {
+    return guard([&] { check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize"); });
+}
+
+// ------------------------------------------------------------------- model
+
+int skb_retained_modes(const skb_workload* w, skb_retained_mode* out, uint64_t capacity, uint64_t* count) {
+    return guard([&] {
+        const auto modes = retained_modes(to_workload(w));
+        require(count != nullptr, "count must be non-null");
+        *count = modes.size();
+        if (out == nullptr) return;
+        require(capacity >= modes.size(), "retained mode capacity too small");
+        for (size_t i = 0; i < modes.size(); ++i)
+            out[i] = {modes[i].k, modes[i].l, modes[i].kx, modes[i].ky, modes[i].conj ? 1 : 0, modes[i].radial};
+    });
+}
+
+int skb_squared_wavenumber_groups(const skb_workload* w, skb_mode_group* out, uint64_t capacity, uint64_t* count) {
+    return guard([&] {
+        const auto groups = squared_wavenumber_groups(retained_modes(to_workload(w)));
+        require(count != nullptr, "count must be non-null");
+        *count = groups.size();
+        if (out == nullptr) return;
+        require(capacity >= groups.size(), "group capacity too small");
+        for (size_t i = 0; i < groups.size(); ++i) out[i] = {groups[i].key, groups[i].first, groups[i].count};
+    });
+}
+
+int skb_order_hashes(const skb_workload* w, char* mode_hash, char* group_hash, char* wvm_hash) {
+    return guard([&] {
+        const auto wl = to_workload(w);
+        const auto modes = retained_modes(wl);
+        auto put = [](char* dst, const std::string& s) {
+            if (dst) std::snprintf(dst, 32, "%s", s.c_str());
+        };
+        put(mode_hash, mode_order_hash(modes));
+        put(group_hash, group_order_hash(squared_wavenumber_groups(modes)));
+        if (wvm_hash) put(wvm_hash, wvm_order_hash(wl));
+    });
+}
+
+int skb_make_fixture(const skb_workload* w, int kind, uint64_t seed, double* out) {
+    return guard([&] {
+        require(out != nullptr, "output must be non-null");
+        require(kind >= 0 && kind <= 4, "fixture kind must be 0..4");
+        const auto values = make_fixture(to_workload(w), kind, seed);
+        std::memcpy(out, values.data(), values.size() * sizeof(double));
+    });
+}
+
+int skb_vertical_family(const skb_workload* w, int family, uint64_t seed, double* forward, double* inverse,
+                        uint64_t capacity, uint64_t* groups, char* id) {
+    return guard([&] {
+        const auto wl = to_workload(w);
+        VerticalFamily fam;
+        if (family == SKB_FAMILY_COMMON_DCT2) {
+            fam = orthonormal_family(wl.nz, wl.nj());
+        } else {
+            const auto g = squared_wavenumber_groups(retained_modes(wl));
+            if (family == SKB_FAMILY_K2_ROTATION)
+                fam = k2_rotation_family(wl, g);
+            else if (family == SKB_FAMILY_STURM_LIOUVILLE)
+                fam = sturm_liouville_family(wl, g, seed);
+            else
+                throw Error(SKB_ERR_INVALID_ARGUMENT, "unknown vertical family");
+        }
+        if (groups) *groups = fam.groups;
+        if (id) std::snprintf(id, 96, "%s", fam.id.c_str());
+        if (forward == nullptr && inverse == nullptr) return;
+        require(capacity >= fam.forward.size(), "vertical family capacity too small");
+        if (forward) std::memcpy(forward, fam.forward.data(), fam.forward.size() * sizeof(double));
+        if (inverse) std::memcpy(inverse, fam.inverse.data(), fam.inverse.size() * sizeof(double));
+    });
+}
+
+// --------------------------------------------------------------------- FFT
+
+int skb_fft_create(const skb_workload* w, int precision, skb_fft_provider** out) {
+    return guard([&] {
+        require(out != nullptr, "output handle must be non-null");
+        auto p = std::make_unique<skb_fft_provider>();
+        const auto t0 = Clock::now();
+        p->w = to_workload(w);
+        p->p = to_precision(precision);
+        p->stream = make_stream();
+        p->otherSetup = seconds_since(t0);
+        p->plan = std::make_unique<HorizontalPlan>(p->w, p->p, false, p->w.planes());
+        const auto t1 = Clock::now();
+        const size_t es = element_bytes(p->p);
+        p->real.allocate(es * p->w.realElements());
+        p->spectrum.allocate(2 * es * p->w.spectrumElements());
+        p->retained.allocate(2 * es * std::max<uint64_t>(1, p->plan->modes() * p->w.planes()));
+        p->host.p = p->p;
+        p->allocation = seconds_since(t1) + p->plan->allocationSeconds;
+        *out = p.release();
+    });
+}
+
+int skb_fft_destroy(skb_fft_provider* p) {
+    return guard([&] { delete p; });
+}
+
+int skb_fft_info(const skb_fft_provider* p, skb_provider_info* info) {
+    return guard([&] {
+        require(p != nullptr && info != nullptr, "handle and info must be non-null");
+        std::memset(info, 0, sizeof(*info));
+        info->allocation_seconds = p->allocation;
+        info->planning_seconds = p->plan->planningSeconds;
+        info->other_setup_seconds = p->otherSetup;
+        info->persistent_bytes = p->plan->persistentBytes;
+        info->scratch_bytes = p->plan->scratchBytes;
+        info->planning_bytes = 0;
+        info->active_kx = p->w.nxHalf();
+        info->full_kx = p->w.nxHalf();
+        info->row_transforms_per_direction = p->w.ny * p->w.planes();
+        info->column_transforms_per_direction = p->w.nxHalf() * p->w.planes();
+        info->launches_per_execution = 2;
+        info->precision = p->p == Precision::f64 ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
+        info->destroys_native_input = 0;
+        fill_identity(info, "skb-cuda hand-written sm_100a row/column shared-memory FFT");
+    });
+}
+
+void* skb_fft_stream(skb_fft_provider* p) { return p ? p->stream : nullptr; }
+
+int skb_fft_forward_device(skb_fft_provider* p, const void* real, void* wvm, void* stream) {
+    return guard([&] {
+        require(p && real && wvm, "handle and buffers must be non-null");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->forward_dense(real, wvm, p->w.planes(), s);
+    });
+}
+
+int skb_fft_inverse_device(skb_fft_provider* p, const void* wvm, void* real, void* stream) {
+    return guard([&] {
+        require(p && real && wvm, "handle and buffers must be non-null");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->inverse_dense(wvm, real, p->w.planes(), s);
+    });
+}
+
+int skb_fft_gather_retained_device(skb_fft_provider* p, const void* wvm, const skb_field_view* views,
+                                   uint64_t count, double scale, void* stream) {
+    return guard([&] {
+        require(p && wvm, "handle and buffers must be non-null");
+        require(count == p->w.fields, "one field view per workload field");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->gather_dense(wvm, p->w.planes(), to_views(views, count, p->w.nz), scale, s);
+    });
+}
+
+int skb_fft_embed_retained_device(skb_fft_provider* p, const skb_field_view* views, uint64_t count, void* wvm,
+                                  void* stream) {
+    return guard([&] {
+        require(p && wvm, "handle and buffers must be non-null");
+        require(count == p->w.fields, "one field view per workload field");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->embed_dense(to_views(views, count, p->w.nz), wvm, p->w.planes(), s);
+    });
+}
+
+int skb_fft_forward(skb_fft_provider* p, const double* input, skb_complex* wvm) {
+    return guard([&] {
+        require(p && input && wvm, "handle and buffers must be non-null");
+        p->host.upload(p->real.get(), input, p->w.realElements(), p->stream);
+        p->plan->forward_dense(p->real.get(), p->spectrum.get(), p->w.planes(), p->stream);
+        p->host.download(reinterpret_cast<double*>(wvm), p->spectrum.get(), 2 * p->w.spectrumElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_fft_inverse(skb_fft_provider* p, skb_complex* wvm, double* output) {
+    return guard([&] {
+        require(p && wvm && output, "handle and buffers must be non-null");
+        p->host.upload(p->spectrum.get(), reinterpret_cast<const double*>(wvm), 2 * p->w.spectrumElements(),
+                       p->stream);
+        p->plan->inverse_dense(p->spectrum.get(), p->real.get(), p->w.planes(), p->stream);
+        p->host.download(output, p->real.get(), p->w.realElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_fft_forward_split(skb_fft_provider* p, const double* input, double* re, double* im) {
+    return guard([&] {
+        require(p && input && re && im, "handle and buffers must be non-null");
+        const auto n = p->w.spectrumElements();
+        const size_t es = element_bytes(p->p);
+        if (p->splitRe.bytes() < n * es) {
+            p->splitRe.allocate(n * es);
+            p->splitIm.allocate(n * es);
+        }
+        p->host.upload(p->real.get(), input, p->w.realElements(), p->stream);
+        p->plan->forward_dense(p->real.get(), p->spectrum.get(), p->w.planes(), p->stream);
+        check_cuda(launch_split(p->p == Precision::f64, p->spectrum.get(), p->splitRe.get(), p->splitIm.get(),
+                                (long long)n, p->stream),
+                   "split kernel");
+        p->host.download(re, p->splitRe.get(), n, p->stream);
+        p->host.download(im, p->splitIm.get(), n, p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_fft_inverse_split(skb_fft_provider* p, double* re, double* im, double* output) {
+    return guard([&] {
+        require(p && re && im && output, "handle and buffers must be non-null");
+        const auto n = p->w.spectrumElements();
+        const size_t es = element_bytes(p->p);
+        if (p->splitRe.bytes() < n * es) {
+            p->splitRe.allocate(n * es);
+            p->splitIm.allocate(n * es);
+        }
+        p->host.upload(p->splitRe.get(), re, n, p->stream);
+        p->host.upload(p->splitIm.get(), im, n, p->stream);
+        check_cuda(launch_interleave(p->p == Precision::f64, p->splitRe.get(), p->splitIm.get(), p->spectrum.get(),
+                                     (long long)n, p->stream),
+                   "interleave kernel");
+        p->plan->inverse_dense(p->spectrum.get(), p->real.get(), p->w.planes(), p->stream);
+        p->host.download(output, p->real.get(), p->w.realElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_fft_gather_retained(skb_fft_provider* p, const skb_complex* wvm, skb_complex* retained) {
+    return guard([&] {
+        require(p && wvm && retained, "handle and buffers must be non-null");
+        const size_t ces = 2 * element_bytes(p->p);
+        p->host.upload(p->spectrum.get(), reinterpret_cast<const double*>(wvm), 2 * p->w.spectrumElements(),
+                       p->stream);
+        p->plan->gather_dense(p->spectrum.get(), p->w.planes(), retained_views(p->retained.get(), p->w, ces), 1.0,
+                              p->stream);
+        p->host.download(reinterpret_cast<double*>(retained), p->retained.get(),
+                         2 * p->plan->modes() * p->w.planes(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_fft_embed_retained(skb_fft_provider* p, const skb_complex* retained, skb_complex* wvm) {
+    return guard([&] {
+        require(p && wvm && retained, "handle and buffers must be non-null");
+        const size_t ces = 2 * element_bytes(p->p);
+        p->host.upload(p->retained.get(), reinterpret_cast<const double*>(retained),
+                       2 * p->plan->modes() * p->w.planes(), p->stream);
+        p->plan->embed_dense(retained_views(p->retained.get(), p->w, ces), p->spectrum.get(), p->w.planes(),
+                             p->stream);
+        p->host.download(reinterpret_cast<double*>(wvm), p->spectrum.get(), 2 * p->w.spectrumElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_fft_gather_retained_to_split(skb_fft_provider* p, const skb_complex* wvm, double* re, double* im,
+                                     double scale) {
+    return guard([&] {
+        require(p && wvm && re && im, "handle and buffers must be non-null");
+        const auto n = p->plan->modes() * p->w.planes();
+        const size_t es = element_bytes(p->p);
+        if (p->splitRe.bytes() < std::max<uint64_t>(n, p->w.spectrumElements()) * es) {
+            p->splitRe.allocate(std::max<uint64_t>(n, p->w.spectrumElements()) * es);
+            p->splitIm.allocate(std::max<uint64_t>(n, p->w.spectrumElements()) * es);
+        }
+        p->host.upload(p->spectrum.get(), reinterpret_cast<const double*>(wvm), 2 * p->w.spectrumElements(),
+                       p->stream);
+        p->plan->gather_dense(p->spectrum.get(), p->w.planes(),
+                              retained_split_views(p->splitRe.get(), p->splitIm.get(), p->w, es), scale, p->stream);
+        p->host.download(re, p->splitRe.get(), n, p->stream);
+        p->host.download(im, p->splitIm.get(), n, p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_fft_embed_retained_from_split(skb_fft_provider* p, const double* re, const double* im, skb_complex* wvm) {
+    return guard([&] {
+        require(p && wvm && re && im, "handle and buffers must be non-null");
+        const auto n = p->plan->modes() * p->w.planes();
+        const size_t es = element_bytes(p->p);
+        if (p->splitRe.bytes() < std::max<uint64_t>(n, p->w.spectrumElements()) * es) {
+            p->splitRe.allocate(std::max<uint64_t>(n, p->w.spectrumElements()) * es);
+            p->splitIm.allocate(std::max<uint64_t>(n, p->w.spectrumElements()) * es);
+        }
+        p->host.upload(p->splitRe.get(), re, n, p->stream);
+        p->host.upload(p->splitIm.get(), im, n, p->stream);
+        p->plan->embed_dense(retained_split_views(p->splitRe.get(), p->splitIm.get(), p->w, es), p->spectrum.get(),
+                             p->w.planes(), p->stream);
+        p->host.download(reinterpret_cast<double*>(wvm), p->spectrum.get(), 2 * p->w.spectrumElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+// ------------------------------------------------------------------ pruned
+
+int skb_pruned_create(const skb_workload* w, int precision, skb_pruned_provider** out) {
+    return guard([&] {
+        require(out != nullptr, "output handle must be non-null");
+        auto p = std::make_unique<skb_pruned_provider>();
+        const auto t0 = Clock::now();
+        p->w = to_workload(w);
+        p->p = to_precision(precision);
+        p->stream = make_stream();
+        p->otherSetup = seconds_since(t0);
+        p->plan = std::make_unique<HorizontalPlan>(p->w, p->p, true, p->w.planes());
+        const auto t1 = Clock::now();
+        const size_t es = element_bytes(p->p);
+        p->real.allocate(es * p->w.realElements());
+        p->retained.allocate(2 * es * p->plan->modes() * p->w.planes());
+        p->retainedIm.allocate(es * p->plan->modes() * p->w.planes());
+        p->host.p = p->p;
+        p->allocation = seconds_since(t1) + p->plan->allocationSeconds;
+        *out = p.release();
+    });
+}
+
+int skb_pruned_destroy(skb_pruned_provider* p) {
+    return guard([&] { delete p; });
+}
+
+int skb_pruned_info(const skb_pruned_provider* p, skb_provider_info* info) {
+    return guard([&] {
+        require(p != nullptr && info != nullptr, "handle and info must be non-null");
+        std::memset(info, 0, sizeof(*info));
+        info->allocation_seconds = p->allocation;
+        info->planning_seconds = p->plan->planningSeconds;
+        info->other_setup_seconds = p->otherSetup;
+        info->persistent_bytes = p->plan->persistentBytes;
+        info->scratch_bytes = p->plan->scratchBytes;
+        info->active_kx = static_cast<uint64_t>(p->plan->keep());
+        info->full_kx = p->w.nxHalf();
+        info->row_transforms_per_direction = p->w.ny * p->w.planes();
+        info->column_transforms_per_direction = info->active_kx * p->w.planes();
+        info->omitted_column_transforms_per_direction = (info->full_kx - info->active_kx) * p->w.planes();
+        info->launches_per_execution = 2;
+        info->precision = p->p == Precision::f64 ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
+        fill_identity(info, "skb-cuda hand-written sm_100a pruned row/active-column FFT with fused retention");
+    });
+}
+
+void* skb_pruned_stream(skb_pruned_provider* p) { return p ? p->stream : nullptr; }
+
+int skb_pruned_forward_device(skb_pruned_provider* p, const void* real, const skb_field_view* fields, uint64_t count,
+                              double scale, void* stream) {
+    return guard([&] {
+        require(p && real, "handle and buffers must be non-null");
+        require(count == p->w.fields, "one field view per workload field");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->forward(real, p->w.planes(), to_views(fields, count, p->w.nz), scale, s);
+    });
+}
+
+int skb_pruned_inverse_device(skb_pruned_provider* p, const skb_field_view* fields, uint64_t count, void* real,
+                              void* stream) {
+    return guard([&] {
+        require(p && real, "handle and buffers must be non-null");
+        require(count == p->w.fields, "one field view per workload field");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->inverse(to_views(fields, count, p->w.nz), real, s);
+    });
+}
+
+int skb_pruned_forward_rows_device(skb_pruned_provider* p, const void* real, void* stream) {
+    return guard([&] {
+        require(p && real, "handle and buffers must be non-null");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->forward_rows(real, p->w.planes(), s);
+    });
+}
+
+int skb_pruned_forward_columns_device(skb_pruned_provider* p, const skb_field_view* fields, uint64_t count,
+                                      double scale, void* stream) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        require(count == p->w.fields, "one field view per workload field");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->forward_columns(to_views(fields, count, p->w.nz), scale, s);
+    });
+}
+
+int skb_pruned_inverse_columns_device(skb_pruned_provider* p, const skb_field_view* fields, uint64_t count,
+                                      void* stream) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        require(count == p->w.fields, "one field view per workload field");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->inverse_columns(to_views(fields, count, p->w.nz), s);
+    });
+}
+
+int skb_pruned_inverse_rows_device(skb_pruned_provider* p, void* real, void* stream) {
+    return guard([&] {
+        require(p && real, "handle and buffers must be non-null");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->plan->inverse_rows(real, p->w.planes(), s);
+    });
+}
+
+int skb_pruned_forward(skb_pruned_provider* p, const double* input, skb_complex* retained) {
+    return guard([&] {
+        require(p && input && retained, "handle and buffers must be non-null");
+        const size_t ces = 2 * element_bytes(p->p);
+        p->host.upload(p->real.get(), input, p->w.realElements(), p->stream);
+        p->plan->forward(p->real.get(), p->w.planes(), retained_views(p->retained.get(), p->w, ces), 1.0, p->stream);
+        p->host.download(reinterpret_cast<double*>(retained), p->retained.get(), 2 * p->plan->modes() * p->w.planes(),
+                         p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_pruned_forward_split(skb_pruned_provider* p, const double* input, double* re, double* im, double scale) {
+    return guard([&] {
+        require(p && input && re && im, "handle and buffers must be non-null");
+        const size_t es = element_bytes(p->p);
+        const auto n = p->plan->modes() * p->w.planes();
+        p->host.upload(p->real.get(), input, p->w.realElements(), p->stream);
+        p->plan->forward(p->real.get(), p->w.planes(),
+                         retained_split_views(p->retained.get(), p->retainedIm.get(), p->w, es), scale, p->stream);
+        p->host.download(re, p->retained.get(), n, p->stream);
+        p->host.download(im, p->retainedIm.get(), n, p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_pruned_inverse(skb_pruned_provider* p, const skb_complex* retained, double* output) {
+    return guard([&] {
+        require(p && output && retained, "handle and buffers must be non-null");
+        const size_t ces = 2 * element_bytes(p->p);
+        p->host.upload(p->retained.get(), reinterpret_cast<const double*>(retained),
+                       2 * p->plan->modes() * p->w.planes(), p->stream);
+        p->plan->inverse(retained_views(p->retained.get(), p->w, ces), p->real.get(), p->stream);
+        p->host.download(output, p->real.get(), p->w.realElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_pruned_inverse_split(skb_pruned_provider* p, const double* re, const double* im, double* output) {
+    return guard([&] {
+        require(p && output && re && im, "handle and buffers must be non-null");
+        const size_t es = element_bytes(p->p);
+        const auto n = p->plan->modes() * p->w.planes();
+        p->host.upload(p->retained.get(), re, n, p->stream);
+        p->host.upload(p->retainedIm.get(), im, n, p->stream);
+        p->plan->inverse(retained_split_views(p->retained.get(), p->retainedIm.get(), p->w, es), p->real.get(),
+                         p->stream);
+        p->host.download(output, p->real.get(), p->w.realElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_pruned_forward_split_fields(skb_pruned_provider* p, const double* input, const skb_field_view* fields,
+                                    uint64_t count, double scale) {
+    return guard([&] {
+        require(p && input && fields, "handle and buffers must be non-null");
+        require(count == p->w.fields, "Streaming pruned output field views must match the workload field count.");
+        for (uint64_t f = 0; f < count; ++f)
+            require(fields[f].real && fields[f].imag && fields[f].mode_stride >= p->w.nz,
+                    "Streaming pruned output field view is invalid.");
+        const size_t es = element_bytes(p->p);
+        const auto H = p->plan->modes(), nz = p->w.nz;
+        p->host.upload(p->real.get(), input, p->w.realElements(), p->stream);
+        // Device-side compact split fields [field][mode][z], then strided copies out.
+        ViewSet v{};
+        v.count = static_cast<int>(count);
+        for (uint64_t f = 0; f < count; ++f)
+            v.v[f] = {p->retained.get<unsigned char>() + es * f * H * nz,
+                      p->retainedIm.get<unsigned char>() + es * f * H * nz, static_cast<long long>(nz)};
+        p->plan->forward(p->real.get(), p->w.planes(), v, scale, p->stream);
+        if (p->p == Precision::f64) {
+            for (uint64_t f = 0; f < count; ++f) {
+                check_cuda(cudaMemcpy2DAsync(fields[f].real, fields[f].mode_stride * sizeof(double),
+                                             p->retained.get<unsigned char>() + es * f * H * nz, nz * es, nz * es, H,
+                                             cudaMemcpyDeviceToHost, p->stream),
+                           "cudaMemcpy2DAsync");
+                check_cuda(cudaMemcpy2DAsync(fields[f].imag, fields[f].mode_stride * sizeof(double),
+                                             p->retainedIm.get<unsigned char>() + es * f * H * nz, nz * es, nz * es,
+                                             H, cudaMemcpyDeviceToHost, p->stream),
+                           "cudaMemcpy2DAsync");
+            }
+            sync(p->stream);
+        } else {
+            std::vector<double> re(H * nz), im(H * nz);
+            for (uint64_t f = 0; f < count; ++f) {
+                p->host.download(re.data(), p->retained.get<unsigned char>() + es * f * H * nz, H * nz, p->stream);
+                p->host.download(im.data(), p->retainedIm.get<unsigned char>() + es * f * H * nz, H * nz, p->stream);
+                sync(p->stream);
+                auto* dr = static_cast<double*>(fields[f].real);
+                auto* di = static_cast<double*>(fields[f].imag);
+                for (uint64_t m = 0; m < H; ++m)
+                    for (uint64_t z = 0; z < nz; ++z) {
+                        dr[z + fields[f].mode_stride * m] = re[z + nz * m];
+                        di[z + fields[f].mode_stride * m] = im[z + nz * m];
+                    }
+            }
+        }
+    });
+}
+
+int skb_pruned_inverse_split_fields(skb_pruned_provider* p, const skb_field_view* fields, uint64_t count,
+                                    double* output) {
+    return guard([&] {
+        require(p && output && fields, "handle and buffers must be non-null");
+        require(count == p->w.fields, "Streaming pruned input field views must match the workload field count.");
+        for (uint64_t f = 0; f < count; ++f)
+            require(fields[f].real && fields[f].imag && fields[f].mode_stride >= p->w.nz,
+                    "Streaming pruned input field view is invalid.");
+        const size_t es = element_bytes(p->p);
+        const auto H = p->plan->modes(), nz = p->w.nz;
+        std::vector<double> re(H * nz), im(H * nz);
+        for (uint64_t f = 0; f < count; ++f) {
+            const auto* sr = static_cast<const double*>(fields[f].real);
+            const auto* si = static_cast<const double*>(fields[f].imag);
+            for (uint64_t m = 0; m < H; ++m)
+                for (uint64_t z = 0; z < nz; ++z) {
+                    re[z + nz * m] = sr[z + fields[f].mode_stride * m];
+                    im[z + nz * m] = si[z + fields[f].mode_stride * m];
+                }
+            p->host.upload(p->retained.get<unsigned char>() + es * f * H * nz, re.data(), H * nz, p->stream);
+            p->host.upload(p->retainedIm.get<unsigned char>() + es * f * H * nz, im.data(), H * nz, p->stream);
+            sync(p->stream);
+        }
+        ViewSet v{};
+        v.count = static_cast<int>(count);
+        for (uint64_t f = 0; f < count; ++f)
+            v.v[f] = {p->retained.get<unsigned char>() + es * f * H * nz,
+                      p->retainedIm.get<unsigned char>() + es * f * H * nz, static_cast<long long>(nz)};
+        p->plan->inverse(v, p->real.get(), p->stream);
+        p->host.download(output, p->real.get(), p->w.realElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+// ---------------------------------------------------------------- vertical
+
+int skb_vertical_create(const skb_workload* w, const skb_mode_group* groups, uint64_t group_count,
+                        const double* forward, const double* inverse, int layout, int policy, int gemm_precision,
+                        skb_vertical_provider** out) {
+    return guard([&] {
+        require(out != nullptr, "output handle must be non-null");
+        require(groups != nullptr && group_count > 0, "Vertical GEMM requires at least one horizontal mode and field.");
+        require(layout == SKB_LAYOUT_INTERLEAVED || layout == SKB_LAYOUT_SPLIT, "unknown layout");
+        require(policy >= SKB_BUFFERS_BIDIRECTIONAL && policy <= SKB_BUFFERS_INVERSE_ONLY, "unknown buffer policy");
+        auto p = std::make_unique<skb_vertical_provider>();
+        p->w = to_workload(w);
+        p->layout = layout;
+        p->policy = policy;
+        if (gemm_precision == SKB_GEMM_FP64) {
+            p->gp = GemmPrecision::f64;
+            p->p = Precision::f64;
+        } else if (gemm_precision == SKB_GEMM_FP32) {
+            p->gp = GemmPrecision::f32;
+            p->p = Precision::f32;
+        } else {
+            throw Error(SKB_ERR_RUNTIME, "unsupported: tensor-core split GEMM precision is not built in this library");
+        }
+        p->host.p = p->p;
+        const auto prepStart = Clock::now();
+        std::vector<ModeGroup> g(group_count);
+        uint64_t modes = 0;
+        for (uint64_t i = 0; i < group_count; ++i) {
+            g[i] = {groups[i].squared_mode_key, groups[i].first_mode, groups[i].mode_count};
+            modes += groups[i].mode_count;
+        }
+        VerticalFamily fam;
+        fam.nz = p->w.nz;
+        fam.nj = p->w.nj();
+        require(fam.nj > 0, "Vertical GEMM requires Nz >= 2.");
+        const bool fwd = policy != SKB_BUFFERS_INVERSE_ONLY, inv = policy != SKB_BUFFERS_FORWARD_ONLY;
+        require(!fwd || forward != nullptr, "forward matrices must be non-null");
+        require(!inv || inverse != nullptr, "inverse matrices must be non-null");
+        fam.groups = group_count;
+        const auto elems = fam.nz * fam.nj * group_count;
+        fam.forward.assign(elems, 0.0);
+        fam.inverse.assign(elems, 0.0);
+        if (fwd) std::memcpy(fam.forward.data(), forward, elems * sizeof(double));
+        if (inv) std::memcpy(fam.inverse.data(), inverse, elems * sizeof(double));
+        p->stream = make_stream();
+        if (fwd)
+            p->forward = std::make_unique<VerticalPlan>(p->gp, static_cast<int>(fam.nj), static_cast<int>(fam.nz), g,
+                                                        p->w.fields, 1, transpose_family(fam, true));
+        if (inv)
+            p->inverse = std::make_unique<VerticalPlan>(p->gp, static_cast<int>(fam.nz), static_cast<int>(fam.nj), g,
+                                                        p->w.fields, 1, transpose_family(fam, false));
+        p->preparation = seconds_since(prepStart);
+        p->groups = group_count;
+        p->columns = modes * p->w.fields;
+        const auto allocStart = Clock::now();
+        const size_t es = element_bytes(p->p);
+        const size_t mult = layout == SKB_LAYOUT_SPLIT ? 1 : 2;
+        if (fwd) {
+            p->physIn.allocate(mult * es * p->columns * fam.nz);
+            p->modalOut.allocate(mult * es * p->columns * fam.nj);
+            if (layout == SKB_LAYOUT_SPLIT) {
+                p->physInIm.allocate(es * p->columns * fam.nz);
+                p->modalOutIm.allocate(es * p->columns * fam.nj);
+            }
+        }
+        if (inv) {
+            p->modalIn.allocate(mult * es * p->columns * fam.nj);
+            p->physOut.allocate(mult * es * p->columns * fam.nz);
+            if (layout == SKB_LAYOUT_SPLIT) {
+                p->modalInIm.allocate(es * p->columns * fam.nj);
+                p->physOutIm.allocate(es * p->columns * fam.nz);
+            }
+        }
+        p->allocation = seconds_since(allocStart);
+        *out = p.release();
+    });
+}
+
+int skb_vertical_destroy(skb_vertical_provider* p) {
+    return guard([&] { delete p; });
+}
+
+int skb_vertical_info(const skb_vertical_provider* p, skb_provider_info* info) {
+    return guard([&] {
+        require(p != nullptr && info != nullptr, "handle and info must be non-null");
+        std::memset(info, 0, sizeof(*info));
+        info->allocation_seconds = p->allocation;
+        info->planning_seconds = p->preparation;
+        info->persistent_bytes = (p->forward ? p->forward->persistentBytes() : 0) +
+                                 (p->inverse ? p->inverse->persistentBytes() : 0) + p->physIn.bytes() +
+                                 p->physInIm.bytes() + p->modalOut.bytes() + p->modalOutIm.bytes() +
+                                 p->modalIn.bytes() + p->modalInIm.bytes() + p->physOut.bytes() + p->physOutIm.bytes();
+        info->launches_per_execution = 1;
+        info->precision = p->p == Precision::f64 ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
+        info->column_transforms_per_direction = p->columns;
+        fill_identity(info, "skb-cuda hand-written sm_100a K2-grouped GEMM (one launch for all groups)");
+    });
+}
+
+void* skb_vertical_stream(skb_vertical_provider* p) { return p ? p->stream : nullptr; }
+
+namespace {
+const VerticalPlan& need(const std::unique_ptr<VerticalPlan>& plan, const char* what) {
+    if (!plan) throw Error(SKB_ERR_LOGIC, what);
+    return *plan;
+}
+}  // namespace
+
+int skb_vertical_forward_device(skb_vertical_provider* p, const void* in_re, const void* in_im, void* out_re,
+                                void* out_im, void* stream) {
+    return guard([&] {
+        require(p && in_re && out_re, "handle and buffers must be non-null");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        need(p->forward, "Forward GEMM component requested from an inverse-only provider.")
+            .execute({const_cast<void*>(in_re), const_cast<void*>(in_im)}, {out_re, out_im}, s);
+    });
+}
+
+int skb_vertical_inverse_device(skb_vertical_provider* p, const void* in_re, const void* in_im, void* out_re,
+                                void* out_im, void* stream) {
+    return guard([&] {
+        require(p && in_re && out_re, "handle and buffers must be non-null");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        need(p->inverse, "Inverse GEMM component requested from a forward-only provider.")
+            .execute({const_cast<void*>(in_re), const_cast<void*>(in_im)}, {out_re, out_im}, s);
+    });
+}
+
+namespace {
+void require_layout(const skb_vertical_provider* p, int layout) {
+    if (p->layout != layout)
+        throw Error(SKB_ERR_LOGIC, layout == SKB_LAYOUT_SPLIT
+                                       ? "Split GEMM component requested from the complex GEMM provider."
+                                       : "Interleaved GEMM component requested from the split GEMM provider.");
+}
+}  // namespace
+
+int skb_vertical_load_physical_input(skb_vertical_provider* p, const skb_complex* input) {
+    return guard([&] {
+        require(p && input, "handle and input must be non-null");
+        require_layout(p, SKB_LAYOUT_INTERLEAVED);
+        need(p->forward, "Forward GEMM component requested from an inverse-only provider.");
+        p->host.upload(p->physIn.get(), reinterpret_cast<const double*>(input), 2 * p->columns * p->w.nz, p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_load_modal_input(skb_vertical_provider* p, const skb_complex* input) {
+    return guard([&] {
+        require(p && input, "handle and input must be non-null");
+        require_layout(p, SKB_LAYOUT_INTERLEAVED);
+        need(p->inverse, "Inverse GEMM component requested from a forward-only provider.");
+        p->host.upload(p->modalIn.get(), reinterpret_cast<const double*>(input), 2 * p->columns * p->w.nj(),
+                       p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_load_physical_input_split(skb_vertical_provider* p, const double* re, const double* im) {
+    return guard([&] {
+        require(p && re && im, "handle and inputs must be non-null");
+        require_layout(p, SKB_LAYOUT_SPLIT);
+        need(p->forward, "Forward GEMM component requested from an inverse-only provider.");
+        p->host.upload(p->physIn.get(), re, p->columns * p->w.nz, p->stream);
+        p->host.upload(p->physInIm.get(), im, p->columns * p->w.nz, p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_load_modal_input_split(skb_vertical_provider* p, const double* re, const double* im) {
+    return guard([&] {
+        require(p && re && im, "handle and inputs must be non-null");
+        require_layout(p, SKB_LAYOUT_SPLIT);
+        need(p->inverse, "Inverse GEMM component requested from a forward-only provider.");
+        p->host.upload(p->modalIn.get(), re, p->columns * p->w.nj(), p->stream);
+        p->host.upload(p->modalInIm.get(), im, p->columns * p->w.nj(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_execute_forward(skb_vertical_provider* p) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        need(p->forward, "Forward GEMM component requested from an inverse-only provider.")
+            .execute({p->physIn.get(), p->physInIm.get()}, {p->modalOut.get(), p->modalOutIm.get()}, p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_execute_inverse(skb_vertical_provider* p) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        need(p->inverse, "Inverse GEMM component requested from a forward-only provider.")
+            .execute({p->modalIn.get(), p->modalInIm.get()}, {p->physOut.get(), p->physOutIm.get()}, p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_copy_forward_output(skb_vertical_provider* p, skb_complex* output) {
+    return guard([&] {
+        require(p && output, "handle and output must be non-null");
+        require_layout(p, SKB_LAYOUT_INTERLEAVED);
+        need(p->forward, "Forward GEMM component requested from an inverse-only provider.");
+        p->host.download(reinterpret_cast<double*>(output), p->modalOut.get(), 2 * p->columns * p->w.nj(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_copy_inverse_output(skb_vertical_provider* p, skb_complex* output) {
+    return guard([&] {
+        require(p && output, "handle and output must be non-null");
+        require_layout(p, SKB_LAYOUT_INTERLEAVED);
+        need(p->inverse, "Inverse GEMM component requested from a forward-only provider.");
+        p->host.download(reinterpret_cast<double*>(output), p->physOut.get(), 2 * p->columns * p->w.nz, p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_copy_forward_output_split(skb_vertical_provider* p, double* re, double* im) {
+    return guard([&] {
+        require(p && re && im, "handle and outputs must be non-null");
+        require_layout(p, SKB_LAYOUT_SPLIT);
+        need(p->forward, "Forward GEMM component requested from an inverse-only provider.");
+        p->host.download(re, p->modalOut.get(), p->columns * p->w.nj(), p->stream);
+        p->host.download(im, p->modalOutIm.get(), p->columns * p->w.nj(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_vertical_copy_inverse_output_split(skb_vertical_provider* p, double* re, double* im) {
+    return guard([&] {
+        require(p && re && im, "handle and outputs must be non-null");
+        require_layout(p, SKB_LAYOUT_SPLIT);
+        need(p->inverse, "Inverse GEMM component requested from a forward-only provider.");
+        p->host.download(re, p->physOut.get(), p->columns * p->w.nz, p->stream);
+        p->host.download(im, p->physOutIm.get(), p->columns * p->w.nz, p->stream);
+        sync(p->stream);
+    });
+}
+
+// --------------------------------------------------------------- pointwise
+
+int skb_pointwise_create(uint64_t volume, double scale, int precision, skb_pointwise_executor** out) {
+    return guard([&] {
+        require(out != nullptr, "output handle must be non-null");
+        require(volume > 0, "Pointwise advection volume must be positive.");
+        auto p = std::make_unique<skb_pointwise_executor>();
+        p->volume = volume;
+        p->scale = scale;
+        p->p = to_precision(precision);
+        p->host.p = p->p;
+        p->stream = make_stream();
+        *out = p.release();
+    });
+}
+
+int skb_pointwise_destroy(skb_pointwise_executor* p) {
+    return guard([&] { delete p; });
+}
+
+void* skb_pointwise_stream(skb_pointwise_executor* p) { return p ? p->stream : nullptr; }
+
+int skb_pointwise_execute_device(skb_pointwise_executor* p, const void* shared, const void* derivative, void* target,
+                                 void* stream) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        require(shared && derivative && target, "Pointwise advection buffers must be non-null.");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        check_cuda(launch_pointwise(p->p == Precision::f64, static_cast<long long>(p->volume), p->scale, shared,
+                                    derivative, target, sm_count(), s),
+                   "pointwise advection kernel");
+    });
+}
+
+int skb_pointwise_execute(skb_pointwise_executor* p, const double* shared, const double* derivative,
+                          double* target) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        require(shared && derivative && target, "Pointwise advection buffers must be non-null.");
+        const size_t es = element_bytes(p->p);
+        if (p->shared.bytes() == 0) {
+            p->shared.allocate(3 * es * p->volume);
+            p->derivative.allocate(3 * es * p->volume);
+            p->target.allocate(es * p->volume);
+        }
+        p->host.upload(p->shared.get(), shared, 3 * p->volume, p->stream);
+        p->host.upload(p->derivative.get(), derivative, 3 * p->volume, p->stream);
+        check_cuda(launch_pointwise(p->p == Precision::f64, static_cast<long long>(p->volume), p->scale,
+                                    p->shared.get(), p->derivative.get(), p->target.get(), sm_count(), p->stream),
+                   "pointwise advection kernel");
+        p->host.download(target, p->target.get(), p->volume, p->stream);
+        sync(p->stream);
+    });
+}
+
+// -------------------------------------------------------------------- flux
+
+int skb_flux_create(const skb_flux_options* o, skb_flux** out) {
+    return guard([&] {
+        require(o != nullptr && out != nullptr, "options and output handle must be non-null");
+        require(o->mode >= SKB_FLUX_FP64_PLAIN && o->mode <= SKB_FLUX_SPLIT_BF16X3, "unknown flux mode");
+        FluxConfig cfg;
+        cfg.n = o->n;
+        cfg.nz = o->nz;
+        cfg.targets = o->targets;
+        cfg.members = o->members;
+        cfg.mode = static_cast<FluxMode>(o->mode);
+        cfg.family = o->family;
+        cfg.familySeed = o->family_seed;
+        require(cfg.family == SKB_FAMILY_K2_ROTATION || cfg.family == SKB_FAMILY_STURM_LIOUVILLE,
+                "flux family must be K2 rotation or Sturm-Liouville");
+        auto p = std::make_unique<skb_flux>();
+        p->pipeline = std::make_unique<FluxPipeline>(cfg);
+        p->stream = make_stream();
+        *out = p.release();
+    });
+}
+
+int skb_flux_destroy(skb_flux* p) {
+    return guard([&] { delete p; });
+}
+
+int skb_flux_info(const skb_flux* p, skb_provider_info* info) {
+    return guard([&] {
+        require(p != nullptr && info != nullptr, "handle and info must be non-null");
+        std::memset(info, 0, sizeof(*info));
+        const auto& f = *p->pipeline;
+        info->allocation_seconds = f.allocationSeconds;
+        info->planning_seconds = f.planningSeconds;
+        info->persistent_bytes = f.persistentBytes;
+        info->scratch_bytes = f.scratchBytes;
+        info->launches_per_execution = f.launchesPerExecution();
+        info->precision = f.f64() ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
+        fill_identity(info, f.familyId.c_str());
+    });
+}
+
+void* skb_flux_stream(skb_flux* p) { return p ? p->stream : nullptr; }
+
+int skb_flux_sizes(const skb_flux* p, uint64_t* modes, uint64_t* nj, uint64_t* in, uint64_t* out) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        if (modes) *modes = p->pipeline->modes();
+        if (nj) *nj = p->pipeline->nj();
+        if (in) *in = p->pipeline->inputElements();
+        if (out) *out = p->pipeline->outputElements();
+    });
+}
+
+int skb_flux_execute_device(skb_flux* p, const void* in, void* out, void* stream) {
+    return guard([&] {
+        require(p && in && out, "handle and buffers must be non-null");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->pipeline->execute(in, out, s);
+    });
+}
+
+int skb_flux_execute(skb_flux* p, const skb_complex* in, skb_complex* out) {
+    return guard([&] {
+        require(p && in && out, "handle and buffers must be non-null");
+        auto& f = *p->pipeline;
+        const size_t es = f.f64() ? sizeof(double) : sizeof(float);
+        if (p->in.bytes() == 0) {
+            p->in.allocate(2 * es * f.inputElements());
+            p->out.allocate(2 * es * f.outputElements());
+        }
+        p->host.p = f.f64() ? Precision::f64 : Precision::f32;
+        p->host.ensure(2 * std::max(f.inputElements(), f.outputElements()));
+        p->host.upload(p->in.get(), reinterpret_cast<const double*>(in), 2 * f.inputElements(), p->stream);
+        f.execute(p->in.get(), p->out.get(), p->stream);
+        p->host.download(reinterpret_cast<double*>(out), p->out.get(), 2 * f.outputElements(), p->stream);
+        sync(p->stream);
+    });
+}
+
+int skb_flux_capture_graph(skb_flux* p, const void* in, void* out) {
+    return guard([&] {
+        require(p && in && out, "handle and buffers must be non-null");
+        p->pipeline->capture(in, out, p->stream);
+    });
+}
+
+int skb_flux_replay_graph(skb_flux* p, void* stream) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        p->pipeline->replay(stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    });
+}
+
+// ------------------------------------------------------------------ timing
+
+int skb_timer_create(skb_timer** out) {
+    return guard([&] {
+        require(out != nullptr, "output handle must be non-null");
+        auto t = std::make_unique<skb_timer>();
+        check_cuda(cudaEventCreate(&t->start), "cudaEventCreate");
+        check_cuda(cudaEventCreate(&t->stop), "cudaEventCreate");
+        *out = t.release();
+    });
+}
+
+int skb_timer_destroy(skb_timer* t) {
+    return guard([&] { delete t; });
+}
+
+int skb_timer_start(skb_timer* t, void* stream) {
+    return guard([&] { check_cuda(cudaEventRecord(t->start, static_cast<cudaStream_t>(stream)), "cudaEventRecord"); });
+}
+
+int skb_timer_stop(skb_timer* t, void* stream) {
+    return guard([&] { check_cuda(cudaEventRecord(t->stop, static_cast<cudaStream_t>(stream)), "cudaEventRecord"); });
+}
+
+int skb_timer_elapsed_ms(skb_timer* t, double* ms) {
+    return guard([&] {
+        require(t && ms, "timer and output must be non-null");
+        check_cuda(cudaEventSynchronize(t->stop), "cudaEventSynchronize");
+        float f = 0.0f;
+        check_cuda(cudaEventElapsedTime(&f, t->start, t->stop), "cudaEventElapsedTime");
+        *ms = f;
+    });
+}
+
+// ----------------------------------------------------------------- buffers
+
+int skb_device_alloc(uint64_t bytes, void** ptr) {
+    return guard([&] {
+        require(ptr != nullptr, "output pointer must be non-null");
+        check_cuda(cudaMalloc(ptr, bytes), "cudaMalloc");
+    });
+}
+
+int skb_device_free(void* ptr) {
+    return guard([&] { check_cuda(cudaFree(ptr), "cudaFree"); });
+}
+
+int skb_host_alloc_pinned(uint64_t bytes, void** ptr) {
+    return guard([&] {
+        require(ptr != nullptr, "output pointer must be non-null");
+        check_cuda(cudaMallocHost(ptr, bytes), "cudaMallocHost");
+    });
+}
+
+int skb_host_free_pinned(void* ptr) {
+    return guard([&] { check_cuda(cudaFreeHost(ptr), "cudaFreeHost"); });
+}
+
+int skb_copy_to_device(void* dst, const void* src, uint64_t bytes, void* stream) {
+    return guard([&] {
+        check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream)),
+                   "cudaMemcpyAsync H2D");
+    });
+}
+
+int skb_copy_to_host(void* dst, const void* src, uint64_t bytes, void* stream) {
+    return guard([&] {
+        check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)),
+                   "cudaMemcpyAsync D2H");
+    });
+}
+
+int skb_stream_synchronize(void* stream) {
+    return guard([&] { check_cuda(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "cudaStreamSynchronize"); });
+}
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// The composed 15 -> 4 (or 12 -> 3) antialiased flux on the device.
+//
+// Order and normalisation follow runProductionLifetimeFluxBenchmark's
+// streamed graph (src/benchmark.cpp:4328-4424): inverse vertical GEMM of all
+// input fields, inverse pruned horizontal of [U,V,W] once, then per target the
+// inverse of its derivative triple, the pointwise product
+// -1/(Nx*Ny)^2 (u qx + v qy + w qz), the forward pruned horizontal with
+// retention, and finally the forward vertical GEMM of the targets.  Input slot
+// map (benchmark.cpp:4138): slots 0..2 are [U,V,W]; slots 3+3t..5+3t are
+// [q_t,x, q_t,y, q_t,z].  Ensemble members are independent and batched into
+// every launch.
+
+#pragma once
+
+#include <cstdint>
+#include <memory>
+
+#include "runtime.hpp"
+
+namespace skb {
+
+enum class FluxMode { fp64_plain = 0, fp32 = 1, split_tf32x3 = 2, split_bf16x3 = 3 };
+
+struct FluxConfig {
+    std::uint64_t n = 0, nz = 0, targets = 4, members = 1;
+    FluxMode mode = FluxMode::fp64_plain;
+    int family = 1;  // SKB_FAMILY_K2_ROTATION or SKB_FAMILY_STURM_LIOUVILLE
+    std::uint64_t familySeed = 0;
+};
+
+class FluxPipeline {
+public:
+    explicit FluxPipeline(const FluxConfig& cfg);
+    ~FluxPipeline();
+
+    // Device arrays of the pipeline's I/O precision (double for fp64_plain,
+    // float otherwise): modal input [member][mode][3+3T][j], output
+    // [member][mode][T][j].
+    void execute(const void* modalIn, void* modalOut, cudaStream_t s);
+    void capture(const void* modalIn, void* modalOut, cudaStream_t s);
+    void replay(cudaStream_t s);
+
+    std::uint64_t modes() const { return modes_; }
+    std::uint64_t nj() const { return nj_; }
+    std::uint64_t fieldsIn() const { return fieldsIn_; }
+    std::uint64_t inputElements() const { return cfg_.members * modes_ * fieldsIn_ * nj_; }
+    std::uint64_t outputElements() const { return cfg_.members * modes_ * cfg_.targets * nj_; }
+    bool f64() const { return cfg_.mode == FluxMode::fp64_plain; }
+    const FluxConfig& config() const { return cfg_; }
+    std::uint64_t launchesPerExecution() const { return launches_; }
+
+    double allocationSeconds = 0.0, planningSeconds = 0.0;
+    std::uint64_t persistentBytes = 0, scratchBytes = 0;
+    std::string familyId;
+
+private:
+    FluxConfig cfg_;
+    Workload wOut_;
+    std::uint64_t modes_ = 0, nj_ = 0, fieldsIn_ = 0, volume_ = 0;
+    std::unique_ptr<HorizontalPlan> horizontal_;
+    std::unique_ptr<VerticalPlan> inverseGemm_, forwardGemm_;
+    DeviceBuffer physIn_, shared_, deriv_, target_, physOut_;
+    std::uint64_t launches_ = 0;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graphExec_ = nullptr;
+};
+
+}  // namespace skb

@@ -1,0 +1,260 @@
+#include "runtime.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+#include "util.hpp"
+
+namespace skb {
+
+void throw_cuda(cudaError_t err, const char* what) {
+    const int code = err == cudaErrorMemoryAllocation ? -4 : -2;
+    throw Error(code, std::string(what) + ": " + cudaGetErrorName(err) + " (" + cudaGetErrorString(err) + ")");
+}
+
+void DeviceBuffer::allocate(size_t bytes) {
+    release();
+    if (bytes == 0) return;
+    check_cuda(cudaMalloc(&ptr_, bytes), "cudaMalloc");
+    bytes_ = bytes;
+}
+
+void DeviceBuffer::release() noexcept {
+    if (ptr_ != nullptr) cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+}
+
+void DeviceBuffer::upload(const void* src, size_t bytes, cudaStream_t stream) {
+    if (bytes > bytes_) throw Error(-1, "upload larger than the device buffer");
+    if (stream == nullptr) {
+        check_cuda(cudaMemcpy(ptr_, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+    } else {
+        check_cuda(cudaMemcpyAsync(ptr_, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync H2D");
+    }
+}
+
+int sm_count() {
+    int device = 0, count = 0;
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+    return count;
+}
+
+size_t element_bytes(Precision p) { return p == Precision::f64 ? sizeof(double) : sizeof(float); }
+
+DeviceBuffer upload_real_table(const std::vector<double>& values, Precision p) {
+    if (p == Precision::f64) return upload_vector(values);
+    std::vector<float> f(values.begin(), values.end());
+    return upload_vector(f);
+}
+
+namespace {
+std::uint64_t active_columns(const std::vector<RetainedMode>& modes) {
+    std::uint64_t active = 0;
+    for (const auto& m : modes) active = std::max<std::uint64_t>(active, m.kx + 1);
+    return active;
+}
+}  // namespace
+
+HorizontalPlan::HorizontalPlan(const Workload& w, Precision p, bool pruned, std::uint64_t maxPlanes)
+    : w_(w), p_(p), maxPlanes_(maxPlanes) {
+    validate_workload(w);
+    if (!supported_length(static_cast<long long>(w.nx)) || !supported_length(static_cast<long long>(w.ny)))
+        throw Error(-2, "unsupported: the cuda provider transforms power-of-two Nx and Ny in [2, 1024]; got " +
+                            std::to_string(w.nx) + "x" + std::to_string(w.ny));
+    const auto planStart = Clock::now();
+    const auto modes = retained_modes(w);
+    modeCount_ = modes.size();
+    if (pruned && modes.empty()) throw Error(-1, "The pruned provider requires retained modes.");
+    keep_ = static_cast<int>(pruned ? active_columns(modes) : w.nxHalf());
+    const auto columnsForTables = pruned ? static_cast<std::uint64_t>(keep_) : w.nxHalf();
+    const auto tables = column_tables(w, modes, columnsForTables);
+    const auto twHalf = twiddle_table(std::max<std::uint64_t>(1, w.nx / 2));
+    const auto twFull = twiddle_table(w.nx);
+    const auto twCol = twiddle_table(w.ny);
+    planningSeconds = seconds_since(planStart);
+
+    const auto allocStart = Clock::now();
+    twHalf_ = upload_real_table(twHalf, p);
+    twFull_ = upload_real_table(twFull, p);
+    twCol_ = upload_real_table(twCol, p);
+    cellMap_ = upload_vector(tables.cellMap);
+    colStart_ = upload_vector(tables.colStart);
+    colKy_ = upload_vector(tables.colKy);
+    colMode_ = upload_vector(tables.colMode);
+    modeKx_ = upload_vector(tables.modeKx);
+    modeKy_ = upload_vector(tables.modeKy);
+    modeConj_ = upload_vector(tables.modeConj);
+    const size_t binBytes = static_cast<size_t>(w.ny) * keep_ * maxPlanes * 2 * element_bytes(p);
+    bins_.allocate(binBytes);
+    allocationSeconds = seconds_since(allocStart);
+    persistentBytes = twHalf_.bytes() + twFull_.bytes() + twCol_.bytes() + cellMap_.bytes() + colStart_.bytes() +
+                      colKy_.bytes() + colMode_.bytes() + modeKx_.bytes() + modeKy_.bytes() + modeConj_.bytes();
+    scratchBytes = bins_.bytes();
+}
+
+ModeTables HorizontalPlan::tables() const {
+    return {cellMap_.get<int>(), colStart_.get<int>(), colKy_.get<int>(), colMode_.get<int>()};
+}
+
+void HorizontalPlan::forward_rows(const void* real, std::uint64_t planes, cudaStream_t s) const {
+    if (planes > maxPlanes_) throw Error(-1, "plane count exceeds the plan's scratch");
+    check_cuda(launch_rows_forward(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny),
+                                   static_cast<long long>(planes), keep_, real, scratch(planes), twHalf_.get(),
+                                   twFull_.get(), s),
+               "row r2c kernel");
+}
+
+void HorizontalPlan::forward_columns(const ViewSet& views, double scale, cudaStream_t s) const {
+    const auto planes = static_cast<std::uint64_t>(views.count) * w_.nz;
+    if (planes > maxPlanes_) throw Error(-1, "plane count exceeds the plan's scratch");
+    check_cuda(launch_columns_gather(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, scratch(planes),
+                                     views, tables(), scale, twCol_.get(), s),
+               "column c2c + retention kernel");
+}
+
+void HorizontalPlan::inverse_columns(const ViewSet& views, cudaStream_t s) const {
+    const auto planes = static_cast<std::uint64_t>(views.count) * w_.nz;
+    if (planes > maxPlanes_) throw Error(-1, "plane count exceeds the plan's scratch");
+    check_cuda(launch_columns_embed(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, views, tables(),
+                                    scratch(planes), twCol_.get(), s),
+               "embedding + column c2c kernel");
+}
+
+void HorizontalPlan::inverse_rows(void* real, std::uint64_t planes, cudaStream_t s) const {
+    if (planes > maxPlanes_) throw Error(-1, "plane count exceeds the plan's scratch");
+    check_cuda(launch_rows_inverse(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny),
+                                   static_cast<long long>(planes), keep_, scratch(planes), real, twHalf_.get(),
+                                   twFull_.get(), s),
+               "row c2r kernel");
+}
+
+void HorizontalPlan::forward(const void* real, std::uint64_t planes, const ViewSet& views, double scale,
+                             cudaStream_t s) const {
+    if (planes != static_cast<std::uint64_t>(views.count) * w_.nz)
+        throw Error(-1, "field views must cover every real plane");
+    forward_rows(real, planes, s);
+    forward_columns(views, scale, s);
+}
+
+void HorizontalPlan::inverse(const ViewSet& views, void* real, cudaStream_t s) const {
+    inverse_columns(views, s);
+    inverse_rows(real, static_cast<std::uint64_t>(views.count) * w_.nz, s);
+}
+
+void HorizontalPlan::forward_dense(const void* real, void* wvm, std::uint64_t planes, cudaStream_t s) const {
+    if (keep_ != static_cast<int>(w_.nxHalf())) throw Error(-3, "dense transform requested from a pruned plan");
+    const DenseBins out{wvm, static_cast<long long>(planes), static_cast<long long>(w_.nxHalf())};
+    check_cuda(launch_rows_forward(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny),
+                                   static_cast<long long>(planes), keep_, real, out, twHalf_.get(), twFull_.get(), s),
+               "row r2c kernel");
+    check_cuda(launch_columns_dense(p_, -1, static_cast<int>(w_.ny), keep_, static_cast<long long>(planes), out, out,
+                                    twCol_.get(), s),
+               "column c2c kernel");
+}
+
+void HorizontalPlan::inverse_dense(const void* wvm, void* real, std::uint64_t planes, cudaStream_t s) const {
+    if (keep_ != static_cast<int>(w_.nxHalf())) throw Error(-3, "dense transform requested from a pruned plan");
+    if (planes > maxPlanes_) throw Error(-1, "plane count exceeds the plan's scratch");
+    const DenseBins in{const_cast<void*>(wvm), static_cast<long long>(planes), static_cast<long long>(w_.nxHalf())};
+    check_cuda(launch_columns_dense(p_, +1, static_cast<int>(w_.ny), keep_, static_cast<long long>(planes), in,
+                                    scratch(planes), twCol_.get(), s),
+               "column c2c kernel");
+    check_cuda(launch_rows_inverse(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny),
+                                   static_cast<long long>(planes), keep_, scratch(planes), real, twHalf_.get(),
+                                   twFull_.get(), s),
+               "row c2r kernel");
+}
+
+void HorizontalPlan::gather_dense(const void* wvm, std::uint64_t planes, const ViewSet& views, double scale,
+                                  cudaStream_t s) const {
+    const DenseBins in{const_cast<void*>(wvm), static_cast<long long>(planes), static_cast<long long>(w_.nxHalf())};
+    check_cuda(launch_gather_dense(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz),
+                                   static_cast<long long>(modeCount_), modeKx_.get<int>(), modeKy_.get<int>(),
+                                   modeConj_.get<unsigned char>(), in, views, scale, s),
+               "retention kernel");
+}
+
+void HorizontalPlan::embed_dense(const ViewSet& views, void* wvm, std::uint64_t planes, cudaStream_t s) const {
+    if (keep_ != static_cast<int>(w_.nxHalf())) throw Error(-3, "dense embedding requested from a pruned plan");
+    const DenseBins out{wvm, static_cast<long long>(planes), static_cast<long long>(w_.nxHalf())};
+    check_cuda(launch_embed_dense(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, views, tables(), out,
+                                  s),
+               "embedding kernel");
+}
+
+std::vector<double> transpose_family(const VerticalFamily& fam, bool forward) {
+    const auto nz = fam.nz, nj = fam.nj;
+    const auto elems = nz * nj;
+    std::vector<double> out(fam.groups * elems);
+    for (std::uint64_t g = 0; g < fam.groups; ++g) {
+        const double* F = fam.forward.data() + g * elems;
+        const double* I = fam.inverse.data() + g * elems;
+        double* At = out.data() + g * elems;
+        if (forward) {
+            // R = Nj rows, S = Nz: At[z][j] = F[j][z].
+            for (std::uint64_t z = 0; z < nz; ++z)
+                for (std::uint64_t j = 0; j < nj; ++j) At[z * nj + j] = F[j * nz + z];
+        } else {
+            // R = Nz rows, S = Nj: At[j][z] = I[z][j].
+            for (std::uint64_t j = 0; j < nj; ++j)
+                for (std::uint64_t z = 0; z < nz; ++z) At[j * nz + z] = I[z * nj + j];
+        }
+    }
+    return out;
+}
+
+VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::vector<ModeGroup>& groups,
+                           std::uint64_t fields, std::uint64_t members, const std::vector<double>& transposed)
+    : p_(p), R_(rowsOut), S_(inner) {
+    if (groups.empty() || fields == 0 || members == 0) throw Error(-1, "Vertical GEMM requires groups and fields.");
+    const auto matrixElems = static_cast<std::uint64_t>(rowsOut) * inner;
+    if (transposed.size() != groups.size() * matrixElems && transposed.size() != matrixElems)
+        throw Error(-1, "Vertical GEMM matrix family size does not match the groups.");
+    const bool common = transposed.size() == matrixElems && groups.size() > 1;
+    const int width = gemm_tile_columns(p);
+    std::vector<int> tg, tc, tn;
+    std::uint64_t expected = 0;
+    std::uint64_t perMember = 0;
+    for (const auto& g : groups) perMember += g.count * fields;
+    for (std::uint64_t m = 0; m < members; ++m) {
+        expected = 0;
+        for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
+            const auto& g = groups[gi];
+            if (g.count == 0 || g.first != expected)
+                throw Error(-1, "Vertical GEMM groups must be nonempty and contiguous.");
+            expected += g.count;
+            const std::uint64_t c0 = m * perMember + g.first * fields;
+            const std::uint64_t n = g.count * fields;
+            for (std::uint64_t c = 0; c < n; c += width) {
+                tg.push_back(common ? 0 : static_cast<int>(gi));
+                tc.push_back(static_cast<int>(c0 + c));
+                tn.push_back(static_cast<int>(std::min<std::uint64_t>(width, n - c)));
+            }
+        }
+    }
+    if (members * perMember > static_cast<std::uint64_t>(INT32_MAX)) throw Error(-1, "too many GEMM columns");
+    columns_ = members * perMember;
+    tiles_ = static_cast<int>(tg.size());
+    if (p == GemmPrecision::f64) {
+        matrices_ = upload_vector(transposed);
+    } else {
+        std::vector<float> f(transposed.begin(), transposed.end());
+        matrices_ = upload_vector(f);
+    }
+    tileGroup_ = upload_vector(tg);
+    tileColumn_ = upload_vector(tc);
+    tileCount_ = upload_vector(tn);
+}
+
+std::uint64_t VerticalPlan::persistentBytes() const {
+    return matrices_.bytes() + tileGroup_.bytes() + tileColumn_.bytes() + tileCount_.bytes();
+}
+
+void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s) const {
+    const GroupTiles t{tileGroup_.get<int>(), tileColumn_.get<int>(), tileCount_.get<int>(), tiles_};
+    check_cuda(launch_grouped_gemm(p_, R_, S_, matrices_.get(), t, in, out, s), "grouped vertical GEMM kernel");
+}
+
+}  // namespace skb

@@ -1,0 +1,157 @@
+// Host runtime shared by every C-ABI handle: status errors, owned device
+// buffers, and the horizontal / vertical plans (set-up tables + scratch) that
+// the providers and the flux pipeline are built from.
+
+#pragma once
+
+#include <chrono>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "horizontal.hpp"
+#include "model.hpp"
+#include "vertical.hpp"
+
+namespace skb {
+
+// Error carrying one of the SKB_ERR_* status codes.
+class Error : public std::runtime_error {
+public:
+    Error(int code, const std::string& what) : std::runtime_error(what), code_(code) {}
+    int code() const noexcept { return code_; }
+
+private:
+    int code_;
+};
+
+[[noreturn]] void throw_cuda(cudaError_t err, const char* what);
+inline void check_cuda(cudaError_t err, const char* what) {
+    if (err != cudaSuccess) throw_cuda(err, what);
+}
+
+using Clock = std::chrono::steady_clock;
+inline double seconds_since(Clock::time_point t) {
+    return std::chrono::duration<double>(Clock::now() - t).count();
+}
+
+// Owned device allocation.
+class DeviceBuffer {
+public:
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t bytes) { allocate(bytes); }
+    ~DeviceBuffer() { release(); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr_(o.ptr_), bytes_(o.bytes_) {
+        o.ptr_ = nullptr;
+        o.bytes_ = 0;
+    }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        if (this != &o) {
+            release();
+            ptr_ = o.ptr_;
+            bytes_ = o.bytes_;
+            o.ptr_ = nullptr;
+            o.bytes_ = 0;
+        }
+        return *this;
+    }
+    void allocate(size_t bytes);
+    void release() noexcept;
+    template <typename T = void>
+    T* get() const {
+        return static_cast<T*>(ptr_);
+    }
+    size_t bytes() const noexcept { return bytes_; }
+    void upload(const void* src, size_t bytes, cudaStream_t stream = nullptr);
+
+private:
+    void* ptr_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+template <typename T>
+DeviceBuffer upload_vector(const std::vector<T>& v) {
+    DeviceBuffer b(v.size() * sizeof(T) + (v.empty() ? sizeof(T) : 0));
+    if (!v.empty()) b.upload(v.data(), v.size() * sizeof(T));
+    return b;
+}
+
+int sm_count();
+size_t element_bytes(Precision p);
+
+// Upload a double table in the plan's precision.
+DeviceBuffer upload_real_table(const std::vector<double>& values, Precision p);
+
+// Horizontal plan: twiddles, column tables and the dense bin scratch for a
+// grid, a kept kx band and a maximum plane count.
+class HorizontalPlan {
+public:
+    HorizontalPlan(const Workload& w, Precision p, bool pruned, std::uint64_t maxPlanes);
+
+    const Workload& workload() const { return w_; }
+    Precision precision() const { return p_; }
+    int keep() const { return keep_; }
+    std::uint64_t modes() const { return modeCount_; }
+    ModeTables tables() const;
+    DenseBins scratch(std::uint64_t planes) const {
+        return {bins_.get(), static_cast<long long>(planes), static_cast<long long>(keep_)};
+    }
+
+    // x then y (forward) into views; y then x (inverse) from views.
+    void forward(const void* real, std::uint64_t planes, const ViewSet& views, double scale, cudaStream_t s) const;
+    void inverse(const ViewSet& views, void* real, cudaStream_t s) const;
+    void forward_rows(const void* real, std::uint64_t planes, cudaStream_t s) const;
+    void forward_columns(const ViewSet& views, double scale, cudaStream_t s) const;
+    void inverse_columns(const ViewSet& views, cudaStream_t s) const;
+    void inverse_rows(void* real, std::uint64_t planes, cudaStream_t s) const;
+    // Full-grid dense forms (keep = Nx/2+1): WVM spectrum with `planes` planes.
+    void forward_dense(const void* real, void* wvm, std::uint64_t planes, cudaStream_t s) const;
+    void inverse_dense(const void* wvm, void* real, std::uint64_t planes, cudaStream_t s) const;
+    void gather_dense(const void* wvm, std::uint64_t planes, const ViewSet& views, double scale,
+                      cudaStream_t s) const;
+    void embed_dense(const ViewSet& views, void* wvm, std::uint64_t planes, cudaStream_t s) const;
+
+    double allocationSeconds = 0.0, planningSeconds = 0.0;
+    std::uint64_t persistentBytes = 0, scratchBytes = 0;
+
+private:
+    Workload w_;
+    Precision p_;
+    int keep_ = 0;
+    std::uint64_t maxPlanes_ = 0;
+    std::uint64_t modeCount_ = 0;
+    DeviceBuffer twHalf_, twFull_, twCol_;
+    DeviceBuffer cellMap_, colStart_, colKy_, colMode_, modeKx_, modeKy_, modeConj_;
+    DeviceBuffer bins_;
+};
+
+// Vertical plan: transposed matrices and tile tables for one direction.
+class VerticalPlan {
+public:
+    // rows_out x inner per group; matrices given as At[g][s][r].
+    VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::vector<ModeGroup>& groups,
+                 std::uint64_t fields, std::uint64_t members, const std::vector<double>& transposed);
+    void execute(ComplexOperand in, ComplexOperand out, cudaStream_t s) const;
+    GemmPrecision precision() const { return p_; }
+    std::uint64_t columns() const { return columns_; }
+    std::uint64_t matrixBytes() const { return matrices_.bytes(); }
+    std::uint64_t persistentBytes() const;
+    int tiles() const { return tiles_; }
+
+private:
+    GemmPrecision p_;
+    int R_, S_;
+    std::uint64_t columns_ = 0;
+    int tiles_ = 0;
+    DeviceBuffer matrices_, tileGroup_, tileColumn_, tileCount_;
+};
+
+// At[g][s][r] for the forward (Nj x Nz) or inverse (Nz x Nj) matrices of a family.
+std::vector<double> transpose_family(const VerticalFamily& fam, bool forward);
+
+}  // namespace skb

@@ -1,0 +1,150 @@
+// SIMT grouped vertical GEMM (FP64 / FP32).  See vertical.hpp.
+//
+// One CTA of 256 threads computes a tile of 32 complex columns of one K^2
+// group, all R output rows.  The inner dimension S is streamed through shared
+// memory in chunks of 32: the chunk of the group's transposed matrix
+// At[s][r] (prepared at set-up) and of the input columns in[c][s].  Lane l of
+// warp w owns rows r = l + 32k and columns c = w + 8m, so each step of s reads
+// a 32-wide contiguous row of At (conflict-free) and a broadcast input value,
+// and the final stores of out[c][r] are contiguous across the warp.
+
+#include "vertical.hpp"
+
+#include "fft_device.cuh"
+
+namespace skb {
+namespace {
+
+constexpr int kTileCols = 32;
+constexpr int kChunk = 32;
+constexpr int kThreads = 256;
+
+template <typename T, bool SPLIT>
+__device__ __forceinline__ cx<T> load_operand(const ComplexOperand& op, long long i) {
+    if (SPLIT) return {reinterpret_cast<const T*>(op.re)[i], reinterpret_cast<const T*>(op.im)[i]};
+    return reinterpret_cast<const cx<T>*>(op.re)[i];
+}
+
+template <typename T, bool SPLIT>
+__device__ __forceinline__ void store_operand(const ComplexOperand& op, long long i, cx<T> v) {
+    if (SPLIT) {
+        reinterpret_cast<T*>(op.re)[i] = v.x;
+        reinterpret_cast<T*>(op.im)[i] = v.y;
+    } else {
+        reinterpret_cast<cx<T>*>(op.re)[i] = v;
+    }
+}
+
+template <typename T, int KR, bool SPLIT>
+__global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, const T* __restrict__ At,
+                                                                GroupTiles tiles, ComplexOperand in,
+                                                                ComplexOperand out) {
+    using V = cx<T>;
+    constexpr int RP = 32 * KR;
+    extern __shared__ unsigned char smem_raw[];
+    V(*sX)[kChunk + 1] = reinterpret_cast<V(*)[kChunk + 1]>(smem_raw);
+    T(*sA)[RP] = reinterpret_cast<T(*)[RP]>(smem_raw + sizeof(V) * kTileCols * (kChunk + 1));
+    const int tile = blockIdx.x;
+    const int g = __ldg(tiles.tileGroup + tile);
+    const int c0 = __ldg(tiles.tileColumn + tile);
+    const int ncols = __ldg(tiles.tileCount + tile);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const T* A = At + (long long)g * R * S;
+
+    V acc[KR][kTileCols / 8];
+#pragma unroll
+    for (int k = 0; k < KR; ++k)
+#pragma unroll
+        for (int m = 0; m < kTileCols / 8; ++m) acc[k][m] = {T(0), T(0)};
+
+    for (int s0 = 0; s0 < S; s0 += kChunk) {
+        const int sc = min(kChunk, S - s0);
+        for (int i = threadIdx.x; i < kChunk * RP; i += kThreads) {
+            const int s = i / RP, r = i % RP;
+            sA[s][r] = (s < sc && r < R) ? __ldg(A + (long long)(s0 + s) * R + r) : T(0);
+        }
+        for (int i = threadIdx.x; i < kTileCols * kChunk; i += kThreads) {
+            const int c = i / kChunk, s = i % kChunk;
+            V v = {T(0), T(0)};
+            if (c < ncols && s < sc) v = load_operand<T, SPLIT>(in, (long long)(c0 + c) * S + s0 + s);
+            sX[c][s] = v;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int s = 0; s < sc; ++s) {
+            T a[KR];
+#pragma unroll
+            for (int k = 0; k < KR; ++k) a[k] = sA[s][lane + 32 * k];
+#pragma unroll
+            for (int m = 0; m < kTileCols / 8; ++m) {
+                const V x = sX[warp + 8 * m][s];
+#pragma unroll
+                for (int k = 0; k < KR; ++k) {
+                    acc[k][m].x = fma(a[k], x.x, acc[k][m].x);
+                    acc[k][m].y = fma(a[k], x.y, acc[k][m].y);
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int m = 0; m < kTileCols / 8; ++m) {
+        const int c = warp + 8 * m;
+        if (c >= ncols) continue;
+#pragma unroll
+        for (int k = 0; k < KR; ++k) {
+            const int r = lane + 32 * k;
+            if (r < R) store_operand<T, SPLIT>(out, (long long)(c0 + c) * R + r, acc[k][m]);
+        }
+    }
+}
+
+template <typename T, int KR>
+cudaError_t launch_kr(int R, int S, const void* At, const GroupTiles& tiles, ComplexOperand in, ComplexOperand out,
+                      cudaStream_t stream) {
+    const bool split = in.im != nullptr;
+    if (split != (out.im != nullptr)) return cudaErrorInvalidValue;
+    const size_t bytes = sizeof(cx<T>) * kTileCols * (kChunk + 1) + sizeof(T) * kChunk * 32 * KR;
+    auto kernel = split ? grouped_gemm_kernel<T, KR, true> : grouped_gemm_kernel<T, KR, false>;
+    if (bytes > 48 * 1024) {
+        const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        if (err != cudaSuccess) return err;
+    }
+    kernel<<<tiles.tiles, kThreads, bytes, stream>>>(R, S, static_cast<const T*>(At), tiles, in, out);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_t(int R, int S, const void* At, const GroupTiles& tiles, ComplexOperand in, ComplexOperand out,
+                     cudaStream_t stream) {
+    const int kr = (R + 31) / 32;
+    switch (kr) {
+        case 1: return launch_kr<T, 1>(R, S, At, tiles, in, out, stream);
+        case 2: return launch_kr<T, 2>(R, S, At, tiles, in, out, stream);
+        case 3: return launch_kr<T, 3>(R, S, At, tiles, in, out, stream);
+        case 4: return launch_kr<T, 4>(R, S, At, tiles, in, out, stream);
+        case 5: return launch_kr<T, 5>(R, S, At, tiles, in, out, stream);
+        case 6: return launch_kr<T, 6>(R, S, At, tiles, in, out, stream);
+        case 7:
+        case 8:
+        case 9: return launch_kr<T, 9>(R, S, At, tiles, in, out, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+int gemm_tile_columns(GemmPrecision) { return kTileCols; }
+
+cudaError_t launch_grouped_gemm(GemmPrecision p, int R, int S, const void* matrices, const GroupTiles& tiles,
+                                ComplexOperand in, ComplexOperand out, cudaStream_t stream) {
+    if (tiles.tiles <= 0) return cudaSuccess;
+    switch (p) {
+        case GemmPrecision::f64: return launch_t<double>(R, S, matrices, tiles, in, out, stream);
+        case GemmPrecision::f32: return launch_t<float>(R, S, matrices, tiles, in, out, stream);
+        default: return cudaErrorNotSupported;
+    }
+}
+
+}  // namespace skb
