@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Benchmark of the composed antialiased flux on B200.
+
+Workload: the full 15 -> 4 flux (inverse K^2-grouped vertical GEMM, inverse
+pruned 2-D transforms, pointwise advection, forward pruned transforms with 2/3
+truncation, forward vertical GEMM) at 512 x 512 horizontal, Nz = 129, 4 target
+fields, 8 ensemble members per launch, replayed from one CUDA graph.  Metric:
+flux evaluations per second (one evaluation = one member's 15 -> 4 flux).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--mode split|fp32|fp64]
+    python bench.py --impl reference ...     # CPU arm, rank 0 only
+
+Under torchrun every rank runs an independent replica (the path shards over
+members with no exchange); a gloo barrier brackets the timed region and the
+step time is the max over ranks.  Prints one JSON line on rank 0.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "spectral-kernel-benchmarks_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "flux evals/s (512²×129,f4) split-prec vs FP64-plain at ≤1e-6 rel err; p99 ms"
+UNIT = "evals/s"
+FALLBACK_HBM_GBS = 6650.0
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    p.add_argument("--mode", choices=["split", "fp32", "fp64"], default="split")
+    p.add_argument("--n", type=int, default=512)
+    p.add_argument("--nz", type=int, default=129)
+    p.add_argument("--members", type=int, default=8)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--skip-cpu-baseline", action="store_true")
+    p.add_argument("--skip-e2e", action="store_true")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------ distribution
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, value):
+        if not self.pg:
+            return value
+        import torch
+
+        t = torch.tensor([float(value)], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                                  parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ inputs
+
+def power_law_inputs(n, nz, members, targets=4, seed=129):
+    """Seeded k^-3 power-law modal spectra: amplitude (1 + |k|^2)^(-3/2) times a
+    uniform random phase, for every (member, mode, field, j)."""
+    from oracle import oracle as orc  # mode table only; the values are synthetic
+
+    modes = orc.retained_modes(n, n)
+    nj = 2 * (nz - 1) // 3
+    fields = 3 + 3 * targets
+    rng = np.random.default_rng(seed)
+    k2 = (modes.k.astype(np.float64) ** 2 + modes.l.astype(np.float64) ** 2)
+    amp = (1.0 + k2) ** -1.5
+    shape = (members, len(modes), fields, nj)
+    phase = rng.uniform(0.0, 2.0 * np.pi, shape)
+    mag = rng.uniform(0.5, 1.5, shape)
+    x = (amp[None, :, None, None] * mag) * np.exp(1j * phase)
+    dc = (modes.k == 0) & (modes.l == 0)
+    x[:, dc, :, :] = x[:, dc, :, :].real
+    return np.ascontiguousarray(x.reshape(-1))
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel_stage):
+    """Per-launch DRAM bytes of a stage from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "flux_traffic.json")
+    try:
+        with open(path) as fh:
+            table = json.load(fh)
+        return table.get(kernel_stage)
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------- CUDA arm
+
+def cuda_arm(args, dist):
+    import skb_cuda as S
+
+    S.set_device(dist.local)
+    mode = {"split": S.FLUX_SPLIT_BF16X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
+    try:
+        flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode)
+        mode_name = args.mode
+    except RuntimeError:
+        if args.mode != "split":
+            raise
+        mode, mode_name = S.FLUX_FP32, "fp32"
+        flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode)
+    dtype = flux.device_dtype
+    x = power_law_inputs(args.n, args.nz, args.members, seed=129 + dist.rank)
+    din = S.DeviceArray.from_numpy(x.astype(dtype))
+    dout = S.DeviceArray(flux.output_elements * np.dtype(dtype).itemsize)
+    stream = flux.stream
+
+    # Warm-up through the graph path (captures once, then replays).
+    flux.execute_device(din.ptr, dout.ptr)
+    flux.capture_graph(din.ptr, dout.ptr)
+    for _ in range(args.warmup):
+        flux.replay_graph()
+    S.synchronize()
+
+    timer = S.Timer()
+    with ClockSampler(dist.local) as clocks:
+        dist.barrier()
+        S.synchronize()
+        timer.start(stream)
+        for _ in range(args.steps):
+            flux.replay_graph()
+        timer.stop(stream)
+        S.synchronize()
+        dist.barrier()
+    ms = timer.elapsed_ms() / args.steps
+    ms_max = dist.max(ms)
+    value = dist.world * args.members * 1000.0 / ms_max
+
+    stages = flux.profile(din.ptr, dout.ptr)
+    info = flux.info()
+
+    # Accuracy of this run's mode against the FP64-plain CUDA path on the same inputs.
+    rel_err = None
+    if mode != S.FLUX_FP64_PLAIN:
+        out = dout.download(dtype, flux.output_elements).astype(np.complex128)
+        ref_flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=S.FLUX_FP64_PLAIN)
+        ref = ref_flux.execute(x)
+        num = float(np.linalg.norm(out - ref))
+        den = float(np.linalg.norm(ref))
+        rel_err = num / den if den else num
+        del ref_flux
+
+    # End to end through the public host API: pinned FP64 host arrays, H2D,
+    # compute, D2H every step.
+    e2e = None
+    if not args.skip_e2e:
+        hin = S.PinnedArray(np.complex128, flux.input_elements)
+        hout = S.PinnedArray(np.complex128, flux.output_elements)
+        hin.array[:] = x
+        flux.execute_host_ptr(hin.ptr, hout.ptr)
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            flux.execute_host_ptr(hin.ptr, hout.ptr)
+        t1 = time.perf_counter()
+        dist.barrier()
+        e2e_ms = dist.max((t1 - t0) * 1000.0 / args.e2e_steps)
+        e2e = {"value": dist.world * args.members * 1000.0 / e2e_ms, "unit": UNIT,
+               "h2d_bytes_per_step": int(hin.array.nbytes), "d2h_bytes_per_step": int(hout.array.nbytes),
+               "ms_per_step": e2e_ms, "steps": args.e2e_steps}
+        hin.free()
+        hout.free()
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.skip_cpu_baseline:
+        cpu = cpu_baseline(args)
+
+    if dist.rank != 0:
+        return None
+    peak, peak_kind = measured_peak()
+    dominant = max(stages, key=lambda s: s["ms"])
+    per_launch_ms = dominant["ms"] / max(1, dominant["launches"])
+    per_launch_bytes = dominant["bytes"] / max(1, dominant["launches"])
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    total_ms = sum(s["ms"] for s in stages)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": dist.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if mode == S.FLUX_FP64_PLAIN else ("f32" if mode == S.FLUX_FP32 else "bf16x3+f32"),
+        "data": "synthetic (seeded k^-3 power-law modal spectra, K^2 pair-rotation vertical family)",
+        "config": {"workload": f"15->4 flux {args.n}x{args.n}, Nz={args.nz}, 4 targets, {args.members} members "
+                               "per launch, CUDA graph replay",
+                   "n": args.n, "nz": args.nz, "targets": 4, "members_per_gpu": args.members, "mode": mode_name,
+                   "evals_per_step_per_gpu": args.members, "l2": "inputs larger than L2 (%.2f GB modal input)"
+                   % (din.nbytes / 1e9), "parallelism": f"replicas x{dist.world}"},
+        "rel_err_vs_fp64": rel_err,
+        "roofline": {"bound": "hbm", "kernel": dominant["name"], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": ncu_traffic(dominant["name"]),
+                     "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": per_launch_ms},
+        "stages": [{"name": s["name"], "ms": round(s["ms"], 4), "share": round(s["ms"] / total_ms, 4),
+                    "launches": s["launches"], "GBps": (s["bytes"] / (s["ms"] * 1e-3) / 1e9) if s["ms"] else None}
+                   for s in stages],
+        "e2e": e2e,
+        "gpu_launches": int(info["launches_per_execution"]) * args.steps,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    return line
+
+
+# ------------------------------------------------------------- CPU arms
+
+def cpu_flux_once(n, nz, seed, workers):
+    """One member's 15 -> 4 flux on the host: threaded pocketfft FP64 transforms,
+    per-group BLAS GEMMs and the threaded pointwise product (oracle port)."""
+    from oracle import oracle as orc
+
+    modes = orc.retained_modes(n, n)
+    fam = orc.k2_family(orc.Workload(n, n, nz, 4))
+    x = orc.flux_inputs(modes, 15, 2 * (nz - 1) // 3, seed)
+    t0 = time.perf_counter()
+    orc.flux(n, nz, x, family=fam, modes=modes, workers=workers)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(args):
+    workers = os.cpu_count() or 1
+    seconds = cpu_flux_once(args.n, args.nz, 129, workers)
+    return {"value": 1.0 / seconds, "unit": UNIT, "cores": workers, "kind": "port",
+            "sample": f"one 15->4 evaluation of one member at {args.n}x{args.n}, Nz={args.nz} "
+                      f"(threaded pocketfft FP64 + BLAS + threaded pointwise; FFTW 3.3.11 is not on this host)"}
+
+
+def reference_arm(args, dist):
+    if dist.rank != 0:
+        return None
+    workers = os.cpu_count() or 1
+    warm = max(0, min(args.warmup, 1))
+    for _ in range(warm):
+        cpu_flux_once(args.n, args.nz, 129, workers)
+    # Bound the timed sample to about two minutes of host work.
+    times = []
+    budget = 120.0
+    for i in range(args.steps):
+        times.append(cpu_flux_once(args.n, args.nz, 129 + i, workers))
+        if sum(times) > budget:
+            break
+    sec = statistics.mean(times)
+    value = 1.0 / sec
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1000.0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference modal fixture generator)",
+        "config": {"workload": f"15->4 flux {args.n}x{args.n}, Nz={args.nz}, 4 targets, one member per step",
+                   "n": args.n, "nz": args.nz, "targets": 4},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                         "sample": f"{len(times)} of {args.steps} steps timed (one evaluation each; "
+                                   "FFTW 3.3.11 absent, threaded pocketfft stand-in)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        line = reference_arm(args, dist) if args.impl == "reference" else cuda_arm(args, dist)
+        if line is not None and dist.rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -135,6 +135,8 @@ typedef struct skb_provider_info {
 SKB_API const char* skb_last_error(void);
 SKB_API const char* skb_version(void);
 SKB_API int skb_device_count(int* count);
+/* Select the device this library's calls on the calling thread use. */
+SKB_API int skb_set_device(int device);
 /* Synchronise the current device (host-side barrier for timing). */
 SKB_API int skb_device_synchronize(void);
 
@@ -298,6 +300,18 @@ SKB_API int skb_flux_sizes(const skb_flux* p, uint64_t* modes, uint64_t* nj, uin
 SKB_API int skb_flux_execute(skb_flux* p, const skb_complex* modal_input, skb_complex* modal_output);
 /* Device arrays: FP64 complex for SKB_FLUX_FP64_PLAIN, FP32 complex otherwise. */
 SKB_API int skb_flux_execute_device(skb_flux* p, const void* modal_input, void* modal_output, void* stream);
+/* One execute_device with CUDA events between stages: per stage the device
+ * milliseconds, kernel launches and algorithmic bytes / flops (for roofline
+ * reporting).  `count` receives the number of stages. */
+typedef struct skb_stage_time {
+    char name[48];
+    double ms;
+    uint64_t launches;
+    double algorithmic_bytes;
+    double flops;
+} skb_stage_time;
+SKB_API int skb_flux_profile(skb_flux* p, const void* modal_input, void* modal_output, skb_stage_time* stages,
+                             uint64_t capacity, uint64_t* count);
 /* Capture execute_device on these buffers into a CUDA graph and replay it. */
 SKB_API int skb_flux_capture_graph(skb_flux* p, const void* modal_input, void* modal_output);
 SKB_API int skb_flux_replay_graph(skb_flux* p, void* stream);

@@ -165,20 +165,31 @@ def direct_c2r(w: Workload, wvm):
     return out
 
 
-def fft_r2c(w: Workload, real):
+def fft_r2c(w: Workload, real, workers=1):
     """FFTWProvider::forward (fftw_provider.cpp:537-572) restated with pocketfft:
-    unnormalised 2-D r2c of every plane, written frequency-major (WVM)."""
+    unnormalised 2-D r2c of every plane, written frequency-major (WVM).
+    workers > 1 uses scipy.fft's threaded pocketfft (timing baselines)."""
     planes = np.asarray(real, dtype=np.float64).reshape(w.planes, w.ny, w.nx)
-    spec = np.fft.rfft2(planes, axes=(1, 2))  # [plane][ky][kx]
+    if workers > 1:
+        import scipy.fft
+
+        spec = scipy.fft.rfft2(planes, axes=(1, 2), workers=workers)
+    else:
+        spec = np.fft.rfft2(planes, axes=(1, 2))  # [plane][ky][kx]
     return np.ascontiguousarray(spec.transpose(1, 2, 0)).reshape(-1)
 
 
-def fft_c2r(w: Workload, wvm):
+def fft_c2r(w: Workload, wvm, workers=1):
     """FFTWProvider::inverse (fftw_provider.cpp:574-610): unnormalised c2r with
     FFTW's half-spectrum semantics (columns c2c, then rows c2r; the imaginary
     parts of the kx = 0 and kx = Nx/2 bins of each row are ignored)."""
     spec = np.asarray(wvm, dtype=np.complex128).reshape(w.ny, w.nx_half, w.planes).transpose(2, 0, 1)
-    real = np.fft.irfft2(spec, s=(w.ny, w.nx), axes=(1, 2), norm="forward")
+    if workers > 1:
+        import scipy.fft
+
+        real = scipy.fft.irfft2(spec, s=(w.ny, w.nx), axes=(1, 2), norm="forward", workers=workers)
+    else:
+        real = np.fft.irfft2(spec, s=(w.ny, w.nx), axes=(1, 2), norm="forward")
     return np.ascontiguousarray(real).reshape(-1)
 
 
@@ -238,7 +249,7 @@ def pointwise(volume, scale, shared, derivative, workers=1):
     return out
 
 
-def flux(n, nz, modal_in, targets=4, family=None, modes=None):
+def flux(n, nz, modal_in, targets=4, family=None, modes=None, workers=1):
     """The 15 -> 4 streamed flux of runProductionLifetimeFluxBenchmark
     (benchmark.cpp:4182-4241 oracle order, 4405-4424 executeAll): inverse
     vertical GEMM of all input fields, inverse horizontal of [U,V,W] once, then per
@@ -256,13 +267,13 @@ def flux(n, nz, modal_in, targets=4, family=None, modes=None):
     H = len(modes)
     phys = grouped_vertical(w_in, family, "inverse", modal_in).reshape(H, fields_in, nz)
     scale = 1.0 / float((n * n) ** 2)
-    shared = fft_c2r(w3, embed_retained(w3, modes, phys[:, 0:3, :].reshape(-1)))
+    shared = fft_c2r(w3, embed_retained(w3, modes, phys[:, 0:3, :].reshape(-1)), workers)
     phys_out = np.empty((H, targets, nz), np.complex128)
     for t in range(targets):
         trip = phys[:, 3 + 3 * t:6 + 3 * t, :].reshape(-1)
-        deriv = fft_c2r(w3, embed_retained(w3, modes, trip))
-        target = pointwise(n * n * nz, scale, shared, deriv)
-        phys_out[:, t, :] = gather_retained(w1, modes, fft_r2c(w1, target)).reshape(H, nz)
+        deriv = fft_c2r(w3, embed_retained(w3, modes, trip), workers)
+        target = pointwise(n * n * nz, scale, shared, deriv, workers)
+        phys_out[:, t, :] = gather_retained(w1, modes, fft_r2c(w1, target, workers)).reshape(H, nz)
     return grouped_vertical(w_out, family, "forward", phys_out.reshape(-1))
 
 

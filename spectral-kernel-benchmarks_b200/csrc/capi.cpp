@@ -231,6 +231,10 @@ int skb_device_count(int* count) {
     });
 }
 
+int skb_set_device(int device) {
+    return guard([&] { check_cuda(cudaSetDevice(device), "cudaSetDevice"); });
+}
+
 int skb_device_synchronize(void) {
     return guard([&] { check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize"); });
 }
@@ -1130,6 +1134,25 @@ int skb_flux_execute(skb_flux* p, const skb_complex* in, skb_complex* out) {
         f.execute(p->in.get(), p->out.get(), p->stream);
         p->host.download(reinterpret_cast<double*>(out), p->out.get(), 2 * f.outputElements(), p->stream);
         sync(p->stream);
+    });
+}
+
+int skb_flux_profile(skb_flux* p, const void* in, void* out, skb_stage_time* stages, uint64_t capacity,
+                     uint64_t* count) {
+    return guard([&] {
+        require(p && in && out && count, "handle, buffers and count must be non-null");
+        const auto result = p->pipeline->profile(in, out, p->stream);
+        *count = result.size();
+        if (stages == nullptr) return;
+        require(capacity >= result.size(), "stage capacity too small");
+        for (size_t i = 0; i < result.size(); ++i) {
+            std::memset(&stages[i], 0, sizeof(stages[i]));
+            std::snprintf(stages[i].name, sizeof(stages[i].name), "%s", result[i].name.c_str());
+            stages[i].ms = result[i].ms;
+            stages[i].launches = result[i].launches;
+            stages[i].algorithmic_bytes = result[i].bytes;
+            stages[i].flops = result[i].flops;
+        }
     });
 }
 

@@ -66,12 +66,70 @@ FluxPipeline::~FluxPipeline() {
     if (graph_ != nullptr) cudaGraphDestroy(graph_);
 }
 
-void FluxPipeline::execute(const void* modalIn, void* modalOut, cudaStream_t s) {
+// Optional stage timing: events recorded on the stream between stages.
+struct FluxPipeline::Recorder {
+    cudaStream_t stream;
+    std::vector<cudaEvent_t> events;
+    std::vector<int> stageOf;
+    std::vector<StageTime> stages;
+    explicit Recorder(cudaStream_t s) : stream(s) { mark(-1); }
+    ~Recorder() {
+        for (auto e : events) cudaEventDestroy(e);
+    }
+    int stage(const std::string& name) {
+        for (size_t i = 0; i < stages.size(); ++i)
+            if (stages[i].name == name) return static_cast<int>(i);
+        stages.push_back({name});
+        return static_cast<int>(stages.size() - 1);
+    }
+    void mark(int stageIndex) {
+        cudaEvent_t e;
+        check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+        check_cuda(cudaEventRecord(e, stream), "cudaEventRecord");
+        events.push_back(e);
+        stageOf.push_back(stageIndex);
+    }
+    void end(const std::string& name, std::uint64_t launches, double bytes, double flops) {
+        const int i = stage(name);
+        stages[i].launches += launches;
+        stages[i].bytes += bytes;
+        stages[i].flops += flops;
+        mark(i);
+    }
+    std::vector<StageTime> finish() {
+        check_cuda(cudaEventSynchronize(events.back()), "cudaEventSynchronize");
+        for (size_t k = 1; k < events.size(); ++k) {
+            float ms = 0.0f;
+            check_cuda(cudaEventElapsedTime(&ms, events[k - 1], events[k]), "cudaEventElapsedTime");
+            stages[stageOf[k]].ms += ms;
+        }
+        return stages;
+    }
+};
+
+void FluxPipeline::execute(const void* modalIn, void* modalOut, cudaStream_t s) { run(modalIn, modalOut, s, nullptr); }
+
+std::vector<FluxPipeline::StageTime> FluxPipeline::profile(const void* modalIn, void* modalOut, cudaStream_t s) {
+    Recorder rec(s);
+    run(modalIn, modalOut, s, &rec);
+    return rec.finish();
+}
+
+void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec) {
     const auto H = modes_, nz = cfg_.nz, T = cfg_.targets, M = cfg_.members;
-    const size_t ces = 2 * element_bytes(horizontal_->precision());  // complex element bytes
+    const size_t es = element_bytes(horizontal_->precision());
+    const size_t ces = 2 * es;  // complex element bytes
+    const double n = static_cast<double>(cfg_.n);
+    const double keep = horizontal_->keep();
     auto* physIn = physIn_.get<unsigned char>();
     auto* physOut = physOut_.get<unsigned char>();
+    // Algorithmic bytes of one plane through each horizontal stage.
+    const double binsPlane = n * keep * ces, realPlane = n * n * es, compactPlane = double(H) * ces;
+    const double gemmIn = double(M) * H * fieldsIn_ * (nj_ + nz) * ces + inverseGemm_->matrixBytes();
+    const double gemmOut = double(M) * H * T * (nj_ + nz) * ces + forwardGemm_->matrixBytes();
+
     inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s);
+    if (rec) rec->end("gemm_inverse", 1, gemmIn, 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
 
     auto triple = [&](std::uint64_t firstField) {
         ViewSet v{};
@@ -82,12 +140,19 @@ void FluxPipeline::execute(const void* modalIn, void* modalOut, cudaStream_t s) 
                                   static_cast<long long>(fieldsIn_ * nz)};
         return v;
     };
-    horizontal_->inverse(triple(0), shared_.get(), s);
-    const double scale = 1.0 / (static_cast<double>(cfg_.n * cfg_.n) * static_cast<double>(cfg_.n * cfg_.n));
-    const size_t es = element_bytes(horizontal_->precision());
+    const double triplePlanes = 3.0 * M * nz;
+    auto inverseTriple = [&](std::uint64_t firstField, void* real) {
+        const ViewSet v = triple(firstField);
+        horizontal_->inverse_columns(v, s);
+        if (rec) rec->end("columns_inverse_embed", 1, triplePlanes * (compactPlane + binsPlane), 0.0);
+        horizontal_->inverse_rows(real, 3 * M * nz, s);
+        if (rec) rec->end("rows_inverse_c2r", 1, triplePlanes * (binsPlane + realPlane), 0.0);
+    };
+    inverseTriple(0, shared_.get());
+    const double scale = 1.0 / (n * n * n * n);
     const int sms = sm_count();
     for (std::uint64_t t = 0; t < T; ++t) {
-        horizontal_->inverse(triple(3 + 3 * t), deriv_.get(), s);
+        inverseTriple(3 + 3 * t, deriv_.get());
         for (std::uint64_t m = 0; m < M; ++m) {
             check_cuda(launch_pointwise(f64(), static_cast<long long>(volume_), scale,
                                         shared_.get<unsigned char>() + es * 3 * m * volume_,
@@ -95,13 +160,18 @@ void FluxPipeline::execute(const void* modalIn, void* modalOut, cudaStream_t s) 
                                         target_.get<unsigned char>() + es * m * volume_, sms, s),
                        "pointwise advection kernel");
         }
+        if (rec) rec->end("pointwise", M, 7.0 * es * double(volume_) * M, 6.0 * double(volume_) * M);
         ViewSet out{};
         out.count = static_cast<int>(M);
         for (std::uint64_t m = 0; m < M; ++m)
             out.v[m] = {physOut + ces * ((m * H * T + t) * nz), nullptr, static_cast<long long>(T * nz)};
-        horizontal_->forward(target_.get(), M * nz, out, 1.0, s);
+        horizontal_->forward_rows(target_.get(), M * nz, s);
+        if (rec) rec->end("rows_forward_r2c", 1, double(M) * nz * (realPlane + binsPlane), 0.0);
+        horizontal_->forward_columns(out, 1.0, s);
+        if (rec) rec->end("columns_forward_gather", 1, double(M) * nz * (binsPlane + compactPlane), 0.0);
     }
     forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s);
+    if (rec) rec->end("gemm_forward", 1, gemmOut, 4.0 * nz * nj_ * double(M) * H * T);
 }
 
 void FluxPipeline::capture(const void* modalIn, void* modalOut, cudaStream_t s) {

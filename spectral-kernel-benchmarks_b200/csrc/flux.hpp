@@ -14,6 +14,8 @@
 
 #include <cstdint>
 #include <memory>
+#include <string>
+#include <vector>
 
 #include "runtime.hpp"
 
@@ -37,6 +39,16 @@ public:
     // float otherwise): modal input [member][mode][3+3T][j], output
     // [member][mode][T][j].
     void execute(const void* modalIn, void* modalOut, cudaStream_t s);
+
+    // One evaluation with CUDA events between stages; per stage the summed
+    // device milliseconds, launches and algorithmic bytes / flops.
+    struct StageTime {
+        std::string name;
+        double ms = 0.0;
+        std::uint64_t launches = 0;
+        double bytes = 0.0, flops = 0.0;
+    };
+    std::vector<StageTime> profile(const void* modalIn, void* modalOut, cudaStream_t s);
     void capture(const void* modalIn, void* modalOut, cudaStream_t s);
     void replay(cudaStream_t s);
 
@@ -61,6 +73,8 @@ private:
     std::unique_ptr<VerticalPlan> inverseGemm_, forwardGemm_;
     DeviceBuffer physIn_, shared_, deriv_, target_, physOut_;
     std::uint64_t launches_ = 0;
+    struct Recorder;
+    void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec);
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graphExec_ = nullptr;
 };

@@ -109,6 +109,11 @@ class ProviderInfo(ctypes.Structure):
         return out
 
 
+class StageTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("ms", ctypes.c_double), ("launches", ctypes.c_uint64),
+                ("algorithmic_bytes", ctypes.c_double), ("flops", ctypes.c_double)]
+
+
 class FluxOptions(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint64), ("nz", ctypes.c_uint64), ("targets", ctypes.c_uint64),
                 ("members", ctypes.c_uint64), ("mode", ctypes.c_int32), ("family", ctypes.c_int32),
@@ -165,6 +170,10 @@ def device_count():
     n = ctypes.c_int(0)
     check(library().skb_device_count(ctypes.byref(n)))
     return n.value
+
+
+def set_device(device):
+    check(library().skb_set_device(ctypes.c_int(device)))
 
 
 def synchronize():
@@ -684,6 +693,15 @@ class Flux:
     def execute_device(self, in_ptr, out_ptr, stream=None):
         check(library().skb_flux_execute_device(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr),
                                                 ctypes.c_void_p(stream)))
+
+    def profile(self, in_ptr, out_ptr):
+        """One device execution with per-stage event timing -> list of dicts."""
+        arr = (StageTime * 32)()
+        n = ctypes.c_uint64()
+        check(library().skb_flux_profile(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), arr, _u64(32),
+                                         ctypes.byref(n)))
+        return [dict(name=a.name.decode(), ms=a.ms, launches=a.launches, bytes=a.algorithmic_bytes, flops=a.flops)
+                for a in arr[: n.value]]
 
     def capture_graph(self, in_ptr, out_ptr):
         check(library().skb_flux_capture_graph(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr)))
