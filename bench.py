@@ -194,7 +194,7 @@ def cuda_arm(args, dist):
     import skb_cuda as S
 
     S.set_device(dist.local)
-    mode = {"split": S.FLUX_SPLIT_BF16X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
+    mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
     try:
         flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode)
         mode_name = args.mode
@@ -227,6 +227,7 @@ def cuda_arm(args, dist):
         S.synchronize()
         dist.barrier()
     ms = timer.elapsed_ms() / args.steps
+    flux.check_device()
     ms_max = dist.max(ms)
     value = dist.world * args.members * 1000.0 / ms_max
 
@@ -288,7 +289,7 @@ def cuda_arm(args, dist):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if mode == S.FLUX_FP64_PLAIN else ("f32" if mode == S.FLUX_FP32 else "bf16x3+f32"),
+        "dtype": "f64" if mode == S.FLUX_FP64_PLAIN else ("f32" if mode == S.FLUX_FP32 else "tf32x3+f32"),
         "data": "synthetic (seeded k^-3 power-law modal spectra, K^2 pair-rotation vertical family)",
         "config": {"workload": f"15->4 flux {args.n}x{args.n}, Nz={args.nz}, 4 targets, {args.members} members "
                                "per launch, CUDA graph replay",

@@ -312,6 +312,10 @@ typedef struct skb_stage_time {
 } skb_stage_time;
 SKB_API int skb_flux_profile(skb_flux* p, const void* modal_input, void* modal_output, skb_stage_time* stages,
                              uint64_t capacity, uint64_t* count);
+/* Raises SKB_ERR_RUNTIME if a bounded wait inside a tensor-core kernel of
+ * this handle expired since creation (the kernel then skipped its work and
+ * released its tensor memory instead of hanging). */
+SKB_API int skb_flux_check_device(skb_flux* p);
 /* Capture execute_device on these buffers into a CUDA graph and replay it. */
 SKB_API int skb_flux_capture_graph(skb_flux* p, const void* modal_input, void* modal_output);
 SKB_API int skb_flux_replay_graph(skb_flux* p, void* stream);

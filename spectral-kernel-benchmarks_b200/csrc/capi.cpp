@@ -782,8 +782,12 @@ int skb_vertical_create(const skb_workload* w, const skb_mode_group* groups, uin
         } else if (gemm_precision == SKB_GEMM_FP32) {
             p->gp = GemmPrecision::f32;
             p->p = Precision::f32;
+        } else if (gemm_precision == SKB_GEMM_TF32X3) {
+            require(layout == SKB_LAYOUT_INTERLEAVED, "the split-TF32x3 tensor-core form takes the interleaved layout");
+            p->gp = GemmPrecision::tf32x3;
+            p->p = Precision::f32;
         } else {
-            throw Error(SKB_ERR_RUNTIME, "unsupported: tensor-core split GEMM precision is not built in this library");
+            throw Error(SKB_ERR_RUNTIME, "unsupported: the split-BF16x3 GEMM form is not built in this library");
         }
         p->host.p = p->p;
         const auto prepStart = Clock::now();
@@ -809,10 +813,10 @@ int skb_vertical_create(const skb_workload* w, const skb_mode_group* groups, uin
         p->stream = make_stream();
         if (fwd)
             p->forward = std::make_unique<VerticalPlan>(p->gp, static_cast<int>(fam.nj), static_cast<int>(fam.nz), g,
-                                                        p->w.fields, 1, transpose_family(fam, true));
+                                                        p->w.fields, 1, fam.forward);
         if (inv)
             p->inverse = std::make_unique<VerticalPlan>(p->gp, static_cast<int>(fam.nz), static_cast<int>(fam.nj), g,
-                                                        p->w.fields, 1, transpose_family(fam, false));
+                                                        p->w.fields, 1, fam.inverse);
         p->preparation = seconds_since(prepStart);
         p->groups = group_count;
         p->columns = modes * p->w.fields;
@@ -948,6 +952,7 @@ int skb_vertical_execute_forward(skb_vertical_provider* p) {
         need(p->forward, "Forward GEMM component requested from an inverse-only provider.")
             .execute({p->physIn.get(), p->physInIm.get()}, {p->modalOut.get(), p->modalOutIm.get()}, p->stream);
         sync(p->stream);
+        p->forward->check_device_error();
     });
 }
 
@@ -957,6 +962,7 @@ int skb_vertical_execute_inverse(skb_vertical_provider* p) {
         need(p->inverse, "Inverse GEMM component requested from a forward-only provider.")
             .execute({p->modalIn.get(), p->modalInIm.get()}, {p->physOut.get(), p->physOutIm.get()}, p->stream);
         sync(p->stream);
+        p->inverse->check_device_error();
     });
 }
 
@@ -1134,6 +1140,7 @@ int skb_flux_execute(skb_flux* p, const skb_complex* in, skb_complex* out) {
         f.execute(p->in.get(), p->out.get(), p->stream);
         p->host.download(reinterpret_cast<double*>(out), p->out.get(), 2 * f.outputElements(), p->stream);
         sync(p->stream);
+        f.check_device_errors();
     });
 }
 
@@ -1153,6 +1160,14 @@ int skb_flux_profile(skb_flux* p, const void* in, void* out, skb_stage_time* sta
             stages[i].algorithmic_bytes = result[i].bytes;
             stages[i].flops = result[i].flops;
         }
+    });
+}
+
+int skb_flux_check_device(skb_flux* p) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        sync(p->stream);
+        p->pipeline->check_device_errors();
     });
 }
 

@@ -10,8 +10,8 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
     if (cfg.members == 0) throw Error(-1, "flux requires at least one ensemble member");
     if (3 * cfg.members > static_cast<std::uint64_t>(kMaxViews))
         throw Error(-1, "at most " + std::to_string(kMaxViews / 3) + " ensemble members per flux handle");
-    if (cfg.mode == FluxMode::split_tf32x3 || cfg.mode == FluxMode::split_bf16x3)
-        throw Error(-2, "unsupported: split tensor-core flux mode is not built in this library");
+    if (cfg.mode == FluxMode::split_bf16x3)
+        throw Error(-2, "unsupported: the split-BF16x3 flux mode is not built in this library (use split-TF32x3)");
     const auto planStart = Clock::now();
     wOut_ = Workload{cfg.n, cfg.n, cfg.nz, cfg.targets, 1.0, 1.0, true};
     fieldsIn_ = 3 + 3 * cfg.targets;
@@ -23,13 +23,13 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
     VerticalFamily fam = cfg.family == 2 ? sturm_liouville_family(wOut_, groups, cfg.familySeed)
                                          : k2_rotation_family(wOut_, groups);
     familyId = fam.id;
-    const auto fwdT = transpose_family(fam, true);
-    const auto invT = transpose_family(fam, false);
     planningSeconds = seconds_since(planStart);
 
     const auto allocStart = Clock::now();
     const Precision hp = f64() ? Precision::f64 : Precision::f32;
-    const GemmPrecision gp = f64() ? GemmPrecision::f64 : GemmPrecision::f32;
+    const GemmPrecision gp = f64() ? GemmPrecision::f64
+                             : cfg.mode == FluxMode::split_tf32x3 ? GemmPrecision::tf32x3
+                                                                  : GemmPrecision::f32;
     const size_t es = element_bytes(hp);
     // Admission by device memory: refuse before allocating what cannot fit.
     const std::uint64_t maxPlanes = 3 * cfg.members * cfg.nz;
@@ -44,9 +44,9 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
     horizontal_ = std::make_unique<HorizontalPlan>(Workload{cfg.n, cfg.n, cfg.nz, 3, 1.0, 1.0, true}, hp, true,
                                                    maxPlanes);
     inverseGemm_ = std::make_unique<VerticalPlan>(gp, static_cast<int>(cfg.nz), static_cast<int>(nj_), groups,
-                                                  fieldsIn_, cfg.members, invT);
+                                                  fieldsIn_, cfg.members, fam.inverse);
     forwardGemm_ = std::make_unique<VerticalPlan>(gp, static_cast<int>(nj_), static_cast<int>(cfg.nz), groups,
-                                                  cfg.targets, cfg.members, fwdT);
+                                                  cfg.targets, cfg.members, fam.forward);
     physIn_.allocate(2 * es * cfg.members * modes_ * fieldsIn_ * cfg.nz);
     physOut_.allocate(2 * es * cfg.members * modes_ * cfg.targets * cfg.nz);
     shared_.allocate(es * 3 * cfg.members * volume_);
@@ -172,6 +172,11 @@ void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Reco
     }
     forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s);
     if (rec) rec->end("gemm_forward", 1, gemmOut, 4.0 * nz * nj_ * double(M) * H * T);
+}
+
+void FluxPipeline::check_device_errors() const {
+    inverseGemm_->check_device_error();
+    forwardGemm_->check_device_error();
 }
 
 void FluxPipeline::capture(const void* modalIn, void* modalOut, cudaStream_t s) {

@@ -50,6 +50,8 @@ public:
     };
     std::vector<StageTime> profile(const void* modalIn, void* modalOut, cudaStream_t s);
     void capture(const void* modalIn, void* modalOut, cudaStream_t s);
+    // Raises if a bounded device wait inside a tensor-core kernel expired.
+    void check_device_errors() const;
     void replay(cudaStream_t s);
 
     std::uint64_t modes() const { return modes_; }

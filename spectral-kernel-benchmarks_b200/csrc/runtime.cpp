@@ -184,47 +184,83 @@ void HorizontalPlan::embed_dense(const ViewSet& views, void* wvm, std::uint64_t 
                "embedding kernel");
 }
 
-std::vector<double> transpose_family(const VerticalFamily& fam, bool forward) {
-    const auto nz = fam.nz, nj = fam.nj;
-    const auto elems = nz * nj;
-    std::vector<double> out(fam.groups * elems);
-    for (std::uint64_t g = 0; g < fam.groups; ++g) {
-        const double* F = fam.forward.data() + g * elems;
-        const double* I = fam.inverse.data() + g * elems;
-        double* At = out.data() + g * elems;
-        if (forward) {
-            // R = Nj rows, S = Nz: At[z][j] = F[j][z].
-            for (std::uint64_t z = 0; z < nz; ++z)
-                for (std::uint64_t j = 0; j < nj; ++j) At[z * nj + j] = F[j * nz + z];
-        } else {
-            // R = Nz rows, S = Nj: At[j][z] = I[z][j].
-            for (std::uint64_t j = 0; j < nj; ++j)
-                for (std::uint64_t z = 0; z < nz; ++z) At[j * nz + z] = I[z * nj + j];
-        }
-    }
-    return out;
-}
-
 VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::vector<ModeGroup>& groups,
-                           std::uint64_t fields, std::uint64_t members, const std::vector<double>& transposed)
+                           std::uint64_t fields, std::uint64_t members, const std::vector<double>& natural)
     : p_(p), R_(rowsOut), S_(inner) {
     if (groups.empty() || fields == 0 || members == 0) throw Error(-1, "Vertical GEMM requires groups and fields.");
     const auto matrixElems = static_cast<std::uint64_t>(rowsOut) * inner;
-    if (transposed.size() != groups.size() * matrixElems && transposed.size() != matrixElems)
+    if (natural.size() != groups.size() * matrixElems && natural.size() != matrixElems)
         throw Error(-1, "Vertical GEMM matrix family size does not match the groups.");
-    const bool common = transposed.size() == matrixElems && groups.size() > 1;
+    const bool common = natural.size() == matrixElems && groups.size() > 1;
+    std::uint64_t expected = 0;
+    for (const auto& g : groups) {
+        if (g.count == 0 || g.first != expected) throw Error(-1, "Vertical GEMM groups must be nonempty and contiguous.");
+        expected += g.count;
+    }
+    const std::uint64_t perMember = expected * fields;
+    if (members * perMember > static_cast<std::uint64_t>(INT32_MAX)) throw Error(-1, "too many GEMM columns");
+    columns_ = members * perMember;
+    memberColumns_ = static_cast<long long>(perMember);
+    const std::uint64_t groupsCount = common ? 1 : groups.size();
+
+    if (p == GemmPrecision::tf32x3) {
+        if (!tc_gemm_supported(rowsOut, inner))
+            throw Error(-2, "unsupported: tensor-core GEMM needs the padded group matrix and two data stages in "
+                            "227 KB of shared memory (R=" + std::to_string(rowsOut) + ", S=" + std::to_string(inner) +
+                            ")");
+        // Natural-layout FP32 matrices, one per group (a common matrix is
+        // replicated); the kernel splits them into TF32 hi/lo.
+        std::vector<float> f(groups.size() * matrixElems);
+        for (std::uint64_t gi = 0; gi < groups.size(); ++gi)
+            for (std::uint64_t e = 0; e < matrixElems; ++e)
+                f[gi * matrixElems + e] = static_cast<float>(natural[(common ? 0 : gi) * matrixElems + e]);
+        matrices_ = upload_vector(f);
+        std::vector<int> gc(groups.size()), gf(groups.size());
+        for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
+            gc[gi] = static_cast<int>(groups[gi].count * fields);
+            gf[gi] = static_cast<int>(groups[gi].first * fields);
+        }
+        // Units: runs of up to unit_tiles * 64 virtual (member, column) pairs of
+        // one group, largest first so the long units start early.
+        struct Unit {
+            int g, col, count;
+        };
+        std::vector<Unit> units;
+        const int span = tc_gemm_unit_tiles() * 64;
+        for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
+            const int total = static_cast<int>(members) * gc[gi];
+            for (int c = 0; c < total; c += span) units.push_back({static_cast<int>(gi), c, std::min(span, total - c)});
+        }
+        std::stable_sort(units.begin(), units.end(), [](const Unit& a, const Unit& b) { return a.count > b.count; });
+        std::vector<int> ug, uc, un;
+        for (const auto& u : units) {
+            ug.push_back(u.g);
+            uc.push_back(u.col);
+            un.push_back(u.count);
+        }
+        units_ = static_cast<int>(ug.size());
+        unitGroup_ = upload_vector(ug);
+        unitColumn_ = upload_vector(uc);
+        unitCount_ = upload_vector(un);
+        groupColumns_ = upload_vector(gc);
+        groupFirst_ = upload_vector(gf);
+        error_.allocate(sizeof(int));
+        check_cuda(cudaMemset(error_.get(), 0, sizeof(int)), "cudaMemset");
+        return;
+    }
+
+    // SIMT forms read the transposed matrices At[g][s][r].
+    std::vector<double> At(groupsCount * matrixElems);
+    for (std::uint64_t g = 0; g < groupsCount; ++g)
+        for (int r = 0; r < rowsOut; ++r)
+            for (int s = 0; s < inner; ++s)
+                At[g * matrixElems + static_cast<std::uint64_t>(s) * rowsOut + r] =
+                    natural[g * matrixElems + static_cast<std::uint64_t>(r) * inner + s];
     const int width = gemm_tile_columns(p);
     std::vector<int> tg, tc, tn;
-    std::uint64_t expected = 0;
-    std::uint64_t perMember = 0;
-    for (const auto& g : groups) perMember += g.count * fields;
     for (std::uint64_t m = 0; m < members; ++m) {
-        expected = 0;
         for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
             const auto& g = groups[gi];
-            if (g.count == 0 || g.first != expected)
-                throw Error(-1, "Vertical GEMM groups must be nonempty and contiguous.");
-            expected += g.count;
             const std::uint64_t c0 = m * perMember + g.first * fields;
             const std::uint64_t n = g.count * fields;
             for (std::uint64_t c = 0; c < n; c += width) {
@@ -234,13 +270,11 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
             }
         }
     }
-    if (members * perMember > static_cast<std::uint64_t>(INT32_MAX)) throw Error(-1, "too many GEMM columns");
-    columns_ = members * perMember;
     tiles_ = static_cast<int>(tg.size());
     if (p == GemmPrecision::f64) {
-        matrices_ = upload_vector(transposed);
+        matrices_ = upload_vector(At);
     } else {
-        std::vector<float> f(transposed.begin(), transposed.end());
+        std::vector<float> f(At.begin(), At.end());
         matrices_ = upload_vector(f);
     }
     tileGroup_ = upload_vector(tg);
@@ -249,12 +283,42 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
 }
 
 std::uint64_t VerticalPlan::persistentBytes() const {
-    return matrices_.bytes() + tileGroup_.bytes() + tileColumn_.bytes() + tileCount_.bytes();
+    return matrices_.bytes() + tileGroup_.bytes() + tileColumn_.bytes() + tileCount_.bytes() + unitGroup_.bytes() +
+           unitColumn_.bytes() + unitCount_.bytes() + groupColumns_.bytes() + groupFirst_.bytes() + error_.bytes();
 }
 
 void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s) const {
+    if (p_ == GemmPrecision::tf32x3) {
+        if (in.im != nullptr || out.im != nullptr)
+            throw Error(-3, "the tensor-core GEMM form takes interleaved complex operands");
+        TcGemmArgs a{};
+        a.B = matrices_.get<float>();
+        a.R = R_;
+        a.S = S_;
+        a.NP = (R_ + 15) / 16 * 16;
+        a.KCH = (S_ + 31) / 32;
+        a.unitGroup = unitGroup_.get<int>();
+        a.unitColumn = unitColumn_.get<int>();
+        a.unitCount = unitCount_.get<int>();
+        a.units = units_;
+        a.groupColumns = groupColumns_.get<int>();
+        a.groupFirst = groupFirst_.get<int>();
+        a.memberColumns = memberColumns_;
+        a.in = static_cast<const float2*>(in.re);
+        a.out = static_cast<float2*>(out.re);
+        a.error = error_.get<int>();
+        check_cuda(launch_tc_gemm(a, s), "tensor-core grouped vertical GEMM kernel");
+        return;
+    }
     const GroupTiles t{tileGroup_.get<int>(), tileColumn_.get<int>(), tileCount_.get<int>(), tiles_};
     check_cuda(launch_grouped_gemm(p_, R_, S_, matrices_.get(), t, in, out, s), "grouped vertical GEMM kernel");
+}
+
+void VerticalPlan::check_device_error() const {
+    if (error_.bytes() == 0) return;
+    int flag = 0;
+    check_cuda(cudaMemcpy(&flag, error_.get(), sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
+    if (flag != 0) throw Error(-2, "tensor-core GEMM: a bounded device wait expired (MMA completion not observed)");
 }
 
 }  // namespace skb

@@ -130,28 +130,32 @@ private:
     DeviceBuffer bins_;
 };
 
-// Vertical plan: transposed matrices and tile tables for one direction.
+// Vertical plan for one direction: the group matrices prepared for the chosen
+// GEMM form and the tile / work-unit tables of every group and member.
 class VerticalPlan {
 public:
-    // rows_out x inner per group; matrices given as At[g][s][r].
+    // rowsOut x inner matrices per group, natural layout A[g][r][s]
+    // (forward: F[g][j][z], inverse: I[g][z][j]); one matrix for all groups
+    // when `natural` holds a single rowsOut x inner block.
     VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::vector<ModeGroup>& groups,
-                 std::uint64_t fields, std::uint64_t members, const std::vector<double>& transposed);
+                 std::uint64_t fields, std::uint64_t members, const std::vector<double>& natural);
     void execute(ComplexOperand in, ComplexOperand out, cudaStream_t s) const;
+    // Raises if a bounded device wait of the tensor-core form expired.
+    void check_device_error() const;
     GemmPrecision precision() const { return p_; }
     std::uint64_t columns() const { return columns_; }
     std::uint64_t matrixBytes() const { return matrices_.bytes(); }
     std::uint64_t persistentBytes() const;
-    int tiles() const { return tiles_; }
+    int launches() const { return 1; }
 
 private:
     GemmPrecision p_;
     int R_, S_;
     std::uint64_t columns_ = 0;
-    int tiles_ = 0;
+    int tiles_ = 0, units_ = 0;
+    long long memberColumns_ = 0;
     DeviceBuffer matrices_, tileGroup_, tileColumn_, tileCount_;
+    DeviceBuffer unitGroup_, unitColumn_, unitCount_, groupColumns_, groupFirst_, error_;
 };
-
-// At[g][s][r] for the forward (Nj x Nz) or inverse (Nz x Nj) matrices of a family.
-std::vector<double> transpose_family(const VerticalFamily& fam, bool forward);
 
 }  // namespace skb

@@ -1,0 +1,343 @@
+// Tensor-core (tcgen05, sm_100a) grouped vertical GEMM in split TF32x3.
+//
+// Problem (see vertical.hpp): for each K^2 group g, out[c][r] = sum_s
+// A_g[r][s] in[c][s] over the group's complex columns c.  It is issued as the
+// transposed real product
+//     D[m][n] = sum_k Aop[m][k] * Bop[n][k]
+// with m = (column, re/im part) of the data (M = 128 rows = 64 complex
+// columns per tile), n = r (N = R padded to a multiple of 16) and k = s.  Both
+// operands are K-major: Bop is the group matrix in its natural row-major
+// [r][s] layout, Aop is the data row in[c][0..S).
+//
+// Split precision: x = hi + lo with hi = rna_tf32(x), lo = rna_tf32(x - hi);
+// D = Ahi*Bhi + Ahi*Blo + Alo*Bhi accumulated in FP32 in tensor memory.  The
+// dropped lo*lo term is ~2^-22 relative, so results carry FP32-level error.
+//
+// CTA work unit: one group and a run of up to kUnitTiles M-tiles of its
+// (member, column) list.  The group matrix is split and written once into
+// shared memory (all K chunks) and stays resident; data chunks of 32 k
+// stream through a two-stage buffer.  Operands use the canonical K-major
+// SWIZZLE_128B layout: 8-row atoms of 8 x 128 bytes, 16-byte chunk q of row
+// n stored at chunk (q xor n%8).  One elected thread issues the MMAs and
+// commits them to the stage's mbarrier; every wait is bounded and reports
+// through `error` instead of hanging.
+
+#include <cstdint>
+
+#include "vertical.hpp"
+
+namespace skb {
+namespace {
+
+constexpr int kTileRows = 128;    // M
+constexpr int kChunkK = 32;       // tf32 elements per 128-byte row
+constexpr int kThreads = 256;
+constexpr int kTmemCols = 256;
+constexpr int kStageBytes = 2 * kTileRows * 128;  // hi + lo
+constexpr long long kWaitLimit = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity to complete.
+// Gives up early once any CTA of the launch has reported an expired wait.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const int* error) {
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 1023) == 1023 && *reinterpret_cast<const volatile int*>(error) != 0) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t slot, uint32_t cols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(cols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    const uint32_t mask = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(mask)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// K-major SWIZZLE_128B descriptor: SBO = 1024 B between 8-row atoms, LBO
+// unused (16 B), descriptor version 1, layout type 2.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(1) << 16) |
+           (static_cast<uint64_t>(1024 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
+           (static_cast<uint64_t>(2) << 61);
+}
+
+// Byte offset of (row, 16-byte chunk q) inside a swizzled operand.
+__device__ __forceinline__ uint32_t sw128_offset(int row, int q) {
+    return static_cast<uint32_t>((row >> 3) * 1024 + (row & 7) * 128 + ((q ^ (row & 7)) << 4));
+}
+
+struct Split4 {
+    float4 hi, lo;
+};
+
+__device__ __forceinline__ Split4 split4(float a, float b, float c, float d) {
+    Split4 s;
+    s.hi = make_float4(tf32_rna(a), tf32_rna(b), tf32_rna(c), tf32_rna(d));
+    s.lo = make_float4(tf32_rna(a - s.hi.x), tf32_rna(b - s.hi.y), tf32_rna(c - s.hi.z), tf32_rna(d - s.hi.w));
+    return s;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) tc_gemm_tf32x3_kernel(TcGemmArgs p) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* base =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int NP = p.NP, KCH = p.KCH, R = p.R, S = p.S;
+    unsigned char* sBhi = base;
+    unsigned char* sBlo = sBhi + KCH * NP * 128;
+    unsigned char* sA = sBlo + KCH * NP * 128;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sA + 2 * kStageBytes);
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(bars + 2);
+
+    const int unit = blockIdx.x;
+    const int g = __ldg(p.unitGroup + unit);
+    const int vc0 = __ldg(p.unitColumn + unit);
+    const int vcN = __ldg(p.unitCount + unit);
+    const int gcols = __ldg(p.groupColumns + g);
+    const long long gfirst = __ldg(p.groupFirst + g);
+
+    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar1, 1);
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(smem_u32(tmemSlot), kTmemCols);
+        tmem_relinquish();
+    }
+
+    // Resident group matrix, split hi/lo, zero-padded to NP x KCH*32.
+    const float* Bg = p.B + static_cast<long long>(g) * R * S;
+    for (int item = tid; item < NP * KCH * 8; item += kThreads) {
+        const int q = item & 7;
+        const int rest = item >> 3;
+        const int kc = rest % KCH;
+        const int n = rest / KCH;
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int s = kc * kChunkK + q * 4 + j;
+            v[j] = (n < R && s < S) ? __ldg(Bg + static_cast<long long>(n) * S + s) : 0.0f;
+        }
+        const Split4 sp = split4(v[0], v[1], v[2], v[3]);
+        const uint32_t off = kc * NP * 128 + sw128_offset(n, q);
+        *reinterpret_cast<float4*>(sBhi + off) = sp.hi;
+        *reinterpret_cast<float4*>(sBlo + off) = sp.lo;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmemSlot;
+
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(NP >> 3) << 17) |
+                           (static_cast<uint32_t>(kTileRows >> 4) << 24);
+    int commits0 = 0, commits1 = 0, waits0 = 0, waits1 = 0;
+    bool aborted = false;
+    auto drain = [&](int stage) -> bool {
+        // Wait until every commit on this stage's barrier has completed.
+        int& w = stage ? waits1 : waits0;
+        const int c = stage ? commits1 : commits0;
+        bool ok = true;
+        while (w < c && ok) {
+            ok = mbar_wait(stage ? bar1 : bar0, static_cast<uint32_t>(w & 1), p.error);
+            ++w;
+        }
+        return ok;
+    };
+
+    const int tiles = (vcN + 63) / 64;
+    int it = 0;
+    for (int t = 0; t < tiles && !aborted; ++t) {
+        const int tv0 = vc0 + t * 64;
+        const int tcount = min(64, vc0 + vcN - tv0);
+        for (int kc = 0; kc < KCH && !aborted; ++kc, ++it) {
+            const int st = it & 1;
+            if (__syncthreads_or(!drain(st))) {
+                aborted = true;
+                break;
+            }
+            unsigned char* aHi = sA + st * kStageBytes;
+            unsigned char* aLo = aHi + kTileRows * 128;
+            for (int item = tid; item < 64 * 8; item += kThreads) {
+                const int q = item & 7;
+                const int cl = item >> 3;
+                float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
+                if (cl < tcount) {
+                    const int vc = tv0 + cl;
+                    const int member = vc / gcols;
+                    const long long C = static_cast<long long>(member) * p.memberColumns + gfirst + (vc - member * gcols);
+                    const float2* src = p.in + C * S;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int s = kc * kChunkK + q * 4 + j;
+                        if (s < S) {
+                            const float2 x = __ldg(src + s);
+                            re[j] = x.x;
+                            im[j] = x.y;
+                        }
+                    }
+                }
+                const Split4 r4 = split4(re[0], re[1], re[2], re[3]);
+                const Split4 i4 = split4(im[0], im[1], im[2], im[3]);
+                const uint32_t o0 = sw128_offset(2 * cl, q), o1 = sw128_offset(2 * cl + 1, q);
+                *reinterpret_cast<float4*>(aHi + o0) = r4.hi;
+                *reinterpret_cast<float4*>(aLo + o0) = r4.lo;
+                *reinterpret_cast<float4*>(aHi + o1) = i4.hi;
+                *reinterpret_cast<float4*>(aLo + o1) = i4.lo;
+            }
+            fence_proxy_async();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t aH = smem_u32(aHi), aL = smem_u32(aLo);
+                const uint32_t bH = smem_u32(sBhi + kc * NP * 128), bL = smem_u32(sBlo + kc * NP * 128);
+                const int ksteps = min(4, (S - kc * kChunkK + 7) / 8);
+                for (int j = 0; j < ksteps; ++j) {
+                    const uint32_t off = j * 32;
+                    const uint32_t acc = (kc > 0 || j > 0) ? 1u : 0u;
+                    mma_tf32(tmem, sw128_desc(aH + off), sw128_desc(bH + off), idesc, acc);
+                    mma_tf32(tmem, sw128_desc(aH + off), sw128_desc(bL + off), idesc, 1u);
+                    mma_tf32(tmem, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
+                }
+                mma_commit(st ? bar1 : bar0);
+            }
+            if (st)
+                ++commits1;
+            else
+                ++commits0;
+        }
+        if (aborted) break;
+        // The last commit covers every MMA of this tile.
+        const int last = (it - 1) & 1;
+        if (__syncthreads_or(!drain(last))) {
+            aborted = true;
+            break;
+        }
+        tc_fence_after();
+        const int quarter = warp & 3;
+        const int half = warp >> 2;
+        const int m = quarter * 32 + lane;
+        const int cl = m >> 1;
+        const int part = m & 1;
+        const bool valid = cl < tcount;
+        long long C = 0;
+        if (valid) {
+            const int vc = tv0 + cl;
+            const int member = vc / gcols;
+            C = static_cast<long long>(member) * p.memberColumns + gfirst + (vc - member * gcols);
+        }
+        const int nHalf = NP / 2;
+        for (int col = half * nHalf; col < (half + 1) * nHalf; col += 8) {
+            uint32_t v[8];
+            tmem_ld_x8(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(col), v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float x = __uint_as_float(v[j]);
+                const float y = __shfl_xor_sync(0xffffffffu, x, 1);
+                const int n = col + j;
+                if ((j & 1) == part && valid && n < R)
+                    p.out[C * R + n] = part == 0 ? make_float2(x, y) : make_float2(y, x);
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (aborted) {
+        // Give outstanding MMAs a bounded chance to finish before freeing TMEM.
+        drain(0);
+        drain(1);
+        if (tid == 0) atomicExch(p.error, 1);
+    }
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+}
+
+}  // namespace
+
+size_t tc_gemm_smem_bytes(int R, int S) {
+    const int NP = (R + 15) / 16 * 16;
+    const int KCH = (S + kChunkK - 1) / kChunkK;
+    return 1024 + 2 * static_cast<size_t>(KCH) * NP * 128 + 2 * kStageBytes + 64;
+}
+
+bool tc_gemm_supported(int R, int S) {
+    const int NP = (R + 15) / 16 * 16;
+    return NP <= 256 && NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
+}
+
+int tc_gemm_unit_tiles() { return 16; }
+
+cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream) {
+    if (args.units <= 0) return cudaSuccess;
+    if (!tc_gemm_supported(args.R, args.S)) return cudaErrorInvalidValue;
+    const size_t bytes = tc_gemm_smem_bytes(args.R, args.S);
+    cudaError_t err =
+        cudaFuncSetAttribute(tc_gemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (err != cudaSuccess) return err;
+    tc_gemm_tf32x3_kernel<<<args.units, kThreads, bytes, stream>>>(args);
+    return cudaGetLastError();
+}
+
+}  // namespace skb

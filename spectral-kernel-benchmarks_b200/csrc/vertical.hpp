@@ -10,6 +10,8 @@
 
 #pragma once
 
+#include <cstddef>
+
 #include <cuda_runtime.h>
 
 namespace skb {
@@ -31,6 +33,29 @@ struct ComplexOperand {
 
 // Column tile width (complex columns per CTA) used to build GroupTiles.
 int gemm_tile_columns(GemmPrecision p);
+
+// Tensor-core split-TF32x3 form (tc_gemm.cu).  Work units are runs of the
+// (member, column) list of one group: virtual column v of group g is member
+// v / groupColumns[g], column groupFirst[g] + v % groupColumns[g] of that
+// member, i.e. global complex column member*memberColumns + ...
+struct TcGemmArgs {
+    const float* B;  // group matrices in natural layout [g][R][S], FP32
+    int R, S, NP, KCH;
+    const int* unitGroup;
+    const int* unitColumn;  // first virtual column of the unit
+    const int* unitCount;   // virtual columns in the unit
+    int units;
+    const int* groupColumns;  // complex columns per member in each group
+    const int* groupFirst;    // first complex column of each group within a member
+    long long memberColumns;
+    const float2* in;  // [column][S] complex FP32
+    float2* out;       // [column][R] complex FP32
+    int* error;        // set to nonzero if a bounded wait expired
+};
+bool tc_gemm_supported(int R, int S);
+size_t tc_gemm_smem_bytes(int R, int S);
+int tc_gemm_unit_tiles();
+cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream);
 
 cudaError_t launch_grouped_gemm(GemmPrecision p, int R, int S, const void* matrices, const GroupTiles& tiles,
                                 ComplexOperand in, ComplexOperand out, cudaStream_t stream);

@@ -703,6 +703,9 @@ class Flux:
         return [dict(name=a.name.decode(), ms=a.ms, launches=a.launches, bytes=a.algorithmic_bytes, flops=a.flops)
                 for a in arr[: n.value]]
 
+    def check_device(self):
+        check(library().skb_flux_check_device(self.h))
+
     def capture_graph(self, in_ptr, out_ptr):
         check(library().skb_flux_capture_graph(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr)))
 

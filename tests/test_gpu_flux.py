@@ -70,3 +70,28 @@ def test_flux_graph_replay_equals_direct():
     flux.replay_graph()
     skb_cuda.synchronize()
     assert np.array_equal(dout.download(np.complex128, flux.output_elements), direct)
+
+
+def test_flux_tf32x3_error_against_fp64():
+    n, nz, members = 64, 17, 2
+    modes = orc.retained_modes(n, n)
+    nj = 2 * (nz - 1) // 3
+    xs = [orc.flux_inputs(modes, 15, nj, 129 + m) for m in range(members)]
+    out = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3).execute(np.concatenate(xs))
+    out = out.reshape(members, -1)
+    for m in range(members):
+        assert orc.rel_l2_error(out[m], orc.flux(n, nz, xs[m])) <= 1e-6
+
+
+def test_flux_tf32x3_full_size_against_fp64_cuda():
+    # 512x512, Nz=129, 4 targets, 2 members: split precision versus the
+    # FP64-plain CUDA path on the same inputs (1e-6).
+    n, nz, members = 512, 129, 2
+    modes = orc.retained_modes(n, n)
+    nj = 2 * (nz - 1) // 3
+    x = np.concatenate([orc.flux_inputs(modes, 15, nj, 300 + m) for m in range(members)])
+    ref = skb_cuda.Flux(n, nz, members=members).execute(x)
+    fast = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    out = fast.execute(x)
+    fast.check_device()
+    assert orc.rel_l2_error(out, ref) <= 1e-6

@@ -120,3 +120,37 @@ def test_pointwise_large_volume():
     assert orc.max_rel_error(out, ref) <= 1e-15
     out32 = skb_cuda.PointwiseAdvectionExecutor(n, scale, skb_cuda.FP32).execute(s, d)
     assert orc.rel_l2_error(out32, ref) <= 1e-6
+
+
+# ------------------------------------------------------- tensor-core form
+
+@pytest.mark.parametrize("shape", [(16, 16, 9, 3), (16, 16, 7, 2), (256, 256, 65, 3), (128, 128, 33, 4),
+                                   (512, 512, 129, 15)])
+def test_tf32x3_tensor_core_matches_oracle(shape):
+    # Split TF32x3 on tcgen05, FP32 accumulation: FP32-level error against FP64.
+    w = skb_cuda.Workload(*shape)
+    o = orc.Workload(*shape)
+    fam = orc.k2_family(o)
+    H = len(orc.retained_modes(w.nx, w.ny))
+    rng = np.random.default_rng(12)
+    phys = rng.uniform(-1, 1, H * w.fields * w.nz) + 1j * rng.uniform(-1, 1, H * w.fields * w.nz)
+    modal = rng.uniform(-1, 1, H * w.fields * w.nj) + 1j * rng.uniform(-1, 1, H * w.fields * w.nj)
+    vp = provider(w, precision=skb_cuda.GEMM_TF32X3)
+    vp.load_physical_input(phys)
+    vp.execute_forward()
+    got = vp.copy_forward_output()
+    ref = orc.grouped_vertical(o, fam, "forward", phys)
+    assert orc.rel_l2_error(got, ref) <= 1e-6
+    assert orc.max_rel_error(got, ref) <= 2e-6
+    vp.load_modal_input(modal)
+    vp.execute_inverse()
+    got = vp.copy_inverse_output()
+    ref = orc.grouped_vertical(o, fam, "inverse", modal)
+    assert orc.rel_l2_error(got, ref) <= 1e-6
+    assert orc.max_rel_error(got, ref) <= 2e-6
+
+
+def test_tf32x3_rejects_split_layout():
+    w = skb_cuda.Workload(16, 16, 9, 3)
+    with pytest.raises(ValueError):
+        provider(w, layout=skb_cuda.SPLIT, precision=skb_cuda.GEMM_TF32X3)
