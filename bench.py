@@ -195,14 +195,8 @@ def cuda_arm(args, dist):
 
     S.set_device(dist.local)
     mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
-    try:
-        flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode)
-        mode_name = args.mode
-    except RuntimeError:
-        if args.mode != "split":
-            raise
-        mode, mode_name = S.FLUX_FP32, "fp32"
-        flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode)
+    flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode)
+    mode_name = {"split": "split-tf32x3"}.get(args.mode, args.mode)
     dtype = flux.device_dtype
     x = power_law_inputs(args.n, args.nz, args.members, seed=129 + dist.rank)
     din = S.DeviceArray.from_numpy(x.astype(dtype))
