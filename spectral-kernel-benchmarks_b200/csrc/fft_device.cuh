@@ -125,10 +125,12 @@ __device__ __forceinline__ V twiddle(const V* __restrict__ tw, int k) {
 
 constexpr int fft_threads(int N) { return N >= 8 ? N / 8 : 1; }
 
-// Transform B sequences of length N in shared memory.  Must be called by all
-// fft_threads(N)*B threads (tid in [0, that)); other threads of the CTA must
-// still reach the __syncthreads() calls, which is why `active` exists.
-template <typename T, int N, int B, int SIGN>
+// Transform B sequences of length N in shared memory, element (n, b) at
+// data[n * LD + b] (LD = B, or B + 1 where callers also walk along n).  Must
+// be called by all fft_threads(N)*B threads (tid in [0, that)); other threads
+// of the CTA must still reach the __syncthreads() calls, which is why
+// `active` exists.
+template <typename T, int N, int B, int SIGN, int LD = B>
 __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ tw, int tid, bool active) {
     using V = cx<T>;
     if constexpr (N == 1) {
@@ -139,7 +141,7 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
             V v[N];
             const int b = tid;
 #pragma unroll
-            for (int n = 0; n < N; ++n) v[n] = data[n * B + b];
+            for (int n = 0; n < N; ++n) v[n] = data[n * LD + b];
             if constexpr (N == 2) {
                 dft2<SIGN>(v[0], v[1]);
             } else {
@@ -151,7 +153,7 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
                 v[3] = t3;
             }
 #pragma unroll
-            for (int n = 0; n < N; ++n) data[n * B + b] = v[n];
+            for (int n = 0; n < N; ++n) data[n * LD + b] = v[n];
         }
         __syncthreads();
     } else {
@@ -164,7 +166,7 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
             V v[8];
             if (active) {
 #pragma unroll
-                for (int r = 0; r < 8; ++r) v[r] = data[(j + r * (N / 8)) * B + b];
+                for (int r = 0; r < 8; ++r) v[r] = data[(j + r * (N / 8)) * LD + b];
                 const int k = j % Ns;
                 if (Ns > 1) {
                     const int step = k * (N / (Ns * 8));
@@ -178,7 +180,7 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
                 const int k = j % Ns;
                 const int base = (j / Ns) * Ns * 8 + k;
 #pragma unroll
-                for (int r = 0; r < 8; ++r) data[(base + r * Ns) * B + b] = v[r];
+                for (int r = 0; r < 8; ++r) data[(base + r * Ns) * LD + b] = v[r];
             }
             __syncthreads();
             Ns *= 8;
@@ -197,7 +199,7 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
                 for (int s = 0; s < 2; ++s) {
                     const int jj = j + s * (N / 8);
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) v[4 * s + r] = data[(jj + r * ns) * B + b];
+                    for (int r = 0; r < 4; ++r) v[4 * s + r] = data[(jj + r * ns) * LD + b];
 #pragma unroll
                     for (int r = 1; r < 4; ++r) v[4 * s + r] = cmul(v[4 * s + r], twiddle<SIGN>(tw, jj * r));
                     dft4<SIGN>(v[4 * s], v[4 * s + 1], v[4 * s + 2], v[4 * s + 3]);
@@ -209,7 +211,7 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
                 for (int s = 0; s < 2; ++s) {
                     const int jj = j + s * (N / 8);
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) data[(jj + r * ns) * B + b] = v[4 * s + r];
+                    for (int r = 0; r < 4; ++r) data[(jj + r * ns) * LD + b] = v[4 * s + r];
                 }
             }
             __syncthreads();
@@ -221,8 +223,8 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     const int jj = j + s * (N / 8);
-                    v[2 * s] = data[jj * B + b];
-                    v[2 * s + 1] = cmul(data[(jj + ns) * B + b], twiddle<SIGN>(tw, jj));
+                    v[2 * s] = data[jj * LD + b];
+                    v[2 * s + 1] = cmul(data[(jj + ns) * LD + b], twiddle<SIGN>(tw, jj));
                     dft2<SIGN>(v[2 * s], v[2 * s + 1]);
                 }
             }
@@ -231,8 +233,8 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     const int jj = j + s * (N / 8);
-                    data[jj * B + b] = v[2 * s];
-                    data[(jj + ns) * B + b] = v[2 * s + 1];
+                    data[jj * LD + b] = v[2 * s];
+                    data[(jj + ns) * LD + b] = v[2 * s + 1];
                 }
             }
             __syncthreads();

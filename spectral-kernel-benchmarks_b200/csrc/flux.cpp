@@ -1,5 +1,6 @@
 #include "flux.hpp"
 
+#include "flux_rows.hpp"
 #include "pointwise.hpp"
 
 namespace skb {
@@ -31,11 +32,13 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
                              : cfg.mode == FluxMode::split_tf32x3 ? GemmPrecision::tf32x3
                                                                   : GemmPrecision::f32;
     const size_t es = element_bytes(hp);
+    fused_ = cfg.mode == FluxMode::split_tf32x3 && rows_flux_supported(static_cast<long long>(cfg.n));
     // Admission by device memory: refuse before allocating what cannot fit.
-    const std::uint64_t maxPlanes = 3 * cfg.members * cfg.nz;
+    const std::uint64_t maxPlanes = fused_ ? 1 : 3 * cfg.members * cfg.nz;
+    const std::uint64_t binPlanes = fused_ ? cfg.members * cfg.nz * (fieldsIn_ + cfg.targets) : maxPlanes;
     std::uint64_t need = 2 * es * cfg.members * modes_ * cfg.nz * (fieldsIn_ + cfg.targets)  // physIn, physOut
-                         + es * volume_ * cfg.members * 7                                   // 3+3+1 volumes
-                         + 2 * es * cfg.n * (cfg.n / 2 + 1) * maxPlanes;                    // bin scratch bound
+                         + (fused_ ? 0 : es * volume_ * cfg.members * 7)                   // 3+3+1 volumes
+                         + 2 * es * cfg.n * (cfg.n / 2 + 1) * binPlanes;                   // bin scratch bound
     size_t freeBytes = 0, totalBytes = 0;
     check_cuda(cudaMemGetInfo(&freeBytes, &totalBytes), "cudaMemGetInfo");
     if (need > freeBytes)
@@ -49,16 +52,23 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
                                                   cfg.targets, cfg.members, fam.forward);
     physIn_.allocate(2 * es * cfg.members * modes_ * fieldsIn_ * cfg.nz);
     physOut_.allocate(2 * es * cfg.members * modes_ * cfg.targets * cfg.nz);
-    shared_.allocate(es * 3 * cfg.members * volume_);
-    deriv_.allocate(es * 3 * cfg.members * volume_);
-    target_.allocate(es * cfg.members * volume_);
+    if (fused_) {
+        const std::uint64_t keep = static_cast<std::uint64_t>(horizontal_->keep());
+        binsIn_.allocate(2 * es * cfg.n * keep * cfg.members * fieldsIn_ * cfg.nz);
+        binsOut_.allocate(2 * es * cfg.n * keep * cfg.members * cfg.targets * cfg.nz);
+    } else {
+        shared_.allocate(es * 3 * cfg.members * volume_);
+        deriv_.allocate(es * 3 * cfg.members * volume_);
+        target_.allocate(es * cfg.members * volume_);
+    }
     allocationSeconds = seconds_since(allocStart) + horizontal_->allocationSeconds;
     planningSeconds += horizontal_->planningSeconds;
     persistentBytes = horizontal_->persistentBytes + inverseGemm_->persistentBytes() + forwardGemm_->persistentBytes();
     scratchBytes = horizontal_->scratchBytes + physIn_.bytes() + physOut_.bytes() + shared_.bytes() +
-                   deriv_.bytes() + target_.bytes();
-    // 2 GEMMs, 2 launches per inverse / forward horizontal, members pointwise per target.
-    launches_ = 2 + 2 + cfg.targets * (2 + cfg.members + 2);
+                   deriv_.bytes() + target_.bytes() + binsIn_.bytes() + binsOut_.bytes();
+    // Staged: 2 GEMMs, 2 launches per inverse / forward horizontal, members pointwise per target.
+    // Fused: GEMM, embed+columns, fused rows, columns+retention, GEMM.
+    launches_ = fused_ ? 5 : 2 + 2 + cfg.targets * (2 + cfg.members + 2);
 }
 
 FluxPipeline::~FluxPipeline() {
@@ -115,7 +125,65 @@ std::vector<FluxPipeline::StageTime> FluxPipeline::profile(const void* modalIn, 
     return rec.finish();
 }
 
+void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec) {
+    const auto H = modes_, nz = cfg_.nz, T = cfg_.targets, M = cfg_.members;
+    const size_t ces = 2 * sizeof(float);
+    const double n = static_cast<double>(cfg_.n);
+    const long long keep = horizontal_->keep();
+    auto* physIn = physIn_.get<unsigned char>();
+    auto* physOut = physOut_.get<unsigned char>();
+    const double binsPlane = n * keep * ces, compactPlane = double(H) * ces;
+    const double gemmIn = double(M) * H * fieldsIn_ * (nj_ + nz) * ces + inverseGemm_->matrixBytes();
+    const double gemmOut = double(M) * H * T * (nj_ + nz) * ces + forwardGemm_->matrixBytes();
+    const long long inPlanes = static_cast<long long>(M * fieldsIn_ * nz);
+    const long long outPlanes = static_cast<long long>(M * T * nz);
+
+    inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s);
+    if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
+
+    ViewSet inViews{};
+    inViews.count = static_cast<int>(M * fieldsIn_);
+    for (std::uint64_t m = 0; m < M; ++m)
+        for (std::uint64_t f = 0; f < fieldsIn_; ++f)
+            inViews.v[m * fieldsIn_ + f] = {physIn + ces * ((m * H * fieldsIn_ + f) * nz), nullptr,
+                                            static_cast<long long>(fieldsIn_ * nz)};
+    const DenseBins binsIn{binsIn_.get(), inPlanes, keep};
+    horizontal_->inverse_columns_into(inViews, binsIn, s);
+    if (rec) rec->end("columns_inverse_embed", 1, double(inPlanes) * (compactPlane + binsPlane), 0.0);
+
+    RowFluxArgs a{};
+    a.nx = static_cast<int>(cfg_.n);
+    a.ny = static_cast<int>(cfg_.n);
+    a.nz = static_cast<int>(nz);
+    a.keep = static_cast<int>(keep);
+    a.members = static_cast<int>(M);
+    a.fieldsIn = static_cast<int>(fieldsIn_);
+    a.targets = static_cast<int>(T);
+    a.scale = static_cast<float>(1.0 / (n * n * n * n));
+    a.binsIn = binsIn;
+    a.binsOut = {binsOut_.get(), outPlanes, keep};
+    a.twHalf = horizontal_->twiddlesHalf();
+    a.twFull = horizontal_->twiddlesFull();
+    check_cuda(launch_rows_flux(a, s), "fused row flux kernel");
+    if (rec) rec->end("rows_flux_fused", 1, double(inPlanes + outPlanes) * binsPlane, 0.0);
+
+    ViewSet outViews{};
+    outViews.count = static_cast<int>(M * T);
+    for (std::uint64_t m = 0; m < M; ++m)
+        for (std::uint64_t t = 0; t < T; ++t)
+            outViews.v[m * T + t] = {physOut + ces * ((m * H * T + t) * nz), nullptr, static_cast<long long>(T * nz)};
+    horizontal_->forward_columns_from(a.binsOut, outViews, 1.0, s);
+    if (rec) rec->end("columns_forward_gather", 1, double(outPlanes) * (binsPlane + compactPlane), 0.0);
+
+    forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s);
+    if (rec) rec->end("gemm_forward_tf32x3", 1, gemmOut, 3.0 * 4.0 * nz * nj_ * double(M) * H * T);
+}
+
 void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec) {
+    if (fused_) {
+        runFused(modalIn, modalOut, s, rec);
+        return;
+    }
     const auto H = modes_, nz = cfg_.nz, T = cfg_.targets, M = cfg_.members;
     const size_t es = element_bytes(horizontal_->precision());
     const size_t ces = 2 * es;  // complex element bytes

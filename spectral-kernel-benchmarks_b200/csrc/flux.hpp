@@ -74,8 +74,13 @@ private:
     std::unique_ptr<HorizontalPlan> horizontal_;
     std::unique_ptr<VerticalPlan> inverseGemm_, forwardGemm_;
     DeviceBuffer physIn_, shared_, deriv_, target_, physOut_;
+    // Fused split-precision path: column-transformed bins of every input slot
+    // and of every target.
+    bool fused_ = false;
+    DeviceBuffer binsIn_, binsOut_;
     std::uint64_t launches_ = 0;
     struct Recorder;
+    void runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec);
     void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec);
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graphExec_ = nullptr;

@@ -1,0 +1,159 @@
+// Fused row stage of the split-precision flux (FP32).
+//
+// One CTA owns one row y of B consecutive z-planes of one ensemble member and
+// does, entirely on chip, what the staged path spreads over three kernels and
+// seven real volumes (benchmark.cpp:4405-4424 order):
+//   U,V,W rows      <- c2r of the column-transformed bins of input slots 0..2,
+//                      kept in registers;
+//   for each target t:
+//     q_t,x/y/z rows <- c2r of slots 3+3t .. 5+3t;
+//     target row     = -scale*(u*q_x + v*q_y + w*q_z)   (pointwise_advection.cpp:143-147)
+//     target bins    <- r2c of the target row, kx < keep.
+// The c2r / r2c are the same half-length complex FFT formulation as the
+// staged row kernels (horizontal.cu), so both paths share their numerics.
+// Every thread keeps the same eight (plane, x-pair) positions across all
+// transforms, which is what lets U,V,W and the product stay in registers.
+
+#include "flux_rows.hpp"
+
+#include "fft_device.cuh"
+
+namespace skb {
+namespace {
+
+template <int M, int B>
+struct RowFluxShape {
+    static constexpr int threads = fft_threads(M) * B;
+    static constexpr int per = M * B / threads;  // positions per thread (8 for M >= 8)
+};
+
+template <int M, int B>
+__global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(RowFluxArgs a) {
+    using V = float2;
+    constexpr int NT = RowFluxShape<M, B>::threads;
+    constexpr int PER = RowFluxShape<M, B>::per;
+    __shared__ V data[M * B];
+    const int tid = threadIdx.x;
+    const int zChunks = (a.nz + B - 1) / B;
+    const int member = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int y = blockIdx.y;
+    const V* twHalf = static_cast<const V*>(a.twHalf);
+    const V* twFull = static_cast<const V*>(a.twFull);
+    const V* in = static_cast<const V*>(a.binsIn.data);
+    V* out = static_cast<V*>(a.binsOut.data);
+    const long long inRow = a.binsIn.planes;   // stride between kx
+    const long long outRow = a.binsOut.planes;
+
+    // Inverse row transform of input slot f into per-thread registers r[].
+    auto inverse_row = [&](int f, V (&r)[PER]) {
+        const long long pBase = (static_cast<long long>(member) * a.fieldsIn + f) * a.nz + z0;
+        auto load = [&](int k, int b) -> V {
+            if (k >= a.keep || z0 + b >= a.nz) return V{0.f, 0.f};
+            V v = in[pBase + b + inRow * (static_cast<long long>(k) + a.binsIn.kxStride * y)];
+            if (k == 0 || k == M) v.y = 0.f;
+            return v;
+        };
+        constexpr int pairs = M / 2 + 1;
+        for (int idx = tid; idx < pairs * B; idx += NT) {
+            const int b = idx % B;
+            const int k = idx / B;
+            if (k == 0) {
+                const V x0 = load(0, b);
+                const V xm = load(M, b);
+                data[b] = {x0.x + xm.x, x0.x - xm.x};
+                continue;
+            }
+            const int kk = M - k;
+            const V xk = load(k, b);
+            const V xm = load(kk, b);
+            {
+                const V s = cadd(xk, cconj(xm));
+                const V d = csub(xk, cconj(xm));
+                const V t = cmulc(d, __ldg(twFull + k));
+                data[k * B + b] = {s.x - t.y, s.y + t.x};
+            }
+            if (kk != k) {
+                const V s = cadd(xm, cconj(xk));
+                const V d = csub(xm, cconj(xk));
+                const V t = cmulc(d, __ldg(twFull + kk));
+                data[kk * B + b] = {s.x - t.y, s.y + t.x};
+            }
+        }
+        __syncthreads();
+        fft_smem<float, M, B, +1>(data, twHalf, tid, true);
+#pragma unroll
+        for (int e = 0; e < PER; ++e) r[e] = data[tid + e * NT];
+        __syncthreads();
+    };
+
+    V u[PER], v[PER], w[PER];
+    inverse_row(0, u);
+    inverse_row(1, v);
+    inverse_row(2, w);
+    const float scale = a.scale;
+    for (int t = 0; t < a.targets; ++t) {
+        V acc[PER], q[PER];
+        inverse_row(3 + 3 * t, q);
+#pragma unroll
+        for (int e = 0; e < PER; ++e) acc[e] = {u[e].x * q[e].x, u[e].y * q[e].y};
+        inverse_row(4 + 3 * t, q);
+#pragma unroll
+        for (int e = 0; e < PER; ++e) acc[e] = {acc[e].x + v[e].x * q[e].x, acc[e].y + v[e].y * q[e].y};
+        inverse_row(5 + 3 * t, q);
+#pragma unroll
+        for (int e = 0; e < PER; ++e) {
+            acc[e] = {acc[e].x + w[e].x * q[e].x, acc[e].y + w[e].y * q[e].y};
+            data[tid + e * NT] = {-scale * acc[e].x, -scale * acc[e].y};
+        }
+        __syncthreads();
+        fft_smem<float, M, B, -1>(data, twHalf, tid, true);
+        // Real-spectrum split of the half-length FFT, kx < keep.
+        const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.nz + z0;
+        for (int idx = tid; idx < a.keep * B; idx += NT) {
+            const int b = idx % B;
+            const int k = idx / B;
+            if (z0 + b >= a.nz) continue;
+            V X;
+            const V zz = data[b];
+            if (k == 0) {
+                X = {zz.x + zz.y, 0.f};
+            } else if (k == M) {
+                X = {zz.x - zz.y, 0.f};
+            } else {
+                const V zk = data[k * B + b];
+                const V zm = cconj(data[(M - k) * B + b]);
+                const V ev = cscale(cadd(zk, zm), 0.5f);
+                const V d = csub(zk, zm);
+                const V o = {0.5f * d.y, -0.5f * d.x};
+                X = cadd(ev, cmul(__ldg(twFull + k), o));
+            }
+            out[pOut + b + outRow * (static_cast<long long>(k) + a.binsOut.kxStride * y)] = X;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
+    const int M = a.nx / 2;
+    constexpr int B = 8;
+    const int zChunks = (a.nz + B - 1) / B;
+    dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
+    switch (M) {
+        case 8: rows_flux_kernel<8, B><<<grid, RowFluxShape<8, B>::threads, 0, stream>>>(a); break;
+        case 16: rows_flux_kernel<16, B><<<grid, RowFluxShape<16, B>::threads, 0, stream>>>(a); break;
+        case 32: rows_flux_kernel<32, B><<<grid, RowFluxShape<32, B>::threads, 0, stream>>>(a); break;
+        case 64: rows_flux_kernel<64, B><<<grid, RowFluxShape<64, B>::threads, 0, stream>>>(a); break;
+        case 128: rows_flux_kernel<128, B><<<grid, RowFluxShape<128, B>::threads, 0, stream>>>(a); break;
+        case 256: rows_flux_kernel<256, B><<<grid, RowFluxShape<256, B>::threads, 0, stream>>>(a); break;
+        case 512: rows_flux_kernel<512, B><<<grid, RowFluxShape<512, B>::threads, 0, stream>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+bool rows_flux_supported(long long nx) { return nx >= 16 && nx <= 1024 && (nx & (nx - 1)) == 0; }
+
+}  // namespace skb

@@ -1,0 +1,23 @@
+// Fused row stage of the split-precision flux (flux_rows.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "horizontal.hpp"
+
+namespace skb {
+
+struct RowFluxArgs {
+    int nx, ny, nz, keep;
+    int members, fieldsIn, targets;
+    float scale;          // 1/(Nx*Ny)^2 (benchmark.cpp:4040-4041)
+    DenseBins binsIn;     // column-transformed input slots, plane (member*fieldsIn + slot)*nz + z
+    DenseBins binsOut;    // target bins, plane (member*targets + t)*nz + z
+    const void* twHalf;   // exp(-2 pi i k/(nx/2)), float2
+    const void* twFull;   // exp(-2 pi i k/nx), float2
+};
+
+bool rows_flux_supported(long long nx);
+cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream);
+
+}  // namespace skb

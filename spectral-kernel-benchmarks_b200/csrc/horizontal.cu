@@ -41,16 +41,18 @@ __global__ void __launch_bounds__(cta_threads<T, M>()) rows_forward_kernel(
     const long long p0 = (long long)blockIdx.x * B;
     const int y = blockIdx.y;
     constexpr int NX = 2 * M;
+    constexpr int LD = B + 1;  // padded so the walk along x below is conflict-free
+    // Consecutive threads take consecutive x-pairs of one row: full-line loads.
     for (int idx = tid; idx < M * B; idx += NT) {
-        const int b = idx % B;
-        const int m = idx / B;
+        const int m = idx % M;
+        const int b = idx / M;
         const long long p = p0 + b;
         V v = {T(0), T(0)};
         if (p < planes) v = *reinterpret_cast<const V*>(real + (p * ny + y) * NX + 2 * m);
-        data[m * B + b] = v;
+        data[m * LD + b] = v;
     }
     __syncthreads();
-    fft_smem<T, M, B, -1>(data, twHalf, tid, true);
+    fft_smem<T, M, B, -1, LD>(data, twHalf, tid, true);
     V* out = reinterpret_cast<V*>(bins.data);
     for (int idx = tid; idx < keep * B; idx += NT) {
         const int b = idx % B;
@@ -64,8 +66,8 @@ __global__ void __launch_bounds__(cta_threads<T, M>()) rows_forward_kernel(
         } else if (k == M) {
             X = {z0.x - z0.y, T(0)};
         } else {
-            const V zk = data[k * B + b];
-            const V zm = cconj(data[(M - k) * B + b]);
+            const V zk = data[k * LD + b];
+            const V zm = cconj(data[(M - k) * LD + b]);
             const V e = cscale(cadd(zk, zm), T(0.5));
             const V d = csub(zk, zm);
             // o = -i/2 * d
@@ -93,6 +95,7 @@ __global__ void __launch_bounds__(cta_threads<T, M>()) rows_inverse_kernel(
     const long long p0 = (long long)blockIdx.x * B;
     const int y = blockIdx.y;
     constexpr int NX = 2 * M;
+    constexpr int LD = B + 1;
     const V* in = reinterpret_cast<const V*>(bins.data);
     auto load = [&](int k, int b) -> V {
         const long long p = p0 + b;
@@ -119,22 +122,23 @@ __global__ void __launch_bounds__(cta_threads<T, M>()) rows_inverse_kernel(
             const V s = cadd(xk, cconj(xm));
             const V d = csub(xk, cconj(xm));
             const V t = cmulc(d, __ldg(twFull + k));  // d * e^{+2 pi i k/NX}
-            data[k * B + b] = {s.x - t.y, s.y + t.x};    // s + i t
+            data[k * LD + b] = {s.x - t.y, s.y + t.x};   // s + i t
         }
         if (kk != k) {
             const V s = cadd(xm, cconj(xk));
             const V d = csub(xm, cconj(xk));
             const V t = cmulc(d, __ldg(twFull + kk));
-            data[kk * B + b] = {s.x - t.y, s.y + t.x};
+            data[kk * LD + b] = {s.x - t.y, s.y + t.x};
         }
     }
     __syncthreads();
-    fft_smem<T, M, B, +1>(data, twHalf, tid, true);
+    fft_smem<T, M, B, +1, LD>(data, twHalf, tid, true);
+    // Consecutive threads write consecutive x-pairs of one row.
     for (int idx = tid; idx < M * B; idx += NT) {
-        const int b = idx % B;
-        const int m = idx / B;
+        const int m = idx % M;
+        const int b = idx / M;
         const long long p = p0 + b;
-        if (p < planes) *reinterpret_cast<V*>(real + (p * ny + y) * NX + 2 * m) = data[m * B + b];
+        if (p < planes) *reinterpret_cast<V*>(real + (p * ny + y) * NX + 2 * m) = data[m * LD + b];
     }
 }
 
@@ -344,6 +348,12 @@ size_t smem_bytes() {
     return size_t(N) * batch_width<T, N>() * sizeof(cx<T>);
 }
 
+// Row kernels pad each shared row by one element (stride B + 1).
+template <typename T, int N>
+size_t row_smem_bytes() {
+    return size_t(N) * (batch_width<T, N>() + 1) * sizeof(cx<T>);
+}
+
 template <typename K>
 cudaError_t allow_smem(K kernel, size_t bytes) {
     if (bytes <= 48 * 1024) return cudaSuccess;
@@ -378,7 +388,7 @@ cudaError_t rows_forward_t(int nx, int ny, long long planes, int keep, const voi
     SKB_LENGTH_SWITCH(M, {
         constexpr int B = batch_width<T, L>();
         auto kernel = rows_forward_kernel<T, L>;
-        const size_t bytes = smem_bytes<T, L>();
+        const size_t bytes = row_smem_bytes<T, L>();
         cudaError_t err = allow_smem(kernel, bytes);
         if (err != cudaSuccess) return err;
         dim3 grid(unsigned((planes + B - 1) / B), unsigned(ny));
@@ -402,7 +412,7 @@ cudaError_t rows_inverse_t(int nx, int ny, long long planes, int keep, DenseBins
     SKB_LENGTH_SWITCH(M, {
         constexpr int B = batch_width<T, L>();
         auto kernel = rows_inverse_kernel<T, L>;
-        const size_t bytes = smem_bytes<T, L>();
+        const size_t bytes = row_smem_bytes<T, L>();
         cudaError_t err = allow_smem(kernel, bytes);
         if (err != cudaSuccess) return err;
         dim3 grid(unsigned((planes + B - 1) / B), unsigned(ny));

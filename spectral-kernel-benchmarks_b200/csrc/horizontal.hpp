@@ -20,7 +20,7 @@
 
 namespace skb {
 
-constexpr int kMaxViews = 64;
+constexpr int kMaxViews = 128;
 
 // One field of retained (compact) coefficients: element (mode, z) lives at
 // z + modeStride*mode.  Interleaved complex when imag == nullptr (re points at

@@ -122,6 +122,20 @@ void HorizontalPlan::inverse_columns(const ViewSet& views, cudaStream_t s) const
                "embedding + column c2c kernel");
 }
 
+void HorizontalPlan::inverse_columns_into(const ViewSet& views, DenseBins out, cudaStream_t s) const {
+    if (out.kxStride != keep_) throw Error(-1, "bin array must hold keep() columns per row");
+    check_cuda(launch_columns_embed(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, views, tables(), out,
+                                    twCol_.get(), s),
+               "embedding + column c2c kernel");
+}
+
+void HorizontalPlan::forward_columns_from(DenseBins in, const ViewSet& views, double scale, cudaStream_t s) const {
+    if (in.kxStride != keep_) throw Error(-1, "bin array must hold keep() columns per row");
+    check_cuda(launch_columns_gather(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, in, views,
+                                     tables(), scale, twCol_.get(), s),
+               "column c2c + retention kernel");
+}
+
 void HorizontalPlan::inverse_rows(void* real, std::uint64_t planes, cudaStream_t s) const {
     if (planes > maxPlanes_) throw Error(-1, "plane count exceeds the plan's scratch");
     check_cuda(launch_rows_inverse(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny),

@@ -114,6 +114,11 @@ public:
     void inverse_dense(const void* wvm, void* real, std::uint64_t planes, cudaStream_t s) const;
     void gather_dense(const void* wvm, std::uint64_t planes, const ViewSet& views, double scale,
                       cudaStream_t s) const;
+    // Column stages against caller-owned bin arrays (kxStride = keep()).
+    void inverse_columns_into(const ViewSet& views, DenseBins out, cudaStream_t s) const;
+    void forward_columns_from(DenseBins in, const ViewSet& views, double scale, cudaStream_t s) const;
+    const void* twiddlesHalf() const { return twHalf_.get(); }
+    const void* twiddlesFull() const { return twFull_.get(); }
     void embed_dense(const ViewSet& views, void* wvm, std::uint64_t planes, cudaStream_t s) const;
 
     double allocationSeconds = 0.0, planningSeconds = 0.0;
