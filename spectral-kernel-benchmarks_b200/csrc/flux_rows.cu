@@ -13,6 +13,8 @@
 // staged row kernels (horizontal.cu), so both paths share their numerics.
 // Every thread keeps the same eight (plane, x-pair) positions across all
 // transforms, which is what lets U,V,W and the product stay in registers.
+// The 3+3T slots are consumed in order, so the bins of slot f+1 are copied
+// into a second shared stage with cp.async while slot f is transformed.
 
 #include "flux_rows.hpp"
 
@@ -27,12 +29,25 @@ struct RowFluxShape {
     static constexpr int per = M * B / threads;  // positions per thread (8 for M >= 8)
 };
 
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int srcBytes) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(srcBytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <int M, int B>
 __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(RowFluxArgs a) {
     using V = float2;
     constexpr int NT = RowFluxShape<M, B>::threads;
     constexpr int PER = RowFluxShape<M, B>::per;
-    __shared__ V data[M * B];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* data = reinterpret_cast<V*>(smem_raw);
+    V* stage0 = data + M * B;
+    V* stage1 = stage0 + a.keep * B;
     const int tid = threadIdx.x;
     const int zChunks = (a.nz + B - 1) / B;
     const int member = blockIdx.x / zChunks;
@@ -42,15 +57,38 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
     const V* twFull = static_cast<const V*>(a.twFull);
     const V* in = static_cast<const V*>(a.binsIn.data);
     V* out = static_cast<V*>(a.binsOut.data);
-    const long long inRow = a.binsIn.planes;   // stride between kx
+    const long long inRow = a.binsIn.planes;  // stride between kx
     const long long outRow = a.binsOut.planes;
+    const int keep = a.keep;
 
-    // Inverse row transform of input slot f into per-thread registers r[].
-    auto inverse_row = [&](int f, V (&r)[PER]) {
+    // Asynchronous copy of slot f's bins of this row (kx < keep, B planes) into
+    // a stage buffer [k][b]; planes beyond Nz are zero-filled.
+    auto issue = [&](int f, V* stage) {
         const long long pBase = (static_cast<long long>(member) * a.fieldsIn + f) * a.nz + z0;
+        const long long rowBase = a.binsIn.kxStride * y;
+        for (int idx = tid; idx < keep * B; idx += NT) {
+            const int b = idx % B;
+            const int k = idx / B;
+            const bool ok = z0 + b < a.nz;
+            const V* src = ok ? in + pBase + b + inRow * (static_cast<long long>(k) + rowBase) : in;
+            cp_async8(stage + idx, src, ok ? 8 : 0);
+        }
+        cp_async_commit();
+    };
+
+    // Inverse row transform of slot f (already staged) into registers r[].
+    auto inverse_row = [&](int f, V (&r)[PER]) {
+        if (f + 1 < a.fieldsIn) {
+            issue(f + 1, ((f + 1) & 1) ? stage1 : stage0);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const V* st = (f & 1) ? stage1 : stage0;
         auto load = [&](int k, int b) -> V {
-            if (k >= a.keep || z0 + b >= a.nz) return V{0.f, 0.f};
-            V v = in[pBase + b + inRow * (static_cast<long long>(k) + a.binsIn.kxStride * y)];
+            if (k >= keep) return V{0.f, 0.f};
+            V v = st[k * B + b];
             if (k == 0 || k == M) v.y = 0.f;
             return v;
         };
@@ -87,6 +125,7 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
         __syncthreads();
     };
 
+    issue(0, stage0);
     V u[PER], v[PER], w[PER];
     inverse_row(0, u);
     inverse_row(1, v);
@@ -110,7 +149,7 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
         fft_smem<float, M, B, -1>(data, twHalf, tid, true);
         // Real-spectrum split of the half-length FFT, kx < keep.
         const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.nz + z0;
-        for (int idx = tid; idx < a.keep * B; idx += NT) {
+        for (int idx = tid; idx < keep * B; idx += NT) {
             const int b = idx % B;
             const int k = idx / B;
             if (z0 + b >= a.nz) continue;
@@ -136,22 +175,35 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
 
 }  // namespace
 
+template <int M>
+cudaError_t launch_m(const RowFluxArgs& a, dim3 grid, cudaStream_t stream) {
+    constexpr int B = 8;
+    auto kernel = rows_flux_kernel<M, B>;
+    const size_t bytes = sizeof(float2) * (size_t(M) * B + 2 * size_t(a.keep) * B);
+    if (bytes > 48 * 1024) {
+        const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        if (err != cudaSuccess) return err;
+    }
+    kernel<<<grid, RowFluxShape<M, B>::threads, bytes, stream>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
     const int M = a.nx / 2;
     constexpr int B = 8;
+    if (a.keep < 1 || a.keep > M + 1 || a.fieldsIn != 3 + 3 * a.targets) return cudaErrorInvalidValue;
     const int zChunks = (a.nz + B - 1) / B;
     dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
     switch (M) {
-        case 8: rows_flux_kernel<8, B><<<grid, RowFluxShape<8, B>::threads, 0, stream>>>(a); break;
-        case 16: rows_flux_kernel<16, B><<<grid, RowFluxShape<16, B>::threads, 0, stream>>>(a); break;
-        case 32: rows_flux_kernel<32, B><<<grid, RowFluxShape<32, B>::threads, 0, stream>>>(a); break;
-        case 64: rows_flux_kernel<64, B><<<grid, RowFluxShape<64, B>::threads, 0, stream>>>(a); break;
-        case 128: rows_flux_kernel<128, B><<<grid, RowFluxShape<128, B>::threads, 0, stream>>>(a); break;
-        case 256: rows_flux_kernel<256, B><<<grid, RowFluxShape<256, B>::threads, 0, stream>>>(a); break;
-        case 512: rows_flux_kernel<512, B><<<grid, RowFluxShape<512, B>::threads, 0, stream>>>(a); break;
+        case 8: return launch_m<8>(a, grid, stream);
+        case 16: return launch_m<16>(a, grid, stream);
+        case 32: return launch_m<32>(a, grid, stream);
+        case 64: return launch_m<64>(a, grid, stream);
+        case 128: return launch_m<128>(a, grid, stream);
+        case 256: return launch_m<256>(a, grid, stream);
+        case 512: return launch_m<512>(a, grid, stream);
         default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 bool rows_flux_supported(long long nx) { return nx >= 16 && nx <= 1024 && (nx & (nx - 1)) == 0; }

@@ -10,8 +10,9 @@
 // [r][s] layout, Aop is the data row in[c][0..S).
 //
 // Split precision: x = hi + lo with hi = rna_tf32(x), lo = rna_tf32(x - hi);
-// D = Ahi*Bhi + Ahi*Blo + Alo*Bhi accumulated in FP32 in tensor memory.  The
-// dropped lo*lo term is ~2^-22 relative, so results carry FP32-level error.
+// D = Ahi*Blo + Alo*Bhi + Ahi*Bhi accumulated in FP32 in tensor memory, one
+// accumulator per 32-wide K chunk, chunk sums added in FP32 registers.  The
+// dropped lo*lo term is ~2^-22 relative.
 //
 // CTA work unit: one group and a run of up to kUnitTiles M-tiles of its
 // (member, column) list.  The group matrix is split and written once into
@@ -32,7 +33,7 @@ namespace {
 constexpr int kTileRows = 128;    // M
 constexpr int kChunkK = 32;       // tf32 elements per 128-byte row
 constexpr int kThreads = 256;
-constexpr int kTmemCols = 256;
+constexpr int kTmemCols = 512;  // one FP32 accumulator of NP columns per K chunk
 constexpr int kStageBytes = 2 * kTileRows * 128;  // hi + lo
 constexpr long long kWaitLimit = 1LL << 22;
 
@@ -253,12 +254,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_tf32x3_kernel(TcGemmArgs 
                 const uint32_t aH = smem_u32(aHi), aL = smem_u32(aLo);
                 const uint32_t bH = smem_u32(sBhi + kc * NP * 128), bL = smem_u32(sBlo + kc * NP * 128);
                 const int ksteps = min(4, (S - kc * kChunkK + 7) / 8);
+                // Each K chunk accumulates into its own TMEM columns; the chunk
+                // partial sums are added in FP32 registers in the epilogue,
+                // which keeps the in-MMA accumulation depth at 12 terms.
+                const uint32_t dChunk = tmem + static_cast<uint32_t>(kc * NP);
                 for (int j = 0; j < ksteps; ++j) {
                     const uint32_t off = j * 32;
-                    const uint32_t acc = (kc > 0 || j > 0) ? 1u : 0u;
-                    mma_tf32(tmem, sw128_desc(aH + off), sw128_desc(bH + off), idesc, acc);
-                    mma_tf32(tmem, sw128_desc(aH + off), sw128_desc(bL + off), idesc, 1u);
-                    mma_tf32(tmem, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
+                    const uint32_t acc = j > 0 ? 1u : 0u;
+                    mma_tf32(dChunk, sw128_desc(aH + off), sw128_desc(bL + off), idesc, acc);
+                    mma_tf32(dChunk, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
+                    mma_tf32(dChunk, sw128_desc(aH + off), sw128_desc(bH + off), idesc, 1u);
                 }
                 mma_commit(st ? bar1 : bar0);
             }
@@ -289,12 +294,19 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_tf32x3_kernel(TcGemmArgs 
         }
         const int nHalf = NP / 2;
         for (int col = half * nHalf; col < (half + 1) * nHalf; col += 8) {
-            uint32_t v[8];
-            tmem_ld_x8(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(col), v);
-            tmem_wait_ld();
+            float sum[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int kc = 0; kc < KCH; ++kc) {
+                uint32_t v[8];
+                tmem_ld_x8(tmem + (static_cast<uint32_t>(quarter * 32) << 16) +
+                               static_cast<uint32_t>(kc * NP + col),
+                           v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 8; ++j) sum[j] += __uint_as_float(v[j]);
+            }
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const float x = __uint_as_float(v[j]);
+                const float x = sum[j];
                 const float y = __shfl_xor_sync(0xffffffffu, x, 1);
                 const int n = col + j;
                 if ((j & 1) == part && valid && n < R)
@@ -324,7 +336,8 @@ size_t tc_gemm_smem_bytes(int R, int S) {
 
 bool tc_gemm_supported(int R, int S) {
     const int NP = (R + 15) / 16 * 16;
-    return NP <= 256 && NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
+    const int KCH = (S + kChunkK - 1) / kChunkK;
+    return NP <= 256 && KCH * NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
 }
 
 int tc_gemm_unit_tiles() { return 16; }

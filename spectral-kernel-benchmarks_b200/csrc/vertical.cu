@@ -2,8 +2,9 @@
 //
 // One CTA of 256 threads computes a tile of 32 complex columns of one K^2
 // group, all R output rows.  The inner dimension S is streamed through shared
-// memory in chunks of 32: the chunk of the group's transposed matrix
-// At[s][r] (prepared at set-up) and of the input columns in[c][s].  Lane l of
+// memory in chunks of 32 with a two-stage cp.async pipeline (chunk c+1 is in
+// flight while chunk c is consumed): the chunk of the group's transposed
+// matrix At[s][r] (prepared at set-up) and of the input columns in[c][s].  Lane l of
 // warp w owns rows r = l + 32k and columns c = w + 8m, so each step of s reads
 // a 32-wide contiguous row of At (conflict-free) and a broadcast input value,
 // and the final stores of out[c][r] are contiguous across the warp.
@@ -35,15 +36,28 @@ __device__ __forceinline__ void store_operand(const ComplexOperand& op, long lon
     }
 }
 
+// Asynchronous 4/8/16-byte global->shared copy; src_bytes = 0 writes zeros.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src, int src_bytes) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(src), "n"(BYTES), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <typename T, int KR, bool SPLIT>
 __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, const T* __restrict__ At,
                                                                 GroupTiles tiles, ComplexOperand in,
                                                                 ComplexOperand out) {
     using V = cx<T>;
     constexpr int RP = 32 * KR;
-    extern __shared__ unsigned char smem_raw[];
-    V(*sX)[kChunk + 1] = reinterpret_cast<V(*)[kChunk + 1]>(smem_raw);
-    T(*sA)[RP] = reinterpret_cast<T(*)[RP]>(smem_raw + sizeof(V) * kTileCols * (kChunk + 1));
+    constexpr size_t xBytes = sizeof(V) * kTileCols * (kChunk + 1);
+    constexpr size_t aBytes = sizeof(T) * kChunk * RP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tile = blockIdx.x;
     const int g = __ldg(tiles.tileGroup + tile);
     const int c0 = __ldg(tiles.tileColumn + tile);
@@ -51,6 +65,37 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const T* A = At + (long long)g * R * S;
+    const int chunks = (S + kChunk - 1) / kChunk;
+
+    auto stageX = [&](int b) { return reinterpret_cast<V(*)[kChunk + 1]>(smem_raw + b * (xBytes + aBytes)); };
+    auto stageA = [&](int b) { return reinterpret_cast<T(*)[RP]>(smem_raw + b * (xBytes + aBytes) + xBytes); };
+
+    // Issue the copies of chunk c into stage buffer b (zero-filled padding).
+    auto issue = [&](int c, int b) {
+        const int s0 = c * kChunk;
+        T(*sA)[RP] = stageA(b);
+        V(*sX)[kChunk + 1] = stageX(b);
+        for (int i = threadIdx.x; i < kChunk * RP; i += kThreads) {
+            const int s = i / RP, r = i % RP;
+            const bool ok = s0 + s < S && r < R;
+            const T* src = ok ? A + (long long)(s0 + s) * R + r : A;
+            cp_async<sizeof(T)>(&sA[s][r], src, ok ? int(sizeof(T)) : 0);
+        }
+        for (int i = threadIdx.x; i < kTileCols * kChunk; i += kThreads) {
+            const int c = i / kChunk, s = i % kChunk;
+            const bool ok = c < ncols && s0 + s < S;
+            const long long idx = ok ? (long long)(c0 + c) * S + s0 + s : 0;
+            if (SPLIT) {
+                // Split operands: two scalar copies into the complex slot.
+                T* slot = reinterpret_cast<T*>(&sX[c][s]);
+                cp_async<sizeof(T)>(slot, reinterpret_cast<const T*>(in.re) + idx, ok ? int(sizeof(T)) : 0);
+                cp_async<sizeof(T)>(slot + 1, reinterpret_cast<const T*>(in.im) + idx, ok ? int(sizeof(T)) : 0);
+            } else {
+                cp_async<sizeof(V)>(&sX[c][s], reinterpret_cast<const V*>(in.re) + idx, ok ? int(sizeof(V)) : 0);
+            }
+        }
+        cp_async_commit();
+    };
 
     V acc[KR][kTileCols / 8];
 #pragma unroll
@@ -58,19 +103,18 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
 #pragma unroll
         for (int m = 0; m < kTileCols / 8; ++m) acc[k][m] = {T(0), T(0)};
 
-    for (int s0 = 0; s0 < S; s0 += kChunk) {
-        const int sc = min(kChunk, S - s0);
-        for (int i = threadIdx.x; i < kChunk * RP; i += kThreads) {
-            const int s = i / RP, r = i % RP;
-            sA[s][r] = (s < sc && r < R) ? __ldg(A + (long long)(s0 + s) * R + r) : T(0);
-        }
-        for (int i = threadIdx.x; i < kTileCols * kChunk; i += kThreads) {
-            const int c = i / kChunk, s = i % kChunk;
-            V v = {T(0), T(0)};
-            if (c < ncols && s < sc) v = load_operand<T, SPLIT>(in, (long long)(c0 + c) * S + s0 + s);
-            sX[c][s] = v;
+    issue(0, 0);
+    for (int c = 0; c < chunks; ++c) {
+        if (c + 1 < chunks) {
+            issue(c + 1, (c + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
+        T(*sA)[RP] = stageA(c & 1);
+        V(*sX)[kChunk + 1] = stageX(c & 1);
+        const int sc = min(kChunk, S - c * kChunk);
 #pragma unroll 4
         for (int s = 0; s < sc; ++s) {
             T a[KR];
@@ -105,7 +149,7 @@ cudaError_t launch_kr(int R, int S, const void* At, const GroupTiles& tiles, Com
                       cudaStream_t stream) {
     const bool split = in.im != nullptr;
     if (split != (out.im != nullptr)) return cudaErrorInvalidValue;
-    const size_t bytes = sizeof(cx<T>) * kTileCols * (kChunk + 1) + sizeof(T) * kChunk * 32 * KR;
+    const size_t bytes = 2 * (sizeof(cx<T>) * kTileCols * (kChunk + 1) + sizeof(T) * kChunk * 32 * KR);
     auto kernel = split ? grouped_gemm_kernel<T, KR, true> : grouped_gemm_kernel<T, KR, false>;
     if (bytes > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
