@@ -44,9 +44,12 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
     using V = float2;
     constexpr int NT = RowFluxShape<M, B>::threads;
     constexpr int PER = RowFluxShape<M, B>::per;
+    // Shared rows padded to B+1: with 64-byte rows the radix-8 passes' strided
+    // stores would otherwise alias onto half the banks.
+    constexpr int LD = B + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* data = reinterpret_cast<V*>(smem_raw);
-    V* stage0 = data + M * B;
+    V* stage0 = data + M * LD;
     V* stage1 = stage0 + a.keep * B;
     const int tid = threadIdx.x;
     const int zChunks = (a.nz + B - 1) / B;
@@ -60,6 +63,9 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
     const long long inRow = a.binsIn.planes;  // stride between kx
     const long long outRow = a.binsOut.planes;
     const int keep = a.keep;
+
+    // Shared position of the e-th element a thread owns: (n, b) at n*LD + b.
+    auto pos = [](int idx) { return (idx / B) * LD + idx % B; };
 
     // Asynchronous copy of slot f's bins of this row (kx < keep, B planes) into
     // a stage buffer [k][b]; planes beyond Nz are zero-filled.
@@ -109,19 +115,19 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
                 const V s = cadd(xk, cconj(xm));
                 const V d = csub(xk, cconj(xm));
                 const V t = cmulc(d, __ldg(twFull + k));
-                data[k * B + b] = {s.x - t.y, s.y + t.x};
+                data[k * LD + b] = {s.x - t.y, s.y + t.x};
             }
             if (kk != k) {
                 const V s = cadd(xm, cconj(xk));
                 const V d = csub(xm, cconj(xk));
                 const V t = cmulc(d, __ldg(twFull + kk));
-                data[kk * B + b] = {s.x - t.y, s.y + t.x};
+                data[kk * LD + b] = {s.x - t.y, s.y + t.x};
             }
         }
         __syncthreads();
-        fft_smem<float, M, B, +1>(data, twHalf, tid, true);
+        fft_smem<float, M, B, +1, LD>(data, twHalf, tid, true);
 #pragma unroll
-        for (int e = 0; e < PER; ++e) r[e] = data[tid + e * NT];
+        for (int e = 0; e < PER; ++e) r[e] = data[pos(tid + e * NT)];
         __syncthreads();
     };
 
@@ -143,10 +149,10 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
 #pragma unroll
         for (int e = 0; e < PER; ++e) {
             acc[e] = {acc[e].x + w[e].x * q[e].x, acc[e].y + w[e].y * q[e].y};
-            data[tid + e * NT] = {-scale * acc[e].x, -scale * acc[e].y};
+            data[pos(tid + e * NT)] = {-scale * acc[e].x, -scale * acc[e].y};
         }
         __syncthreads();
-        fft_smem<float, M, B, -1>(data, twHalf, tid, true);
+        fft_smem<float, M, B, -1, LD>(data, twHalf, tid, true);
         // Real-spectrum split of the half-length FFT, kx < keep.
         const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.nz + z0;
         for (int idx = tid; idx < keep * B; idx += NT) {
@@ -160,8 +166,8 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
             } else if (k == M) {
                 X = {zz.x - zz.y, 0.f};
             } else {
-                const V zk = data[k * B + b];
-                const V zm = cconj(data[(M - k) * B + b]);
+                const V zk = data[k * LD + b];
+                const V zm = cconj(data[(M - k) * LD + b]);
                 const V ev = cscale(cadd(zk, zm), 0.5f);
                 const V d = csub(zk, zm);
                 const V o = {0.5f * d.y, -0.5f * d.x};
@@ -179,7 +185,7 @@ template <int M>
 cudaError_t launch_m(const RowFluxArgs& a, dim3 grid, cudaStream_t stream) {
     constexpr int B = 8;
     auto kernel = rows_flux_kernel<M, B>;
-    const size_t bytes = sizeof(float2) * (size_t(M) * B + 2 * size_t(a.keep) * B);
+    const size_t bytes = sizeof(float2) * (size_t(M) * (B + 1) + 2 * size_t(a.keep) * B);
     if (bytes > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (err != cudaSuccess) return err;

@@ -14,10 +14,11 @@
 // accumulator per 32-wide K chunk, chunk sums added in FP32 registers.  The
 // dropped lo*lo term is ~2^-22 relative.
 //
-// CTA work unit: one group and a run of up to kUnitTiles M-tiles of its
-// (member, column) list.  The group matrix is split and written once into
-// shared memory (all K chunks) and stays resident; data chunks of 32 k
-// stream through a two-stage buffer.  Operands use the canonical K-major
+// CTA work unit: one group and a run of up to 16 M-tiles of its (member,
+// column) list.  The group matrix is split and written once into shared
+// memory (all K chunks) and stays resident; data chunks of 32 k stream
+// through a three-stage ring filled by producer warps while one MMA lane and
+// the epilogue warps work on earlier chunks (warp specialisation below).  Operands use the canonical K-major
 // SWIZZLE_128B layout: 8-row atoms of 8 x 128 bytes, 16-byte chunk q of row
 // n stored at chunk (q xor n%8).  One elected thread issues the MMAs and
 // commits them to the stage's mbarrier; every wait is bounded and reports
@@ -32,8 +33,7 @@ namespace {
 
 constexpr int kTileRows = 128;    // M
 constexpr int kChunkK = 32;       // tf32 elements per 128-byte row
-constexpr int kThreads = 256;
-constexpr int kTmemCols = 512;  // one FP32 accumulator of NP columns per K chunk
+constexpr int kTmemCols = 512;  // two chunk accumulators + the running sum, NP columns each
 constexpr int kStageBytes = 2 * kTileRows * 128;  // hi + lo
 constexpr long long kWaitLimit = 1LL << 22;
 
@@ -107,6 +107,13 @@ __device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, uint32_t (&v)[8]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+__device__ __forceinline__ void tmem_st_x8(uint32_t taddr, const uint32_t (&v)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ float tf32_rna(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -137,18 +144,51 @@ __device__ __forceinline__ Split4 split4(float a, float b, float c, float d) {
     return s;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) tc_gemm_tf32x3_kernel(TcGemmArgs p) {
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Warp roles of the pipelined kernel.
+constexpr int kProducerWarps = 8;
+constexpr int kMmaWarp = kProducerWarps;
+constexpr int kEpilogueWarps = 8;
+constexpr int kPipeThreads = (kProducerWarps + 1 + kEpilogueWarps) * 32;
+constexpr int kStages = 3;
+constexpr int kAccumulators = 2;
+
+struct PipeState {
+    uint64_t full[kStages], empty[kStages], accFull[kAccumulators], accEmpty[kAccumulators], done;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ long long virtual_column(const TcGemmArgs& p, int vc, int gcols, long long gfirst) {
+    const int member = vc / gcols;
+    return static_cast<long long>(member) * p.memberColumns + gfirst + (vc - member * gcols);
+}
+
+// Warp-specialised split-TF32x3 grouped GEMM.
+//   producer warps 0-7: data chunk (64 columns x 32 k) -> registers -> TF32
+//       hi/lo -> swizzled A stage of a 3-deep ring; arrive full[stage].
+//   MMA warp 8 (one lane): per chunk, 3 MMAs per k-step into one of two
+//       ping-pong TMEM chunk accumulators; commit empty[stage] and accFull.
+//   epilogue warps 9-16: add each chunk accumulator into an FP32 running sum
+//       kept in TMEM (tcgen05.ld / tcgen05.st), release it (accEmpty), and
+//       after the tile's last chunk write the tile's outputs.
+// NPH = NP/16: x8 column blocks per epilogue half.
+template <int NPH>
+__global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArgs p) {
+    constexpr int NP = NPH * 16;
+    constexpr int HALF = NP / 2;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int NP = p.NP, KCH = p.KCH, R = p.R, S = p.S;
+    const int KCH = p.KCH, R = p.R, S = p.S;
     unsigned char* sBhi = base;
     unsigned char* sBlo = sBhi + KCH * NP * 128;
     unsigned char* sA = sBlo + KCH * NP * 128;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sA + 2 * kStageBytes);
-    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(bars + 2);
+    PipeState* st = reinterpret_cast<PipeState*>(sA + kStages * kStageBytes);
 
     const int unit = blockIdx.x;
     const int g = __ldg(p.unitGroup + unit);
@@ -156,21 +196,27 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_tf32x3_kernel(TcGemmArgs 
     const int vcN = __ldg(p.unitCount + unit);
     const int gcols = __ldg(p.groupColumns + g);
     const long long gfirst = __ldg(p.groupFirst + g);
+    const int tiles = (vcN + 63) / 64;
 
-    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
     if (tid == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar1, 1);
+        for (int i = 0; i < kStages; ++i) {
+            mbar_init(smem_u32(&st->full[i]), kProducerWarps * 32);
+            mbar_init(smem_u32(&st->empty[i]), 1);
+        }
+        for (int i = 0; i < kAccumulators; ++i) {
+            mbar_init(smem_u32(&st->accFull[i]), 1);
+            mbar_init(smem_u32(&st->accEmpty[i]), kEpilogueWarps * 32);
+        }
+        mbar_init(smem_u32(&st->done), 1);
         fence_barrier_init();
     }
-    if (warp == 0) {
-        tmem_alloc(smem_u32(tmemSlot), kTmemCols);
+    if (warp == kMmaWarp) {
+        tmem_alloc(smem_u32(&st->tmem), kTmemCols);
         tmem_relinquish();
     }
-
     // Resident group matrix, split hi/lo, zero-padded to NP x KCH*32.
     const float* Bg = p.B + static_cast<long long>(g) * R * S;
-    for (int item = tid; item < NP * KCH * 8; item += kThreads) {
+    for (int item = tid; item < NP * KCH * 8; item += kPipeThreads) {
         const int q = item & 7;
         const int rest = item >> 3;
         const int kc = rest % KCH;
@@ -186,144 +232,156 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_tf32x3_kernel(TcGemmArgs 
         *reinterpret_cast<float4*>(sBhi + off) = sp.hi;
         *reinterpret_cast<float4*>(sBlo + off) = sp.lo;
     }
+    fence_proxy_async();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tmemSlot;
+    const uint32_t tmem = st->tmem;
+    bool failed = false;
 
-    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(NP >> 3) << 17) |
-                           (static_cast<uint32_t>(kTileRows >> 4) << 24);
-    int commits0 = 0, commits1 = 0, waits0 = 0, waits1 = 0;
-    bool aborted = false;
-    auto drain = [&](int stage) -> bool {
-        // Wait until every commit on this stage's barrier has completed.
-        int& w = stage ? waits1 : waits0;
-        const int c = stage ? commits1 : commits0;
-        bool ok = true;
-        while (w < c && ok) {
-            ok = mbar_wait(stage ? bar1 : bar0, static_cast<uint32_t>(w & 1), p.error);
-            ++w;
-        }
-        return ok;
-    };
-
-    const int tiles = (vcN + 63) / 64;
-    int it = 0;
-    for (int t = 0; t < tiles && !aborted; ++t) {
-        const int tv0 = vc0 + t * 64;
-        const int tcount = min(64, vc0 + vcN - tv0);
-        for (int kc = 0; kc < KCH && !aborted; ++kc, ++it) {
-            const int st = it & 1;
-            if (__syncthreads_or(!drain(st))) {
-                aborted = true;
-                break;
-            }
-            unsigned char* aHi = sA + st * kStageBytes;
-            unsigned char* aLo = aHi + kTileRows * 128;
-            for (int item = tid; item < 64 * 8; item += kThreads) {
-                const int q = item & 7;
-                const int cl = item >> 3;
-                float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
-                if (cl < tcount) {
-                    const int vc = tv0 + cl;
-                    const int member = vc / gcols;
-                    const long long C = static_cast<long long>(member) * p.memberColumns + gfirst + (vc - member * gcols);
-                    const float2* src = p.in + C * S;
+    if (warp < kProducerWarps) {
+        // ---------------------------------------------------------- producer
+        int it = 0;
+        for (int t = 0; t < tiles && !failed; ++t) {
+            const int tv0 = vc0 + t * 64;
+            const int tcount = min(64, vc0 + vcN - tv0);
+            for (int kc = 0; kc < KCH; ++kc, ++it) {
+                const int stage = it % kStages;
+                const int round = it / kStages;
+                if (round > 0 && !mbar_wait(smem_u32(&st->empty[stage]), (round - 1) & 1, p.error)) {
+                    failed = true;
+                    break;
+                }
+                unsigned char* aHi = sA + stage * kStageBytes;
+                unsigned char* aLo = aHi + kTileRows * 128;
+                for (int item = tid; item < 64 * 8; item += kProducerWarps * 32) {
+                    const int q = item & 7;
+                    const int cl = item >> 3;
+                    float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
+                    if (cl < tcount) {
+                        const float2* src = p.in + virtual_column(p, tv0 + cl, gcols, gfirst) * S;
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int s = kc * kChunkK + q * 4 + j;
-                        if (s < S) {
-                            const float2 x = __ldg(src + s);
-                            re[j] = x.x;
-                            im[j] = x.y;
+                        for (int j = 0; j < 4; ++j) {
+                            const int s = kc * kChunkK + q * 4 + j;
+                            if (s < S) {
+                                const float2 x = __ldg(src + s);
+                                re[j] = x.x;
+                                im[j] = x.y;
+                            }
                         }
                     }
+                    const Split4 r4 = split4(re[0], re[1], re[2], re[3]);
+                    const Split4 i4 = split4(im[0], im[1], im[2], im[3]);
+                    const uint32_t o0 = sw128_offset(2 * cl, q), o1 = sw128_offset(2 * cl + 1, q);
+                    *reinterpret_cast<float4*>(aHi + o0) = r4.hi;
+                    *reinterpret_cast<float4*>(aLo + o0) = r4.lo;
+                    *reinterpret_cast<float4*>(aHi + o1) = i4.hi;
+                    *reinterpret_cast<float4*>(aLo + o1) = i4.lo;
                 }
-                const Split4 r4 = split4(re[0], re[1], re[2], re[3]);
-                const Split4 i4 = split4(im[0], im[1], im[2], im[3]);
-                const uint32_t o0 = sw128_offset(2 * cl, q), o1 = sw128_offset(2 * cl + 1, q);
-                *reinterpret_cast<float4*>(aHi + o0) = r4.hi;
-                *reinterpret_cast<float4*>(aLo + o0) = r4.lo;
-                *reinterpret_cast<float4*>(aHi + o1) = i4.hi;
-                *reinterpret_cast<float4*>(aLo + o1) = i4.lo;
+                fence_proxy_async();
+                mbar_arrive(smem_u32(&st->full[stage]));
             }
-            fence_proxy_async();
-            __syncthreads();
-            if (tid == 0) {
-                tc_fence_after();
-                const uint32_t aH = smem_u32(aHi), aL = smem_u32(aLo);
-                const uint32_t bH = smem_u32(sBhi + kc * NP * 128), bL = smem_u32(sBlo + kc * NP * 128);
-                const int ksteps = min(4, (S - kc * kChunkK + 7) / 8);
-                // Each K chunk accumulates into its own TMEM columns; the chunk
-                // partial sums are added in FP32 registers in the epilogue,
-                // which keeps the in-MMA accumulation depth at 12 terms.
-                const uint32_t dChunk = tmem + static_cast<uint32_t>(kc * NP);
-                for (int j = 0; j < ksteps; ++j) {
-                    const uint32_t off = j * 32;
-                    const uint32_t acc = j > 0 ? 1u : 0u;
-                    mma_tf32(dChunk, sw128_desc(aH + off), sw128_desc(bL + off), idesc, acc);
-                    mma_tf32(dChunk, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
-                    mma_tf32(dChunk, sw128_desc(aH + off), sw128_desc(bH + off), idesc, 1u);
+        }
+    } else if (warp == kMmaWarp) {
+        // --------------------------------------------------------------- MMA
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(NP >> 3) << 17) |
+                                   (static_cast<uint32_t>(kTileRows >> 4) << 24);
+            int it = 0;
+            for (int t = 0; t < tiles && !failed; ++t) {
+                for (int kc = 0; kc < KCH; ++kc, ++it) {
+                    const int stage = it % kStages;
+                    const int acc = it % kAccumulators;
+                    const int accRound = it / kAccumulators;
+                    if (!mbar_wait(smem_u32(&st->full[stage]), (it / kStages) & 1, p.error) ||
+                        (accRound > 0 &&
+                         !mbar_wait(smem_u32(&st->accEmpty[acc]), (accRound - 1) & 1, p.error))) {
+                        failed = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t aH = smem_u32(sA + stage * kStageBytes);
+                    const uint32_t aL = aH + kTileRows * 128;
+                    const uint32_t bH = smem_u32(sBhi + kc * NP * 128), bL = smem_u32(sBlo + kc * NP * 128);
+                    const uint32_t d = tmem + static_cast<uint32_t>(acc * NP);
+                    const int ksteps = min(4, (S - kc * kChunkK + 7) / 8);
+                    for (int j = 0; j < ksteps; ++j) {
+                        const uint32_t off = j * 32;
+                        mma_tf32(d, sw128_desc(aH + off), sw128_desc(bL + off), idesc, j > 0 ? 1u : 0u);
+                        mma_tf32(d, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
+                        mma_tf32(d, sw128_desc(aH + off), sw128_desc(bH + off), idesc, 1u);
+                    }
+                    mma_commit(smem_u32(&st->empty[stage]));
+                    mma_commit(smem_u32(&st->accFull[acc]));
                 }
-                mma_commit(st ? bar1 : bar0);
             }
-            if (st)
-                ++commits1;
-            else
-                ++commits0;
+            // Every issued MMA has completed once this commit lands.
+            mma_commit(smem_u32(&st->done));
+            if (!mbar_wait(smem_u32(&st->done), 0, p.error)) failed = true;
         }
-        if (aborted) break;
-        // The last commit covers every MMA of this tile.
-        const int last = (it - 1) & 1;
-        if (__syncthreads_or(!drain(last))) {
-            aborted = true;
-            break;
-        }
-        tc_fence_after();
-        const int quarter = warp & 3;
-        const int half = warp >> 2;
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------------- epilogue
+        // Running chunk sums live in a third TMEM region (columns 2*NP ..),
+        // read-added-stored eight columns at a time, so only 16 values are
+        // live per thread.  The final chunk's sum goes straight to global.
+        const int quarter = warp & 3;  // TMEM lanes this warp may access
+        const int half = (warp - kMmaWarp - 1) >> 2;
         const int m = quarter * 32 + lane;
         const int cl = m >> 1;
         const int part = m & 1;
-        const bool valid = cl < tcount;
-        long long C = 0;
-        if (valid) {
-            const int vc = tv0 + cl;
-            const int member = vc / gcols;
-            C = static_cast<long long>(member) * p.memberColumns + gfirst + (vc - member * gcols);
-        }
-        const int nHalf = NP / 2;
-        for (int col = half * nHalf; col < (half + 1) * nHalf; col += 8) {
-            float sum[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            for (int kc = 0; kc < KCH; ++kc) {
-                uint32_t v[8];
-                tmem_ld_x8(tmem + (static_cast<uint32_t>(quarter * 32) << 16) +
-                               static_cast<uint32_t>(kc * NP + col),
-                           v);
-                tmem_wait_ld();
+        const uint32_t laneBase = static_cast<uint32_t>(quarter * 32) << 16;
+        const uint32_t sumBase = tmem + laneBase + static_cast<uint32_t>(kAccumulators * NP + half * HALF);
+        int it = 0;
+        for (int t = 0; t < tiles && !failed; ++t) {
+            const int tv0 = vc0 + t * 64;
+            const int tcount = min(64, vc0 + vcN - tv0);
+            const bool valid = cl < tcount;
+            const long long C = valid ? virtual_column(p, tv0 + cl, gcols, gfirst) : 0;
+            for (int kc = 0; kc < KCH; ++kc, ++it) {
+                const int acc = it % kAccumulators;
+                if (!mbar_wait(smem_u32(&st->accFull[acc]), (it / kAccumulators) & 1, p.error)) {
+                    failed = true;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t accBase = tmem + laneBase + static_cast<uint32_t>(acc * NP + half * HALF);
+                const bool first = kc == 0, last = kc == KCH - 1;
+#pragma unroll 1
+                for (int blk = 0; blk < HALF / 8; ++blk) {
+                    uint32_t a[8], b[8];
+                    tmem_ld_x8(accBase + blk * 8, a);
+                    if (!first) tmem_ld_x8(sumBase + blk * 8, b);
+                    tmem_wait_ld();
+                    float x8[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) sum[j] += __uint_as_float(v[j]);
-            }
+                    for (int j = 0; j < 8; ++j)
+                        x8[j] = first ? __uint_as_float(a[j]) : __uint_as_float(b[j]) + __uint_as_float(a[j]);
+                    if (!last) {
+                        uint32_t o[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const float x = sum[j];
-                const float y = __shfl_xor_sync(0xffffffffu, x, 1);
-                const int n = col + j;
-                if ((j & 1) == part && valid && n < R)
-                    p.out[C * R + n] = part == 0 ? make_float2(x, y) : make_float2(y, x);
+                        for (int j = 0; j < 8; ++j) o[j] = __float_as_uint(x8[j]);
+                        tmem_st_x8(sumBase + blk * 8, o);
+                        tmem_wait_st();
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const float y = __shfl_xor_sync(0xffffffffu, x8[j], 1);
+                            const int n = half * HALF + blk * 8 + j;
+                            if ((j & 1) == part && valid && n < R)
+                                p.out[C * R + n] = part == 0 ? make_float2(x8[j], y) : make_float2(y, x8[j]);
+                        }
+                    }
+                }
+                tc_fence_before();
+                mbar_arrive(smem_u32(&st->accEmpty[acc]));
             }
         }
-        tc_fence_before();
-        __syncthreads();
     }
-    if (aborted) {
-        // Give outstanding MMAs a bounded chance to finish before freeing TMEM.
-        drain(0);
-        drain(1);
-        if (tid == 0) atomicExch(p.error, 1);
-    }
+    if (failed) atomicExch(p.error, 1);
+    tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+    if (warp == kMmaWarp) tmem_dealloc(tmem, kTmemCols);
 }
 
 }  // namespace
@@ -331,26 +389,44 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_tf32x3_kernel(TcGemmArgs 
 size_t tc_gemm_smem_bytes(int R, int S) {
     const int NP = (R + 15) / 16 * 16;
     const int KCH = (S + kChunkK - 1) / kChunkK;
-    return 1024 + 2 * static_cast<size_t>(KCH) * NP * 128 + 2 * kStageBytes + 64;
+    return 1024 + 2 * static_cast<size_t>(KCH) * NP * 128 + kStages * kStageBytes + sizeof(PipeState) + 16;
 }
 
 bool tc_gemm_supported(int R, int S) {
     const int NP = (R + 15) / 16 * 16;
-    const int KCH = (S + kChunkK - 1) / kChunkK;
-    return NP <= 256 && KCH * NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
+    return NP >= 16 && (kAccumulators + 1) * NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
 }
 
 int tc_gemm_unit_tiles() { return 16; }
 
+namespace {
+template <int NPH>
+cudaError_t launch_np(const TcGemmArgs& args, cudaStream_t stream) {
+    const size_t bytes = tc_gemm_smem_bytes(args.R, args.S);
+    auto kernel = tc_gemm_pipe_kernel<NPH>;
+    const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (err != cudaSuccess) return err;
+    kernel<<<args.units, kPipeThreads, bytes, stream>>>(args);
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream) {
     if (args.units <= 0) return cudaSuccess;
-    if (!tc_gemm_supported(args.R, args.S)) return cudaErrorInvalidValue;
-    const size_t bytes = tc_gemm_smem_bytes(args.R, args.S);
-    cudaError_t err =
-        cudaFuncSetAttribute(tc_gemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-    if (err != cudaSuccess) return err;
-    tc_gemm_tf32x3_kernel<<<args.units, kThreads, bytes, stream>>>(args);
-    return cudaGetLastError();
+    if (!tc_gemm_supported(args.R, args.S) || args.NP != (args.R + 15) / 16 * 16) return cudaErrorInvalidValue;
+    switch (args.NP / 16) {
+        case 1: return launch_np<1>(args, stream);
+        case 2: return launch_np<2>(args, stream);
+        case 3: return launch_np<3>(args, stream);
+        case 4: return launch_np<4>(args, stream);
+        case 5: return launch_np<5>(args, stream);
+        case 6: return launch_np<6>(args, stream);
+        case 7: return launch_np<7>(args, stream);
+        case 8: return launch_np<8>(args, stream);
+        case 9: return launch_np<9>(args, stream);
+        case 10: return launch_np<10>(args, stream);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace skb
