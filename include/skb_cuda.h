@@ -298,6 +298,9 @@ SKB_API int skb_flux_sizes(const skb_flux* p, uint64_t* modes, uint64_t* nj, uin
                    uint64_t* output_elements);
 /* Host arrays (double complex), blocking. */
 SKB_API int skb_flux_execute(skb_flux* p, const skb_complex* modal_input, skb_complex* modal_output);
+/* Device arrays, the first `members` (1..capacity) ensemble members only. */
+SKB_API int skb_flux_execute_device_members(skb_flux* p, const void* modal_input, void* modal_output,
+                                            uint64_t members, void* stream);
 /* Device arrays: FP64 complex for SKB_FLUX_FP64_PLAIN, FP32 complex otherwise. */
 SKB_API int skb_flux_execute_device(skb_flux* p, const void* modal_input, void* modal_output, void* stream);
 /* One execute_device with CUDA events between stages: per stage the device
@@ -319,6 +322,41 @@ SKB_API int skb_flux_check_device(skb_flux* p);
 /* Capture execute_device on these buffers into a CUDA graph and replay it. */
 SKB_API int skb_flux_capture_graph(skb_flux* p, const void* modal_input, void* modal_output);
 SKB_API int skb_flux_replay_graph(skb_flux* p, void* stream);
+
+/* ------------------------------------------------------ serving loop */
+/* A continuous-batching request loop over flux size classes (no counterpart
+ * in the reference, which has no serving path).  Each class gets one or more
+ * slots — a flux pipeline for `max_batch` members on its own stream — while
+ * they fit `hbm_budget_bytes`; queued requests of a class join the next free
+ * slot's batch, and slots of all classes run concurrently.  Inputs are host
+ * FP64 complex arrays of one member ([mode][field][j]) or resident states
+ * loaded once; results are written to the caller's host array (pinned memory
+ * keeps the copy asynchronous).  A member's result does not depend on the
+ * other requests in its batch. */
+typedef struct skb_server_class {
+    uint64_t n, nz, targets, max_batch;
+    int32_t mode; /* SKB_FLUX_* */
+} skb_server_class;
+
+typedef struct skb_server_stats {
+    uint64_t submitted, completed, batches, slots, resident_states;
+    uint64_t slot_bytes, state_bytes, budget_bytes;
+} skb_server_stats;
+
+typedef struct skb_server skb_server;
+SKB_API int skb_server_create(const skb_server_class* classes, uint64_t class_count, uint64_t hbm_budget_bytes,
+                              int max_slots_per_class, skb_server** out);
+SKB_API int skb_server_destroy(skb_server* s);
+SKB_API int skb_server_sizes(skb_server* s, int size_class, uint64_t* input_elements, uint64_t* output_elements);
+SKB_API int skb_server_submit(skb_server* s, int size_class, const skb_complex* input, skb_complex* output,
+                              uint64_t* ticket);
+/* Admission by HBM footprint: SKB_ERR_OUT_OF_MEMORY when the state does not fit. */
+SKB_API int skb_server_load_state(skb_server* s, int size_class, const skb_complex* input, int64_t* state);
+SKB_API int skb_server_release_state(skb_server* s, int64_t state);
+SKB_API int skb_server_submit_state(skb_server* s, int64_t state, skb_complex* output, uint64_t* ticket);
+/* *done = 1 when finished within timeout_seconds; latency = submit -> result in host memory. */
+SKB_API int skb_server_wait(skb_server* s, uint64_t ticket, double timeout_seconds, int* done, double* latency_ms);
+SKB_API int skb_server_get_stats(skb_server* s, skb_server_stats* stats);
 
 /* --------------------------------------------------------------- timing */
 /* Events on a handle's stream, for benchmark harnesses. */

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "flux.hpp"
+#include "server.hpp"
 #include "pointwise.hpp"
 #include "runtime.hpp"
 #include "util.hpp"
@@ -1125,6 +1126,14 @@ int skb_flux_execute_device(skb_flux* p, const void* in, void* out, void* stream
     });
 }
 
+int skb_flux_execute_device_members(skb_flux* p, const void* in, void* out, uint64_t members, void* stream) {
+    return guard([&] {
+        require(p && in && out, "handle and buffers must be non-null");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+        p->pipeline->execute(in, out, s, members);
+    });
+}
+
 int skb_flux_execute(skb_flux* p, const skb_complex* in, skb_complex* out) {
     return guard([&] {
         require(p && in && out, "handle and buffers must be non-null");
@@ -1182,6 +1191,81 @@ int skb_flux_replay_graph(skb_flux* p, void* stream) {
     return guard([&] {
         require(p != nullptr, "handle must be non-null");
         p->pipeline->replay(stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    });
+}
+
+// ----------------------------------------------------------------- server
+
+int skb_server_create(const skb_server_class* classes, uint64_t count, uint64_t budget, int maxSlots,
+                      skb_server** out) {
+    return guard([&] {
+        require(classes != nullptr && count > 0 && out != nullptr, "classes and output handle must be non-null");
+        std::vector<ServerClass> cs;
+        for (uint64_t i = 0; i < count; ++i) {
+            require(classes[i].mode >= SKB_FLUX_FP64_PLAIN && classes[i].mode <= SKB_FLUX_SPLIT_BF16X3,
+                    "unknown flux mode");
+            cs.push_back({classes[i].n, classes[i].nz, classes[i].targets, classes[i].max_batch,
+                          static_cast<FluxMode>(classes[i].mode)});
+        }
+        *out = reinterpret_cast<skb_server*>(new Server(cs, budget, maxSlots));
+    });
+}
+
+int skb_server_destroy(skb_server* s) {
+    return guard([&] { delete reinterpret_cast<Server*>(s); });
+}
+
+int skb_server_sizes(skb_server* s, int cls, uint64_t* in, uint64_t* out) {
+    return guard([&] {
+        require(s != nullptr, "handle must be non-null");
+        auto* srv = reinterpret_cast<Server*>(s);
+        if (in) *in = srv->inputElements(cls);
+        if (out) *out = srv->outputElements(cls);
+    });
+}
+
+int skb_server_submit(skb_server* s, int cls, const skb_complex* in, skb_complex* out, uint64_t* ticket) {
+    return guard([&] {
+        require(s != nullptr && ticket != nullptr, "handle and ticket must be non-null");
+        *ticket = reinterpret_cast<Server*>(s)->submit(cls, reinterpret_cast<const double*>(in),
+                                                       reinterpret_cast<double*>(out));
+    });
+}
+
+int skb_server_load_state(skb_server* s, int cls, const skb_complex* in, int64_t* state) {
+    return guard([&] {
+        require(s != nullptr && state != nullptr, "handle and state must be non-null");
+        *state = reinterpret_cast<Server*>(s)->loadState(cls, reinterpret_cast<const double*>(in));
+    });
+}
+
+int skb_server_release_state(skb_server* s, int64_t state) {
+    return guard([&] {
+        require(s != nullptr, "handle must be non-null");
+        reinterpret_cast<Server*>(s)->releaseState(state);
+    });
+}
+
+int skb_server_submit_state(skb_server* s, int64_t state, skb_complex* out, uint64_t* ticket) {
+    return guard([&] {
+        require(s != nullptr && ticket != nullptr, "handle and ticket must be non-null");
+        *ticket = reinterpret_cast<Server*>(s)->submitState(state, reinterpret_cast<double*>(out));
+    });
+}
+
+int skb_server_wait(skb_server* s, uint64_t ticket, double timeout, int* done, double* latency) {
+    return guard([&] {
+        require(s != nullptr && done != nullptr, "handle and done flag must be non-null");
+        *done = reinterpret_cast<Server*>(s)->wait(ticket, timeout, latency) ? 1 : 0;
+    });
+}
+
+int skb_server_get_stats(skb_server* s, skb_server_stats* st) {
+    return guard([&] {
+        require(s != nullptr && st != nullptr, "handle and stats must be non-null");
+        const auto x = reinterpret_cast<Server*>(s)->stats();
+        *st = {x.submitted, x.completed, x.batches, x.slots, x.residentStates, x.slotBytes, x.stateBytes,
+               x.budgetBytes};
     });
 }
 

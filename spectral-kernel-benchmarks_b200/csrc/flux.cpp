@@ -117,16 +117,25 @@ struct FluxPipeline::Recorder {
     }
 };
 
-void FluxPipeline::execute(const void* modalIn, void* modalOut, cudaStream_t s) { run(modalIn, modalOut, s, nullptr); }
+void FluxPipeline::execute(const void* modalIn, void* modalOut, cudaStream_t s) {
+    run(modalIn, modalOut, s, nullptr, cfg_.members);
+}
+
+void FluxPipeline::execute(const void* modalIn, void* modalOut, cudaStream_t s, std::uint64_t members) {
+    if (members == 0 || members > cfg_.members)
+        throw Error(-1, "active members must be between 1 and the handle's capacity");
+    run(modalIn, modalOut, s, nullptr, members);
+}
 
 std::vector<FluxPipeline::StageTime> FluxPipeline::profile(const void* modalIn, void* modalOut, cudaStream_t s) {
     Recorder rec(s);
-    run(modalIn, modalOut, s, &rec);
+    run(modalIn, modalOut, s, &rec, cfg_.members);
     return rec.finish();
 }
 
-void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec) {
-    const auto H = modes_, nz = cfg_.nz, T = cfg_.targets, M = cfg_.members;
+void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec,
+                            std::uint64_t members) {
+    const auto H = modes_, nz = cfg_.nz, T = cfg_.targets, M = members;
     const size_t ces = 2 * sizeof(float);
     const double n = static_cast<double>(cfg_.n);
     const long long keep = horizontal_->keep();
@@ -138,7 +147,7 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
     const long long inPlanes = static_cast<long long>(M * fieldsIn_ * nz);
     const long long outPlanes = static_cast<long long>(M * T * nz);
 
-    inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s);
+    inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s, M);
     if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
 
     ViewSet inViews{};
@@ -175,16 +184,16 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
     horizontal_->forward_columns_from(a.binsOut, outViews, 1.0, s);
     if (rec) rec->end("columns_forward_gather", 1, double(outPlanes) * (binsPlane + compactPlane), 0.0);
 
-    forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s);
+    forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s, M);
     if (rec) rec->end("gemm_forward_tf32x3", 1, gemmOut, 3.0 * 4.0 * nz * nj_ * double(M) * H * T);
 }
 
-void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec) {
+void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members) {
     if (fused_) {
-        runFused(modalIn, modalOut, s, rec);
+        runFused(modalIn, modalOut, s, rec, members);
         return;
     }
-    const auto H = modes_, nz = cfg_.nz, T = cfg_.targets, M = cfg_.members;
+    const auto H = modes_, nz = cfg_.nz, T = cfg_.targets, M = members;
     const size_t es = element_bytes(horizontal_->precision());
     const size_t ces = 2 * es;  // complex element bytes
     const double n = static_cast<double>(cfg_.n);
@@ -196,7 +205,7 @@ void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Reco
     const double gemmIn = double(M) * H * fieldsIn_ * (nj_ + nz) * ces + inverseGemm_->matrixBytes();
     const double gemmOut = double(M) * H * T * (nj_ + nz) * ces + forwardGemm_->matrixBytes();
 
-    inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s);
+    inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s, M);
     if (rec) rec->end("gemm_inverse", 1, gemmIn, 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
 
     auto triple = [&](std::uint64_t firstField) {
@@ -238,7 +247,7 @@ void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Reco
         horizontal_->forward_columns(out, 1.0, s);
         if (rec) rec->end("columns_forward_gather", 1, double(M) * nz * (binsPlane + compactPlane), 0.0);
     }
-    forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s);
+    forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s, M);
     if (rec) rec->end("gemm_forward", 1, gemmOut, 4.0 * nz * nj_ * double(M) * H * T);
 }
 

@@ -39,6 +39,8 @@ public:
     // float otherwise): modal input [member][mode][3+3T][j], output
     // [member][mode][T][j].
     void execute(const void* modalIn, void* modalOut, cudaStream_t s);
+    // The first `members` (<= capacity) ensemble members only, for partial batches.
+    void execute(const void* modalIn, void* modalOut, cudaStream_t s, std::uint64_t members);
 
     // One evaluation with CUDA events between stages; per stage the summed
     // device milliseconds, launches and algorithmic bytes / flops.
@@ -80,8 +82,8 @@ private:
     DeviceBuffer binsIn_, binsOut_;
     std::uint64_t launches_ = 0;
     struct Recorder;
-    void runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec);
-    void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec);
+    void runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
+    void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graphExec_ = nullptr;
 };

@@ -214,6 +214,7 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
     const std::uint64_t perMember = expected * fields;
     if (members * perMember > static_cast<std::uint64_t>(INT32_MAX)) throw Error(-1, "too many GEMM columns");
     columns_ = members * perMember;
+    members_ = members;
     memberColumns_ = static_cast<long long>(perMember);
     const std::uint64_t groupsCount = common ? 1 : groups.size();
 
@@ -235,27 +236,34 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
             gf[gi] = static_cast<int>(groups[gi].first * fields);
         }
         // Units: runs of up to unit_tiles * 64 virtual (member, column) pairs of
-        // one group, largest first so the long units start early.
+        // one group, largest first so the long units start early.  One table
+        // per active member count so partial batches launch only their units.
         struct Unit {
             int g, col, count;
         };
-        std::vector<Unit> units;
         const int span = tc_gemm_unit_tiles() * 64;
-        for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
-            const int total = static_cast<int>(members) * gc[gi];
-            for (int c = 0; c < total; c += span) units.push_back({static_cast<int>(gi), c, std::min(span, total - c)});
+        for (std::uint64_t active = 1; active <= members; ++active) {
+            std::vector<Unit> units;
+            for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
+                const int total = static_cast<int>(active) * gc[gi];
+                for (int c = 0; c < total; c += span)
+                    units.push_back({static_cast<int>(gi), c, std::min(span, total - c)});
+            }
+            std::stable_sort(units.begin(), units.end(),
+                             [](const Unit& a, const Unit& b) { return a.count > b.count; });
+            std::vector<int> ug, uc, un;
+            for (const auto& u : units) {
+                ug.push_back(u.g);
+                uc.push_back(u.col);
+                un.push_back(u.count);
+            }
+            UnitTable table;
+            table.units = static_cast<int>(ug.size());
+            table.group = upload_vector(ug);
+            table.column = upload_vector(uc);
+            table.count = upload_vector(un);
+            unitTables_.push_back(std::move(table));
         }
-        std::stable_sort(units.begin(), units.end(), [](const Unit& a, const Unit& b) { return a.count > b.count; });
-        std::vector<int> ug, uc, un;
-        for (const auto& u : units) {
-            ug.push_back(u.g);
-            uc.push_back(u.col);
-            un.push_back(u.count);
-        }
-        units_ = static_cast<int>(ug.size());
-        unitGroup_ = upload_vector(ug);
-        unitColumn_ = upload_vector(uc);
-        unitCount_ = upload_vector(un);
         groupColumns_ = upload_vector(gc);
         groupFirst_ = upload_vector(gf);
         error_.allocate(sizeof(int));
@@ -297,24 +305,29 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
 }
 
 std::uint64_t VerticalPlan::persistentBytes() const {
-    return matrices_.bytes() + tileGroup_.bytes() + tileColumn_.bytes() + tileCount_.bytes() + unitGroup_.bytes() +
-           unitColumn_.bytes() + unitCount_.bytes() + groupColumns_.bytes() + groupFirst_.bytes() + error_.bytes();
+    std::uint64_t units = 0;
+    for (const auto& t : unitTables_) units += t.group.bytes() + t.column.bytes() + t.count.bytes();
+    return matrices_.bytes() + tileGroup_.bytes() + tileColumn_.bytes() + tileCount_.bytes() + units +
+           groupColumns_.bytes() + groupFirst_.bytes() + error_.bytes();
 }
 
-void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s) const {
+void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s, std::uint64_t members) const {
+    if (members == 0) members = members_;
+    if (members > members_) throw Error(-1, "more ensemble members than the plan was built for");
     if (p_ == GemmPrecision::tf32x3) {
         if (in.im != nullptr || out.im != nullptr)
             throw Error(-3, "the tensor-core GEMM form takes interleaved complex operands");
+        const UnitTable& table = unitTables_[members - 1];
         TcGemmArgs a{};
         a.B = matrices_.get<float>();
         a.R = R_;
         a.S = S_;
         a.NP = (R_ + 15) / 16 * 16;
         a.KCH = (S_ + 31) / 32;
-        a.unitGroup = unitGroup_.get<int>();
-        a.unitColumn = unitColumn_.get<int>();
-        a.unitCount = unitCount_.get<int>();
-        a.units = units_;
+        a.unitGroup = table.group.get<int>();
+        a.unitColumn = table.column.get<int>();
+        a.unitCount = table.count.get<int>();
+        a.units = table.units;
         a.groupColumns = groupColumns_.get<int>();
         a.groupFirst = groupFirst_.get<int>();
         a.memberColumns = memberColumns_;
@@ -324,7 +337,9 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
         check_cuda(launch_tc_gemm(a, s), "tensor-core grouped vertical GEMM kernel");
         return;
     }
-    const GroupTiles t{tileGroup_.get<int>(), tileColumn_.get<int>(), tileCount_.get<int>(), tiles_};
+    // SIMT tiles are member-major: the first members' tiles form a prefix.
+    const int tiles = static_cast<int>(static_cast<std::uint64_t>(tiles_) / members_ * members);
+    const GroupTiles t{tileGroup_.get<int>(), tileColumn_.get<int>(), tileCount_.get<int>(), tiles};
     check_cuda(launch_grouped_gemm(p_, R_, S_, matrices_.get(), t, in, out, s), "grouped vertical GEMM kernel");
 }
 

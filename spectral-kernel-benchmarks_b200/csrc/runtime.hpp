@@ -144,7 +144,9 @@ public:
     // when `natural` holds a single rowsOut x inner block.
     VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::vector<ModeGroup>& groups,
                  std::uint64_t fields, std::uint64_t members, const std::vector<double>& natural);
-    void execute(ComplexOperand in, ComplexOperand out, cudaStream_t s) const;
+    // `members` <= the capacity given at construction (0 = all): the first
+    // `members` ensemble members are computed.
+    void execute(ComplexOperand in, ComplexOperand out, cudaStream_t s, std::uint64_t members = 0) const;
     // Raises if a bounded device wait of the tensor-core form expired.
     void check_device_error() const;
     GemmPrecision precision() const { return p_; }
@@ -157,10 +159,17 @@ private:
     GemmPrecision p_;
     int R_, S_;
     std::uint64_t columns_ = 0;
-    int tiles_ = 0, units_ = 0;
+    int tiles_ = 0;
+    std::uint64_t members_ = 1;
     long long memberColumns_ = 0;
     DeviceBuffer matrices_, tileGroup_, tileColumn_, tileCount_;
-    DeviceBuffer unitGroup_, unitColumn_, unitCount_, groupColumns_, groupFirst_, error_;
+    // Tensor-core work units, one table per active member count 1..members.
+    struct UnitTable {
+        DeviceBuffer group, column, count;
+        int units = 0;
+    };
+    std::vector<UnitTable> unitTables_;
+    DeviceBuffer groupColumns_, groupFirst_, error_;
 };
 
 }  // namespace skb

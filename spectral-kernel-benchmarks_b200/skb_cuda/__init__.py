@@ -690,9 +690,14 @@ class Flux:
     def execute_host_ptr(self, in_ptr, out_ptr):
         check(library().skb_flux_execute(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr)))
 
-    def execute_device(self, in_ptr, out_ptr, stream=None):
-        check(library().skb_flux_execute_device(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr),
-                                                ctypes.c_void_p(stream)))
+    def execute_device(self, in_ptr, out_ptr, stream=None, members=None):
+        if members is None:
+            check(library().skb_flux_execute_device(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr),
+                                                    ctypes.c_void_p(stream)))
+        else:
+            check(library().skb_flux_execute_device_members(self.h, ctypes.c_void_p(in_ptr),
+                                                            ctypes.c_void_p(out_ptr), _u64(members),
+                                                            ctypes.c_void_p(stream)))
 
     def profile(self, in_ptr, out_ptr):
         """One device execution with per-stage event timing -> list of dicts."""
@@ -715,6 +720,88 @@ class Flux:
     def close(self):
         if self.h:
             check(library().skb_flux_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------ serving loop
+
+class ServerClass(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("nz", ctypes.c_uint64), ("targets", ctypes.c_uint64),
+                ("max_batch", ctypes.c_uint64), ("mode", ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in ("submitted", "completed", "batches", "slots", "resident_states",
+                                                     "slot_bytes", "state_bytes", "budget_bytes")]
+
+
+class Server:
+    """Continuous-batching flux request loop over size classes.
+
+    classes: list of (n, nz, targets, max_batch, mode).  Outputs are written
+    into caller arrays; keep them alive until wait() returns."""
+
+    def __init__(self, classes, hbm_budget_bytes, max_slots_per_class=2):
+        arr = (ServerClass * len(classes))(*[ServerClass(*c) for c in classes])
+        h = ctypes.c_void_p()
+        check(library().skb_server_create(arr, _u64(len(classes)), _u64(hbm_budget_bytes),
+                                          ctypes.c_int(max_slots_per_class), ctypes.byref(h)))
+        self.h = h
+        self.sizes = []
+        for i in range(len(classes)):
+            a, b = ctypes.c_uint64(), ctypes.c_uint64()
+            check(library().skb_server_sizes(self.h, ctypes.c_int(i), ctypes.byref(a), ctypes.byref(b)))
+            self.sizes.append((a.value, b.value))
+        self._keep = {}
+
+    def submit(self, size_class, modal_input, output=None):
+        x = _complex(modal_input)
+        assert x.size == self.sizes[size_class][0]
+        out = output if output is not None else np.empty(self.sizes[size_class][1], np.complex128)
+        t = ctypes.c_uint64()
+        check(library().skb_server_submit(self.h, ctypes.c_int(size_class), _p(x), _p(out), ctypes.byref(t)))
+        self._keep[t.value] = (x, out)
+        return t.value
+
+    def load_state(self, size_class, modal_input):
+        x = _complex(modal_input)
+        sid = ctypes.c_int64()
+        check(library().skb_server_load_state(self.h, ctypes.c_int(size_class), _p(x), ctypes.byref(sid)))
+        return sid.value
+
+    def release_state(self, state):
+        check(library().skb_server_release_state(self.h, ctypes.c_int64(state)))
+
+    def submit_state(self, state, output):
+        t = ctypes.c_uint64()
+        check(library().skb_server_submit_state(self.h, ctypes.c_int64(state), _p(output), ctypes.byref(t)))
+        self._keep[t.value] = (None, output)
+        return t.value
+
+    def wait(self, ticket, timeout=60.0):
+        """-> (output array, latency_ms); raises TimeoutError if not finished."""
+        done, lat = ctypes.c_int(), ctypes.c_double()
+        check(library().skb_server_wait(self.h, _u64(ticket), ctypes.c_double(timeout), ctypes.byref(done),
+                                        ctypes.byref(lat)))
+        if not done.value:
+            raise TimeoutError(f"request {ticket} not finished within {timeout} s")
+        _, out = self._keep.pop(ticket)
+        return out, lat.value
+
+    def stats(self):
+        st = ServerStats()
+        check(library().skb_server_get_stats(self.h, ctypes.byref(st)))
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            check(library().skb_server_destroy(self.h))
             self.h = None
 
     def __del__(self):
