@@ -357,6 +357,9 @@ SKB_API int skb_server_submit_state(skb_server* s, int64_t state, skb_complex* o
 /* *done = 1 when finished within timeout_seconds; latency = submit -> result in host memory. */
 SKB_API int skb_server_wait(skb_server* s, uint64_t ticket, double timeout_seconds, int* done, double* latency_ms);
 SKB_API int skb_server_get_stats(skb_server* s, skb_server_stats* stats);
+/* held = 1: queued requests wait and no new batch starts (running batches
+ * finish); held = 0 releases them, so a burst submitted meanwhile is batched. */
+SKB_API int skb_server_hold(skb_server* s, int held);
 
 /* --------------------------------------------------------------- timing */
 /* Events on a handle's stream, for benchmark harnesses. */

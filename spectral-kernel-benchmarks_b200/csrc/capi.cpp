@@ -1269,6 +1269,13 @@ int skb_server_get_stats(skb_server* s, skb_server_stats* st) {
     });
 }
 
+int skb_server_hold(skb_server* s, int held) {
+    return guard([&] {
+        require(s != nullptr, "handle must be non-null");
+        reinterpret_cast<Server*>(s)->hold(held != 0);
+    });
+}
+
 // ------------------------------------------------------------------ timing
 
 int skb_timer_create(skb_timer** out) {

@@ -242,4 +242,108 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-level variant: one warp transforms one length-N sequence held in
+// shared memory at x[pad8(n)] (one spare slot per 8 elements, so the
+// stride-8 stores of the first radix-8 pass spread over all banks).  Only
+// __syncwarp() separates the passes.  Lane l owns butterflies l + 32q.
+
+__device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
+
+template <typename T, int N, int SIGN>
+__device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw, int lane) {
+    using V = cx<T>;
+    static_assert(N >= 8 && (N & (N - 1)) == 0, "warp_fft needs a power of two >= 8");
+    constexpr int BF = N / 8;
+    constexpr int Q = (BF + 31) / 32;
+    int Ns = 1;
+#pragma unroll
+    for (int pass = 0; pass < 12; ++pass) {
+        if (Ns * 8 > N) break;
+        V v[Q][8];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            if (j < BF) {
+#pragma unroll
+                for (int r = 0; r < 8; ++r) v[q][r] = x[pad8(j + r * BF)];
+                const int k = j % Ns;
+                if (Ns > 1) {
+                    const int step = k * (N / (Ns * 8));
+#pragma unroll
+                    for (int r = 1; r < 8; ++r) v[q][r] = cmul(v[q][r], twiddle<SIGN>(tw, step * r));
+                }
+                dft8<SIGN>(v[q]);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            if (j < BF) {
+                const int k = j % Ns;
+                const int base = (j / Ns) * Ns * 8 + k;
+#pragma unroll
+                for (int r = 0; r < 8; ++r) x[pad8(base + r * Ns)] = v[q][r];
+            }
+        }
+        __syncwarp();
+        Ns *= 8;
+    }
+    constexpr int rest = [] {
+        int ns = 1;
+        while (ns * 8 <= N) ns *= 8;
+        return N / ns;
+    }();
+    if constexpr (rest == 4) {
+        constexpr int ns = N / 4;
+        constexpr int Q4 = (ns + 31) / 32;
+        V v[Q4][4];
+#pragma unroll
+        for (int q = 0; q < Q4; ++q) {
+            const int jj = lane + 32 * q;
+            if (jj < ns) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) v[q][r] = x[pad8(jj + r * ns)];
+#pragma unroll
+                for (int r = 1; r < 4; ++r) v[q][r] = cmul(v[q][r], twiddle<SIGN>(tw, jj * r));
+                dft4<SIGN>(v[q][0], v[q][1], v[q][2], v[q][3]);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < Q4; ++q) {
+            const int jj = lane + 32 * q;
+            if (jj < ns) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) x[pad8(jj + r * ns)] = v[q][r];
+            }
+        }
+        __syncwarp();
+    } else if constexpr (rest == 2) {
+        constexpr int ns = N / 2;
+        constexpr int Q2 = (ns + 31) / 32;
+        V v[Q2][2];
+#pragma unroll
+        for (int q = 0; q < Q2; ++q) {
+            const int jj = lane + 32 * q;
+            if (jj < ns) {
+                v[q][0] = x[pad8(jj)];
+                v[q][1] = cmul(x[pad8(jj + ns)], twiddle<SIGN>(tw, jj));
+                dft2<SIGN>(v[q][0], v[q][1]);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < Q2; ++q) {
+            const int jj = lane + 32 * q;
+            if (jj < ns) {
+                x[pad8(jj)] = v[q][0];
+                x[pad8(jj + ns)] = v[q][1];
+            }
+        }
+        __syncwarp();
+    }
+}
+
 }  // namespace skb

@@ -11,10 +11,12 @@
 //     target bins    <- r2c of the target row, kx < keep.
 // The c2r / r2c are the same half-length complex FFT formulation as the
 // staged row kernels (horizontal.cu), so both paths share their numerics.
-// Every thread keeps the same eight (plane, x-pair) positions across all
+// Each warp owns one z-plane and transforms it with warp-synchronous passes
+// (warp_fft); every lane keeps the same Nx/64 x-pairs of its plane across all
 // transforms, which is what lets U,V,W and the product stay in registers.
 // The 3+3T slots are consumed in order, so the bins of slot f+1 are copied
-// into a second shared stage with cp.async while slot f is transformed.
+// into a second shared stage with cp.async while slot f is transformed; the
+// only CTA-wide barriers are one per slot and one per target.
 
 #include "flux_rows.hpp"
 
@@ -23,35 +25,34 @@
 namespace skb {
 namespace {
 
-template <int M, int B>
-struct RowFluxShape {
-    static constexpr int threads = fft_threads(M) * B;
-    static constexpr int per = M * B / threads;  // positions per thread (8 for M >= 8)
-};
-
 __device__ __forceinline__ void cp_async8(void* dst, const void* src, int srcBytes) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(srcBytes) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Per-warp padded sequence region (pad8 of the largest index, plus slack).
+template <int M>
+constexpr int region() {
+    return M + M / 8 + 8;
 }
 
 template <int M, int B>
-__global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(RowFluxArgs a) {
+__global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
     using V = float2;
-    constexpr int NT = RowFluxShape<M, B>::threads;
-    constexpr int PER = RowFluxShape<M, B>::per;
-    // Shared rows padded to B+1: with 64-byte rows the radix-8 passes' strided
-    // stores would otherwise alias onto half the banks.
-    constexpr int LD = B + 1;
+    constexpr int NT = 32 * B;
+    constexpr int PER = M / 32;  // elements of its plane each lane keeps in registers
+    constexpr int XP = region<M>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V* data = reinterpret_cast<V*>(smem_raw);
-    V* stage0 = data + M * LD;
-    V* stage1 = stage0 + a.keep * B;
+    const int keep = a.keep;
+    const int KP = keep | 1;  // odd stage row stride: the 8 planes of one kx hit distinct banks
+    V* xs = reinterpret_cast<V*>(smem_raw);
+    V* stage0 = xs + B * XP;
+    V* stage1 = stage0 + B * KP;
+    V* outTile = stage1 + B * KP;  // [k][b], row stride B + 1
     const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
     const int zChunks = (a.nz + B - 1) / B;
     const int member = blockIdx.x / zChunks;
     const int z0 = (blockIdx.x % zChunks) * B;
@@ -62,13 +63,11 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
     V* out = static_cast<V*>(a.binsOut.data);
     const long long inRow = a.binsIn.planes;  // stride between kx
     const long long outRow = a.binsOut.planes;
-    const int keep = a.keep;
+    V* x = xs + warp * XP;  // this warp's plane
 
-    // Shared position of the e-th element a thread owns: (n, b) at n*LD + b.
-    auto pos = [](int idx) { return (idx / B) * LD + idx % B; };
-
-    // Asynchronous copy of slot f's bins of this row (kx < keep, B planes) into
-    // a stage buffer [k][b]; planes beyond Nz are zero-filled.
+    // Asynchronous copy of slot f's bins of this row into a plane-major stage
+    // [b][k]; consecutive threads read consecutive planes of one kx (the
+    // planes-innermost global rows), planes beyond Nz are zero-filled.
     auto issue = [&](int f, V* stage) {
         const long long pBase = (static_cast<long long>(member) * a.fieldsIn + f) * a.nz + z0;
         const long long rowBase = a.binsIn.kxStride * y;
@@ -77,58 +76,53 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
             const int k = idx / B;
             const bool ok = z0 + b < a.nz;
             const V* src = ok ? in + pBase + b + inRow * (static_cast<long long>(k) + rowBase) : in;
-            cp_async8(stage + idx, src, ok ? 8 : 0);
+            cp_async8(stage + b * KP + k, src, ok ? 8 : 0);
         }
         cp_async_commit();
     };
 
-    // Inverse row transform of slot f (already staged) into registers r[].
+    // Inverse row transform of slot f into this lane's registers r[]: element
+    // lane + 32e of the warp's plane.
     auto inverse_row = [&](int f, V (&r)[PER]) {
-        if (f + 1 < a.fieldsIn) {
-            issue(f + 1, ((f + 1) & 1) ? stage1 : stage0);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        cp_async_wait_all();
         __syncthreads();
-        const V* st = (f & 1) ? stage1 : stage0;
-        auto load = [&](int k, int b) -> V {
+        if (f + 1 < a.fieldsIn) issue(f + 1, ((f + 1) & 1) ? stage1 : stage0);
+        const V* st = ((f & 1) ? stage1 : stage0) + warp * KP;
+        auto load = [&](int k) -> V {
             if (k >= keep) return V{0.f, 0.f};
-            V v = st[k * B + b];
+            V v = st[k];
             if (k == 0 || k == M) v.y = 0.f;
             return v;
         };
         constexpr int pairs = M / 2 + 1;
-        for (int idx = tid; idx < pairs * B; idx += NT) {
-            const int b = idx % B;
-            const int k = idx / B;
+        for (int k = lane; k < pairs; k += 32) {
             if (k == 0) {
-                const V x0 = load(0, b);
-                const V xm = load(M, b);
-                data[b] = {x0.x + xm.x, x0.x - xm.x};
+                const V x0 = load(0);
+                const V xm = load(M);
+                x[pad8(0)] = {x0.x + xm.x, x0.x - xm.x};
                 continue;
             }
             const int kk = M - k;
-            const V xk = load(k, b);
-            const V xm = load(kk, b);
+            const V xk = load(k);
+            const V xm = load(kk);
             {
                 const V s = cadd(xk, cconj(xm));
                 const V d = csub(xk, cconj(xm));
                 const V t = cmulc(d, __ldg(twFull + k));
-                data[k * LD + b] = {s.x - t.y, s.y + t.x};
+                x[pad8(k)] = {s.x - t.y, s.y + t.x};
             }
             if (kk != k) {
                 const V s = cadd(xm, cconj(xk));
                 const V d = csub(xm, cconj(xk));
                 const V t = cmulc(d, __ldg(twFull + kk));
-                data[kk * LD + b] = {s.x - t.y, s.y + t.x};
+                x[pad8(kk)] = {s.x - t.y, s.y + t.x};
             }
         }
-        __syncthreads();
-        fft_smem<float, M, B, +1, LD>(data, twHalf, tid, true);
+        __syncwarp();
+        warp_fft<float, M, +1>(x, twHalf, lane);
 #pragma unroll
-        for (int e = 0; e < PER; ++e) r[e] = data[pos(tid + e * NT)];
-        __syncthreads();
+        for (int e = 0; e < PER; ++e) r[e] = x[pad8(lane + 32 * e)];
+        __syncwarp();
     };
 
     issue(0, stage0);
@@ -149,33 +143,38 @@ __global__ void __launch_bounds__(RowFluxShape<M, B>::threads) rows_flux_kernel(
 #pragma unroll
         for (int e = 0; e < PER; ++e) {
             acc[e] = {acc[e].x + w[e].x * q[e].x, acc[e].y + w[e].y * q[e].y};
-            data[pos(tid + e * NT)] = {-scale * acc[e].x, -scale * acc[e].y};
+            x[pad8(lane + 32 * e)] = {-scale * acc[e].x, -scale * acc[e].y};
         }
-        __syncthreads();
-        fft_smem<float, M, B, -1, LD>(data, twHalf, tid, true);
-        // Real-spectrum split of the half-length FFT, kx < keep.
-        const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.nz + z0;
-        for (int idx = tid; idx < keep * B; idx += NT) {
-            const int b = idx % B;
-            const int k = idx / B;
-            if (z0 + b >= a.nz) continue;
+        __syncwarp();
+        warp_fft<float, M, -1>(x, twHalf, lane);
+        // Real-spectrum split of the half-length FFT, kx < keep, into [k][b].
+        const V zz = x[pad8(0)];
+        for (int k = lane; k < keep; k += 32) {
             V X;
-            const V zz = data[b];
             if (k == 0) {
                 X = {zz.x + zz.y, 0.f};
             } else if (k == M) {
                 X = {zz.x - zz.y, 0.f};
             } else {
-                const V zk = data[k * LD + b];
-                const V zm = cconj(data[(M - k) * LD + b]);
+                const V zk = x[pad8(k)];
+                const V zm = cconj(x[pad8(M - k)]);
                 const V ev = cscale(cadd(zk, zm), 0.5f);
                 const V d = csub(zk, zm);
                 const V o = {0.5f * d.y, -0.5f * d.x};
                 X = cadd(ev, cmul(__ldg(twFull + k), o));
             }
-            out[pOut + b + outRow * (static_cast<long long>(k) + a.binsOut.kxStride * y)] = X;
+            outTile[k * (B + 1) + warp] = X;
         }
         __syncthreads();
+        // Coalesced rows of B planes per kx.
+        const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.nz + z0;
+        for (int idx = tid; idx < keep * B; idx += NT) {
+            const int b = idx % B;
+            const int k = idx / B;
+            if (z0 + b < a.nz)
+                out[pOut + b + outRow * (static_cast<long long>(k) + a.binsOut.kxStride * y)] = outTile[k * (B + 1) + b];
+        }
+        // The next outTile write happens after the next inverse_row's barrier.
     }
 }
 
@@ -185,12 +184,13 @@ template <int M>
 cudaError_t launch_m(const RowFluxArgs& a, dim3 grid, cudaStream_t stream) {
     constexpr int B = 8;
     auto kernel = rows_flux_kernel<M, B>;
-    const size_t bytes = sizeof(float2) * (size_t(M) * (B + 1) + 2 * size_t(a.keep) * B);
+    const size_t bytes =
+        sizeof(float2) * (size_t(B) * region<M>() + 2 * size_t(B) * (a.keep | 1) + size_t(a.keep) * (B + 1));
     if (bytes > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (err != cudaSuccess) return err;
     }
-    kernel<<<grid, RowFluxShape<M, B>::threads, bytes, stream>>>(a);
+    kernel<<<grid, 32 * B, bytes, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -201,17 +201,14 @@ cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
     const int zChunks = (a.nz + B - 1) / B;
     dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
     switch (M) {
-        case 8: return launch_m<8>(a, grid, stream);
-        case 16: return launch_m<16>(a, grid, stream);
         case 32: return launch_m<32>(a, grid, stream);
         case 64: return launch_m<64>(a, grid, stream);
         case 128: return launch_m<128>(a, grid, stream);
         case 256: return launch_m<256>(a, grid, stream);
-        case 512: return launch_m<512>(a, grid, stream);
         default: return cudaErrorInvalidValue;
     }
 }
 
-bool rows_flux_supported(long long nx) { return nx >= 16 && nx <= 1024 && (nx & (nx - 1)) == 0; }
+bool rows_flux_supported(long long nx) { return nx >= 64 && nx <= 512 && (nx & (nx - 1)) == 0; }
 
 }  // namespace skb

@@ -293,6 +293,14 @@ void Server::finish(Slot& slot) {
     done_.notify_all();
 }
 
+void Server::hold(bool held) {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        held_ = held;
+    }
+    work_.notify_all();
+}
+
 void Server::loop() {
     cudaSetDevice(device_);
     std::unique_lock<std::mutex> lk(mu_);
@@ -339,7 +347,7 @@ void Server::loop() {
             break;
         }
         for (auto& s : slots_) {
-            if (s->busy || classes_[s->cls].queue.empty()) continue;
+            if (held_ || s->busy || classes_[s->cls].queue.empty()) continue;
             launch(*s);
             progress = true;
         }

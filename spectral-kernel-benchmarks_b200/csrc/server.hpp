@@ -59,6 +59,9 @@ public:
     // Wait up to timeoutSeconds; returns true when finished and fills the
     // latency (submit -> result in host memory) in milliseconds.
     bool wait(std::uint64_t ticket, double timeoutSeconds, double* latencyMs);
+    // While held, queued requests wait and no new batch starts (running
+    // batches finish); releasing lets a burst that queued meanwhile be batched.
+    void hold(bool held);
     ServerStats stats();
 
 private:
@@ -106,6 +109,7 @@ private:
     std::condition_variable work_, done_;
     std::thread worker_;
     bool stop_ = false;
+    bool held_ = false;
     int device_ = 0;
     std::uint64_t nextTicket_ = 1;
     std::int64_t nextState_ = 1;

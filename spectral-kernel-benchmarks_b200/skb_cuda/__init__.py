@@ -794,6 +794,10 @@ class Server:
         _, out = self._keep.pop(ticket)
         return out, lat.value
 
+    def hold(self, held=True):
+        """While held, no new batch starts; release with hold(False)."""
+        check(library().skb_server_hold(self.h, 1 if held else 0))
+
     def stats(self):
         st = ServerStats()
         check(library().skb_server_get_stats(self.h, ctypes.byref(st)))
