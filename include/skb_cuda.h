@@ -186,6 +186,25 @@ SKB_API int skb_fft_gather_retained_device(skb_fft_provider* p, const void* wvm_
                                    uint64_t view_count, double scale, void* stream);
 SKB_API int skb_fft_embed_retained_device(skb_fft_provider* p, const skb_field_view* views, uint64_t view_count,
                                   void* wvm_spectrum, void* stream);
+/* Handle-free dense inverse that allocates nothing.  It has no counterpart in
+ * the reference.  It is for callers that may not allocate device memory while
+ * they run: a host that enforces its own device-memory budget through its own
+ * allocator, or a plugin whose host forbids cudaMalloc / cudaFree inside its
+ * compute callbacks (an allocation can fail once the budget is reserved, and
+ * cudaFree stalls every stream on the device).  The result is that of
+ * skb_fft_inverse_device for the same workload and precision; the spectrum is
+ * preserved.  The scratch (twiddle tables and the column-transformed
+ * spectrum) is a fixed 64 MiB device array inside this library, which every
+ * GPU that loads the library holds until the process exits; a workload that
+ * needs more is refused with SKB_ERR_INVALID_ARGUMENT.  The first call on each
+ * device looks the array's address up and may make the driver load the
+ * library's device code, so make that call before any stream capture begins.
+ * Each call writes everything it later reads, so nothing has to start at zero,
+ * but all calls share the one array: calls whose GPU work overlaps (other
+ * streams, other threads) race and corrupt each other; serialise them.
+ * stream NULL is the legacy default stream. */
+SKB_API int skb_fft_inverse_device_noalloc(const skb_workload* w, int precision, const void* wvm_spectrum, void* real,
+                                           void* stream);
 
 /* ------------------------------------------- pruned horizontal provider */
 /* Replaces FFTWPrunedProvider (skbench.hpp:467-520) and

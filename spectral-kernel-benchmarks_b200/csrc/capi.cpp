@@ -8,6 +8,7 @@
 #include <string>
 
 #include "flux.hpp"
+#include "noalloc.hpp"
 #include "server.hpp"
 #include "pointwise.hpp"
 #include "runtime.hpp"
@@ -375,6 +376,13 @@ int skb_fft_inverse_device(skb_fft_provider* p, const void* wvm, void* real, voi
         require(p && real && wvm, "handle and buffers must be non-null");
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
         p->plan->inverse_dense(wvm, real, p->w.planes(), s);
+    });
+}
+
+int skb_fft_inverse_device_noalloc(const skb_workload* w, int precision, const void* wvm, void* real, void* stream) {
+    return guard([&] {
+        require(wvm && real, "buffers must be non-null");
+        inverse_dense_static(to_workload(w), to_precision(precision), wvm, real, static_cast<cudaStream_t>(stream));
     });
 }
 
