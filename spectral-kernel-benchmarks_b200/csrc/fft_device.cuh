@@ -244,11 +244,12 @@ __device__ __forceinline__ void fft_smem(cx<T>* data, const cx<T>* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // Warp-level variant: one warp transforms one length-N sequence held in
-// shared memory at x[pad8(n)] (one spare slot per 8 elements, so the
-// stride-8 stores of the first radix-8 pass spread over all banks).  Only
-// __syncwarp() separates the passes.  Lane l owns butterflies l + 32q.
+// shared memory at x[pad16(n)] (one spare slot per 16 elements: the stride-8
+// stores of the first radix-8 pass then spread over all banks of a half-warp,
+// while runs of 16 consecutive elements stay contiguous).  Only __syncwarp()
+// separates the passes.  Lane l owns butterflies l + 32q.
 
-__device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 
 template <typename T, int N, int SIGN>
 __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw, int lane) {
@@ -266,7 +267,7 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
             const int j = lane + 32 * q;
             if (j < BF) {
 #pragma unroll
-                for (int r = 0; r < 8; ++r) v[q][r] = x[pad8(j + r * BF)];
+                for (int r = 0; r < 8; ++r) v[q][r] = x[pad16(j + r * BF)];
                 const int k = j % Ns;
                 if (Ns > 1) {
                     const int step = k * (N / (Ns * 8));
@@ -284,7 +285,7 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
                 const int k = j % Ns;
                 const int base = (j / Ns) * Ns * 8 + k;
 #pragma unroll
-                for (int r = 0; r < 8; ++r) x[pad8(base + r * Ns)] = v[q][r];
+                for (int r = 0; r < 8; ++r) x[pad16(base + r * Ns)] = v[q][r];
             }
         }
         __syncwarp();
@@ -304,7 +305,7 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
             const int jj = lane + 32 * q;
             if (jj < ns) {
 #pragma unroll
-                for (int r = 0; r < 4; ++r) v[q][r] = x[pad8(jj + r * ns)];
+                for (int r = 0; r < 4; ++r) v[q][r] = x[pad16(jj + r * ns)];
 #pragma unroll
                 for (int r = 1; r < 4; ++r) v[q][r] = cmul(v[q][r], twiddle<SIGN>(tw, jj * r));
                 dft4<SIGN>(v[q][0], v[q][1], v[q][2], v[q][3]);
@@ -316,7 +317,7 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
             const int jj = lane + 32 * q;
             if (jj < ns) {
 #pragma unroll
-                for (int r = 0; r < 4; ++r) x[pad8(jj + r * ns)] = v[q][r];
+                for (int r = 0; r < 4; ++r) x[pad16(jj + r * ns)] = v[q][r];
             }
         }
         __syncwarp();
@@ -328,8 +329,8 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
         for (int q = 0; q < Q2; ++q) {
             const int jj = lane + 32 * q;
             if (jj < ns) {
-                v[q][0] = x[pad8(jj)];
-                v[q][1] = cmul(x[pad8(jj + ns)], twiddle<SIGN>(tw, jj));
+                v[q][0] = x[pad16(jj)];
+                v[q][1] = cmul(x[pad16(jj + ns)], twiddle<SIGN>(tw, jj));
                 dft2<SIGN>(v[q][0], v[q][1]);
             }
         }
@@ -338,8 +339,8 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
         for (int q = 0; q < Q2; ++q) {
             const int jj = lane + 32 * q;
             if (jj < ns) {
-                x[pad8(jj)] = v[q][0];
-                x[pad8(jj + ns)] = v[q][1];
+                x[pad16(jj)] = v[q][0];
+                x[pad16(jj + ns)] = v[q][1];
             }
         }
         __syncwarp();

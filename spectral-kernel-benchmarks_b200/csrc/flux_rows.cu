@@ -32,10 +32,10 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, int srcByt
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Per-warp padded sequence region (pad8 of the largest index, plus slack).
+// Per-warp padded sequence region (pad16 of the largest index, plus slack).
 template <int M>
 constexpr int region() {
-    return M + M / 8 + 8;
+    return M + M / 16 + 8;
 }
 
 template <int M, int B>
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
             if (k == 0) {
                 const V x0 = load(0);
                 const V xm = load(M);
-                x[pad8(0)] = {x0.x + xm.x, x0.x - xm.x};
+                x[pad16(0)] = {x0.x + xm.x, x0.x - xm.x};
                 continue;
             }
             const int kk = M - k;
@@ -109,19 +109,19 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
                 const V s = cadd(xk, cconj(xm));
                 const V d = csub(xk, cconj(xm));
                 const V t = cmulc(d, __ldg(twFull + k));
-                x[pad8(k)] = {s.x - t.y, s.y + t.x};
+                x[pad16(k)] = {s.x - t.y, s.y + t.x};
             }
             if (kk != k) {
                 const V s = cadd(xm, cconj(xk));
                 const V d = csub(xm, cconj(xk));
                 const V t = cmulc(d, __ldg(twFull + kk));
-                x[pad8(kk)] = {s.x - t.y, s.y + t.x};
+                x[pad16(kk)] = {s.x - t.y, s.y + t.x};
             }
         }
         __syncwarp();
         warp_fft<float, M, +1>(x, twHalf, lane);
 #pragma unroll
-        for (int e = 0; e < PER; ++e) r[e] = x[pad8(lane + 32 * e)];
+        for (int e = 0; e < PER; ++e) r[e] = x[pad16(lane + 32 * e)];
         __syncwarp();
     };
 
@@ -143,12 +143,12 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
 #pragma unroll
         for (int e = 0; e < PER; ++e) {
             acc[e] = {acc[e].x + w[e].x * q[e].x, acc[e].y + w[e].y * q[e].y};
-            x[pad8(lane + 32 * e)] = {-scale * acc[e].x, -scale * acc[e].y};
+            x[pad16(lane + 32 * e)] = {-scale * acc[e].x, -scale * acc[e].y};
         }
         __syncwarp();
         warp_fft<float, M, -1>(x, twHalf, lane);
         // Real-spectrum split of the half-length FFT, kx < keep, into [k][b].
-        const V zz = x[pad8(0)];
+        const V zz = x[pad16(0)];
         for (int k = lane; k < keep; k += 32) {
             V X;
             if (k == 0) {
@@ -156,8 +156,8 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
             } else if (k == M) {
                 X = {zz.x - zz.y, 0.f};
             } else {
-                const V zk = x[pad8(k)];
-                const V zm = cconj(x[pad8(M - k)]);
+                const V zk = x[pad16(k)];
+                const V zm = cconj(x[pad16(M - k)]);
                 const V ev = cscale(cadd(zk, zm), 0.5f);
                 const V d = csub(zk, zm);
                 const V o = {0.5f * d.y, -0.5f * d.x};
