@@ -25,6 +25,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "build")
 LIB = os.path.join(HERE, "libskb_cuda.so")
+HARNESS = os.path.join(HERE, "harness")
+CLI = os.path.join(HERE, "skbench-cuda")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -79,7 +81,23 @@ def build(force=False, checked=False, verbose=False):
         proc = subprocess.run(cmd, capture_output=True, text=True)
         if proc.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), proc.stderr))
+    build_cli(force)
     return LIB
+
+
+def build_cli(force=False):
+    """The skbench-cuda command line (harness/*.cpp) against the C ABI only."""
+    srcs = sorted(glob.glob(os.path.join(HARNESS, "*.cpp")))
+    deps = srcs + glob.glob(os.path.join(HARNESS, "*.hpp")) + [LIB, os.path.join(ROOT, "include", "skb_cuda.h")]
+    if not force and os.path.exists(CLI) and os.path.getmtime(CLI) >= max(os.path.getmtime(d) for d in deps):
+        return CLI
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++20", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include")] + srcs + [
+        "-o", CLI, "-L" + HERE, "-lskb_cuda", "-Wl,-rpath,$ORIGIN"]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError("harness build failed:\n%s\n%s" % (" ".join(cmd), proc.stderr))
+    return CLI
 
 
 if __name__ == "__main__":

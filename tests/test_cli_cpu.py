@@ -1,0 +1,46 @@
+"""The skbench-cuda command line without a GPU: argument handling, profile
+list, exit codes (main.cpp:242-245 maps errors to 2) and `compare` over the
+reference writer's own CSV sample."""
+
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "spectral-kernel-benchmarks_b200", "skbench-cuda")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+pytestmark = pytest.mark.skipif(not os.path.exists(CLI), reason="skbench-cuda is not built")
+
+
+def cli(*args):
+    return subprocess.run([CLI, *args], capture_output=True, text=True, timeout=60)
+
+
+def test_list_names_the_reference_profiles_and_kernels():
+    out = cli("list")
+    assert out.returncode == 0
+    for name in ("smoke: 8x8, Nz=7, fields=2", "quick: 256x256, Nz=65, fields=3",
+                 "wvm-historical-512-nz129-f4: 512x512, Nz=129, fields=4", "wvm-large-1024-nz129-f4"):
+        assert name in out.stdout
+    for kernel in ("fft (alias 2d-rfft)", "pruned-horizontal", "vertical-gemm", "pointwise-advection",
+                   "production-lifetime-flux"):
+        assert kernel in out.stdout
+
+
+@pytest.mark.parametrize("args", [(), ("bogus",), ("list", "extra"), ("run", "--kernel", "bogus"),
+                                  ("run", "--profile", "nope"), ("run", "--warmups"), ("validate", "--x"),
+                                  ("compare",)])
+def test_bad_arguments_exit_2(args):
+    out = cli(*args)
+    assert out.returncode == 2
+    assert args == () or "skbench-cuda:" in out.stderr
+
+
+def test_compare_reads_the_reference_csv():
+    out = cli("compare", "--input", os.path.join(GOLDEN, "reference_report.csv"))
+    assert out.returncode == 0
+    lines = out.stdout.strip().splitlines()
+    assert lines[0] == "provider\tscope\tstage\tdirection\tmedian_ms\tsamples"
+    assert lines[1].split("\t") == ["sample", "primitive", "stage", "forward", "1500.000000", "2"]

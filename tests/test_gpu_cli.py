@@ -1,0 +1,73 @@
+"""skbench-cuda run / validate on the GPU: every kernel writes a report whose
+JSON keys are the reference writer's (the golden schema sample produced by the
+reference's own json.cpp) and whose CSV has the reference's nine columns, and
+`validate` passes against the direct transforms."""
+
+import csv
+import json
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "spectral-kernel-benchmarks_b200", "skbench-cuda")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+pytestmark = pytest.mark.gpu
+
+
+def keys_match(sample, got, path="$"):
+    """Every key of the reference sample exists in `got`, recursively."""
+    if isinstance(sample, dict):
+        assert isinstance(got, dict), path
+        for k, v in sample.items():
+            assert k in got, path + "." + k
+            keys_match(v, got[k], path + "." + k)
+    elif isinstance(sample, list) and sample and got:
+        keys_match(sample[0], got[0], path + "[0]")
+
+
+def run(tmp_path, *args):
+    out_json = tmp_path / "report.json"
+    proc = subprocess.run([CLI, "run", *args, "--output", str(out_json)], capture_output=True, text=True,
+                          timeout=600)
+    assert proc.returncode == 0, proc.stdout + proc.stderr
+    report = json.loads(out_json.read_text())
+    with open(out_json.with_suffix(".csv")) as fh:
+        rows = list(csv.reader(fh))
+    return report, rows
+
+
+@pytest.mark.parametrize("args", [
+    ("--kernel", "fft"),
+    ("--kernel", "2d-rfft", "--precision", "fp32"),
+    ("--kernel", "pruned-horizontal"),
+    ("--kernel", "pruned-horizontal", "--precision", "fp32"),
+    ("--kernel", "vertical-gemm", "--vertical-gemm-family", "common"),
+    ("--kernel", "vertical-gemm", "--vertical-gemm-family", "k2-grouped", "--vertical-gemm-precision", "fp32"),
+    ("--kernel", "pointwise-advection"),
+    ("--kernel", "production-lifetime-flux", "--flux-mode", "fp64-plain", "--nx", "32", "--ny", "32", "--nz", "9"),
+    ("--kernel", "production-lifetime-flux", "--flux-mode", "split-tf32x3", "--nx", "64", "--ny", "64", "--nz",
+     "17", "--members", "2"),
+], ids=lambda a: "-".join(a[1::2]))
+def test_run_writes_the_reference_schema(tmp_path, args):
+    report, rows = run(tmp_path, "--profile", "smoke", *args)
+    with open(os.path.join(GOLDEN, "reference_report.json")) as fh:
+        keys_match(json.load(fh), report)
+    assert report["status"] == "passed"
+    provider = report["providers"][0]
+    assert provider["id"] == "cuda"
+    assert provider["correctness"] and all(m["passed"] for m in provider["correctness"])
+    assert any(t["scope"] == "primitive" and t["medianSeconds"] > 0 for t in provider["timings"])
+    assert rows[0] == ["run_id", "provider", "scope", "stage", "direction", "state", "bytes_moved", "sample_index",
+                       "seconds"]
+    assert len(rows) > 1 and all(len(r) == 9 for r in rows)
+
+
+def test_validate_passes():
+    proc = subprocess.run([CLI, "validate"], capture_output=True, text=True, timeout=600)
+    assert proc.returncode == 0, proc.stdout + proc.stderr
+    assert "validation passed" in proc.stdout
+    assert proc.stdout.count("cuda/") == 10 and proc.stdout.count("cuda-pruned/") == 10
+    assert "cuda-flux/split-tf32x3/32x32x9" in proc.stdout
