@@ -51,6 +51,12 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--skip-cpu-baseline", action="store_true")
     p.add_argument("--skip-e2e", action="store_true")
+    p.add_argument("--serve", action="store_true",
+                   help="serving benchmark: Poisson arrivals over mixed grid sizes with resident states")
+    p.add_argument("--serve-requests", type=int, default=600)
+    p.add_argument("--serve-rate", type=float, default=400.0, help="mean arrivals per second")
+    p.add_argument("--serve-batch", type=int, default=8)
+    p.add_argument("--serve-states", type=int, default=8, help="resident member states per size class")
     return p.parse_args()
 
 
@@ -148,22 +154,27 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ inputs
 
+def mode_wavenumbers(n):
+    """(k, l) of the retained radial-2/3 modes, from the library's own mode table."""
+    import skb_cuda as S
+
+    modes = S.retained_modes(S.Workload(n, n, 1, 1))
+    return (np.array([m.k for m in modes], dtype=np.float64), np.array([m.l for m in modes], dtype=np.float64))
+
+
 def power_law_inputs(n, nz, members, targets=4, seed=129):
     """Seeded k^-3 power-law modal spectra: amplitude (1 + |k|^2)^(-3/2) times a
     uniform random phase, for every (member, mode, field, j)."""
-    from oracle import oracle as orc  # mode table only; the values are synthetic
-
-    modes = orc.retained_modes(n, n)
+    k, l = mode_wavenumbers(n)
     nj = 2 * (nz - 1) // 3
     fields = 3 + 3 * targets
     rng = np.random.default_rng(seed)
-    k2 = (modes.k.astype(np.float64) ** 2 + modes.l.astype(np.float64) ** 2)
-    amp = (1.0 + k2) ** -1.5
-    shape = (members, len(modes), fields, nj)
+    amp = (1.0 + k * k + l * l) ** -1.5
+    shape = (members, len(k), fields, nj)
     phase = rng.uniform(0.0, 2.0 * np.pi, shape)
     mag = rng.uniform(0.5, 1.5, shape)
     x = (amp[None, :, None, None] * mag) * np.exp(1j * phase)
-    dc = (modes.k == 0) & (modes.l == 0)
+    dc = (k == 0) & (l == 0)
     x[:, dc, :, :] = x[:, dc, :, :].real
     return np.ascontiguousarray(x.reshape(-1))
 
@@ -306,6 +317,89 @@ def cuda_arm(args, dist):
     return line
 
 
+# ---------------------------------------------------------------- serving
+
+# Size classes of the serving mix: (n, Nz, targets, share of arrivals);
+# targets 3 is the 12 -> 3 variant, 4 the full 15 -> 4 flux.
+SERVE_CLASSES = [(128, 33, 3, 0.4), (256, 65, 3, 0.4), (512, 129, 4, 0.2)]
+
+
+def serve_arm(args, dist):
+    """Requests with seeded exponential inter-arrival times pick a size class
+    by the mix above and a resident member state of that class; the server
+    batches what queues per class.  Latency = submit -> result in host memory."""
+    import skb_cuda as S
+
+    S.set_device(dist.local)
+    mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
+    classes = [(n, nz, t, args.serve_batch, mode) for n, nz, t, _ in SERVE_CLASSES]
+    server = S.Server(classes, hbm_budget_bytes=64 << 30, max_slots_per_class=2)
+    states = []
+    for c, (n, nz, t, _) in enumerate(SERVE_CLASSES):
+        states.append([server.load_state(c, power_law_inputs(n, nz, 1, targets=t, seed=1000 * c + i + 977 * dist.rank))
+                       for i in range(args.serve_states)])
+    rng = np.random.default_rng(7 + dist.rank)
+    picks = rng.choice(len(SERVE_CLASSES), size=args.serve_requests, p=[c[3] for c in SERVE_CLASSES])
+    gaps = rng.exponential(1.0 / args.serve_rate, size=args.serve_requests)
+    outputs = [S.PinnedArray(np.complex128, server.sizes[c][1]) for c in range(len(SERVE_CLASSES))
+               for _ in range(2)]
+    # Warm-up: every class once, alone.
+    for c in range(len(SERVE_CLASSES)):
+        server.wait(server.submit_state(states[c][0], outputs[2 * c].array), timeout=300)
+    base = server.stats()
+    dist.barrier()
+    tickets = []
+    t0 = time.perf_counter()
+    due = t0
+    with ClockSampler(dist.local) as clocks:
+        for i, c in enumerate(picks):
+            due += gaps[i]
+            while True:
+                now = time.perf_counter()
+                if now >= due:
+                    break
+                if due - now > 2e-4:
+                    time.sleep(due - now - 1e-4)
+            # Two pinned result buffers per class, reused: the results of
+            # this benchmark are not read, only their arrival times.
+            tickets.append((c, server.submit_state(states[c][i % args.serve_states], outputs[2 * c + i % 2].array)))
+        lat = [(c, server.wait(t, timeout=600)[1]) for c, t in tickets]
+        t1 = time.perf_counter()
+    stats = server.stats()
+    server.close()
+    for o in outputs:
+        o.free()
+    if dist.rank != 0:
+        return None
+    all_ms = np.array([x for _, x in lat])
+    span = t1 - t0
+    per_class = {}
+    for c, (n, nz, t, share) in enumerate(SERVE_CLASSES):
+        v = np.array([x for k, x in lat if k == c])
+        per_class[f"{n}x{n}xNz{nz}_f{t}"] = {
+            "requests": int(v.size), "p50_ms": float(np.percentile(v, 50)) if v.size else None,
+            "p99_ms": float(np.percentile(v, 99)) if v.size else None,
+            "evals_per_s": float(v.size / span)}
+    mode_name = {"split": "split-tf32x3"}.get(args.mode, args.mode)
+    return {
+        "metric": "serving p99 latency, mixed flux requests (40% 128²×33 f3, 40% 256²×65 f3, 20% 512²×129 f4)",
+        "value": float(np.percentile(all_ms, 99)), "unit": "ms", "n_gpus": dist.world,
+        "steps": args.serve_requests, "warmup": len(SERVE_CLASSES), "ms_per_step": float(np.mean(all_ms)),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if mode == S.FLUX_FP64_PLAIN else ("f32" if mode == S.FLUX_FP32 else "tf32x3+f32"),
+        "data": "synthetic (seeded k^-3 power-law resident states, seeded Poisson arrivals)",
+        "config": {"workload": "continuous-batching flux server", "mode": mode_name,
+                   "arrival_rate_per_s": args.serve_rate, "requests": args.serve_requests,
+                   "max_batch": args.serve_batch, "resident_states_per_class": args.serve_states,
+                   "parallelism": f"replicas x{dist.world}"},
+        "p50_ms": float(np.percentile(all_ms, 50)), "p99_ms": float(np.percentile(all_ms, 99)),
+        "throughput_evals_per_s": float(len(all_ms) / span), "classes": per_class,
+        "server": {"batches": stats["batches"] - base["batches"], "slots": stats["slots"],
+                   "slot_bytes": stats["slot_bytes"], "state_bytes": stats["state_bytes"]},
+        "clocks": clocks.summary(),
+    }
+
+
 # ------------------------------------------------------------- CPU arms
 
 def cpu_flux_once(n, nz, seed, workers):
@@ -362,7 +456,12 @@ def main():
     args = parse()
     dist = Dist()
     try:
-        line = reference_arm(args, dist) if args.impl == "reference" else cuda_arm(args, dist)
+        if args.impl == "reference":
+            line = reference_arm(args, dist)
+        elif args.serve:
+            line = serve_arm(args, dist)
+        else:
+            line = cuda_arm(args, dist)
         if line is not None and dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -1,0 +1,397 @@
+// Warp-per-plane column transforms with fused retention, FP32, for the fused
+// flux's two column stages.
+//
+// A CTA handles one kx column of B consecutive z-planes of one field view.
+// Global traffic is CTA-wide and coalesced over the planes (B consecutive z of
+// one mode, or of one (ky, kx) bin, are contiguous in HBM); each warp then
+// transforms one plane's Ny-point column in its own padded shared region with
+// warp_fft, so the only CTA-wide barriers are the one after the loads and the
+// one before the stores.  The embed form scatters the retained modes of the
+// column (with the kx = 0 Hermitian partner) and zero-fills the rest; the
+// gather form keeps only the retained ky of the column and writes them, scaled
+// and conjugated where the mode stores its partner, into the view.
+
+#include "columns_warp.hpp"
+#include "async_copy.cuh"
+#include "fft_device.cuh"
+
+namespace skb {
+namespace {
+
+// Per-plane region: pad16 of the largest index plus slack, rounded so that
+// region % 16 == 2 — the B planes of one ky then land in distinct banks when
+// consecutive threads fill or drain consecutive planes.
+template <int N>
+constexpr int plane_region() {
+    constexpr int base = N + N / 16 + 1;
+    return base + ((2 - base % 16) + 16) % 16;
+}
+
+template <int N, int B>
+__global__ void __launch_bounds__(32 * B, 4) columns_embed_warp_kernel(int nz, ViewSet views, ModeTables tables,
+                                                                    DenseBins out, const float2* __restrict__ tw) {
+    constexpr int NT = 32 * B;
+    constexpr int XP = plane_region<N>();
+    constexpr int ITER = N * B / NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int zChunks = (nz + B - 1) / B;
+    const int f = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int kx = blockIdx.y;
+    const FieldView view = views.v[f];
+    const int* map = tables.cellMap + static_cast<long long>(kx) * N;
+    const int b = tid % B;  // NT is a multiple of B: every iteration has the same plane
+    const int z = z0 + b;
+    // Retained cells are copied asynchronously straight into the plane
+    // regions (no register staging, so many copies are in flight per SM);
+    // other cells are zero-filled by the same instruction.
+    int e[ITER];
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) e[it] = __ldg(map + (tid + it * NT) / B);
+    const bool inRange = z < nz;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        float2* dst = xs + b * XP + pad16((tid + it * NT) / B);
+        const bool have = inRange && e[it] >= 0;
+        const long long i = have ? z + view.modeStride * (e[it] >> 1) : 0;
+        if (view.im == nullptr) {
+            cp_async8(dst, reinterpret_cast<const float2*>(view.re) + i, have ? 8 : 0);
+        } else {
+            cp_async4(&dst->x, reinterpret_cast<const float*>(view.re) + i, have ? 4 : 0);
+            cp_async4(&dst->y, reinterpret_cast<const float*>(view.im) + i, have ? 4 : 0);
+        }
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    // Cells that store the conjugate partner: negate in place (each thread
+    // fixes the cells it copied).
+#pragma unroll
+    for (int it = 0; it < ITER; ++it)
+        if (inRange && e[it] >= 0 && (e[it] & 1)) {
+            float2* dst = xs + b * XP + pad16((tid + it * NT) / B);
+            dst->y = -dst->y;
+        }
+    __syncthreads();
+    warp_fft<float, N, +1>(xs + warp * XP, tw, lane);
+    __syncthreads();
+    if (z < nz) {
+        float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * nz + z + out.planes * kx;
+        const long long rowStride = out.planes * out.kxStride;
+#pragma unroll
+        for (int it = 0; it < ITER; ++it) {
+            const int ky = (tid + it * NT) / B;
+            dst[rowStride * ky] = xs[b * XP + pad16(ky)];
+        }
+    }
+}
+
+template <int N, int B>
+__global__ void __launch_bounds__(32 * B, 4) columns_gather_warp_kernel(int nz, DenseBins in, ViewSet views,
+                                                                     ModeTables tables, float scale,
+                                                                     const float2* __restrict__ tw) {
+    constexpr int NT = 32 * B;
+    constexpr int XP = plane_region<N>();
+    constexpr int ITER = N * B / NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int zChunks = (nz + B - 1) / B;
+    const int f = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int kx = blockIdx.y;
+    const int b = tid % B;
+    const int z = z0 + b;
+    {
+        const float2* src =
+            static_cast<const float2*>(in.data) + static_cast<long long>(f) * nz + z + in.planes * kx;
+        const long long rowStride = in.planes * in.kxStride;
+#pragma unroll
+        for (int it = 0; it < ITER; ++it) {
+            const int ky = (tid + it * NT) / B;
+            cp_async8(xs + b * XP + pad16(ky), z < nz ? src + rowStride * ky : src, z < nz ? 8 : 0);
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+    }
+    __syncthreads();
+    warp_fft<float, N, -1>(xs + warp * XP, tw, lane);
+    __syncthreads();
+    if (z >= nz) return;
+    const FieldView view = views.v[f];
+    const int begin = __ldg(tables.colStart + kx);
+    const int end = __ldg(tables.colStart + kx + 1);
+    for (int e = begin + tid / B; e < end; e += NT / B) {
+        const int ky = __ldg(tables.colKy + e);
+        const int mc = __ldg(tables.colMode + e);
+        float2 v = xs[b * XP + pad16(ky)];
+        v.x *= scale;
+        v.y *= (mc & 1) ? -scale : scale;
+        const long long i = z + view.modeStride * (mc >> 1);
+        if (view.im == nullptr) {
+            reinterpret_cast<float2*>(view.re)[i] = v;
+        } else {
+            reinterpret_cast<float*>(view.re)[i] = v.x;
+            reinterpret_cast<float*>(view.im)[i] = v.y;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 512-point columns with the first and last FFT passes at the HBM boundary.
+// Three radix-8 Stockham passes (Ns = 1, 8, 64).  Pass 1 is done by thread
+// (plane b = t % 8, butterflies j) straight from global memory: its eight
+// inputs are ky = j + 64r of plane b, and consecutive threads take
+// consecutive planes, so every load instruction reads 64 contiguous bytes per
+// ky.  Pass 2 is warp-per-plane in shared memory.  Pass 3 is again thread
+// (b, j): its outputs are ky = j + 64r of plane b, stored straight to global
+// memory with the same coalescing.  Each element touches shared memory four
+// times instead of eight.  The butterfly-to-thread maps are chosen so that,
+// with a plane region of 2 mod 4 elements, the pass-1 stores and pass-3 loads
+// are free of bank conflicts: in a half-warp the two butterflies of pass 1
+// differ by 2 and those of pass 3 by 1.
+constexpr int kDirectN = 512;
+constexpr int kDirectRegion = 546;  // >= pad16(511) + 1, and 546 % 4 == 2
+static_assert(kDirectRegion % 4 == 2 && kDirectRegion > 542, "direct plane region");
+
+__device__ __forceinline__ int pass1_butterfly(int t, int q) {
+    const int h = t >> 4;
+    return 4 * (h >> 1) + (h & 1) + 2 * ((t >> 3) & 1) + 32 * q;
+}
+
+template <int SIGN>
+__device__ __forceinline__ void direct_middle_pass(float2* xs, const float2* __restrict__ tw, int warp, int lane) {
+    float2* x = xs + warp * kDirectRegion;
+    float2 v[2][8];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = lane + 32 * q;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[q][r] = x[pad16(j + r * 64)];
+        const int step = (j % 8) * 8;
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[q][r] = cmul(v[q][r], twiddle<SIGN>(tw, step * r));
+        dft8<SIGN>(v[q]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = lane + 32 * q;
+        const int base = (j / 8) * 64 + (j % 8);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) x[pad16(base + r * 8)] = v[q][r];
+    }
+}
+
+__global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, ViewSet views, ModeTables tables,
+                                                                      DenseBins out, const float2* __restrict__ tw) {
+    constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int zChunks = (nz + B - 1) / B;
+    const int f = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int kx = blockIdx.y;
+    const int b = tid & 7;
+    const int z = z0 + b;
+    const bool inRange = z < nz;
+    const int* map = tables.cellMap + static_cast<long long>(kx) * N;
+    {
+        const FieldView view = views.v[f];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = pass1_butterfly(tid, q);
+            int e[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) e[r] = __ldg(map + j + 64 * r);
+            float2 v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                v[r] = make_float2(0.f, 0.f);
+                if (inRange && e[r] >= 0) {
+                    const long long i = z + view.modeStride * (e[r] >> 1);
+                    if (view.im == nullptr) {
+                        v[r] = __ldg(reinterpret_cast<const float2*>(view.re) + i);
+                    } else {
+                        v[r] = make_float2(__ldg(reinterpret_cast<const float*>(view.re) + i),
+                                           __ldg(reinterpret_cast<const float*>(view.im) + i));
+                    }
+                    if (e[r] & 1) v[r].y = -v[r].y;
+                }
+            }
+            dft8<+1>(v);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) xs[b * XP + pad16(j * 8 + r)] = v[r];
+        }
+    }
+    __syncthreads();
+    direct_middle_pass<+1>(xs, tw, warp, lane);
+    __syncthreads();
+    if (!inRange) return;
+    float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * nz + z + out.planes * kx;
+    const long long rowStride = out.planes * out.kxStride;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = (tid >> 3) + 32 * q;
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + pad16(j + r * 64)];
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<+1>(tw, j * r));
+        dft8<+1>(v);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) dst[rowStride * (j + 64 * r)] = v[r];
+    }
+}
+
+__global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, DenseBins in, ViewSet views,
+                                                                       ModeTables tables, float scale,
+                                                                       const float2* __restrict__ tw) {
+    constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int zChunks = (nz + B - 1) / B;
+    const int f = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int kx = blockIdx.y;
+    const int b = tid & 7;
+    const int z = z0 + b;
+    const bool inRange = z < nz;
+    {
+        const float2* src = static_cast<const float2*>(in.data) + static_cast<long long>(f) * nz + z + in.planes * kx;
+        const long long rowStride = in.planes * in.kxStride;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = pass1_butterfly(tid, q);
+            float2 v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = inRange ? __ldg(src + rowStride * (j + 64 * r)) : make_float2(0.f, 0.f);
+            dft8<-1>(v);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) xs[b * XP + pad16(j * 8 + r)] = v[r];
+        }
+    }
+    __syncthreads();
+    direct_middle_pass<-1>(xs, tw, warp, lane);
+    __syncthreads();
+    if (!inRange) return;
+    const FieldView view = views.v[f];
+    const int* map = tables.gatherMap + static_cast<long long>(kx) * N;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = (tid >> 3) + 32 * q;
+        int e[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) e[r] = __ldg(map + j + 64 * r);
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + pad16(j + r * 64)];
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<-1>(tw, j * r));
+        dft8<-1>(v);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            if (e[r] < 0) continue;
+            float2 o = v[r];
+            o.x *= scale;
+            o.y *= (e[r] & 1) ? -scale : scale;
+            const long long i = z + view.modeStride * (e[r] >> 1);
+            if (view.im == nullptr) {
+                reinterpret_cast<float2*>(view.re)[i] = o;
+            } else {
+                reinterpret_cast<float*>(view.re)[i] = o.x;
+                reinterpret_cast<float*>(view.im)[i] = o.y;
+            }
+        }
+    }
+}
+
+constexpr size_t kDirectSmem = sizeof(float2) * 8 * kDirectRegion;
+
+constexpr int kPlanes = 8;
+
+template <int N>
+size_t smem_bytes() {
+    return sizeof(float2) * size_t(kPlanes) * plane_region<N>();
+}
+
+template <typename K>
+cudaError_t prepare(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+
+template <int N>
+cudaError_t embed_n(int nz, int columns, const ViewSet& views, const ModeTables& tables, DenseBins out,
+                    const void* tw, cudaStream_t s) {
+    auto kernel = columns_embed_warp_kernel<N, kPlanes>;
+    const size_t bytes = smem_bytes<N>();
+    cudaError_t err = prepare(kernel, bytes);
+    if (err != cudaSuccess) return err;
+    const int zChunks = (nz + kPlanes - 1) / kPlanes;
+    kernel<<<dim3(unsigned(zChunks * views.count), unsigned(columns)), 32 * kPlanes, bytes, s>>>(
+        nz, views, tables, out, static_cast<const float2*>(tw));
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t gather_n(int nz, int columns, DenseBins in, const ViewSet& views, const ModeTables& tables, double scale,
+                     const void* tw, cudaStream_t s) {
+    auto kernel = columns_gather_warp_kernel<N, kPlanes>;
+    const size_t bytes = smem_bytes<N>();
+    cudaError_t err = prepare(kernel, bytes);
+    if (err != cudaSuccess) return err;
+    const int zChunks = (nz + kPlanes - 1) / kPlanes;
+    kernel<<<dim3(unsigned(zChunks * views.count), unsigned(columns)), 32 * kPlanes, bytes, s>>>(
+        nz, in, views, tables, float(scale), static_cast<const float2*>(tw));
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool columns_warp_supported(long long ny) { return ny >= 32 && ny <= 512 && (ny & (ny - 1)) == 0; }
+
+cudaError_t launch_columns_embed_warp(int ny, int nz, int columns, const ViewSet& views, const ModeTables& tables,
+                                      DenseBins out, const void* tw, cudaStream_t s) {
+    if (views.count <= 0 || columns <= 0) return cudaSuccess;
+    switch (ny) {
+        case 32: return embed_n<32>(nz, columns, views, tables, out, tw, s);
+        case 64: return embed_n<64>(nz, columns, views, tables, out, tw, s);
+        case 128: return embed_n<128>(nz, columns, views, tables, out, tw, s);
+        case 256: return embed_n<256>(nz, columns, views, tables, out, tw, s);
+        case 512: {
+            cudaError_t err = prepare(columns_embed_direct_kernel, kDirectSmem);
+            if (err != cudaSuccess) return err;
+            const int zChunks = (nz + 7) / 8;
+            columns_embed_direct_kernel<<<dim3(unsigned(zChunks * views.count), unsigned(columns)), 256, kDirectSmem,
+                                          s>>>(nz, views, tables, out, static_cast<const float2*>(tw));
+            return cudaGetLastError();
+        }
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_columns_gather_warp(int ny, int nz, int columns, DenseBins in, const ViewSet& views,
+                                       const ModeTables& tables, double scale, const void* tw, cudaStream_t s) {
+    if (views.count <= 0 || columns <= 0) return cudaSuccess;
+    switch (ny) {
+        case 32: return gather_n<32>(nz, columns, in, views, tables, scale, tw, s);
+        case 64: return gather_n<64>(nz, columns, in, views, tables, scale, tw, s);
+        case 128: return gather_n<128>(nz, columns, in, views, tables, scale, tw, s);
+        case 256: return gather_n<256>(nz, columns, in, views, tables, scale, tw, s);
+        case 512: {
+            cudaError_t err = prepare(columns_gather_direct_kernel, kDirectSmem);
+            if (err != cudaSuccess) return err;
+            const int zChunks = (nz + 7) / 8;
+            columns_gather_direct_kernel<<<dim3(unsigned(zChunks * views.count), unsigned(columns)), 256, kDirectSmem,
+                                           s>>>(nz, in, views, tables, float(scale), static_cast<const float2*>(tw));
+            return cudaGetLastError();
+        }
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace skb

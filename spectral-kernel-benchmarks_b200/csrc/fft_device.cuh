@@ -347,4 +347,83 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Register-ended warp FFT for N in {256, 512}: the sequence enters and leaves
+// in registers, element lane + 32e in v[e] (e < N/32).  The first radix-8
+// pass reads its butterflies straight from v (butterfly j = lane + 32q needs
+// elements j + (N/8)r = lane + 32(q + Qr)), the last pass (radix 4 for 256,
+// radix 8 for 512, both with Ns = 64) writes straight back to v (butterfly j
+// produces elements j + 64r = lane + 32(q + 2r)), so only the middle pass
+// round-trips through the padded shared region x.
+template <typename T, int N, int SIGN>
+__device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const cx<T>* __restrict__ tw, int lane) {
+    using V = cx<T>;
+    static_assert(N == 256 || N == 512, "warp_fft_rr handles N = 256 and N = 512");
+    constexpr int Q = N / 256;  // radix-8 butterflies per lane in the first / middle passes
+    // Pass 1: Ns = 1, radix 8, registers -> x.
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        V b[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) b[r] = v[q + Q * r];
+        dft8<SIGN>(b);
+        const int j = lane + 32 * q;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) x[pad16(j * 8 + r)] = b[r];
+    }
+    __syncwarp();
+    // Pass 2: Ns = 8, radix 8, x -> x.
+    {
+        V b[Q][8];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+#pragma unroll
+            for (int r = 0; r < 8; ++r) b[q][r] = x[pad16(j + r * (N / 8))];
+            const int step = (j % 8) * (N / 64);
+#pragma unroll
+            for (int r = 1; r < 8; ++r) b[q][r] = cmul(b[q][r], twiddle<SIGN>(tw, step * r));
+            dft8<SIGN>(b[q]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            const int base = (j / 8) * 64 + (j % 8);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) x[pad16(base + r * 8)] = b[q][r];
+        }
+        __syncwarp();
+    }
+    // Pass 3: Ns = 64, radix N/64, x -> registers.
+    if constexpr (N == 256) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = lane + 32 * q;
+            V b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) b[r] = x[pad16(j + r * 64)];
+#pragma unroll
+            for (int r = 1; r < 4; ++r) b[r] = cmul(b[r], twiddle<SIGN>(tw, j * r));
+            dft4<SIGN>(b[0], b[1], b[2], b[3]);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) v[q + 2 * r] = b[r];
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = lane + 32 * q;
+            V b[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) b[r] = x[pad16(j + r * 64)];
+#pragma unroll
+            for (int r = 1; r < 8; ++r) b[r] = cmul(b[r], twiddle<SIGN>(tw, j * r));
+            dft8<SIGN>(b);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[q + 2 * r] = b[r];
+        }
+    }
+    __syncwarp();
+}
+
 }  // namespace skb

@@ -12,25 +12,20 @@
 // The c2r / r2c are the same half-length complex FFT formulation as the
 // staged row kernels (horizontal.cu), so both paths share their numerics.
 // Each warp owns one z-plane and transforms it with warp-synchronous passes
-// (warp_fft); every lane keeps the same Nx/64 x-pairs of its plane across all
-// transforms, which is what lets U,V,W and the product stay in registers.
+// (warp_fft; for 512-point rows warp_fft_rr, whose first and last passes work
+// in registers); every lane keeps the same Nx/64 x-pairs of its plane across
+// all transforms, which is what lets U,V,W and the product stay in registers.
 // The 3+3T slots are consumed in order, so the bins of slot f+1 are copied
 // into a second shared stage with cp.async while slot f is transformed; the
 // only CTA-wide barriers are one per slot and one per target.
 
 #include "flux_rows.hpp"
 
+#include "async_copy.cuh"
 #include "fft_device.cuh"
 
 namespace skb {
 namespace {
-
-__device__ __forceinline__ void cp_async8(void* dst, const void* src, int srcBytes) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(srcBytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Per-warp padded sequence region (pad16 of the largest index, plus slack).
 template <int M>
@@ -94,35 +89,57 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
             if (k == 0 || k == M) v.y = 0.f;
             return v;
         };
-        constexpr int pairs = M / 2 + 1;
-        for (int k = lane; k < pairs; k += 32) {
-            if (k == 0) {
-                const V x0 = load(0);
-                const V xm = load(M);
-                x[pad16(0)] = {x0.x + xm.x, x0.x - xm.x};
-                continue;
-            }
-            const int kk = M - k;
-            const V xk = load(k);
-            const V xm = load(kk);
-            {
-                const V s = cadd(xk, cconj(xm));
-                const V d = csub(xk, cconj(xm));
-                const V t = cmulc(d, __ldg(twFull + k));
-                x[pad16(k)] = {s.x - t.y, s.y + t.x};
-            }
-            if (kk != k) {
-                const V s = cadd(xm, cconj(xk));
-                const V d = csub(xm, cconj(xk));
-                const V t = cmulc(d, __ldg(twFull + kk));
-                x[pad16(kk)] = {s.x - t.y, s.y + t.x};
-            }
-        }
-        __syncwarp();
-        warp_fft<float, M, +1>(x, twHalf, lane);
+        if constexpr (M == 256) {
+            // Pre-processed half-length spectrum straight into registers
+            // (element k = lane + 32e), then the register-ended FFT.
 #pragma unroll
-        for (int e = 0; e < PER; ++e) r[e] = x[pad16(lane + 32 * e)];
-        __syncwarp();
+            for (int e = 0; e < PER; ++e) {
+                const int k = lane + 32 * e;
+                if (k == 0) {
+                    const V x0 = load(0);
+                    const V xm = load(M);
+                    r[e] = {x0.x + xm.x, x0.x - xm.x};
+                } else {
+                    const V xk = load(k);
+                    const V xm = load(M - k);
+                    const V s = cadd(xk, cconj(xm));
+                    const V d = csub(xk, cconj(xm));
+                    const V t = cmulc(d, __ldg(twFull + k));
+                    r[e] = {s.x - t.y, s.y + t.x};
+                }
+            }
+            warp_fft_rr<float, M, +1>(r, x, twHalf, lane);
+        } else {
+            constexpr int pairs = M / 2 + 1;
+            for (int k = lane; k < pairs; k += 32) {
+                if (k == 0) {
+                    const V x0 = load(0);
+                    const V xm = load(M);
+                    x[pad16(0)] = {x0.x + xm.x, x0.x - xm.x};
+                    continue;
+                }
+                const int kk = M - k;
+                const V xk = load(k);
+                const V xm = load(kk);
+                {
+                    const V s = cadd(xk, cconj(xm));
+                    const V d = csub(xk, cconj(xm));
+                    const V t = cmulc(d, __ldg(twFull + k));
+                    x[pad16(k)] = {s.x - t.y, s.y + t.x};
+                }
+                if (kk != k) {
+                    const V s = cadd(xm, cconj(xk));
+                    const V d = csub(xm, cconj(xk));
+                    const V t = cmulc(d, __ldg(twFull + kk));
+                    x[pad16(kk)] = {s.x - t.y, s.y + t.x};
+                }
+            }
+            __syncwarp();
+            warp_fft<float, M, +1>(x, twHalf, lane);
+#pragma unroll
+            for (int e = 0; e < PER; ++e) r[e] = x[pad16(lane + 32 * e)];
+            __syncwarp();
+        }
     };
 
     issue(0, stage0);
@@ -141,12 +158,19 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
         for (int e = 0; e < PER; ++e) acc[e] = {acc[e].x + v[e].x * q[e].x, acc[e].y + v[e].y * q[e].y};
         inverse_row(5 + 3 * t, q);
 #pragma unroll
-        for (int e = 0; e < PER; ++e) {
-            acc[e] = {acc[e].x + w[e].x * q[e].x, acc[e].y + w[e].y * q[e].y};
-            x[pad16(lane + 32 * e)] = {-scale * acc[e].x, -scale * acc[e].y};
+        for (int e = 0; e < PER; ++e)
+            acc[e] = {-scale * (acc[e].x + w[e].x * q[e].x), -scale * (acc[e].y + w[e].y * q[e].y)};
+        if constexpr (M == 256) {
+            warp_fft_rr<float, M, -1>(acc, x, twHalf, lane);
+#pragma unroll
+            for (int e = 0; e < PER; ++e) x[pad16(lane + 32 * e)] = acc[e];
+        } else {
+#pragma unroll
+            for (int e = 0; e < PER; ++e) x[pad16(lane + 32 * e)] = acc[e];
+            __syncwarp();
+            warp_fft<float, M, -1>(x, twHalf, lane);
         }
         __syncwarp();
-        warp_fft<float, M, -1>(x, twHalf, lane);
         // Real-spectrum split of the half-length FFT, kx < keep, into [k][b].
         const V zz = x[pad16(0)];
         for (int k = lane; k < keep; k += 32) {

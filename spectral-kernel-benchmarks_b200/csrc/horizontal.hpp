@@ -44,6 +44,8 @@ struct ModeTables {
     const int* colStart;
     const int* colKy;
     const int* colMode;
+    // gather map: map[kx*Ny + ky] = (mode << 1 | conj) for stored cells only, or -1.
+    const int* gatherMap;
 };
 
 enum class Precision { f64 = 0, f32 = 1 };

@@ -420,6 +420,7 @@ ColumnTables column_tables(const Workload& w, const std::vector<RetainedMode>& m
     ColumnTables t;
     t.activeKx = columns;
     t.cellMap.assign(columns * w.ny, -1);
+    t.gatherMap.assign(columns * w.ny, -1);
     std::vector<std::vector<std::pair<int, int>>> perColumn(columns);
     t.modeKx.resize(modes.size());
     t.modeKy.resize(modes.size());
@@ -429,6 +430,7 @@ ColumnTables column_tables(const Workload& w, const std::vector<RetainedMode>& m
         if (mode.kx >= columns || mode.ky >= w.ny) throw std::invalid_argument("retained mode outside the column band");
         const int code = static_cast<int>(m << 1) | (mode.conj ? 1 : 0);
         t.cellMap[mode.kx * w.ny + mode.ky] = code;
+        t.gatherMap[mode.kx * w.ny + mode.ky] = code;
         perColumn[mode.kx].push_back({static_cast<int>(mode.ky), code});
         t.modeKx[m] = static_cast<int>(mode.kx);
         t.modeKy[m] = static_cast<int>(mode.ky);

@@ -73,6 +73,7 @@ std::vector<double> twiddle_table(std::uint64_t n);
 struct ColumnTables {
     std::uint64_t activeKx = 0;
     std::vector<int> cellMap;   // activeKx * ny
+    std::vector<int> gatherMap;  // activeKx * ny: stored cells only (no kx = 0 partners)
     std::vector<int> colStart;  // activeKx + 1
     std::vector<int> colKy, colMode;
     std::vector<int> modeKx, modeKy;

@@ -1,5 +1,7 @@
 #include "runtime.hpp"
 
+#include "columns_warp.hpp"
+
 #include <algorithm>
 #include <cstring>
 
@@ -80,6 +82,7 @@ HorizontalPlan::HorizontalPlan(const Workload& w, Precision p, bool pruned, std:
     twFull_ = upload_real_table(twFull, p);
     twCol_ = upload_real_table(twCol, p);
     cellMap_ = upload_vector(tables.cellMap);
+    gatherMap_ = upload_vector(tables.gatherMap);
     colStart_ = upload_vector(tables.colStart);
     colKy_ = upload_vector(tables.colKy);
     colMode_ = upload_vector(tables.colMode);
@@ -89,13 +92,14 @@ HorizontalPlan::HorizontalPlan(const Workload& w, Precision p, bool pruned, std:
     const size_t binBytes = static_cast<size_t>(w.ny) * keep_ * maxPlanes * 2 * element_bytes(p);
     bins_.allocate(binBytes);
     allocationSeconds = seconds_since(allocStart);
-    persistentBytes = twHalf_.bytes() + twFull_.bytes() + twCol_.bytes() + cellMap_.bytes() + colStart_.bytes() +
+    persistentBytes = twHalf_.bytes() + twFull_.bytes() + twCol_.bytes() + cellMap_.bytes() + gatherMap_.bytes() +
+                      colStart_.bytes() +
                       colKy_.bytes() + colMode_.bytes() + modeKx_.bytes() + modeKy_.bytes() + modeConj_.bytes();
     scratchBytes = bins_.bytes();
 }
 
 ModeTables HorizontalPlan::tables() const {
-    return {cellMap_.get<int>(), colStart_.get<int>(), colKy_.get<int>(), colMode_.get<int>()};
+    return {cellMap_.get<int>(), colStart_.get<int>(), colKy_.get<int>(), colMode_.get<int>(), gatherMap_.get<int>()};
 }
 
 void HorizontalPlan::forward_rows(const void* real, std::uint64_t planes, cudaStream_t s) const {
@@ -124,6 +128,12 @@ void HorizontalPlan::inverse_columns(const ViewSet& views, cudaStream_t s) const
 
 void HorizontalPlan::inverse_columns_into(const ViewSet& views, DenseBins out, cudaStream_t s) const {
     if (out.kxStride != keep_) throw Error(-1, "bin array must hold keep() columns per row");
+    if (p_ == Precision::f32 && columns_warp_supported(static_cast<long long>(w_.ny))) {
+        check_cuda(launch_columns_embed_warp(static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, views, tables(),
+                                             out, twCol_.get(), s),
+                   "warp embedding + column c2c kernel");
+        return;
+    }
     check_cuda(launch_columns_embed(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, views, tables(), out,
                                     twCol_.get(), s),
                "embedding + column c2c kernel");
@@ -131,6 +141,12 @@ void HorizontalPlan::inverse_columns_into(const ViewSet& views, DenseBins out, c
 
 void HorizontalPlan::forward_columns_from(DenseBins in, const ViewSet& views, double scale, cudaStream_t s) const {
     if (in.kxStride != keep_) throw Error(-1, "bin array must hold keep() columns per row");
+    if (p_ == Precision::f32 && columns_warp_supported(static_cast<long long>(w_.ny))) {
+        check_cuda(launch_columns_gather_warp(static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, in, views,
+                                              tables(), scale, twCol_.get(), s),
+                   "warp column c2c + retention kernel");
+        return;
+    }
     check_cuda(launch_columns_gather(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, in, views,
                                      tables(), scale, twCol_.get(), s),
                "column c2c + retention kernel");

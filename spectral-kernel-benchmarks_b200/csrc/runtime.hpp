@@ -131,7 +131,7 @@ private:
     std::uint64_t maxPlanes_ = 0;
     std::uint64_t modeCount_ = 0;
     DeviceBuffer twHalf_, twFull_, twCol_;
-    DeviceBuffer cellMap_, colStart_, colKy_, colMode_, modeKx_, modeKy_, modeConj_;
+    DeviceBuffer cellMap_, gatherMap_, colStart_, colKy_, colMode_, modeKx_, modeKy_, modeConj_;
     DeviceBuffer bins_;
 };
 

@@ -155,6 +155,8 @@ constexpr int kEpilogueWarps = 8;
 constexpr int kPipeThreads = (kProducerWarps + 1 + kEpilogueWarps) * 32;
 constexpr int kStages = 3;
 constexpr int kAccumulators = 2;
+constexpr int kEpiStride = 17;  // floats per column row of an epilogue warp's transpose buffer
+constexpr int kEpiBytes = kEpilogueWarps * 16 * kEpiStride * 4;
 
 struct PipeState {
     uint64_t full[kStages], empty[kStages], accFull[kAccumulators], accEmpty[kAccumulators], done;
@@ -214,6 +216,19 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         tmem_alloc(smem_u32(&st->tmem), kTmemCols);
         tmem_relinquish();
     }
+    // L2 prefetch of one tile's data columns (S complex each), 128-byte lines.
+    auto prefetch_tile = [&](int t) {
+        const int tv0 = vc0 + t * 64;
+        const int tcount = min(64, vc0 + vcN - tv0);
+        const int lines = (S * 8 + 127) / 128 + 1;
+        for (int i = tid; i < tcount * lines; i += kProducerWarps * 32) {
+            const int cl = i / lines, l = i % lines;
+            const char* col = reinterpret_cast<const char*>(p.in + virtual_column(p, tv0 + cl, gcols, gfirst) * S);
+            const char* line = reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(col) & ~uintptr_t(127)) + 128 * l;
+            if (line < col + S * 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+        }
+    };
+    if (warp < kProducerWarps) prefetch_tile(0);
     // Resident group matrix, split hi/lo, zero-padded to NP x KCH*32.
     const float* Bg = p.B + static_cast<long long>(g) * R * S;
     for (int item = tid; item < NP * KCH * 8; item += kPipeThreads) {
@@ -241,46 +256,64 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
 
     if (warp < kProducerWarps) {
         // ---------------------------------------------------------- producer
-        int it = 0;
-        for (int t = 0; t < tiles && !failed; ++t) {
-            const int tv0 = vc0 + t * 64;
-            const int tcount = min(64, vc0 + vcN - tv0);
-            for (int kc = 0; kc < KCH; ++kc, ++it) {
-                const int stage = it % kStages;
-                const int round = it / kStages;
-                if (round > 0 && !mbar_wait(smem_u32(&st->empty[stage]), (round - 1) & 1, p.error)) {
-                    failed = true;
-                    break;
-                }
-                unsigned char* aHi = sA + stage * kStageBytes;
-                unsigned char* aLo = aHi + kTileRows * 128;
-                for (int item = tid; item < 64 * 8; item += kProducerWarps * 32) {
-                    const int q = item & 7;
-                    const int cl = item >> 3;
-                    float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
-                    if (cl < tcount) {
-                        const float2* src = p.in + virtual_column(p, tv0 + cl, gcols, gfirst) * S;
+        // Chunk it+1's loads are issued before chunk it is converted, so two
+        // chunks of each warp's loads are in flight.  Warp w converts columns
+        // 8w .. 8w+7 of a tile; lane = k within the chunk, so each load
+        // instruction reads one column's 32 consecutive complex values (256
+        // contiguous bytes) and each shared store fills one 128-byte row.
+        const int total = tiles * KCH;
+        long long colBase[8];
+        int loadTile = -1, loadCount = 0;
+        auto load_chunk = [&](int it, float2 (&x)[8]) {
+            const int t = it / KCH, kc = it % KCH;
+            if (t != loadTile) {
+                loadTile = t;
+                const int tv0 = vc0 + t * 64;
+                loadCount = min(64, vc0 + vcN - tv0);
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int s = kc * kChunkK + q * 4 + j;
-                            if (s < S) {
-                                const float2 x = __ldg(src + s);
-                                re[j] = x.x;
-                                im[j] = x.y;
-                            }
-                        }
-                    }
-                    const Split4 r4 = split4(re[0], re[1], re[2], re[3]);
-                    const Split4 i4 = split4(im[0], im[1], im[2], im[3]);
-                    const uint32_t o0 = sw128_offset(2 * cl, q), o1 = sw128_offset(2 * cl + 1, q);
-                    *reinterpret_cast<float4*>(aHi + o0) = r4.hi;
-                    *reinterpret_cast<float4*>(aLo + o0) = r4.lo;
-                    *reinterpret_cast<float4*>(aHi + o1) = i4.hi;
-                    *reinterpret_cast<float4*>(aLo + o1) = i4.lo;
+                for (int c = 0; c < 8; ++c) {
+                    const int cl = warp * 8 + c;
+                    colBase[c] = cl < loadCount ? virtual_column(p, tv0 + cl, gcols, gfirst) * S : 0;
                 }
-                fence_proxy_async();
-                mbar_arrive(smem_u32(&st->full[stage]));
+                // Pull the following tile's columns towards L2 meanwhile.
+                if (t + 1 < tiles) prefetch_tile(t + 1);
             }
+            const int s = kc * kChunkK + lane;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                x[c] = make_float2(0.f, 0.f);
+                if (warp * 8 + c < loadCount && s < S) x[c] = __ldg(p.in + colBase[c] + s);
+            }
+        };
+        float2 next[8];
+        load_chunk(0, next);
+        for (int it = 0; it < total && !failed; ++it) {
+            float2 x[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) x[c] = next[c];
+            if (it + 1 < total) load_chunk(it + 1, next);
+            const int stage = it % kStages;
+            const int round = it / kStages;
+            if (round > 0 && !mbar_wait(smem_u32(&st->empty[stage]), (round - 1) & 1, p.error)) {
+                failed = true;
+                break;
+            }
+            unsigned char* aHi = sA + stage * kStageBytes;
+            unsigned char* aLo = aHi + kTileRows * 128;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int cl = warp * 8 + c;
+                const float rh = tf32_rna(x[c].x), ih = tf32_rna(x[c].y);
+                const float rl = tf32_rna(x[c].x - rh), il = tf32_rna(x[c].y - ih);
+                const uint32_t o0 = sw128_offset(2 * cl, lane >> 2) + 4 * (lane & 3);
+                const uint32_t o1 = sw128_offset(2 * cl + 1, lane >> 2) + 4 * (lane & 3);
+                *reinterpret_cast<float*>(aHi + o0) = rh;
+                *reinterpret_cast<float*>(aLo + o0) = rl;
+                *reinterpret_cast<float*>(aHi + o1) = ih;
+                *reinterpret_cast<float*>(aLo + o1) = il;
+            }
+            fence_proxy_async();
+            mbar_arrive(smem_u32(&st->full[stage]));
         }
     } else if (warp == kMmaWarp) {
         // --------------------------------------------------------------- MMA
@@ -327,17 +360,23 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         // live per thread.  The final chunk's sum goes straight to global.
         const int quarter = warp & 3;  // TMEM lanes this warp may access
         const int half = (warp - kMmaWarp - 1) >> 2;
-        const int m = quarter * 32 + lane;
-        const int cl = m >> 1;
-        const int part = m & 1;
+        const int part = lane & 1;
+        float* ebuf = reinterpret_cast<float*>(st + 1) + (warp - kMmaWarp - 1) * 16 * kEpiStride;
         const uint32_t laneBase = static_cast<uint32_t>(quarter * 32) << 16;
         const uint32_t sumBase = tmem + laneBase + static_cast<uint32_t>(kAccumulators * NP + half * HALF);
         int it = 0;
         for (int t = 0; t < tiles && !failed; ++t) {
             const int tv0 = vc0 + t * 64;
             const int tcount = min(64, vc0 + vcN - tv0);
-            const bool valid = cl < tcount;
-            const long long C = valid ? virtual_column(p, tv0 + cl, gcols, gfirst) : 0;
+            // The four columns this lane stores in the transposed epilogue.
+            bool storeValid[4];
+            long long storeColumn[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int sc = quarter * 16 + 4 * k + (lane >> 3);
+                storeValid[k] = sc < tcount;
+                storeColumn[k] = storeValid[k] ? virtual_column(p, tv0 + sc, gcols, gfirst) : 0;
+            }
             for (int kc = 0; kc < KCH; ++kc, ++it) {
                 const int acc = it % kAccumulators;
                 if (!mbar_wait(smem_u32(&st->accFull[acc]), (it / kAccumulators) & 1, p.error)) {
@@ -364,13 +403,22 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                         tmem_st_x8(sumBase + blk * 8, o);
                         tmem_wait_st();
                     } else {
+                        // Transpose through this warp's shared buffer so that
+                        // each store instruction writes 64 contiguous bytes
+                        // (8 complex outputs) of four columns.
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const float y = __shfl_xor_sync(0xffffffffu, x8[j], 1);
-                            const int n = half * HALF + blk * 8 + j;
-                            if ((j & 1) == part && valid && n < R)
-                                p.out[C * R + n] = part == 0 ? make_float2(x8[j], y) : make_float2(y, x8[j]);
+                        for (int j = 0; j < 8; ++j) ebuf[(lane >> 1) * kEpiStride + 2 * j + part] = x8[j];
+                        __syncwarp();
+                        const int n = half * HALF + blk * 8 + (lane & 7);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int lc = 4 * k + (lane >> 3);
+                            if (storeValid[k] && n < R)
+                                p.out[storeColumn[k] * R + n] =
+                                    make_float2(ebuf[lc * kEpiStride + 2 * (lane & 7)],
+                                                ebuf[lc * kEpiStride + 2 * (lane & 7) + 1]);
                         }
+                        __syncwarp();
                     }
                 }
                 tc_fence_before();
@@ -389,7 +437,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
 size_t tc_gemm_smem_bytes(int R, int S) {
     const int NP = (R + 15) / 16 * 16;
     const int KCH = (S + kChunkK - 1) / kChunkK;
-    return 1024 + 2 * static_cast<size_t>(KCH) * NP * 128 + kStages * kStageBytes + sizeof(PipeState) + 16;
+    return 1024 + 2 * static_cast<size_t>(KCH) * NP * 128 + kStages * kStageBytes + sizeof(PipeState) + 16 +
+           kEpiBytes;
 }
 
 bool tc_gemm_supported(int R, int S) {
