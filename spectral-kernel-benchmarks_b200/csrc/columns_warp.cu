@@ -28,7 +28,7 @@ constexpr int plane_region() {
 }
 
 template <int N, int B>
-__global__ void __launch_bounds__(32 * B, 4) columns_embed_warp_kernel(int nz, ViewSet views, ModeTables tables,
+__global__ void __launch_bounds__(32 * B, 4) columns_embed_warp_kernel(int nz, int zStride, ViewSet views, ModeTables tables,
                                                                     DenseBins out, const float2* __restrict__ tw) {
     constexpr int NT = 32 * B;
     constexpr int XP = plane_region<N>();
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(32 * B, 4) columns_embed_warp_kernel(int nz, V
     warp_fft<float, N, +1>(xs + warp * XP, tw, lane);
     __syncthreads();
     if (z < nz) {
-        float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * nz + z + out.planes * kx;
+        float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * zStride + z + out.planes * kx;
         const long long rowStride = out.planes * out.kxStride;
 #pragma unroll
         for (int it = 0; it < ITER; ++it) {
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(32 * B, 4) columns_embed_warp_kernel(int nz, V
 }
 
 template <int N, int B>
-__global__ void __launch_bounds__(32 * B, 4) columns_gather_warp_kernel(int nz, DenseBins in, ViewSet views,
+__global__ void __launch_bounds__(32 * B, 4) columns_gather_warp_kernel(int nz, int zStride, DenseBins in, ViewSet views,
                                                                      ModeTables tables, float scale,
                                                                      const float2* __restrict__ tw) {
     constexpr int NT = 32 * B;
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(32 * B, 4) columns_gather_warp_kernel(int nz, 
     const int z = z0 + b;
     {
         const float2* src =
-            static_cast<const float2*>(in.data) + static_cast<long long>(f) * nz + z + in.planes * kx;
+            static_cast<const float2*>(in.data) + static_cast<long long>(f) * zStride + z + in.planes * kx;
         const long long rowStride = in.planes * in.kxStride;
 #pragma unroll
         for (int it = 0; it < ITER; ++it) {
@@ -160,6 +160,9 @@ __device__ __forceinline__ int pass1_butterfly(int t, int q) {
     return 4 * (h >> 1) + (h & 1) + 2 * ((t >> 3) & 1) + 32 * q;
 }
 
+// Padded addresses of the passes as per-lane bases plus compile-time offsets
+// (j < 64): pad16(8j + r) = 8j + j/2 + r, pad16(j + 64r) = j + j/16 + 68r,
+// pad16(64(j/8) + j%8 + 8r) = 68(j/8) + j%8 + 8r + r/2.
 template <int SIGN>
 __device__ __forceinline__ void direct_middle_pass(float2* xs, const float2* __restrict__ tw, int warp, int lane) {
     float2* x = xs + warp * kDirectRegion;
@@ -167,8 +170,9 @@ __device__ __forceinline__ void direct_middle_pass(float2* xs, const float2* __r
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int j = lane + 32 * q;
+        const float2* in = x + j + (j >> 4);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[q][r] = x[pad16(j + r * 64)];
+        for (int r = 0; r < 8; ++r) v[q][r] = in[68 * r];
         const int step = (j % 8) * 8;
 #pragma unroll
         for (int r = 1; r < 8; ++r) v[q][r] = cmul(v[q][r], twiddle<SIGN>(tw, step * r));
@@ -178,13 +182,13 @@ __device__ __forceinline__ void direct_middle_pass(float2* xs, const float2* __r
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int j = lane + 32 * q;
-        const int base = (j / 8) * 64 + (j % 8);
+        float2* o = x + 68 * (j / 8) + (j % 8);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) x[pad16(base + r * 8)] = v[q][r];
+        for (int r = 0; r < 8; ++r) o[8 * r + (r >> 1)] = v[q][r];
     }
 }
 
-__global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, ViewSet views, ModeTables tables,
+__global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, int zStride, ViewSet views, ModeTables tables,
                                                                       DenseBins out, const float2* __restrict__ tw) {
     constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -222,22 +226,23 @@ __global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, Vi
                 }
             }
             dft8<+1>(v);
+            float2* o = xs + b * XP + 8 * j + (j >> 1);
 #pragma unroll
-            for (int r = 0; r < 8; ++r) xs[b * XP + pad16(j * 8 + r)] = v[r];
+            for (int r = 0; r < 8; ++r) o[r] = v[r];
         }
     }
     __syncthreads();
     direct_middle_pass<+1>(xs, tw, warp, lane);
     __syncthreads();
     if (!inRange) return;
-    float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * nz + z + out.planes * kx;
+    float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * zStride + z + out.planes * kx;
     const long long rowStride = out.planes * out.kxStride;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int j = (tid >> 3) + 32 * q;
         float2 v[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + pad16(j + r * 64)];
+        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + j + (j >> 4) + 68 * r];
 #pragma unroll
         for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<+1>(tw, j * r));
         dft8<+1>(v);
@@ -246,7 +251,7 @@ __global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, Vi
     }
 }
 
-__global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, DenseBins in, ViewSet views,
+__global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, int zStride, DenseBins in, ViewSet views,
                                                                        ModeTables tables, float scale,
                                                                        const float2* __restrict__ tw) {
     constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
@@ -261,7 +266,7 @@ __global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, D
     const int z = z0 + b;
     const bool inRange = z < nz;
     {
-        const float2* src = static_cast<const float2*>(in.data) + static_cast<long long>(f) * nz + z + in.planes * kx;
+        const float2* src = static_cast<const float2*>(in.data) + static_cast<long long>(f) * zStride + z + in.planes * kx;
         const long long rowStride = in.planes * in.kxStride;
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -270,8 +275,9 @@ __global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, D
 #pragma unroll
             for (int r = 0; r < 8; ++r) v[r] = inRange ? __ldg(src + rowStride * (j + 64 * r)) : make_float2(0.f, 0.f);
             dft8<-1>(v);
+            float2* o = xs + b * XP + 8 * j + (j >> 1);
 #pragma unroll
-            for (int r = 0; r < 8; ++r) xs[b * XP + pad16(j * 8 + r)] = v[r];
+            for (int r = 0; r < 8; ++r) o[r] = v[r];
         }
     }
     __syncthreads();
@@ -288,7 +294,7 @@ __global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, D
         for (int r = 0; r < 8; ++r) e[r] = __ldg(map + j + 64 * r);
         float2 v[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + pad16(j + r * 64)];
+        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + j + (j >> 4) + 68 * r];
 #pragma unroll
         for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<-1>(tw, j * r));
         dft8<-1>(v);
@@ -325,7 +331,7 @@ cudaError_t prepare(K kernel, size_t bytes) {
 }
 
 template <int N>
-cudaError_t embed_n(int nz, int columns, const ViewSet& views, const ModeTables& tables, DenseBins out,
+cudaError_t embed_n(int nz, int zStride, int columns, const ViewSet& views, const ModeTables& tables, DenseBins out,
                     const void* tw, cudaStream_t s) {
     auto kernel = columns_embed_warp_kernel<N, kPlanes>;
     const size_t bytes = smem_bytes<N>();
@@ -333,12 +339,12 @@ cudaError_t embed_n(int nz, int columns, const ViewSet& views, const ModeTables&
     if (err != cudaSuccess) return err;
     const int zChunks = (nz + kPlanes - 1) / kPlanes;
     kernel<<<dim3(unsigned(zChunks * views.count), unsigned(columns)), 32 * kPlanes, bytes, s>>>(
-        nz, views, tables, out, static_cast<const float2*>(tw));
+        nz, zStride, views, tables, out, static_cast<const float2*>(tw));
     return cudaGetLastError();
 }
 
 template <int N>
-cudaError_t gather_n(int nz, int columns, DenseBins in, const ViewSet& views, const ModeTables& tables, double scale,
+cudaError_t gather_n(int nz, int zStride, int columns, DenseBins in, const ViewSet& views, const ModeTables& tables, double scale,
                      const void* tw, cudaStream_t s) {
     auto kernel = columns_gather_warp_kernel<N, kPlanes>;
     const size_t bytes = smem_bytes<N>();
@@ -346,7 +352,241 @@ cudaError_t gather_n(int nz, int columns, DenseBins in, const ViewSet& views, co
     if (err != cudaSuccess) return err;
     const int zChunks = (nz + kPlanes - 1) / kPlanes;
     kernel<<<dim3(unsigned(zChunks * views.count), unsigned(columns)), 32 * kPlanes, bytes, s>>>(
-        nz, in, views, tables, float(scale), static_cast<const float2*>(tw));
+        nz, zStride, in, views, tables, float(scale), static_cast<const float2*>(tw));
+    return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Band forms for the fused flux, in place on the dense bin array.  The
+// retained cells of column kx (with their kx = 0 Hermitian partners) are
+// exactly the band min(ky, Ny - ky) <= band[kx] (checked on the host), and the
+// vertical GEMM reads and writes the retained values at their cells directly,
+// so these kernels need no mode map: the inverse reads the band cells (the
+// rest of the column is zero) and writes the whole column; the forward reads
+// the whole column and writes back only the band cells.  Slot f's planes start
+// at plane f * zStride.
+__device__ __forceinline__ bool in_band(int ky, int n, int band) { return min(ky, n - ky) <= band; }
+
+__global__ void __launch_bounds__(256, 3) columns_inverse_band_kernel(int nz, int zStride, DenseBins bins,
+                                                                      const int* __restrict__ bandOf,
+                                                                      const float2* __restrict__ tw) {
+    constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int zChunks = (nz + B - 1) / B;
+    const int f = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int kx = blockIdx.y;
+    const int b = tid & 7;
+    const int z = z0 + b;
+    const bool inRange = z < nz;
+    const int band = __ldg(bandOf + kx);
+    float2* col = static_cast<float2*>(bins.data) + static_cast<long long>(f) * zStride + z + bins.planes * kx;
+    const long long rowStride = bins.planes * bins.kxStride;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = pass1_butterfly(tid, q);
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int ky = j + 64 * r;
+            v[r] = (inRange && in_band(ky, N, band)) ? col[rowStride * ky] : make_float2(0.f, 0.f);
+        }
+        dft8<+1>(v);
+        float2* o = xs + b * XP + 8 * j + (j >> 1);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) o[r] = v[r];
+    }
+    __syncthreads();
+    direct_middle_pass<+1>(xs, tw, warp, lane);
+    __syncthreads();
+    if (!inRange) return;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = (tid >> 3) + 32 * q;
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + j + (j >> 4) + 68 * r];
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<+1>(tw, j * r));
+        dft8<+1>(v);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) col[rowStride * (j + 64 * r)] = v[r];
+    }
+}
+
+__global__ void __launch_bounds__(256, 3) columns_forward_band_kernel(int nz, int zStride, DenseBins bins,
+                                                                      const int* __restrict__ bandOf, float scale,
+                                                                      const float2* __restrict__ tw) {
+    constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int zChunks = (nz + B - 1) / B;
+    const int f = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int kx = blockIdx.y;
+    const int b = tid & 7;
+    const int z = z0 + b;
+    const bool inRange = z < nz;
+    float2* col = static_cast<float2*>(bins.data) + static_cast<long long>(f) * zStride + z + bins.planes * kx;
+    const long long rowStride = bins.planes * bins.kxStride;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = pass1_butterfly(tid, q);
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = inRange ? col[rowStride * (j + 64 * r)] : make_float2(0.f, 0.f);
+        dft8<-1>(v);
+        float2* o = xs + b * XP + 8 * j + (j >> 1);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) o[r] = v[r];
+    }
+    __syncthreads();
+    direct_middle_pass<-1>(xs, tw, warp, lane);
+    __syncthreads();
+    if (!inRange) return;
+    const int band = __ldg(bandOf + kx);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = (tid >> 3) + 32 * q;
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + j + (j >> 4) + 68 * r];
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<-1>(tw, j * r));
+        dft8<-1>(v);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int ky = j + 64 * r;
+            if (in_band(ky, N, band)) col[rowStride * ky] = make_float2(scale * v[r].x, scale * v[r].y);
+        }
+    }
+}
+
+// Generic-N band forms (warp per plane, cp.async staging).
+template <int N, int B>
+__global__ void __launch_bounds__(32 * B, 4) columns_inverse_band_warp_kernel(int nz, int zStride, DenseBins bins,
+                                                                              const int* __restrict__ bandOf,
+                                                                              const float2* __restrict__ tw) {
+    constexpr int NT = 32 * B;
+    constexpr int XP = plane_region<N>();
+    constexpr int ITER = N * B / NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int zChunks = (nz + B - 1) / B;
+    const int f = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int kx = blockIdx.y;
+    const int b = tid % B;
+    const int z = z0 + b;
+    const bool inRange = z < nz;
+    const int band = __ldg(bandOf + kx);
+    float2* col = static_cast<float2*>(bins.data) + static_cast<long long>(f) * zStride + z + bins.planes * kx;
+    const long long rowStride = bins.planes * bins.kxStride;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int ky = (tid + it * NT) / B;
+        const bool have = inRange && in_band(ky, N, band);
+        cp_async8(xs + b * XP + pad16(ky), have ? col + rowStride * ky : col, have ? 8 : 0);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    warp_fft<float, N, +1>(xs + warp * XP, tw, lane);
+    __syncthreads();
+    if (!inRange) return;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int ky = (tid + it * NT) / B;
+        col[rowStride * ky] = xs[b * XP + pad16(ky)];
+    }
+}
+
+template <int N, int B>
+__global__ void __launch_bounds__(32 * B, 4) columns_forward_band_warp_kernel(int nz, int zStride, DenseBins bins,
+                                                                              const int* __restrict__ bandOf,
+                                                                              float scale,
+                                                                              const float2* __restrict__ tw) {
+    constexpr int NT = 32 * B;
+    constexpr int XP = plane_region<N>();
+    constexpr int ITER = N * B / NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int zChunks = (nz + B - 1) / B;
+    const int f = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int kx = blockIdx.y;
+    const int b = tid % B;
+    const int z = z0 + b;
+    const bool inRange = z < nz;
+    float2* col = static_cast<float2*>(bins.data) + static_cast<long long>(f) * zStride + z + bins.planes * kx;
+    const long long rowStride = bins.planes * bins.kxStride;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int ky = (tid + it * NT) / B;
+        cp_async8(xs + b * XP + pad16(ky), inRange ? col + rowStride * ky : col, inRange ? 8 : 0);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    warp_fft<float, N, -1>(xs + warp * XP, tw, lane);
+    __syncthreads();
+    if (!inRange) return;
+    const int band = __ldg(bandOf + kx);
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int ky = (tid + it * NT) / B;
+        if (in_band(ky, N, band)) {
+            const float2 v = xs[b * XP + pad16(ky)];
+            col[rowStride * ky] = make_float2(scale * v.x, scale * v.y);
+        }
+    }
+}
+
+template <int N>
+cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, const void* tw,
+                           cudaStream_t s) {
+    constexpr int B = 8;
+    const int zChunks = (nz + B - 1) / B;
+    const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
+    if constexpr (N == kDirectN) {
+        cudaError_t err = prepare(columns_inverse_band_kernel, kDirectSmem);
+        if (err != cudaSuccess) return err;
+        columns_inverse_band_kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band,
+                                                                    static_cast<const float2*>(tw));
+    } else {
+        auto kernel = columns_inverse_band_warp_kernel<N, B>;
+        const size_t bytes = sizeof(float2) * size_t(B) * plane_region<N>();
+        cudaError_t err = prepare(kernel, bytes);
+        if (err != cudaSuccess) return err;
+        kernel<<<grid, 32 * B, bytes, s>>>(nz, zStride, bins, band, static_cast<const float2*>(tw));
+    }
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t forward_band_n(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, double scale,
+                           const void* tw, cudaStream_t s) {
+    constexpr int B = 8;
+    const int zChunks = (nz + B - 1) / B;
+    const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
+    if constexpr (N == kDirectN) {
+        cudaError_t err = prepare(columns_forward_band_kernel, kDirectSmem);
+        if (err != cudaSuccess) return err;
+        columns_forward_band_kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band, float(scale),
+                                                                    static_cast<const float2*>(tw));
+    } else {
+        auto kernel = columns_forward_band_warp_kernel<N, B>;
+        const size_t bytes = sizeof(float2) * size_t(B) * plane_region<N>();
+        cudaError_t err = prepare(kernel, bytes);
+        if (err != cudaSuccess) return err;
+        kernel<<<grid, 32 * B, bytes, s>>>(nz, zStride, bins, band, float(scale), static_cast<const float2*>(tw));
+    }
     return cudaGetLastError();
 }
 
@@ -354,42 +594,72 @@ cudaError_t gather_n(int nz, int columns, DenseBins in, const ViewSet& views, co
 
 bool columns_warp_supported(long long ny) { return ny >= 32 && ny <= 512 && (ny & (ny - 1)) == 0; }
 
-cudaError_t launch_columns_embed_warp(int ny, int nz, int columns, const ViewSet& views, const ModeTables& tables,
+cudaError_t launch_columns_embed_warp(int ny, int nz, int zStride, int columns, const ViewSet& views, const ModeTables& tables,
                                       DenseBins out, const void* tw, cudaStream_t s) {
     if (views.count <= 0 || columns <= 0) return cudaSuccess;
     switch (ny) {
-        case 32: return embed_n<32>(nz, columns, views, tables, out, tw, s);
-        case 64: return embed_n<64>(nz, columns, views, tables, out, tw, s);
-        case 128: return embed_n<128>(nz, columns, views, tables, out, tw, s);
-        case 256: return embed_n<256>(nz, columns, views, tables, out, tw, s);
+        case 32: return embed_n<32>(nz, zStride, columns, views, tables, out, tw, s);
+        case 64: return embed_n<64>(nz, zStride, columns, views, tables, out, tw, s);
+        case 128: return embed_n<128>(nz, zStride, columns, views, tables, out, tw, s);
+        case 256: return embed_n<256>(nz, zStride, columns, views, tables, out, tw, s);
         case 512: {
             cudaError_t err = prepare(columns_embed_direct_kernel, kDirectSmem);
             if (err != cudaSuccess) return err;
             const int zChunks = (nz + 7) / 8;
             columns_embed_direct_kernel<<<dim3(unsigned(zChunks * views.count), unsigned(columns)), 256, kDirectSmem,
-                                          s>>>(nz, views, tables, out, static_cast<const float2*>(tw));
+                                          s>>>(nz, zStride, views, tables, out, static_cast<const float2*>(tw));
             return cudaGetLastError();
         }
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_columns_gather_warp(int ny, int nz, int columns, DenseBins in, const ViewSet& views,
+cudaError_t launch_columns_gather_warp(int ny, int nz, int zStride, int columns, DenseBins in, const ViewSet& views,
                                        const ModeTables& tables, double scale, const void* tw, cudaStream_t s) {
     if (views.count <= 0 || columns <= 0) return cudaSuccess;
     switch (ny) {
-        case 32: return gather_n<32>(nz, columns, in, views, tables, scale, tw, s);
-        case 64: return gather_n<64>(nz, columns, in, views, tables, scale, tw, s);
-        case 128: return gather_n<128>(nz, columns, in, views, tables, scale, tw, s);
-        case 256: return gather_n<256>(nz, columns, in, views, tables, scale, tw, s);
+        case 32: return gather_n<32>(nz, zStride, columns, in, views, tables, scale, tw, s);
+        case 64: return gather_n<64>(nz, zStride, columns, in, views, tables, scale, tw, s);
+        case 128: return gather_n<128>(nz, zStride, columns, in, views, tables, scale, tw, s);
+        case 256: return gather_n<256>(nz, zStride, columns, in, views, tables, scale, tw, s);
         case 512: {
             cudaError_t err = prepare(columns_gather_direct_kernel, kDirectSmem);
             if (err != cudaSuccess) return err;
             const int zChunks = (nz + 7) / 8;
             columns_gather_direct_kernel<<<dim3(unsigned(zChunks * views.count), unsigned(columns)), 256, kDirectSmem,
-                                           s>>>(nz, in, views, tables, float(scale), static_cast<const float2*>(tw));
+                                           s>>>(nz, zStride, in, views, tables, float(scale), static_cast<const float2*>(tw));
             return cudaGetLastError();
         }
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace skb
+
+namespace skb {
+
+cudaError_t launch_columns_inverse_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
+                                        const int* band, const void* tw, cudaStream_t s) {
+    if (slots <= 0 || columns <= 0) return cudaSuccess;
+    switch (ny) {
+        case 32: return inverse_band_n<32>(nz, zStride, slots, columns, bins, band, tw, s);
+        case 64: return inverse_band_n<64>(nz, zStride, slots, columns, bins, band, tw, s);
+        case 128: return inverse_band_n<128>(nz, zStride, slots, columns, bins, band, tw, s);
+        case 256: return inverse_band_n<256>(nz, zStride, slots, columns, bins, band, tw, s);
+        case 512: return inverse_band_n<512>(nz, zStride, slots, columns, bins, band, tw, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_columns_forward_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
+                                        const int* band, double scale, const void* tw, cudaStream_t s) {
+    if (slots <= 0 || columns <= 0) return cudaSuccess;
+    switch (ny) {
+        case 32: return forward_band_n<32>(nz, zStride, slots, columns, bins, band, scale, tw, s);
+        case 64: return forward_band_n<64>(nz, zStride, slots, columns, bins, band, scale, tw, s);
+        case 128: return forward_band_n<128>(nz, zStride, slots, columns, bins, band, scale, tw, s);
+        case 256: return forward_band_n<256>(nz, zStride, slots, columns, bins, band, scale, tw, s);
+        case 512: return forward_band_n<512>(nz, zStride, slots, columns, bins, band, scale, tw, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -10,10 +10,21 @@ namespace skb {
 
 // Power-of-two Ny in [32, 512].
 bool columns_warp_supported(long long ny);
-// Same contracts as launch_columns_embed / launch_columns_gather for FP32.
-cudaError_t launch_columns_embed_warp(int ny, int nz, int columns, const ViewSet& views, const ModeTables& tables,
+// Same contracts as launch_columns_embed / launch_columns_gather for FP32,
+// except that view f's planes start at bin plane f * zStride (zStride >= nz;
+// padding planes are neither read nor written).
+cudaError_t launch_columns_embed_warp(int ny, int nz, int zStride, int columns, const ViewSet& views, const ModeTables& tables,
                                       DenseBins out, const void* tw, cudaStream_t s);
-cudaError_t launch_columns_gather_warp(int ny, int nz, int columns, DenseBins in, const ViewSet& views,
+cudaError_t launch_columns_gather_warp(int ny, int nz, int zStride, int columns, DenseBins in, const ViewSet& views,
                                        const ModeTables& tables, double scale, const void* tw, cudaStream_t s);
+
+// Band forms, in place on dense bins [ky][kx < columns][plane] (plane of slot
+// f: f * zStride + z): band[kx] bounds the retained cells of column kx
+// (min(ky, Ny - ky) <= band[kx]).  Inverse: band cells in, whole column out.
+// Forward: whole column in, band cells (times scale) out.
+cudaError_t launch_columns_inverse_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
+                                        const int* band, const void* tw, cudaStream_t s);
+cudaError_t launch_columns_forward_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
+                                        const int* band, double scale, const void* tw, cudaStream_t s);
 
 }  // namespace skb

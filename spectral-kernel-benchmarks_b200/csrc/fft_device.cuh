@@ -360,6 +360,11 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
     using V = cx<T>;
     static_assert(N == 256 || N == 512, "warp_fft_rr handles N = 256 and N = 512");
     constexpr int Q = N / 256;  // radix-8 butterflies per lane in the first / middle passes
+    // Padded addresses as per-lane bases plus compile-time offsets (j < 64,
+    // BF = N/8 a multiple of 16):
+    //   pad16(8j + r)                = 8j + j/2 + r
+    //   pad16(j + BF r)              = j + j/16 + (BF + BF/16) r
+    //   pad16(64(j/8) + j%8 + 8r)    = 68(j/8) + j%8 + 8r + r/2
     // Pass 1: Ns = 1, radix 8, registers -> x.
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -368,8 +373,9 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
         for (int r = 0; r < 8; ++r) b[r] = v[q + Q * r];
         dft8<SIGN>(b);
         const int j = lane + 32 * q;
+        V* o = x + 8 * j + (j >> 1);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) x[pad16(j * 8 + r)] = b[r];
+        for (int r = 0; r < 8; ++r) o[r] = b[r];
     }
     __syncwarp();
     // Pass 2: Ns = 8, radix 8, x -> x.
@@ -378,8 +384,9 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = lane + 32 * q;
+            const V* in = x + j + (j >> 4);
 #pragma unroll
-            for (int r = 0; r < 8; ++r) b[q][r] = x[pad16(j + r * (N / 8))];
+            for (int r = 0; r < 8; ++r) b[q][r] = in[(N / 8 + N / 128) * r];
             const int step = (j % 8) * (N / 64);
 #pragma unroll
             for (int r = 1; r < 8; ++r) b[q][r] = cmul(b[q][r], twiddle<SIGN>(tw, step * r));
@@ -389,39 +396,30 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = lane + 32 * q;
-            const int base = (j / 8) * 64 + (j % 8);
+            V* o = x + 68 * (j / 8) + (j % 8);
 #pragma unroll
-            for (int r = 0; r < 8; ++r) x[pad16(base + r * 8)] = b[q][r];
+            for (int r = 0; r < 8; ++r) o[8 * r + (r >> 1)] = b[q][r];
         }
         __syncwarp();
     }
     // Pass 3: Ns = 64, radix N/64, x -> registers.
-    if constexpr (N == 256) {
+    constexpr int R3 = N / 64;
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int j = lane + 32 * q;
-            V b[4];
+    for (int q = 0; q < 2; ++q) {
+        const int j = lane + 32 * q;
+        const V* in = x + j + (j >> 4);
+        V b[R3];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) b[r] = x[pad16(j + r * 64)];
+        for (int r = 0; r < R3; ++r) b[r] = in[68 * r];
 #pragma unroll
-            for (int r = 1; r < 4; ++r) b[r] = cmul(b[r], twiddle<SIGN>(tw, j * r));
+        for (int r = 1; r < R3; ++r) b[r] = cmul(b[r], twiddle<SIGN>(tw, j * r));
+        if constexpr (R3 == 4) {
             dft4<SIGN>(b[0], b[1], b[2], b[3]);
-#pragma unroll
-            for (int r = 0; r < 4; ++r) v[q + 2 * r] = b[r];
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int j = lane + 32 * q;
-            V b[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) b[r] = x[pad16(j + r * 64)];
-#pragma unroll
-            for (int r = 1; r < 8; ++r) b[r] = cmul(b[r], twiddle<SIGN>(tw, j * r));
+        } else {
             dft8<SIGN>(b);
-#pragma unroll
-            for (int r = 0; r < 8; ++r) v[q + 2 * r] = b[r];
         }
+#pragma unroll
+        for (int r = 0; r < R3; ++r) v[q + 2 * r] = b[r];
     }
     __syncwarp();
 }

@@ -38,7 +38,7 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
     const std::uint64_t binPlanes = fused_ ? cfg.members * cfg.nz * (fieldsIn_ + cfg.targets) : maxPlanes;
     std::uint64_t need = 2 * es * cfg.members * modes_ * cfg.nz * (fieldsIn_ + cfg.targets)  // physIn, physOut
                          + (fused_ ? 0 : es * volume_ * cfg.members * 7)                   // 3+3+1 volumes
-                         + 2 * es * cfg.n * (cfg.n / 2 + 1) * binPlanes;                   // bin scratch bound
+                         + 2 * es * cfg.n * (cfg.n / 2 + 1) * binPlanes * 9 / 8;           // bin scratch bound
     size_t freeBytes = 0, totalBytes = 0;
     check_cuda(cudaMemGetInfo(&freeBytes, &totalBytes), "cudaMemGetInfo");
     if (need > freeBytes)
@@ -50,12 +50,39 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
                                                   fieldsIn_, cfg.members, fam.inverse);
     forwardGemm_ = std::make_unique<VerticalPlan>(gp, static_cast<int>(nj_), static_cast<int>(cfg.nz), groups,
                                                   cfg.targets, cfg.members, fam.forward);
-    physIn_.allocate(2 * es * cfg.members * modes_ * fieldsIn_ * cfg.nz);
-    physOut_.allocate(2 * es * cfg.members * modes_ * cfg.targets * cfg.nz);
+    dense_ = fused_ && horizontal_->band_exact();
+    if (!dense_) {
+        physIn_.allocate(2 * es * cfg.members * modes_ * fieldsIn_ * cfg.nz);
+        physOut_.allocate(2 * es * cfg.members * modes_ * cfg.targets * cfg.nz);
+    }
     if (fused_) {
+        // Bin planes per slot padded to a multiple of 8 (64 bytes of FP32
+        // complex), so every 8-plane run a column or row CTA moves starts on a
+        // 64-byte boundary.
+        zStride_ = (cfg.nz + 7) / 8 * 8;
         const std::uint64_t keep = static_cast<std::uint64_t>(horizontal_->keep());
-        binsIn_.allocate(2 * es * cfg.n * keep * cfg.members * fieldsIn_ * cfg.nz);
-        binsOut_.allocate(2 * es * cfg.n * keep * cfg.members * cfg.targets * cfg.nz);
+        binsIn_.allocate(2 * es * cfg.n * keep * cfg.members * fieldsIn_ * zStride_);
+        binsOut_.allocate(2 * es * cfg.n * keep * cfg.members * cfg.targets * zStride_);
+        if (dense_) {
+            const long long inStored = static_cast<long long>(cfg.members * fieldsIn_ * zStride_);
+            const long long outStored = static_cast<long long>(cfg.members * cfg.targets * zStride_);
+            std::vector<long long> cellIn(modes_), partnerIn(modes_), cellOut(modes_);
+            std::vector<unsigned char> conj(modes_);
+            for (std::uint64_t m = 0; m < modes_; ++m) {
+                const auto& md = modes[m];
+                const long long cell = static_cast<long long>(md.ky * keep + md.kx);
+                cellIn[m] = cell * inStored;
+                cellOut[m] = cell * outStored;
+                partnerIn[m] = (md.kx == 0 && md.ky != 0 && 2 * md.ky != cfg.n)
+                                   ? static_cast<long long>((cfg.n - md.ky) * keep) * inStored
+                                   : -1;
+                conj[m] = md.conj ? 1 : 0;
+            }
+            cellIn_ = upload_vector(cellIn);
+            partnerIn_ = upload_vector(partnerIn);
+            cellOut_ = upload_vector(cellOut);
+            modeConj_ = upload_vector(conj);
+        }
     } else {
         shared_.allocate(es * 3 * cfg.members * volume_);
         deriv_.allocate(es * 3 * cfg.members * volume_);
@@ -146,42 +173,65 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
     const double gemmOut = double(M) * H * T * (nj_ + nz) * ces + forwardGemm_->matrixBytes();
     const long long inPlanes = static_cast<long long>(M * fieldsIn_ * nz);
     const long long outPlanes = static_cast<long long>(M * T * nz);
-
-    inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s, M);
-    if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
-
-    ViewSet inViews{};
-    inViews.count = static_cast<int>(M * fieldsIn_);
-    for (std::uint64_t m = 0; m < M; ++m)
-        for (std::uint64_t f = 0; f < fieldsIn_; ++f)
-            inViews.v[m * fieldsIn_ + f] = {physIn + ces * ((m * H * fieldsIn_ + f) * nz), nullptr,
-                                            static_cast<long long>(fieldsIn_ * nz)};
-    const DenseBins binsIn{binsIn_.get(), inPlanes, keep};
-    horizontal_->inverse_columns_into(inViews, binsIn, s);
-    if (rec) rec->end("columns_inverse_embed", 1, double(inPlanes) * (compactPlane + binsPlane), 0.0);
+    // Stored planes (stride between kx in the bin arrays) include the z-padding.
+    const long long inStored = static_cast<long long>(cfg_.members * fieldsIn_ * zStride_);
+    const long long outStored = static_cast<long long>(cfg_.members * T * zStride_);
+    const DenseBins binsIn{binsIn_.get(), inStored, keep};
+    const DenseBins binsOutArr{binsOut_.get(), outStored, keep};
+    if (dense_) {
+        // GEMM -> retained cells of binsIn -> in-place inverse columns.
+        BinBoundary out{cellIn_.get<long long>(), partnerIn_.get<long long>(), modeConj_.get<unsigned char>(),
+                        static_cast<int>(fieldsIn_), static_cast<int>(zStride_)};
+        inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {binsIn_.get(), nullptr}, s, M, nullptr, &out);
+        if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
+        horizontal_->inverse_columns_band(binsIn, static_cast<int>(M * fieldsIn_), static_cast<int>(zStride_), s);
+        if (rec) rec->end("columns_inverse_embed", 1, double(inPlanes) * (compactPlane + binsPlane), 0.0);
+    } else {
+        inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s, M);
+        if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
+        ViewSet inViews{};
+        inViews.count = static_cast<int>(M * fieldsIn_);
+        for (std::uint64_t m = 0; m < M; ++m)
+            for (std::uint64_t f = 0; f < fieldsIn_; ++f)
+                inViews.v[m * fieldsIn_ + f] = {physIn + ces * ((m * H * fieldsIn_ + f) * nz), nullptr,
+                                                static_cast<long long>(fieldsIn_ * nz)};
+        horizontal_->inverse_columns_into(inViews, binsIn, s, static_cast<int>(zStride_));
+        if (rec) rec->end("columns_inverse_embed", 1, double(inPlanes) * (compactPlane + binsPlane), 0.0);
+    }
 
     RowFluxArgs a{};
     a.nx = static_cast<int>(cfg_.n);
     a.ny = static_cast<int>(cfg_.n);
     a.nz = static_cast<int>(nz);
+    a.zStride = static_cast<int>(zStride_);
     a.keep = static_cast<int>(keep);
     a.members = static_cast<int>(M);
     a.fieldsIn = static_cast<int>(fieldsIn_);
     a.targets = static_cast<int>(T);
     a.scale = static_cast<float>(1.0 / (n * n * n * n));
     a.binsIn = binsIn;
-    a.binsOut = {binsOut_.get(), outPlanes, keep};
+    a.binsOut = binsOutArr;
     a.twHalf = horizontal_->twiddlesHalf();
     a.twFull = horizontal_->twiddlesFull();
     check_cuda(launch_rows_flux(a, s), "fused row flux kernel");
     if (rec) rec->end("rows_flux_fused", 1, double(inPlanes + outPlanes) * binsPlane, 0.0);
 
+    if (dense_) {
+        // In-place forward columns keep the retained cells; the GEMM reads them there.
+        horizontal_->forward_columns_band(binsOutArr, static_cast<int>(M * T), 1.0, static_cast<int>(zStride_), s);
+        if (rec) rec->end("columns_forward_gather", 1, double(outPlanes) * (binsPlane + compactPlane), 0.0);
+        BinBoundary in{cellOut_.get<long long>(), nullptr, modeConj_.get<unsigned char>(), static_cast<int>(T),
+                       static_cast<int>(zStride_)};
+        forwardGemm_->execute({binsOut_.get(), nullptr}, {modalOut, nullptr}, s, M, &in, nullptr);
+        if (rec) rec->end("gemm_forward_tf32x3", 1, gemmOut, 3.0 * 4.0 * nz * nj_ * double(M) * H * T);
+        return;
+    }
     ViewSet outViews{};
     outViews.count = static_cast<int>(M * T);
     for (std::uint64_t m = 0; m < M; ++m)
         for (std::uint64_t t = 0; t < T; ++t)
             outViews.v[m * T + t] = {physOut + ces * ((m * H * T + t) * nz), nullptr, static_cast<long long>(T * nz)};
-    horizontal_->forward_columns_from(a.binsOut, outViews, 1.0, s);
+    horizontal_->forward_columns_from(a.binsOut, outViews, 1.0, s, static_cast<int>(zStride_));
     if (rec) rec->end("columns_forward_gather", 1, double(outPlanes) * (binsPlane + compactPlane), 0.0);
 
     forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s, M);

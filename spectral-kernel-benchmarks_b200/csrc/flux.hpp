@@ -79,7 +79,14 @@ private:
     // Fused split-precision path: column-transformed bins of every input slot
     // and of every target.
     bool fused_ = false;
+    std::uint64_t zStride_ = 0;  // bin planes per slot (Nz padded to a multiple of 8)
     DeviceBuffer binsIn_, binsOut_;
+    // Dense boundary: the GEMMs read / write the retained values at their
+    // cells of the bin arrays (no compact intermediate, no mode map in the
+    // column kernels).  Per mode: cell offsets in binsIn_ (with the kx = 0
+    // partner) and in binsOut_, and the conjugation flag.
+    bool dense_ = false;
+    DeviceBuffer cellIn_, partnerIn_, cellOut_, modeConj_;
     std::uint64_t launches_ = 0;
     struct Recorder;
     void runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
     // [b][k]; consecutive threads read consecutive planes of one kx (the
     // planes-innermost global rows), planes beyond Nz are zero-filled.
     auto issue = [&](int f, V* stage) {
-        const long long pBase = (static_cast<long long>(member) * a.fieldsIn + f) * a.nz + z0;
+        const long long pBase = (static_cast<long long>(member) * a.fieldsIn + f) * a.zStride + z0;
         const long long rowBase = a.binsIn.kxStride * y;
         for (int idx = tid; idx < keep * B; idx += NT) {
             const int b = idx % B;
@@ -162,8 +162,10 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
             acc[e] = {-scale * (acc[e].x + w[e].x * q[e].x), -scale * (acc[e].y + w[e].y * q[e].y)};
         if constexpr (M == 256) {
             warp_fft_rr<float, M, -1>(acc, x, twHalf, lane);
+            // pad16(lane + 32e) = lane + lane/16 + 34e
+            V* o = x + lane + (lane >> 4);
 #pragma unroll
-            for (int e = 0; e < PER; ++e) x[pad16(lane + 32 * e)] = acc[e];
+            for (int e = 0; e < PER; ++e) o[34 * e] = acc[e];
         } else {
 #pragma unroll
             for (int e = 0; e < PER; ++e) x[pad16(lane + 32 * e)] = acc[e];
@@ -191,7 +193,7 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
         }
         __syncthreads();
         // Coalesced rows of B planes per kx.
-        const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.nz + z0;
+        const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.zStride + z0;
         for (int idx = tid; idx < keep * B; idx += NT) {
             const int b = idx % B;
             const int k = idx / B;
@@ -221,7 +223,7 @@ cudaError_t launch_m(const RowFluxArgs& a, dim3 grid, cudaStream_t stream) {
 cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
     const int M = a.nx / 2;
     constexpr int B = 8;
-    if (a.keep < 1 || a.keep > M + 1 || a.fieldsIn != 3 + 3 * a.targets) return cudaErrorInvalidValue;
+    if (a.keep < 1 || a.keep > M + 1 || a.fieldsIn != 3 + 3 * a.targets || a.zStride < a.nz) return cudaErrorInvalidValue;
     const int zChunks = (a.nz + B - 1) / B;
     dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
     switch (M) {

@@ -9,10 +9,11 @@ namespace skb {
 
 struct RowFluxArgs {
     int nx, ny, nz, keep;
+    int zStride;          // bin planes per slot (>= nz; z-padding keeps each slot's planes 64-byte aligned)
     int members, fieldsIn, targets;
     float scale;          // 1/(Nx*Ny)^2 (benchmark.cpp:4040-4041)
-    DenseBins binsIn;     // column-transformed input slots, plane (member*fieldsIn + slot)*nz + z
-    DenseBins binsOut;    // target bins, plane (member*targets + t)*nz + z
+    DenseBins binsIn;     // column-transformed input slots, plane (member*fieldsIn + slot)*zStride + z
+    DenseBins binsOut;    // target bins, plane (member*targets + t)*zStride + z
     const void* twHalf;   // exp(-2 pi i k/(nx/2)), float2
     const void* twFull;   // exp(-2 pi i k/nx), float2
 };

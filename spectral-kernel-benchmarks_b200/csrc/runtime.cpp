@@ -91,6 +91,25 @@ HorizontalPlan::HorizontalPlan(const Workload& w, Precision p, bool pruned, std:
     modeConj_ = upload_vector(tables.modeConj);
     const size_t binBytes = static_cast<size_t>(w.ny) * keep_ * maxPlanes * 2 * element_bytes(p);
     bins_.allocate(binBytes);
+    {
+        // Per-column band of the retained cells, and whether it is exact.
+        std::vector<int> band(static_cast<size_t>(keep_), -1);
+        for (int kx = 0; kx < keep_; ++kx)
+            for (std::uint64_t ky = 0; ky < w.ny; ++ky)
+                if (tables.cellMap[kx * w.ny + ky] >= 0)
+                    band[kx] = std::max(band[kx], static_cast<int>(std::min<std::uint64_t>(ky, w.ny - ky)));
+        bandExact_ = true;
+        for (int kx = 0; kx < keep_ && bandExact_; ++kx)
+            for (std::uint64_t ky = 0; ky < w.ny; ++ky) {
+                const bool cell = tables.cellMap[kx * w.ny + ky] >= 0;
+                const bool inBand = static_cast<int>(std::min<std::uint64_t>(ky, w.ny - ky)) <= band[kx];
+                if (cell != inBand) {
+                    bandExact_ = false;
+                    break;
+                }
+            }
+        band_ = upload_vector(band);
+    }
     allocationSeconds = seconds_since(allocStart);
     persistentBytes = twHalf_.bytes() + twFull_.bytes() + twCol_.bytes() + cellMap_.bytes() + gatherMap_.bytes() +
                       colStart_.bytes() +
@@ -126,30 +145,53 @@ void HorizontalPlan::inverse_columns(const ViewSet& views, cudaStream_t s) const
                "embedding + column c2c kernel");
 }
 
-void HorizontalPlan::inverse_columns_into(const ViewSet& views, DenseBins out, cudaStream_t s) const {
+void HorizontalPlan::inverse_columns_into(const ViewSet& views, DenseBins out, cudaStream_t s, int zStride) const {
     if (out.kxStride != keep_) throw Error(-1, "bin array must hold keep() columns per row");
+    const int nz = static_cast<int>(w_.nz);
+    if (zStride == 0) zStride = nz;
     if (p_ == Precision::f32 && columns_warp_supported(static_cast<long long>(w_.ny))) {
-        check_cuda(launch_columns_embed_warp(static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, views, tables(),
-                                             out, twCol_.get(), s),
+        check_cuda(launch_columns_embed_warp(static_cast<int>(w_.ny), nz, zStride, keep_, views, tables(), out,
+                                             twCol_.get(), s),
                    "warp embedding + column c2c kernel");
         return;
     }
+    if (zStride != nz) throw Error(-3, "padded bin planes need the FP32 warp column kernels");
     check_cuda(launch_columns_embed(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, views, tables(), out,
                                     twCol_.get(), s),
                "embedding + column c2c kernel");
 }
 
-void HorizontalPlan::forward_columns_from(DenseBins in, const ViewSet& views, double scale, cudaStream_t s) const {
+void HorizontalPlan::forward_columns_from(DenseBins in, const ViewSet& views, double scale, cudaStream_t s,
+                                          int zStride) const {
     if (in.kxStride != keep_) throw Error(-1, "bin array must hold keep() columns per row");
+    const int nz = static_cast<int>(w_.nz);
+    if (zStride == 0) zStride = nz;
     if (p_ == Precision::f32 && columns_warp_supported(static_cast<long long>(w_.ny))) {
-        check_cuda(launch_columns_gather_warp(static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, in, views,
-                                              tables(), scale, twCol_.get(), s),
+        check_cuda(launch_columns_gather_warp(static_cast<int>(w_.ny), nz, zStride, keep_, in, views, tables(), scale,
+                                              twCol_.get(), s),
                    "warp column c2c + retention kernel");
         return;
     }
+    if (zStride != nz) throw Error(-3, "padded bin planes need the FP32 warp column kernels");
     check_cuda(launch_columns_gather(p_, static_cast<int>(w_.ny), static_cast<int>(w_.nz), keep_, in, views,
                                      tables(), scale, twCol_.get(), s),
                "column c2c + retention kernel");
+}
+
+void HorizontalPlan::inverse_columns_band(DenseBins bins, int slots, int zStride, cudaStream_t s) const {
+    if (!bandExact_ || p_ != Precision::f32 || !columns_warp_supported(static_cast<long long>(w_.ny)))
+        throw Error(-3, "band column stage needs FP32, an exact retained band and Ny in [32, 512]");
+    check_cuda(launch_columns_inverse_band(static_cast<int>(w_.ny), static_cast<int>(w_.nz), zStride, slots, keep_,
+                                           bins, band_.get<int>(), twCol_.get(), s),
+               "band inverse column kernel");
+}
+
+void HorizontalPlan::forward_columns_band(DenseBins bins, int slots, double scale, int zStride, cudaStream_t s) const {
+    if (!bandExact_ || p_ != Precision::f32 || !columns_warp_supported(static_cast<long long>(w_.ny)))
+        throw Error(-3, "band column stage needs FP32, an exact retained band and Ny in [32, 512]");
+    check_cuda(launch_columns_forward_band(static_cast<int>(w_.ny), static_cast<int>(w_.nz), zStride, slots, keep_,
+                                           bins, band_.get<int>(), scale, twCol_.get(), s),
+               "band forward column kernel");
 }
 
 void HorizontalPlan::inverse_rows(void* real, std::uint64_t planes, cudaStream_t s) const {
@@ -327,7 +369,8 @@ std::uint64_t VerticalPlan::persistentBytes() const {
            groupColumns_.bytes() + groupFirst_.bytes() + error_.bytes();
 }
 
-void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s, std::uint64_t members) const {
+void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s, std::uint64_t members,
+                           const BinBoundary* inBins, const BinBoundary* outBins) const {
     if (members == 0) members = members_;
     if (members > members_) throw Error(-1, "more ensemble members than the plan was built for");
     if (p_ == GemmPrecision::tf32x3) {
@@ -350,9 +393,12 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
         a.in = static_cast<const float2*>(in.re);
         a.out = static_cast<float2*>(out.re);
         a.error = error_.get<int>();
+        if (inBins != nullptr) a.inBins = *inBins;
+        if (outBins != nullptr) a.outBins = *outBins;
         check_cuda(launch_tc_gemm(a, s), "tensor-core grouped vertical GEMM kernel");
         return;
     }
+    if (inBins != nullptr || outBins != nullptr) throw Error(-3, "bin-array operands need the tensor-core GEMM form");
     // SIMT tiles are member-major: the first members' tiles form a prefix.
     const int tiles = static_cast<int>(static_cast<std::uint64_t>(tiles_) / members_ * members);
     const GroupTiles t{tileGroup_.get<int>(), tileColumn_.get<int>(), tileCount_.get<int>(), tiles};

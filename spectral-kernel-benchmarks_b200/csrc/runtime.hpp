@@ -115,8 +115,17 @@ public:
     void gather_dense(const void* wvm, std::uint64_t planes, const ViewSet& views, double scale,
                       cudaStream_t s) const;
     // Column stages against caller-owned bin arrays (kxStride = keep()).
-    void inverse_columns_into(const ViewSet& views, DenseBins out, cudaStream_t s) const;
-    void forward_columns_from(DenseBins in, const ViewSet& views, double scale, cudaStream_t s) const;
+    // zStride: bin planes per view (0 = Nz); values above Nz need the FP32 warp kernels.
+    void inverse_columns_into(const ViewSet& views, DenseBins out, cudaStream_t s, int zStride = 0) const;
+    void forward_columns_from(DenseBins in, const ViewSet& views, double scale, cudaStream_t s,
+                              int zStride = 0) const;
+    // Band form of the column stages (fused flux), in place on dense bins
+    // whose slot f starts at plane f * zStride: valid when band_exact(), i.e.
+    // the retained cells of every column (with the kx = 0 partners) are the
+    // band min(ky, Ny - ky) <= band[kx].  FP32 only.
+    bool band_exact() const { return bandExact_; }
+    void inverse_columns_band(DenseBins bins, int slots, int zStride, cudaStream_t s) const;
+    void forward_columns_band(DenseBins bins, int slots, double scale, int zStride, cudaStream_t s) const;
     const void* twiddlesHalf() const { return twHalf_.get(); }
     const void* twiddlesFull() const { return twFull_.get(); }
     void embed_dense(const ViewSet& views, void* wvm, std::uint64_t planes, cudaStream_t s) const;
@@ -133,6 +142,8 @@ private:
     DeviceBuffer twHalf_, twFull_, twCol_;
     DeviceBuffer cellMap_, gatherMap_, colStart_, colKy_, colMode_, modeKx_, modeKy_, modeConj_;
     DeviceBuffer bins_;
+    DeviceBuffer band_;
+    bool bandExact_ = false;
 };
 
 // Vertical plan for one direction: the group matrices prepared for the chosen
@@ -146,7 +157,10 @@ public:
                  std::uint64_t fields, std::uint64_t members, const std::vector<double>& natural);
     // `members` <= the capacity given at construction (0 = all): the first
     // `members` ensemble members are computed.
-    void execute(ComplexOperand in, ComplexOperand out, cudaStream_t s, std::uint64_t members = 0) const;
+    // inBins / outBins (tensor-core form only): operands in the fused flux's
+    // dense bin array instead of compact [column][len] arrays.
+    void execute(ComplexOperand in, ComplexOperand out, cudaStream_t s, std::uint64_t members = 0,
+                 const BinBoundary* inBins = nullptr, const BinBoundary* outBins = nullptr) const;
     // Raises if a bounded device wait of the tensor-core form expired.
     void check_device_error() const;
     GemmPrecision precision() const { return p_; }

@@ -163,9 +163,23 @@ struct PipeState {
     uint32_t tmem;
 };
 
-__device__ __forceinline__ long long virtual_column(const TcGemmArgs& p, int vc, int gcols, long long gfirst) {
+// Where virtual column vc of a group lives: element offset of its first
+// value, its Hermitian partner (or -1) and whether the stored value is the
+// conjugate.  `len` is the compact column length.
+struct ColumnRef {
+    long long base, partner;
+    bool conj;
+};
+__device__ __forceinline__ ColumnRef column_ref(const TcGemmArgs& p, const BinBoundary& bb, int vc, int gcols,
+                                                long long gfirst, int len) {
     const int member = vc / gcols;
-    return static_cast<long long>(member) * p.memberColumns + gfirst + (vc - member * gcols);
+    const long long c = gfirst + (vc - member * gcols);
+    if (bb.cell == nullptr) return {(static_cast<long long>(member) * p.memberColumns + c) * len, -1, false};
+    const long long mode = c / bb.fields;
+    const int field = static_cast<int>(c - mode * bb.fields);
+    const long long off = (static_cast<long long>(member) * bb.fields + field) * bb.zStride;
+    const long long partner = bb.partner != nullptr ? __ldg(bb.partner + mode) : -1;
+    return {__ldg(bb.cell + mode) + off, partner >= 0 ? partner + off : -1, __ldg(bb.conj + mode) != 0};
 }
 
 // Warp-specialised split-TF32x3 grouped GEMM.
@@ -223,7 +237,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         const int lines = (S * 8 + 127) / 128 + 1;
         for (int i = tid; i < tcount * lines; i += kProducerWarps * 32) {
             const int cl = i / lines, l = i % lines;
-            const char* col = reinterpret_cast<const char*>(p.in + virtual_column(p, tv0 + cl, gcols, gfirst) * S);
+            const char* col =
+                reinterpret_cast<const char*>(p.in + column_ref(p, p.inBins, tv0 + cl, gcols, gfirst, S).base);
             const char* line = reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(col) & ~uintptr_t(127)) + 128 * l;
             if (line < col + S * 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
         }
@@ -263,6 +278,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         // contiguous bytes) and each shared store fills one 128-byte row.
         const int total = tiles * KCH;
         long long colBase[8];
+        unsigned conjMask = 0;  // bit c: column c of the tile is stored conjugated
         int loadTile = -1, loadCount = 0;
         auto load_chunk = [&](int it, float2 (&x)[8]) {
             const int t = it / KCH, kc = it % KCH;
@@ -270,10 +286,16 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                 loadTile = t;
                 const int tv0 = vc0 + t * 64;
                 loadCount = min(64, vc0 + vcN - tv0);
+                conjMask = 0;
 #pragma unroll
                 for (int c = 0; c < 8; ++c) {
                     const int cl = warp * 8 + c;
-                    colBase[c] = cl < loadCount ? virtual_column(p, tv0 + cl, gcols, gfirst) * S : 0;
+                    colBase[c] = 0;
+                    if (cl < loadCount) {
+                        const ColumnRef ref = column_ref(p, p.inBins, tv0 + cl, gcols, gfirst, S);
+                        colBase[c] = ref.base;
+                        conjMask |= ref.conj ? (1u << c) : 0u;
+                    }
                 }
                 // Pull the following tile's columns towards L2 meanwhile.
                 if (t + 1 < tiles) prefetch_tile(t + 1);
@@ -282,7 +304,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 x[c] = make_float2(0.f, 0.f);
-                if (warp * 8 + c < loadCount && s < S) x[c] = __ldg(p.in + colBase[c] + s);
+                if (warp * 8 + c < loadCount && s < S) {
+                    x[c] = __ldg(p.in + colBase[c] + s);
+                    if (conjMask & (1u << c)) x[c].y = -x[c].y;
+                }
             }
         };
         float2 next[8];
@@ -369,13 +394,17 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
             const int tv0 = vc0 + t * 64;
             const int tcount = min(64, vc0 + vcN - tv0);
             // The four columns this lane stores in the transposed epilogue.
-            bool storeValid[4];
-            long long storeColumn[4];
+            bool storeValid[4], storeConj[4];
+            long long storeColumn[4], storePartner[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int sc = quarter * 16 + 4 * k + (lane >> 3);
                 storeValid[k] = sc < tcount;
-                storeColumn[k] = storeValid[k] ? virtual_column(p, tv0 + sc, gcols, gfirst) : 0;
+                const ColumnRef ref =
+                    storeValid[k] ? column_ref(p, p.outBins, tv0 + sc, gcols, gfirst, R) : ColumnRef{0, -1, false};
+                storeColumn[k] = ref.base;
+                storePartner[k] = ref.partner;
+                storeConj[k] = ref.conj;
             }
             for (int kc = 0; kc < KCH; ++kc, ++it) {
                 const int acc = it % kAccumulators;
@@ -413,10 +442,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
                             const int lc = 4 * k + (lane >> 3);
-                            if (storeValid[k] && n < R)
-                                p.out[storeColumn[k] * R + n] =
-                                    make_float2(ebuf[lc * kEpiStride + 2 * (lane & 7)],
-                                                ebuf[lc * kEpiStride + 2 * (lane & 7) + 1]);
+                            if (storeValid[k] && n < R) {
+                                const float re = ebuf[lc * kEpiStride + 2 * (lane & 7)];
+                                const float im = ebuf[lc * kEpiStride + 2 * (lane & 7) + 1];
+                                p.out[storeColumn[k] + n] = make_float2(re, storeConj[k] ? -im : im);
+                                if (storePartner[k] >= 0)
+                                    p.out[storePartner[k] + n] = make_float2(re, storeConj[k] ? im : -im);
+                            }
                         }
                         __syncwarp();
                     }

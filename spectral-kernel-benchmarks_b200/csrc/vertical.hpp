@@ -38,6 +38,20 @@ int gemm_tile_columns(GemmPrecision p);
 // (member, column) list of one group: virtual column v of group g is member
 // v / groupColumns[g], column groupFirst[g] + v % groupColumns[g] of that
 // member, i.e. global complex column member*memberColumns + ...
+// Optional operand in the dense bin array of the fused flux instead of the
+// compact [column][len] layout: complex column (member, mode, field) lives at
+// element cell[mode] + (member * fields + field) * zStride + i (i along Nz).
+// conj[mode] != 0 where the cell holds the conjugate of the retained value;
+// partner[mode] >= 0 (output side) is a second cell, the kx = 0 Hermitian
+// partner, that receives the conjugate of the cell value.
+struct BinBoundary {
+    const long long* cell = nullptr;  // nullptr: compact operand
+    const long long* partner = nullptr;
+    const unsigned char* conj = nullptr;
+    int fields = 1;
+    int zStride = 0;
+};
+
 struct TcGemmArgs {
     const float* B;  // group matrices in natural layout [g][R][S], FP32
     int R, S, NP, KCH;
@@ -48,9 +62,10 @@ struct TcGemmArgs {
     const int* groupColumns;  // complex columns per member in each group
     const int* groupFirst;    // first complex column of each group within a member
     long long memberColumns;
-    const float2* in;  // [column][S] complex FP32
-    float2* out;       // [column][R] complex FP32
+    const float2* in;  // [column][S] complex FP32 (or the bin array, see inBins)
+    float2* out;       // [column][R] complex FP32 (or the bin array, see outBins)
     int* error;        // set to nonzero if a bounded wait expired
+    BinBoundary inBins, outBins;
 };
 bool tc_gemm_supported(int R, int S);
 size_t tc_gemm_smem_bytes(int R, int S);
