@@ -274,6 +274,37 @@ SKB_API int skb_vertical_forward_device(skb_vertical_provider* p, const void* in
 SKB_API int skb_vertical_inverse_device(skb_vertical_provider* p, const void* in_real, const void* in_imag, void* out_real,
                                 void* out_imag, void* stream);
 
+/* ------------------------------------ WVM-direct vertical GEMM provider */
+/* Replaces WvmDirectVerticalGemmProvider (skbench.hpp:220-257,
+ * src/vertical_gemm.cpp:935-1169): per retained mode, the group matrix times
+ * the mode's stored cell of a full WVM spectrum [ky][kx][field][z] (fields are
+ * the columns; the stored values are used as they are, no conjugation),
+ * written to the same cell of a full WVM modal spectrum [ky][kx][field][j];
+ * then the kx = 0 boundary copy (copyModalBoundary / copySpectrumBoundary):
+ * the partner cell (0, Ny - ky) receives the conjugate.  Output cells that
+ * hold no retained mode are not written; initialize_*_output zero a host
+ * output once (initializeModalOutput / initializeSpectrumOutput).  Groups and
+ * matrices as for skb_vertical_create.  One launch per direction. */
+typedef struct skb_vertical_wvm_provider skb_vertical_wvm_provider;
+SKB_API int skb_vertical_wvm_create(const skb_workload* w, const skb_mode_group* groups, uint64_t group_count,
+                                    const double* forward, const double* inverse, int buffer_policy,
+                                    int gemm_precision, skb_vertical_wvm_provider** out);
+SKB_API int skb_vertical_wvm_destroy(skb_vertical_wvm_provider* p);
+SKB_API int skb_vertical_wvm_info(const skb_vertical_wvm_provider* p, skb_provider_info* info);
+/* Complex element counts of the full WVM spectrum and modal spectrum. */
+SKB_API int skb_vertical_wvm_sizes(const skb_vertical_wvm_provider* p, uint64_t* spectrum_elements,
+                                   uint64_t* modal_elements);
+/* executeForward / executeInverse on host FP64 arrays. */
+SKB_API int skb_vertical_wvm_forward(skb_vertical_wvm_provider* p, const skb_complex* spectrum, skb_complex* modal);
+SKB_API int skb_vertical_wvm_inverse(skb_vertical_wvm_provider* p, const skb_complex* modal, skb_complex* spectrum);
+SKB_API int skb_vertical_wvm_initialize_modal_output(const skb_vertical_wvm_provider* p, skb_complex* modal);
+SKB_API int skb_vertical_wvm_initialize_spectrum_output(const skb_vertical_wvm_provider* p, skb_complex* spectrum);
+/* Device forms: FP64 complex for SKB_GEMM_FP64, FP32 complex otherwise. */
+SKB_API int skb_vertical_wvm_forward_device(skb_vertical_wvm_provider* p, const void* spectrum, void* modal,
+                                            void* stream);
+SKB_API int skb_vertical_wvm_inverse_device(skb_vertical_wvm_provider* p, const void* modal, void* spectrum,
+                                            void* stream);
+
 /* ------------------------------------------------- pointwise advection */
 /* Replaces PointwiseAdvectionExecutor (src/pointwise_advection.hpp:18-43). */
 typedef struct skb_pointwise_executor skb_pointwise_executor;
@@ -342,6 +373,30 @@ SKB_API int skb_flux_check_device(skb_flux* p);
 SKB_API int skb_flux_capture_graph(skb_flux* p, const void* modal_input, void* modal_output);
 SKB_API int skb_flux_replay_graph(skb_flux* p, void* stream);
 
+/* ---------------------------------------------- spectral-pipeline round trip */
+/* The spectral-pipeline kernel of skbench (runSpectralPipelineBenchmark,
+ * src/benchmark.cpp:2978-3956; reference order 3072-3110): r2c with radial 2/3
+ * retention, K^2-grouped vertical forward (pair-rotation family), synthetic
+ * modal work (each modal value times syntheticModalWorkWeights,
+ * src/model.cpp:246-274), vertical inverse, embedding with the kx = 0 repair,
+ * and the unnormalised c2r.  SKB_PRECISION_FP64: FP64 transforms and FP64
+ * GEMMs; SKB_PRECISION_FP32: FP32 transforms and split-TF32x3 tensor-core
+ * GEMMs.  Real [field][z][y][x] in and out. */
+typedef struct skb_pipeline skb_pipeline;
+/* syntheticModalWorkWeights: modes*fields*nj doubles, [mode][field][j]. */
+SKB_API int skb_modal_weights(const skb_workload* w, double* out);
+SKB_API int skb_pipeline_create(const skb_workload* w, int precision, skb_pipeline** out);
+SKB_API int skb_pipeline_destroy(skb_pipeline* p);
+SKB_API int skb_pipeline_info(const skb_pipeline* p, skb_provider_info* info);
+/* Host FP64 arrays, blocking. */
+SKB_API int skb_pipeline_execute(skb_pipeline* p, const double* real_in, double* real_out);
+/* Device arrays of the handle's precision, stream-ordered. */
+SKB_API int skb_pipeline_execute_device(skb_pipeline* p, const void* real_in, void* real_out, void* stream);
+/* One device execution with per-stage event times and algorithmic bytes. */
+SKB_API int skb_pipeline_profile(skb_pipeline* p, const void* real_in, void* real_out, skb_stage_time* stages,
+                                 uint64_t capacity, uint64_t* count);
+SKB_API void* skb_pipeline_stream(skb_pipeline* p);
+
 /* ------------------------------------------------------ serving loop */
 /* A continuous-batching request loop over flux size classes (no counterpart
  * in the reference, which has no serving path).  Each class gets one or more
@@ -394,6 +449,7 @@ SKB_API void* skb_pruned_stream(skb_pruned_provider* p);
 SKB_API void* skb_vertical_stream(skb_vertical_provider* p);
 SKB_API void* skb_pointwise_stream(skb_pointwise_executor* p);
 SKB_API void* skb_flux_stream(skb_flux* p);
+SKB_API void* skb_vertical_wvm_stream(skb_vertical_wvm_provider* p);
 
 /* Device buffers for callers without their own allocator (tests, bindings). */
 SKB_API int skb_device_alloc(uint64_t bytes, void** ptr);

@@ -291,3 +291,56 @@ def rel_l2_error(actual, expected):
     num = float(np.sum(np.abs(a - b) ** 2))
     den = float(np.sum(np.abs(b) ** 2))
     return float(np.sqrt(num if den == 0.0 else num / den))
+
+
+def wvm_direct_vertical(w: Workload, family, direction, data, out=None):
+    """WvmDirectVerticalGemmProvider::executeForward / executeInverse
+    (vertical_gemm.cpp:935-1169): per retained mode, the group's real matrix
+    times the mode's stored WVM cell, fields as columns, no conjugation
+    (forwardMode / inverseMode), then the kx = 0 boundary copy: the partner
+    cell (0, Ny - ky) receives the conjugate (copyModalBoundary /
+    copySpectrumBoundary).  forward: WVM spectrum [ky][kx][field][z] -> WVM modal
+    spectrum [ky][kx][field][j]; inverse the reverse.  Cells of `out` that are
+    not written keep their values (the provider's initialize*Output zero them)."""
+    fwd, inv = family
+    modes = retained_modes(w.nx, w.ny)
+    _, first, counts = k2_groups(w.nx, w.ny)
+    group_of = np.repeat(np.arange(len(first)), counts)
+    half = w.nx // 2 + 1
+    rows_in, rows_out, mats = (w.nz, w.nj, fwd) if direction == "forward" else (w.nj, w.nz, inv)
+    x = np.asarray(data, dtype=np.complex128).reshape(w.ny, half, w.fields, rows_in)
+    y = np.zeros((w.ny, half, w.fields, rows_out), np.complex128) if out is None else \
+        np.array(out, dtype=np.complex128).reshape(w.ny, half, w.fields, rows_out)
+    for m in range(len(modes)):
+        kx, ky = int(modes.kx[m]), int(modes.ky[m])
+        y[ky, kx] = x[ky, kx] @ mats[group_of[m]].T
+    for m in range(len(modes)):
+        kx, ky = int(modes.kx[m]), int(modes.ky[m])
+        if kx == 0 and ky != 0 and 2 * ky != w.ny:
+            y[(w.ny - ky) % w.ny, 0] = np.conj(y[ky, 0])
+    return y.reshape(-1)
+
+
+def modal_weights(w: Workload):
+    """syntheticModalWorkWeights (model.cpp:246-267): per (mode, field, j),
+    0.75 + 0.5 * ((17|k| + 29|l| + 7j + 11 field) mod 97) / 96, [mode][field][j]."""
+    modes = retained_modes(w.nx, w.ny)
+    k = np.abs(np.asarray(modes.k, np.int64))
+    l = np.abs(np.asarray(modes.l, np.int64))
+    f = np.arange(w.fields)[None, :, None]
+    j = np.arange(w.nj)[None, None, :]
+    key = (17 * k[:, None, None] + 29 * l[:, None, None] + 7 * j + 11 * f) % 97
+    return (0.75 + 0.5 * key / 96.0).reshape(-1)
+
+
+def spectral_pipeline(w: Workload, real, family=None, workers=1):
+    """The spectral-pipeline round trip (benchmark.cpp:3072-3110 reference order):
+    r2c, retention, K^2 vertical forward, synthetic modal work, vertical inverse,
+    embedding, c2r (unnormalised, FFTW semantics)."""
+    family = k2_family(w) if family is None else family
+    modes = retained_modes(w.nx, w.ny)
+    spec = fft_r2c(w, real, workers)
+    ret = gather_retained(w, modes, spec)
+    modal = grouped_vertical(w, family, "forward", ret) * modal_weights(w)
+    back = grouped_vertical(w, family, "inverse", modal)
+    return fft_c2r(w, embed_retained(w, modes, back), workers)

@@ -208,6 +208,49 @@ int skbref_grouped_vertical(std::uint64_t nx, std::uint64_t ny, std::uint64_t nz
     });
 }
 
+// The spectral-pipeline round trip in the order of runSpectralPipelineBenchmark's
+// reference computation (benchmark.cpp:3072-3110), composed from model.cpp with
+// the direct DFTs in place of FFTW: makeFixture(random, seed) -> directR2C ->
+// gatherRetained -> per-group verticalForward -> applySyntheticModalWorkInterleaved
+// (syntheticModalWorkWeights) -> per-group verticalInverse -> embedRetained ->
+// directC2R (unnormalised).  input: nx*ny*nz*fields doubles; weights:
+// modes*fields*nj doubles; output: like input.
+int skbref_spectral_pipeline(std::uint64_t n, std::uint64_t nz, std::uint64_t fields, std::uint64_t seed,
+                             double* input, double* weights, double* output) {
+    return guarded([&] {
+        const auto workload = makeWorkload(n, n, nz, fields);
+        const auto modes = skbench::retainedHorizontalModes(workload);
+        const auto family = skbench::squaredWavenumberVerticalFixture(workload, modes);
+        const auto nj = family.nj;
+        const auto real = skbench::makeFixture(workload, skbench::FixtureKind::random, seed);
+        std::memcpy(input, real.data(), real.size() * sizeof(double));
+        std::vector<skbench::Complex> spectrum(workload.spectrumElements());
+        skbench::directR2C(workload, real.data(), spectrum.data());
+        std::vector<skbench::Complex> retained(modes.size() * workload.planes());
+        skbench::gatherRetained(workload, modes, spectrum.data(), retained.data());
+        std::vector<skbench::Complex> modal(modes.size() * fields * nj), worked(modal.size());
+        for (std::size_t g = 0; g < family.groups.size(); ++g) {
+            const auto ops = groupSlice(family, g);
+            const auto first = family.groups[g].firstMode;
+            skbench::verticalForward(workload, family.groups[g].modeCount, ops, retained.data() + first * fields * nz,
+                                     modal.data() + first * fields * nj);
+        }
+        const auto w = skbench::syntheticModalWorkWeights(workload, modes);
+        std::memcpy(weights, w.data(), w.size() * sizeof(double));
+        skbench::applySyntheticModalWorkInterleaved(modal.size(), w.data(), modal.data(), worked.data());
+        for (std::size_t g = 0; g < family.groups.size(); ++g) {
+            const auto ops = groupSlice(family, g);
+            const auto first = family.groups[g].firstMode;
+            skbench::verticalInverse(workload, family.groups[g].modeCount, ops, worked.data() + first * fields * nj,
+                                     retained.data() + first * fields * nz);
+        }
+        skbench::embedRetained(workload, modes, retained.data(), spectrum.data());
+        std::vector<double> back(workload.realElements());
+        skbench::directC2R(workload, spectrum.data(), back.data());
+        std::memcpy(output, back.data(), back.size() * sizeof(double));
+    });
+}
+
 // PointwiseAdvectionExecutor (pointwise_advection.cpp:152-240); policy 0 serial,
 // 1 vector-serial, 2 spatial-static.
 int skbref_pointwise(int policy, std::uint64_t workers, std::uint64_t volume, double scale,

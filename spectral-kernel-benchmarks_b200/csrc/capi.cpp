@@ -9,6 +9,7 @@
 
 #include "flux.hpp"
 #include "noalloc.hpp"
+#include "pipeline.hpp"
 #include "server.hpp"
 #include "pointwise.hpp"
 #include "runtime.hpp"
@@ -185,6 +186,34 @@ struct skb_vertical_provider {
     HostAdapter host{Precision::f64, {}};
     double allocation = 0.0, preparation = 0.0;
     ~skb_vertical_provider() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct skb_vertical_wvm_provider {
+    Workload w;
+    GemmPrecision gp = GemmPrecision::f64;
+    Precision p = Precision::f64;
+    cudaStream_t stream = nullptr;
+    std::unique_ptr<VerticalPlan> forward, inverse;
+    // Per retained mode: element offsets of its stored cell in the WVM
+    // spectrum and in the WVM modal spectrum, and of the kx = 0 partner cell.
+    DeviceBuffer cellSpec, partnerSpec, cellModal, partnerModal;
+    DeviceBuffer spectrum, modal;  // device staging of the host forms
+    HostAdapter host{Precision::f64, {}};
+    uint64_t spectrumElements = 0, modalElements = 0;
+    double allocation = 0.0, preparation = 0.0;
+    ~skb_vertical_wvm_provider() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct skb_pipeline {
+    std::unique_ptr<SpectralPipeline> pipe;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer in, out;  // device staging of the host form
+    HostAdapter host{Precision::f64, {}};
+    ~skb_pipeline() {
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -856,6 +885,272 @@ int skb_vertical_create(const skb_workload* w, const skb_mode_group* groups, uin
 int skb_vertical_destroy(skb_vertical_provider* p) {
     return guard([&] { delete p; });
 }
+
+// ------------------------------------------------- WVM-direct vertical GEMM
+
+int skb_vertical_wvm_create(const skb_workload* w, const skb_mode_group* groups, uint64_t group_count,
+                            const double* forward, const double* inverse, int policy, int gemm_precision,
+                            skb_vertical_wvm_provider** out) {
+    return guard([&] {
+        require(out != nullptr, "output handle must be non-null");
+        require(groups != nullptr && group_count > 0, "Direct WVM vertical GEMM requires modes, groups, and fields.");
+        require(policy >= SKB_BUFFERS_BIDIRECTIONAL && policy <= SKB_BUFFERS_INVERSE_ONLY, "unknown buffer policy");
+        auto p = std::make_unique<skb_vertical_wvm_provider>();
+        p->w = to_workload(w);
+        if (gemm_precision == SKB_GEMM_FP64) {
+            p->gp = GemmPrecision::f64;
+            p->p = Precision::f64;
+        } else if (gemm_precision == SKB_GEMM_FP32) {
+            p->gp = GemmPrecision::f32;
+            p->p = Precision::f32;
+        } else if (gemm_precision == SKB_GEMM_TF32X3) {
+            p->gp = GemmPrecision::tf32x3;
+            p->p = Precision::f32;
+        } else {
+            throw Error(SKB_ERR_RUNTIME, "unsupported: the split-BF16x3 GEMM form is not built in this library");
+        }
+        p->host.p = p->p;
+        const auto prepStart = Clock::now();
+        const auto modes = retained_modes(p->w);
+        std::vector<ModeGroup> g(group_count);
+        uint64_t covered = 0;
+        for (uint64_t i = 0; i < group_count; ++i) {
+            g[i] = {groups[i].squared_mode_key, groups[i].first_mode, groups[i].mode_count};
+            require(groups[i].mode_count > 0 && groups[i].first_mode == covered,
+                    "Direct WVM vertical GEMM groups must be nonempty, contiguous, and cover the modes.");
+            covered += groups[i].mode_count;
+        }
+        require(covered == modes.size(), "Direct WVM vertical GEMM groups do not cover every retained mode.");
+        const uint64_t nz = p->w.nz, nj = p->w.nj(), fields = p->w.fields, half = p->w.nxHalf();
+        require(nj > 0, "Vertical GEMM requires Nz >= 2.");
+        const bool fwd = policy != SKB_BUFFERS_INVERSE_ONLY, inv = policy != SKB_BUFFERS_FORWARD_ONLY;
+        require(!fwd || forward != nullptr, "forward matrices must be non-null");
+        require(!inv || inverse != nullptr, "inverse matrices must be non-null");
+        const auto elems = nz * nj * group_count;
+        std::vector<double> F(fwd ? elems : 0), I(inv ? elems : 0);
+        if (fwd) std::memcpy(F.data(), forward, elems * sizeof(double));
+        if (inv) std::memcpy(I.data(), inverse, elems * sizeof(double));
+        std::vector<long long> cs(modes.size()), ps(modes.size()), cm(modes.size()), pm(modes.size());
+        for (size_t m = 0; m < modes.size(); ++m) {
+            const auto& md = modes[m];
+            const long long cell = static_cast<long long>(md.kx + half * md.ky);
+            cs[m] = cell * static_cast<long long>(nz * fields);
+            cm[m] = cell * static_cast<long long>(nj * fields);
+            const bool partner = md.kx == 0 && md.ky != 0 && 2 * md.ky != p->w.ny;
+            const long long pcell = static_cast<long long>(half * ((p->w.ny - md.ky) % p->w.ny));
+            ps[m] = partner ? pcell * static_cast<long long>(nz * fields) : -1;
+            pm[m] = partner ? pcell * static_cast<long long>(nj * fields) : -1;
+        }
+        p->preparation = seconds_since(prepStart);
+        const auto allocStart = Clock::now();
+        p->stream = make_stream();
+        if (fwd)
+            p->forward = std::make_unique<VerticalPlan>(p->gp, static_cast<int>(nj), static_cast<int>(nz), g, fields, 1, F);
+        if (inv)
+            p->inverse = std::make_unique<VerticalPlan>(p->gp, static_cast<int>(nz), static_cast<int>(nj), g, fields, 1, I);
+        p->cellSpec = upload_vector(cs);
+        p->partnerSpec = upload_vector(ps);
+        p->cellModal = upload_vector(cm);
+        p->partnerModal = upload_vector(pm);
+        p->spectrumElements = p->w.spectrumElements();
+        p->modalElements = half * p->w.ny * nj * fields;
+        const size_t es = element_bytes(p->p);
+        p->spectrum.allocate(2 * es * p->spectrumElements);
+        p->modal.allocate(2 * es * p->modalElements);
+        p->allocation = seconds_since(allocStart);
+        *out = p.release();
+    });
+}
+
+int skb_vertical_wvm_destroy(skb_vertical_wvm_provider* p) {
+    return guard([&] { delete p; });
+}
+
+int skb_vertical_wvm_info(const skb_vertical_wvm_provider* p, skb_provider_info* info) {
+    return guard([&] {
+        require(p != nullptr && info != nullptr, "handle and info must be non-null");
+        std::memset(info, 0, sizeof(*info));
+        info->allocation_seconds = p->allocation;
+        info->planning_seconds = p->preparation;
+        info->persistent_bytes = (p->forward ? p->forward->persistentBytes() : 0) +
+                                 (p->inverse ? p->inverse->persistentBytes() : 0) + p->cellSpec.bytes() +
+                                 p->partnerSpec.bytes() + p->cellModal.bytes() + p->partnerModal.bytes();
+        info->scratch_bytes = p->spectrum.bytes() + p->modal.bytes();
+        info->launches_per_execution = 1;
+        info->precision = p->p == Precision::f64 ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
+        fill_identity(info, "skb-cuda hand-written sm_100a direct WVM-order per-mode grouped GEMM");
+    });
+}
+
+int skb_vertical_wvm_sizes(const skb_vertical_wvm_provider* p, uint64_t* spectrum_elements, uint64_t* modal_elements) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        if (spectrum_elements) *spectrum_elements = p->spectrumElements;
+        if (modal_elements) *modal_elements = p->modalElements;
+    });
+}
+
+namespace {
+BinBoundary wvm_boundary(const DeviceBuffer& cell, const DeviceBuffer& partner, uint64_t fields, uint64_t stride,
+                         bool withPartner) {
+    return {cell.get<long long>(), withPartner ? partner.get<long long>() : nullptr, nullptr, static_cast<int>(fields),
+            static_cast<int>(stride)};
+}
+
+void wvm_forward(skb_vertical_wvm_provider* p, const void* spectrum, void* modal, cudaStream_t s) {
+    const BinBoundary in = wvm_boundary(p->cellSpec, p->partnerSpec, p->w.fields, p->w.nz, false);
+    const BinBoundary out = wvm_boundary(p->cellModal, p->partnerModal, p->w.fields, p->w.nj(), true);
+    if (!p->forward) throw std::logic_error("Forward GEMM requested from an inverse-only direct WVM provider.");
+    p->forward->execute({const_cast<void*>(spectrum), nullptr}, {modal, nullptr}, s, 1, &in, &out);
+}
+
+void wvm_inverse(skb_vertical_wvm_provider* p, const void* modal, void* spectrum, cudaStream_t s) {
+    const BinBoundary in = wvm_boundary(p->cellModal, p->partnerModal, p->w.fields, p->w.nj(), false);
+    const BinBoundary out = wvm_boundary(p->cellSpec, p->partnerSpec, p->w.fields, p->w.nz, true);
+    if (!p->inverse) throw std::logic_error("Inverse GEMM requested from a forward-only direct WVM provider.");
+    p->inverse->execute({const_cast<void*>(modal), nullptr}, {spectrum, nullptr}, s, 1, &in, &out);
+}
+}  // namespace
+
+int skb_vertical_wvm_forward_device(skb_vertical_wvm_provider* p, const void* spectrum, void* modal, void* stream) {
+    return guard([&] {
+        require(p && spectrum && modal, "handle and buffers must be non-null");
+        wvm_forward(p, spectrum, modal, stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    });
+}
+
+int skb_vertical_wvm_inverse_device(skb_vertical_wvm_provider* p, const void* modal, void* spectrum, void* stream) {
+    return guard([&] {
+        require(p && spectrum && modal, "handle and buffers must be non-null");
+        wvm_inverse(p, modal, spectrum, stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    });
+}
+
+int skb_vertical_wvm_forward(skb_vertical_wvm_provider* p, const skb_complex* spectrum, skb_complex* modal) {
+    return guard([&] {
+        require(p && spectrum && modal, "handle and buffers must be non-null");
+        // The output's cells without a retained mode keep the caller's values.
+        p->host.upload(p->spectrum.get(), reinterpret_cast<const double*>(spectrum), 2 * p->spectrumElements, p->stream);
+        p->host.upload(p->modal.get(), reinterpret_cast<const double*>(modal), 2 * p->modalElements, p->stream);
+        wvm_forward(p, p->spectrum.get(), p->modal.get(), p->stream);
+        p->host.download(reinterpret_cast<double*>(modal), p->modal.get(), 2 * p->modalElements, p->stream);
+        sync(p->stream);
+        p->forward->check_device_error();
+    });
+}
+
+int skb_vertical_wvm_inverse(skb_vertical_wvm_provider* p, const skb_complex* modal, skb_complex* spectrum) {
+    return guard([&] {
+        require(p && spectrum && modal, "handle and buffers must be non-null");
+        p->host.upload(p->modal.get(), reinterpret_cast<const double*>(modal), 2 * p->modalElements, p->stream);
+        p->host.upload(p->spectrum.get(), reinterpret_cast<const double*>(spectrum), 2 * p->spectrumElements,
+                       p->stream);
+        wvm_inverse(p, p->modal.get(), p->spectrum.get(), p->stream);
+        p->host.download(reinterpret_cast<double*>(spectrum), p->spectrum.get(), 2 * p->spectrumElements, p->stream);
+        sync(p->stream);
+        p->inverse->check_device_error();
+    });
+}
+
+int skb_vertical_wvm_initialize_modal_output(const skb_vertical_wvm_provider* p, skb_complex* modal) {
+    return guard([&] {
+        require(p && modal, "handle and output must be non-null");
+        std::memset(modal, 0, sizeof(skb_complex) * p->modalElements);
+    });
+}
+
+int skb_vertical_wvm_initialize_spectrum_output(const skb_vertical_wvm_provider* p, skb_complex* spectrum) {
+    return guard([&] {
+        require(p && spectrum, "handle and output must be non-null");
+        std::memset(spectrum, 0, sizeof(skb_complex) * p->spectrumElements);
+    });
+}
+
+void* skb_vertical_wvm_stream(skb_vertical_wvm_provider* p) { return p ? p->stream : nullptr; }
+
+// ------------------------------------------------------- spectral pipeline
+
+int skb_modal_weights(const skb_workload* w, double* out) {
+    return guard([&] {
+        require(out != nullptr, "output must be non-null");
+        const Workload wl = to_workload(w);
+        const auto weights = synthetic_modal_weights(wl, retained_modes(wl));
+        std::memcpy(out, weights.data(), weights.size() * sizeof(double));
+    });
+}
+
+int skb_pipeline_create(const skb_workload* w, int precision, skb_pipeline** out) {
+    return guard([&] {
+        require(out != nullptr, "output handle must be non-null");
+        auto p = std::make_unique<skb_pipeline>();
+        const Workload wl = to_workload(w);
+        const Precision pr = to_precision(precision);
+        p->pipe = std::make_unique<SpectralPipeline>(wl, pr);
+        p->stream = make_stream();
+        p->host.p = pr;
+        const size_t es = element_bytes(pr);
+        p->in.allocate(es * wl.realElements());
+        p->out.allocate(es * wl.realElements());
+        *out = p.release();
+    });
+}
+
+int skb_pipeline_destroy(skb_pipeline* p) {
+    return guard([&] { delete p; });
+}
+
+int skb_pipeline_info(const skb_pipeline* p, skb_provider_info* info) {
+    return guard([&] {
+        require(p != nullptr && info != nullptr, "handle and info must be non-null");
+        std::memset(info, 0, sizeof(*info));
+        info->allocation_seconds = p->pipe->allocationSeconds;
+        info->planning_seconds = p->pipe->planningSeconds;
+        info->persistent_bytes = p->pipe->persistentBytes;
+        info->scratch_bytes = p->pipe->scratchBytes + p->in.bytes() + p->out.bytes();
+        info->launches_per_execution = 7;
+        info->precision = p->pipe->precision() == Precision::f64 ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
+        fill_identity(info, p->pipe->precision() == Precision::f64
+                                ? "skb-cuda spectral pipeline: FP64 pruned transforms, FP64 K2-grouped GEMMs"
+                                : "skb-cuda spectral pipeline: FP32 pruned transforms, split-TF32x3 tcgen05 GEMMs");
+    });
+}
+
+int skb_pipeline_execute_device(skb_pipeline* p, const void* real_in, void* real_out, void* stream) {
+    return guard([&] {
+        require(p && real_in && real_out, "handle and buffers must be non-null");
+        p->pipe->execute(real_in, real_out, stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    });
+}
+
+int skb_pipeline_execute(skb_pipeline* p, const double* real_in, double* real_out) {
+    return guard([&] {
+        require(p && real_in && real_out, "handle and buffers must be non-null");
+        const size_t n = p->pipe->workload().realElements();
+        p->host.upload(p->in.get(), real_in, n, p->stream);
+        p->pipe->execute(p->in.get(), p->out.get(), p->stream);
+        p->host.download(real_out, p->out.get(), n, p->stream);
+        sync(p->stream);
+        p->pipe->check_device_error();
+    });
+}
+
+int skb_pipeline_profile(skb_pipeline* p, const void* real_in, void* real_out, skb_stage_time* stages,
+                         uint64_t capacity, uint64_t* count) {
+    return guard([&] {
+        require(p && real_in && real_out && count, "handle, buffers and count must be non-null");
+        const auto st = p->pipe->profile(real_in, real_out, p->stream);
+        *count = st.size();
+        for (size_t i = 0; i < st.size() && i < capacity; ++i) {
+            std::memset(&stages[i], 0, sizeof(skb_stage_time));
+            std::strncpy(stages[i].name, st[i].name.c_str(), sizeof(stages[i].name) - 1);
+            stages[i].ms = st[i].ms;
+            stages[i].launches = st[i].launches;
+            stages[i].algorithmic_bytes = st[i].bytes;
+        }
+    });
+}
+
+void* skb_pipeline_stream(skb_pipeline* p) { return p ? p->stream : nullptr; }
 
 int skb_vertical_info(const skb_vertical_provider* p, skb_provider_info* info) {
     return guard([&] {

@@ -398,11 +398,13 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
         check_cuda(launch_tc_gemm(a, s), "tensor-core grouped vertical GEMM kernel");
         return;
     }
-    if (inBins != nullptr || outBins != nullptr) throw Error(-3, "bin-array operands need the tensor-core GEMM form");
+    if ((inBins != nullptr || outBins != nullptr) && members_ != 1)
+        throw Error(-3, "bin-array operands of the SIMT GEMM need a single-member plan");
     // SIMT tiles are member-major: the first members' tiles form a prefix.
     const int tiles = static_cast<int>(static_cast<std::uint64_t>(tiles_) / members_ * members);
     const GroupTiles t{tileGroup_.get<int>(), tileColumn_.get<int>(), tileCount_.get<int>(), tiles};
-    check_cuda(launch_grouped_gemm(p_, R_, S_, matrices_.get(), t, in, out, s), "grouped vertical GEMM kernel");
+    check_cuda(launch_grouped_gemm(p_, R_, S_, matrices_.get(), t, in, out, s, inBins, outBins),
+               "grouped vertical GEMM kernel");
 }
 
 void VerticalPlan::check_device_error() const {

@@ -173,13 +173,14 @@ struct ColumnRef {
 __device__ __forceinline__ ColumnRef column_ref(const TcGemmArgs& p, const BinBoundary& bb, int vc, int gcols,
                                                 long long gfirst, int len) {
     const int member = vc / gcols;
-    const long long c = gfirst + (vc - member * gcols);
+    const int c = static_cast<int>(gfirst) + (vc - member * gcols);  // column within the member (< 2^31)
     if (bb.cell == nullptr) return {(static_cast<long long>(member) * p.memberColumns + c) * len, -1, false};
-    const long long mode = c / bb.fields;
-    const int field = static_cast<int>(c - mode * bb.fields);
+    const int mode = c / bb.fields;
+    const int field = c - mode * bb.fields;
     const long long off = (static_cast<long long>(member) * bb.fields + field) * bb.zStride;
     const long long partner = bb.partner != nullptr ? __ldg(bb.partner + mode) : -1;
-    return {__ldg(bb.cell + mode) + off, partner >= 0 ? partner + off : -1, __ldg(bb.conj + mode) != 0};
+    const bool conj = bb.conj != nullptr && __ldg(bb.conj + mode) != 0;
+    return {__ldg(bb.cell + mode) + off, partner >= 0 ? partner + off : -1, conj};
 }
 
 // Warp-specialised split-TF32x3 grouped GEMM.

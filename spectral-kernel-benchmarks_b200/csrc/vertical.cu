@@ -49,21 +49,55 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Element offset of column `col` (single member, column = mode * fields +
+// field) in a bin-array operand, with its partner (or -1) and conjugation.
+__device__ __forceinline__ void bin_column(const BinBoundary& bb, int col, long long& base, long long& partner,
+                                           bool& conj) {
+    const int mode = col / bb.fields;
+    const int field = col - mode * bb.fields;
+    const long long off = static_cast<long long>(field) * bb.zStride;
+    base = __ldg(bb.cell + mode) + off;
+    const long long p = bb.partner != nullptr ? __ldg(bb.partner + mode) : -1;
+    partner = p >= 0 ? p + off : -1;
+    conj = bb.conj != nullptr && __ldg(bb.conj + mode) != 0;
+}
+
 template <typename T, int KR, bool SPLIT>
 __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, const T* __restrict__ At,
                                                                 GroupTiles tiles, ComplexOperand in,
-                                                                ComplexOperand out) {
+                                                                ComplexOperand out, BinBoundary inBins,
+                                                                BinBoundary outBins) {
     using V = cx<T>;
     constexpr int RP = 32 * KR;
     constexpr size_t xBytes = sizeof(V) * kTileCols * (kChunk + 1);
     constexpr size_t aBytes = sizeof(T) * kChunk * RP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    // Per tile column: element offsets of the input and output columns (and
+    // the output partner), and the conjugation flags.
+    __shared__ long long colIn[kTileCols], colOut[kTileCols], colPartner[kTileCols];
+    __shared__ signed char conjIn[kTileCols], conjOut[kTileCols];
     const int tile = blockIdx.x;
     const int g = __ldg(tiles.tileGroup + tile);
     const int c0 = __ldg(tiles.tileColumn + tile);
     const int ncols = __ldg(tiles.tileCount + tile);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    if (threadIdx.x < kTileCols) {
+        const int c = threadIdx.x;
+        long long base = static_cast<long long>(c0 + c) * S, partner = -1;
+        bool conj = false;
+        if (inBins.cell != nullptr && c < ncols) bin_column(inBins, c0 + c, base, partner, conj);
+        colIn[c] = base;
+        conjIn[c] = conj ? 1 : 0;
+        base = static_cast<long long>(c0 + c) * R;
+        partner = -1;
+        conj = false;
+        if (outBins.cell != nullptr && c < ncols) bin_column(outBins, c0 + c, base, partner, conj);
+        colOut[c] = base;
+        colPartner[c] = partner;
+        conjOut[c] = conj ? 1 : 0;
+    }
+    __syncthreads();
     const T* A = At + (long long)g * R * S;
     const int chunks = (S + kChunk - 1) / kChunk;
 
@@ -84,7 +118,7 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
         for (int i = threadIdx.x; i < kTileCols * kChunk; i += kThreads) {
             const int c = i / kChunk, s = i % kChunk;
             const bool ok = c < ncols && s0 + s < S;
-            const long long idx = ok ? (long long)(c0 + c) * S + s0 + s : 0;
+            const long long idx = ok ? colIn[c] + s0 + s : 0;
             if (SPLIT) {
                 // Split operands: two scalar copies into the complex slot.
                 T* slot = reinterpret_cast<T*>(&sX[c][s]);
@@ -122,7 +156,8 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
             for (int k = 0; k < KR; ++k) a[k] = sA[s][lane + 32 * k];
 #pragma unroll
             for (int m = 0; m < kTileCols / 8; ++m) {
-                const V x = sX[warp + 8 * m][s];
+                V x = sX[warp + 8 * m][s];
+                if (conjIn[warp + 8 * m]) x.y = -x.y;
 #pragma unroll
                 for (int k = 0; k < KR; ++k) {
                     acc[k][m].x = fma(a[k], x.x, acc[k][m].x);
@@ -139,14 +174,18 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
 #pragma unroll
         for (int k = 0; k < KR; ++k) {
             const int r = lane + 32 * k;
-            if (r < R) store_operand<T, SPLIT>(out, (long long)(c0 + c) * R + r, acc[k][m]);
+            if (r >= R) continue;
+            V v = acc[k][m];
+            if (conjOut[c]) v.y = -v.y;
+            store_operand<T, SPLIT>(out, colOut[c] + r, v);
+            if (colPartner[c] >= 0) store_operand<T, SPLIT>(out, colPartner[c] + r, V{v.x, -v.y});
         }
     }
 }
 
 template <typename T, int KR>
 cudaError_t launch_kr(int R, int S, const void* At, const GroupTiles& tiles, ComplexOperand in, ComplexOperand out,
-                      cudaStream_t stream) {
+                      const BinBoundary& inBins, const BinBoundary& outBins, cudaStream_t stream) {
     const bool split = in.im != nullptr;
     if (split != (out.im != nullptr)) return cudaErrorInvalidValue;
     const size_t bytes = 2 * (sizeof(cx<T>) * kTileCols * (kChunk + 1) + sizeof(T) * kChunk * 32 * KR);
@@ -155,24 +194,25 @@ cudaError_t launch_kr(int R, int S, const void* At, const GroupTiles& tiles, Com
         const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (err != cudaSuccess) return err;
     }
-    kernel<<<tiles.tiles, kThreads, bytes, stream>>>(R, S, static_cast<const T*>(At), tiles, in, out);
+    kernel<<<tiles.tiles, kThreads, bytes, stream>>>(R, S, static_cast<const T*>(At), tiles, in, out, inBins,
+                                                     outBins);
     return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_t(int R, int S, const void* At, const GroupTiles& tiles, ComplexOperand in, ComplexOperand out,
-                     cudaStream_t stream) {
+                     const BinBoundary& ib, const BinBoundary& ob, cudaStream_t stream) {
     const int kr = (R + 31) / 32;
     switch (kr) {
-        case 1: return launch_kr<T, 1>(R, S, At, tiles, in, out, stream);
-        case 2: return launch_kr<T, 2>(R, S, At, tiles, in, out, stream);
-        case 3: return launch_kr<T, 3>(R, S, At, tiles, in, out, stream);
-        case 4: return launch_kr<T, 4>(R, S, At, tiles, in, out, stream);
-        case 5: return launch_kr<T, 5>(R, S, At, tiles, in, out, stream);
-        case 6: return launch_kr<T, 6>(R, S, At, tiles, in, out, stream);
+        case 1: return launch_kr<T, 1>(R, S, At, tiles, in, out, ib, ob, stream);
+        case 2: return launch_kr<T, 2>(R, S, At, tiles, in, out, ib, ob, stream);
+        case 3: return launch_kr<T, 3>(R, S, At, tiles, in, out, ib, ob, stream);
+        case 4: return launch_kr<T, 4>(R, S, At, tiles, in, out, ib, ob, stream);
+        case 5: return launch_kr<T, 5>(R, S, At, tiles, in, out, ib, ob, stream);
+        case 6: return launch_kr<T, 6>(R, S, At, tiles, in, out, ib, ob, stream);
         case 7:
         case 8:
-        case 9: return launch_kr<T, 9>(R, S, At, tiles, in, out, stream);
+        case 9: return launch_kr<T, 9>(R, S, At, tiles, in, out, ib, ob, stream);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -182,11 +222,14 @@ cudaError_t launch_t(int R, int S, const void* At, const GroupTiles& tiles, Comp
 int gemm_tile_columns(GemmPrecision) { return kTileCols; }
 
 cudaError_t launch_grouped_gemm(GemmPrecision p, int R, int S, const void* matrices, const GroupTiles& tiles,
-                                ComplexOperand in, ComplexOperand out, cudaStream_t stream) {
+                                ComplexOperand in, ComplexOperand out, cudaStream_t stream, const BinBoundary* inBins,
+                                const BinBoundary* outBins) {
     if (tiles.tiles <= 0) return cudaSuccess;
+    const BinBoundary ib = inBins ? *inBins : BinBoundary{};
+    const BinBoundary ob = outBins ? *outBins : BinBoundary{};
     switch (p) {
-        case GemmPrecision::f64: return launch_t<double>(R, S, matrices, tiles, in, out, stream);
-        case GemmPrecision::f32: return launch_t<float>(R, S, matrices, tiles, in, out, stream);
+        case GemmPrecision::f64: return launch_t<double>(R, S, matrices, tiles, in, out, ib, ob, stream);
+        case GemmPrecision::f32: return launch_t<float>(R, S, matrices, tiles, in, out, ib, ob, stream);
         default: return cudaErrorNotSupported;
     }
 }

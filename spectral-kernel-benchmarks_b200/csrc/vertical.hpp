@@ -72,7 +72,10 @@ size_t tc_gemm_smem_bytes(int R, int S);
 int tc_gemm_unit_tiles();
 cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream);
 
+// inBins / outBins (optional): operands in a bin array; the SIMT form
+// supports them for a single ensemble member (column = mode * fields + field).
 cudaError_t launch_grouped_gemm(GemmPrecision p, int R, int S, const void* matrices, const GroupTiles& tiles,
-                                ComplexOperand in, ComplexOperand out, cudaStream_t stream);
+                                ComplexOperand in, ComplexOperand out, cudaStream_t stream,
+                                const BinBoundary* inBins = nullptr, const BinBoundary* outBins = nullptr);
 
 }  // namespace skb

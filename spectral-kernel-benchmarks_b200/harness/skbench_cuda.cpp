@@ -690,6 +690,121 @@ ProviderRecord run_pointwise(const Options& o, const skb_workload& w, Report& re
     return rec;
 }
 
+// The spectral-pipeline round trip composed on the host with the direct
+// transforms (benchmark.cpp:3072-3110 order) for the correctness check.
+std::vector<double> host_pipeline(const skb_workload& w, const std::vector<double>& real) {
+    const auto modes = retained_modes(w);
+    const auto groups = k2_groups(w);
+    const std::uint64_t nz = w.nz, nj = 2 * (nz - 1) / 3, F = w.fields;
+    std::vector<double> fwd(groups.size() * nj * nz), inv(groups.size() * nz * nj), weights(modes.size() * F * nj);
+    std::uint64_t familyGroups = 0;
+    char id[128] = {};
+    ok(skb_vertical_family(&w, SKB_FAMILY_K2_ROTATION, 0, fwd.data(), inv.data(), fwd.size(), &familyGroups, id));
+    ok(skb_modal_weights(&w, weights.data()));
+    std::vector<std::uint64_t> groupOf(modes.size());
+    for (std::uint64_t g = 0; g < groups.size(); ++g)
+        for (std::uint64_t m = 0; m < groups[g].mode_count; ++m) groupOf[groups[g].first_mode + m] = g;
+    const auto spec = direct_r2c(w, real.data());
+    const auto ret = gather(w, modes, spec.data());
+    std::vector<cplx> back(ret.size());
+    for (std::size_t m = 0; m < modes.size(); ++m)
+        for (std::uint64_t f = 0; f < F; ++f) {
+            std::vector<lcplx> modal(nj);
+            for (std::uint64_t j = 0; j < nj; ++j) {
+                lcplx acc = 0;
+                for (std::uint64_t z = 0; z < nz; ++z) {
+                    const cplx v = ret[(m * F + f) * nz + z];
+                    acc += static_cast<long double>(fwd[(groupOf[m] * nj + j) * nz + z]) * lcplx(v.real(), v.imag());
+                }
+                modal[j] = lcplx(static_cast<double>(acc.real()), static_cast<double>(acc.imag())) *
+                           static_cast<long double>(weights[(m * F + f) * nj + j]);
+            }
+            for (std::uint64_t z = 0; z < nz; ++z) {
+                lcplx acc = 0;
+                for (std::uint64_t j = 0; j < nj; ++j)
+                    acc += static_cast<long double>(inv[(groupOf[m] * nz + z) * nj + j]) * modal[j];
+                back[(m * F + f) * nz + z] = cplx(double(acc.real()), double(acc.imag()));
+            }
+        }
+    const auto full = embed(w, modes, back.data());
+    return direct_c2r(w, full.data());
+}
+
+ProviderRecord run_pipeline(const Options& o, const skb_workload& w, Report& report) {
+    const int prec = precision_code(o);
+    const bool f32 = prec == SKB_PRECISION_FP32;
+    const std::uint64_t s = f32 ? 4 : 8, planes = w.nz * w.fields, realN = planes * w.nx * w.ny;
+    std::vector<double> input(realN);
+    ok(skb_make_fixture(&w, 2, o.seed, input.data()));
+    skb_pipeline* h = nullptr;
+    ok(skb_pipeline_create(&w, prec, &h));
+    std::unique_ptr<skb_pipeline, int (*)(skb_pipeline*)> guard(h, skb_pipeline_destroy);
+    void* stream = skb_pipeline_stream(h);
+    skb_provider_info info{};
+    ok(skb_pipeline_info(h, &info));
+    ProviderRecord rec;
+    fill_info(rec, info);
+    rec.algorithmId = f32 ? "pruned FP32 transforms + split-TF32x3 tcgen05 K2 GEMMs + modal work"
+                          : "pruned FP64 transforms + FP64 K2 GEMMs + modal work";
+    rec.nativeRepresentationId = "retained [mode][field][z] / modal [mode][field][j] interleaved";
+    rec.modeOrderId = "radial-two-thirds-sorted(radius,k,l); K^2 groups contiguous";
+    rec.planningConfiguration = "streaming-pruned-compact (device-resident); K^2 pair-rotation family";
+    rec.gemmCallsPerExecution = 2;
+    rec.forward.nativePlacement = "out-of-place device arrays";
+    rec.forward.adapterPlacement = "out-of-place host arrays";
+    rec.inverse = rec.forward;
+    DeviceBuffer dIn(realN * s), dOut(realN * s);
+    if (f32) dIn.upload(narrow<float>(input), stream);
+    else dIn.upload(input, stream);
+    const auto modes = retained_modes(w);
+    const std::uint64_t nj = w.nz < 2 ? 0 : 2 * (w.nz - 1) / 3;
+    const std::uint64_t bytes = 2 * realN * s;
+    rec.timings.push_back(series("primitive", "spectral-pipeline round trip", "shared", bytes,
+                                 measure_device(o.warmups, o.samples, stream, [&] {
+                                     ok(skb_pipeline_execute_device(h, dIn.p, dOut.p, stream));
+                                 })));
+    std::vector<double> hostOut(realN);
+    rec.timings.push_back(series("adapter-total", "spectral-pipeline round trip (host arrays)", "shared", bytes,
+                                 measure_host(o.warmups, o.samples, [&] {
+                                     ok(skb_pipeline_execute(h, input.data(), hostOut.data()));
+                                 })));
+    std::vector<skb_stage_time> stages(16);
+    std::uint64_t count = 0;
+    ok(skb_pipeline_profile(h, dIn.p, dOut.p, stages.data(), stages.size(), &count));
+    for (std::uint64_t i = 0; i < count; ++i)
+        rec.timings.push_back(series("primitive-component", stages[i].name, "shared",
+                                     std::uint64_t(stages[i].algorithmic_bytes), {stages[i].ms * 1e-3}));
+    rec.ledger = {{"horizontal forward + retention", StageState::executed, "pruned rows, active-kx columns"},
+                  {"vertical forward", StageState::executed, "one launch for all K^2 groups"},
+                  {"synthetic modal work", StageState::executed, "one elementwise launch"},
+                  {"vertical inverse", StageState::executed, "one launch for all K^2 groups"},
+                  {"embedding + horizontal inverse", StageState::executed, "kx = 0 repair fused into the columns"}};
+    // Correctness: the host composition with direct transforms where cheap,
+    // else FP32 against the FP64 pipeline on the same input.
+    const double tol = f32 ? 1e-5 : 1e-12;
+    const auto got = hostOut;
+    if (w.nx <= 64 && w.ny <= 64) {
+        const auto used = as_used(input, f32);
+        const auto want = host_pipeline(w, used);
+        rec.correctness.push_back(metric("round trip vs direct host composition",
+                                         max_relative_error(got.data(), want.data(), realN, 1.0),
+                                         relative_l2_error(got.data(), want.data(), realN, 1.0), tol));
+    } else if (f32) {
+        skb_pipeline* h64 = nullptr;
+        ok(skb_pipeline_create(&w, SKB_PRECISION_FP64, &h64));
+        std::unique_ptr<skb_pipeline, int (*)(skb_pipeline*)> g64(h64, skb_pipeline_destroy);
+        std::vector<double> want(realN);
+        ok(skb_pipeline_execute(h64, input.data(), want.data()));
+        rec.correctness.push_back(metric("FP32/TF32x3 vs FP64 pipeline",
+                                         max_relative_error(got.data(), want.data(), realN, 1.0),
+                                         relative_l2_error(got.data(), want.data(), realN, 1.0), tol));
+    }
+    (void)modes;
+    (void)nj;
+    report.verticalMatrixFamilyId = "k2-pair-rotation";
+    return rec;
+}
+
 int flux_mode(const std::string& m) {
     if (m == "fp64-plain") return SKB_FLUX_FP64_PLAIN;
     if (m == "fp32") return SKB_FLUX_FP32;
@@ -1005,7 +1120,7 @@ void usage(std::ostream& out) {
         << "  skbench-cuda list\n"
         << "  skbench-cuda validate [--profile NAME]\n"
         << "  skbench-cuda run [--kernel fft|2d-rfft|pruned-horizontal|vertical-gemm|pointwise-advection|"
-           "production-lifetime-flux] [--profile NAME] [--providers cuda]\n"
+           "production-lifetime-flux|spectral-pipeline] [--profile NAME] [--providers cuda]\n"
         << "              [--precision fp64|fp32] [--vertical-gemm-family common|k2-grouped]\n"
         << "              [--vertical-gemm-precision fp64|fp32|tf32x3] [--flux-mode fp64-plain|fp32|split-tf32x3]\n"
         << "              [--members N] [--targets 3|4] [--nx N --ny N --nz N --fields N]\n"
@@ -1020,7 +1135,7 @@ void list() {
                   << "\n    " << p.purpose << '\n';
     std::cout << "providers:\n  cuda: " << skb_version() << "\n"
               << "kernels:\n  fft (alias 2d-rfft)\n  pruned-horizontal\n  vertical-gemm\n  pointwise-advection\n"
-              << "  production-lifetime-flux\n"
+              << "  production-lifetime-flux\n  spectral-pipeline\n"
               << "precisions:\n  fp64\n  fp32\n"
               << "vertical GEMM precisions:\n  fp64\n  fp32\n  tf32x3\n"
               << "vertical GEMM matrix families:\n  common\n  k2-grouped\n"
@@ -1078,10 +1193,11 @@ int run(int argc, char** argv) {
     else if (o.kernel == "vertical-gemm") rec = run_vertical(o, w, report);
     else if (o.kernel == "pointwise-advection") rec = run_pointwise(o, w, report);
     else if (o.kernel == "production-lifetime-flux") rec = run_flux(o, w, report);
+    else if (o.kernel == "spectral-pipeline") rec = run_pipeline(o, w, report);
     else
         throw std::invalid_argument(
-            "kernel must be 'fft', '2d-rfft', 'pruned-horizontal', 'vertical-gemm', 'pointwise-advection' or "
-            "'production-lifetime-flux'.");
+            "kernel must be 'fft', '2d-rfft', 'pruned-horizontal', 'vertical-gemm', 'pointwise-advection', "
+            "'production-lifetime-flux' or 'spectral-pipeline'.");
     rec.compilerFlags = "nvcc -gencode arch=compute_100a,code=sm_100a -O3";
     rec.sourceIdentity = std::string("libskb_cuda ") + skb_version();
     for (const auto& m : rec.correctness)

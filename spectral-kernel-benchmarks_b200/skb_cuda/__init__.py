@@ -134,7 +134,7 @@ def library():
         lib.skb_last_error.restype = ctypes.c_char_p
         lib.skb_version.restype = ctypes.c_char_p
         for name in ("skb_fft_stream", "skb_pruned_stream", "skb_vertical_stream", "skb_pointwise_stream",
-                     "skb_flux_stream"):
+                     "skb_flux_stream", "skb_vertical_wvm_stream", "skb_pipeline_stream"):
             getattr(lib, name).restype = ctypes.c_void_p
             getattr(lib, name).argtypes = [ctypes.c_void_p]
         _LIB = lib
@@ -615,6 +615,132 @@ class VerticalGemmProvider:
 
 
 # -------------------------------------------------------------- pointwise
+
+class WvmDirectVerticalProvider:
+    """WvmDirectVerticalGemmProvider drop-in: per-mode grouped GEMM on full
+    WVM-order spectra [ky][kx][field][z] <-> modal spectra [ky][kx][field][j],
+    with the kx = 0 boundary copy; output cells without a retained mode are
+    left as they are."""
+
+    def __init__(self, workload: Workload, groups, forward, inverse, buffer_policy=BIDIRECTIONAL,
+                 gemm_precision=GEMM_FP64):
+        self.w = workload
+        self.precision = gemm_precision
+        garr = (ModeGroup * len(groups))(*[ModeGroup(g.squared_mode_key, g.first_mode, g.mode_count)
+                                           for g in groups])
+        fwd = np.ascontiguousarray(forward, dtype=np.float64)
+        inv = np.ascontiguousarray(inverse, dtype=np.float64)
+        h = ctypes.c_void_p()
+        check(library().skb_vertical_wvm_create(ctypes.byref(workload), garr, _u64(len(groups)), _p(fwd), _p(inv),
+                                                ctypes.c_int(buffer_policy), ctypes.c_int(gemm_precision),
+                                                ctypes.byref(h)))
+        self.h = h
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        check(library().skb_vertical_wvm_sizes(self.h, ctypes.byref(a), ctypes.byref(b)))
+        self.spectrum_elements, self.modal_elements = a.value, b.value
+
+    @property
+    def stream(self):
+        return library().skb_vertical_wvm_stream(self.h)
+
+    @property
+    def device_dtype(self):
+        return np.complex128 if self.precision == GEMM_FP64 else np.complex64
+
+    def info(self):
+        return _info(library().skb_vertical_wvm_info, self.h)
+
+    def forward(self, spectrum, out=None):
+        x = _complex(spectrum)
+        y = np.zeros(self.modal_elements, np.complex128) if out is None else _complex(out).copy()
+        check(library().skb_vertical_wvm_forward(self.h, _p(x), _p(y)))
+        return y
+
+    def inverse(self, modal, out=None):
+        x = _complex(modal)
+        y = np.zeros(self.spectrum_elements, np.complex128) if out is None else _complex(out).copy()
+        check(library().skb_vertical_wvm_inverse(self.h, _p(x), _p(y)))
+        return y
+
+    def forward_device(self, spectrum_ptr, modal_ptr, stream=None):
+        check(library().skb_vertical_wvm_forward_device(self.h, ctypes.c_void_p(spectrum_ptr),
+                                                        ctypes.c_void_p(modal_ptr), ctypes.c_void_p(stream)))
+
+    def inverse_device(self, modal_ptr, spectrum_ptr, stream=None):
+        check(library().skb_vertical_wvm_inverse_device(self.h, ctypes.c_void_p(modal_ptr),
+                                                        ctypes.c_void_p(spectrum_ptr), ctypes.c_void_p(stream)))
+
+    def close(self):
+        if self.h:
+            check(library().skb_vertical_wvm_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def modal_weights(w: Workload):
+    """syntheticModalWorkWeights: [mode][field][j] doubles."""
+    out = np.empty(len(retained_modes(w)) * w.fields * w.nj)
+    check(library().skb_modal_weights(ctypes.byref(w), _p(out)))
+    return out
+
+
+class SpectralPipeline:
+    """The spectral-pipeline round trip: r2c + retention, K^2 vertical forward,
+    synthetic modal work, vertical inverse, embedding + c2r (unnormalised)."""
+
+    def __init__(self, workload: Workload, precision=FP64):
+        self.w = workload
+        self.precision = precision
+        h = ctypes.c_void_p()
+        check(library().skb_pipeline_create(ctypes.byref(workload), ctypes.c_int(precision), ctypes.byref(h)))
+        self.h = h
+
+    @property
+    def stream(self):
+        return library().skb_pipeline_stream(self.h)
+
+    @property
+    def device_dtype(self):
+        return np.float64 if self.precision == FP64 else np.float32
+
+    def info(self):
+        return _info(library().skb_pipeline_info, self.h)
+
+    def execute(self, real):
+        x = np.ascontiguousarray(real, dtype=np.float64)
+        assert x.size == self.w.real_elements
+        out = np.empty_like(x)
+        check(library().skb_pipeline_execute(self.h, _p(x), _p(out)))
+        return out
+
+    def execute_device(self, in_ptr, out_ptr, stream=None):
+        check(library().skb_pipeline_execute_device(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr),
+                                                    ctypes.c_void_p(stream)))
+
+    def profile(self, in_ptr, out_ptr):
+        stages = (StageTime * 16)()
+        n = ctypes.c_uint64()
+        check(library().skb_pipeline_profile(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), stages,
+                                             _u64(16), ctypes.byref(n)))
+        return [{"name": stages[i].name.decode(), "ms": stages[i].ms, "launches": stages[i].launches,
+                 "bytes": stages[i].algorithmic_bytes} for i in range(n.value)]
+
+    def close(self):
+        if self.h:
+            check(library().skb_pipeline_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 class PointwiseAdvectionExecutor:
     """PointwiseAdvectionExecutor drop-in: target = -scale*(u qx + v qy + w qz)."""

@@ -209,6 +209,16 @@ def main():
         arrays[f"flux{n}_{nz}_in"] = mi.view(np.complex128)
         arrays[f"flux{n}_{nz}_out"] = mo.view(np.complex128)
 
+    # The spectral-pipeline round trip composed from the reference's functions.
+    n, nz, f = 16, 9, 2
+    m = modes(lib, n, nz, f)
+    nj = 2 * (nz - 1) // 3
+    pin = np.zeros(n * n * nz * f)
+    pw = np.zeros(len(m["k"]) * f * nj)
+    pout = np.zeros(n * n * nz * f)
+    check(lib, lib.skbref_spectral_pipeline(U64(n), U64(nz), U64(f), U64(129), p(pin), p(pw), p(pout)))
+    arrays.update(pipeline_in=pin, pipeline_weights=pw, pipeline_out=pout)
+
     np.savez_compressed(os.path.join(HERE, "reference_vectors.npz"), **arrays)
 
     # The reference report writer's own output, for schema key comparison.

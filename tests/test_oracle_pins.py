@@ -127,3 +127,33 @@ def test_flux_restatement_matches_reference(golden_vectors, nz):
     ref = g[f"flux{n}_{nz}_out"]
     assert orc.max_rel_error(out, ref) <= 1e-12
     assert orc.rel_l2_error(out, ref) <= 1e-12
+
+
+def test_wvm_direct_restatement_agrees_with_retained_path():
+    """The WVM-direct provider's per-mode product on stored cells equals the
+    pinned retained path (gather with conjugation, grouped projection) mapped
+    back to the stored cells: F conj(x) = conj(F x) for the real family."""
+    w = orc.Workload(16, 16, 9, 2)
+    fam = orc.k2_family(w)
+    modes = orc.retained_modes(16, 16)
+    rng = np.random.default_rng(3)
+    half = w.nx // 2 + 1
+    n = w.ny * half * w.fields * w.nz
+    spec = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    y = orc.wvm_direct_vertical(w, fam, "forward", spec).reshape(w.ny, half, w.fields, w.nj)
+    ret = orc.gather_retained(w, modes, spec)
+    mod = orc.grouped_vertical(w, fam, "forward", ret).reshape(len(modes), w.fields, w.nj)
+    for m in range(len(modes)):
+        v = np.conj(mod[m]) if modes.conj[m] else mod[m]
+        assert np.allclose(y[modes.ky[m], modes.kx[m]], v, rtol=0, atol=1e-12)
+
+
+def test_spectral_pipeline_restatement_matches_reference(golden_vectors):
+    """Weights and the round trip against the reference's own functions composed
+    in its spectral-pipeline order (tests/golden/make_golden.py)."""
+    g = golden_vectors
+    w = orc.Workload(16, 16, 9, 2)
+    assert np.array_equal(orc.modal_weights(w), g["pipeline_weights"])
+    assert np.array_equal(orc.make_fixture(w, 2, 129), g["pipeline_in"])
+    out = orc.spectral_pipeline(w, g["pipeline_in"])
+    assert orc.max_rel_error(out, g["pipeline_out"]) <= 1e-12
