@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(32 * B, 4) columns_embed_warp_kernel(int nz, i
             dst->y = -dst->y;
         }
     __syncthreads();
-    warp_fft<float, N, +1>(xs + warp * XP, tw, lane);
+    if (z0 + warp < nz) warp_fft<float, N, +1>(xs + warp * XP, tw, lane);
     __syncthreads();
     if (z < nz) {
         float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * zStride + z + out.planes * kx;
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(32 * B, 4) columns_gather_warp_kernel(int nz, 
         cp_async_wait_all();
     }
     __syncthreads();
-    warp_fft<float, N, -1>(xs + warp * XP, tw, lane);
+    if (z0 + warp < nz) warp_fft<float, N, -1>(xs + warp * XP, tw, lane);
     __syncthreads();
     if (z >= nz) return;
     const FieldView view = views.v[f];
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, in
         }
     }
     __syncthreads();
-    direct_middle_pass<+1>(xs, tw, warp, lane);
+    if (z0 + warp < nz) direct_middle_pass<+1>(xs, tw, warp, lane);  // planes beyond Nz stay idle
     __syncthreads();
     if (!inRange) return;
     float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * zStride + z + out.planes * kx;
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, i
         }
     }
     __syncthreads();
-    direct_middle_pass<-1>(xs, tw, warp, lane);
+    if (z0 + warp < nz) direct_middle_pass<-1>(xs, tw, warp, lane);
     __syncthreads();
     if (!inRange) return;
     const FieldView view = views.v[f];
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(256, 3) columns_inverse_band_kernel(int nz, in
         for (int r = 0; r < 8; ++r) o[r] = v[r];
     }
     __syncthreads();
-    direct_middle_pass<+1>(xs, tw, warp, lane);
+    if (z0 + warp < nz) direct_middle_pass<+1>(xs, tw, warp, lane);  // planes beyond Nz stay idle
     __syncthreads();
     if (!inRange) return;
 #pragma unroll
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(256, 3) columns_forward_band_kernel(int nz, in
         for (int r = 0; r < 8; ++r) o[r] = v[r];
     }
     __syncthreads();
-    direct_middle_pass<-1>(xs, tw, warp, lane);
+    if (z0 + warp < nz) direct_middle_pass<-1>(xs, tw, warp, lane);
     __syncthreads();
     if (!inRange) return;
     const int band = __ldg(bandOf + kx);
@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(32 * B, 4) columns_inverse_band_warp_kernel(in
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
-    warp_fft<float, N, +1>(xs + warp * XP, tw, lane);
+    if (z0 + warp < nz) warp_fft<float, N, +1>(xs + warp * XP, tw, lane);
     __syncthreads();
     if (!inRange) return;
 #pragma unroll
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(32 * B, 4) columns_forward_band_warp_kernel(in
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
-    warp_fft<float, N, -1>(xs + warp * XP, tw, lane);
+    if (z0 + warp < nz) warp_fft<float, N, -1>(xs + warp * XP, tw, lane);
     __syncthreads();
     if (!inRange) return;
     const int band = __ldg(bandOf + kx);

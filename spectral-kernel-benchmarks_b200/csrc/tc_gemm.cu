@@ -416,44 +416,57 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                 tc_fence_after();
                 const uint32_t accBase = tmem + laneBase + static_cast<uint32_t>(acc * NP + half * HALF);
                 const bool first = kc == 0, last = kc == KCH - 1;
+                // Blocks of 8 accumulator columns are handled kG at a time:
+                // their TMEM loads are issued together and waited for once.
+                constexpr int kBlocks = HALF / 8, kG = 3;
 #pragma unroll 1
-                for (int blk = 0; blk < HALF / 8; ++blk) {
-                    uint32_t a[8], b[8];
-                    tmem_ld_x8(accBase + blk * 8, a);
-                    if (!first) tmem_ld_x8(sumBase + blk * 8, b);
-                    tmem_wait_ld();
-                    float x8[8];
+                for (int b0 = 0; b0 < kBlocks; b0 += kG) {
+                    uint32_t a[kG][8], b[kG][8];
 #pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        x8[j] = first ? __uint_as_float(a[j]) : __uint_as_float(b[j]) + __uint_as_float(a[j]);
-                    if (!last) {
-                        uint32_t o[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) o[j] = __float_as_uint(x8[j]);
-                        tmem_st_x8(sumBase + blk * 8, o);
-                        tmem_wait_st();
-                    } else {
-                        // Transpose through this warp's shared buffer so that
-                        // each store instruction writes 64 contiguous bytes
-                        // (8 complex outputs) of four columns.
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) ebuf[(lane >> 1) * kEpiStride + 2 * j + part] = x8[j];
-                        __syncwarp();
-                        const int n = half * HALF + blk * 8 + (lane & 7);
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const int lc = 4 * k + (lane >> 3);
-                            if (storeValid[k] && n < R) {
-                                const float re = ebuf[lc * kEpiStride + 2 * (lane & 7)];
-                                const float im = ebuf[lc * kEpiStride + 2 * (lane & 7) + 1];
-                                p.out[storeColumn[k] + n] = make_float2(re, storeConj[k] ? -im : im);
-                                if (storePartner[k] >= 0)
-                                    p.out[storePartner[k] + n] = make_float2(re, storeConj[k] ? im : -im);
-                            }
+                    for (int i = 0; i < kG; ++i)
+                        if (b0 + i < kBlocks) {
+                            tmem_ld_x8(accBase + (b0 + i) * 8, a[i]);
+                            if (!first) tmem_ld_x8(sumBase + (b0 + i) * 8, b[i]);
                         }
-                        __syncwarp();
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int i = 0; i < kG; ++i) {
+                        if (b0 + i >= kBlocks) break;
+                        const int blk = b0 + i;
+                        float x8[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            x8[j] = first ? __uint_as_float(a[i][j])
+                                          : __uint_as_float(b[i][j]) + __uint_as_float(a[i][j]);
+                        if (!last) {
+                            uint32_t o[8];
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) o[j] = __float_as_uint(x8[j]);
+                            tmem_st_x8(sumBase + blk * 8, o);
+                        } else {
+                            // Transpose through this warp's shared buffer so
+                            // that each store instruction writes 64 contiguous
+                            // bytes (8 complex outputs) of four columns.
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) ebuf[(lane >> 1) * kEpiStride + 2 * j + part] = x8[j];
+                            __syncwarp();
+                            const int n = half * HALF + blk * 8 + (lane & 7);
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                const int lc = 4 * k + (lane >> 3);
+                                if (storeValid[k] && n < R) {
+                                    const float re = ebuf[lc * kEpiStride + 2 * (lane & 7)];
+                                    const float im = ebuf[lc * kEpiStride + 2 * (lane & 7) + 1];
+                                    p.out[storeColumn[k] + n] = make_float2(re, storeConj[k] ? -im : im);
+                                    if (storePartner[k] >= 0)
+                                        p.out[storePartner[k] + n] = make_float2(re, storeConj[k] ? im : -im);
+                                }
+                            }
+                            __syncwarp();
+                        }
                     }
                 }
+                if (!last) tmem_wait_st();
                 tc_fence_before();
                 mbar_arrive(smem_u32(&st->accEmpty[acc]));
             }
