@@ -62,7 +62,7 @@ __device__ __forceinline__ void bin_column(const BinBoundary& bb, int col, long 
     conj = bb.conj != nullptr && __ldg(bb.conj + mode) != 0;
 }
 
-template <typename T, int KR, bool SPLIT>
+template <typename T, int KR, bool SPLIT, bool BINS>
 __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, const T* __restrict__ At,
                                                                 GroupTiles tiles, ComplexOperand in,
                                                                 ComplexOperand out, BinBoundary inBins,
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
     const int ncols = __ldg(tiles.tileCount + tile);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    if (threadIdx.x < kTileCols) {
+    if (BINS && threadIdx.x < kTileCols) {
         const int c = threadIdx.x;
         long long base = static_cast<long long>(c0 + c) * S, partner = -1;
         bool conj = false;
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
         colPartner[c] = partner;
         conjOut[c] = conj ? 1 : 0;
     }
-    __syncthreads();
+    if (BINS) __syncthreads();
     const T* A = At + (long long)g * R * S;
     const int chunks = (S + kChunk - 1) / kChunk;
 
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
         for (int i = threadIdx.x; i < kTileCols * kChunk; i += kThreads) {
             const int c = i / kChunk, s = i % kChunk;
             const bool ok = c < ncols && s0 + s < S;
-            const long long idx = ok ? colIn[c] + s0 + s : 0;
+            const long long idx = ok ? (BINS ? colIn[c] : (long long)(c0 + c) * S) + s0 + s : 0;
             if (SPLIT) {
                 // Split operands: two scalar copies into the complex slot.
                 T* slot = reinterpret_cast<T*>(&sX[c][s]);
@@ -156,8 +156,7 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
             for (int k = 0; k < KR; ++k) a[k] = sA[s][lane + 32 * k];
 #pragma unroll
             for (int m = 0; m < kTileCols / 8; ++m) {
-                V x = sX[warp + 8 * m][s];
-                if (conjIn[warp + 8 * m]) x.y = -x.y;
+                const V x = sX[warp + 8 * m][s];
 #pragma unroll
                 for (int k = 0; k < KR; ++k) {
                     acc[k][m].x = fma(a[k], x.x, acc[k][m].x);
@@ -175,8 +174,14 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
         for (int k = 0; k < KR; ++k) {
             const int r = lane + 32 * k;
             if (r >= R) continue;
+            // The matrices are real, so a conjugated input column gives the
+            // conjugate product: both flags are applied here, once.
             V v = acc[k][m];
-            if (conjOut[c]) v.y = -v.y;
+            if (!BINS) {
+                store_operand<T, SPLIT>(out, (long long)(c0 + c) * R + r, v);
+                continue;
+            }
+            if (conjIn[c] != conjOut[c]) v.y = -v.y;
             store_operand<T, SPLIT>(out, colOut[c] + r, v);
             if (colPartner[c] >= 0) store_operand<T, SPLIT>(out, colPartner[c] + r, V{v.x, -v.y});
         }
@@ -189,7 +194,9 @@ cudaError_t launch_kr(int R, int S, const void* At, const GroupTiles& tiles, Com
     const bool split = in.im != nullptr;
     if (split != (out.im != nullptr)) return cudaErrorInvalidValue;
     const size_t bytes = 2 * (sizeof(cx<T>) * kTileCols * (kChunk + 1) + sizeof(T) * kChunk * 32 * KR);
-    auto kernel = split ? grouped_gemm_kernel<T, KR, true> : grouped_gemm_kernel<T, KR, false>;
+    const bool bins = inBins.cell != nullptr || outBins.cell != nullptr;
+    auto kernel = split ? (bins ? grouped_gemm_kernel<T, KR, true, true> : grouped_gemm_kernel<T, KR, true, false>)
+                        : (bins ? grouped_gemm_kernel<T, KR, false, true> : grouped_gemm_kernel<T, KR, false, false>);
     if (bytes > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (err != cudaSuccess) return err;
