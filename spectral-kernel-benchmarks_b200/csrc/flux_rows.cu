@@ -59,7 +59,6 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
     const long long inRow = a.binsIn.planes;  // stride between kx
     const long long outRow = a.binsOut.planes;
     V* x = xs + warp * XP;  // this warp's plane
-    const bool planeActive = z0 + warp < a.nz;
 
     // Asynchronous copy of slot f's bins of this row into a plane-major stage
     // [b][k]; consecutive threads read consecutive planes of one kx (the
@@ -83,9 +82,6 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
         cp_async_wait_all();
         __syncthreads();
         if (f + 1 < a.fieldsIn) issue(f + 1, ((f + 1) & 1) ? stage1 : stage0);
-        // Warps whose plane lies beyond Nz (the last z-chunk) only take part
-        // in the CTA-wide copies and barriers.
-        if (!planeActive) return;
         const V* st = ((f & 1) ? stage1 : stage0) + warp * KP;
         auto load = [&](int k) -> V {
             if (k >= keep) return V{0.f, 0.f};
@@ -161,7 +157,6 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
 #pragma unroll
         for (int e = 0; e < PER; ++e) acc[e] = {acc[e].x + v[e].x * q[e].x, acc[e].y + v[e].y * q[e].y};
         inverse_row(5 + 3 * t, q);
-        if (planeActive) {
 #pragma unroll
         for (int e = 0; e < PER; ++e)
             acc[e] = {-scale * (acc[e].x + w[e].x * q[e].x), -scale * (acc[e].y + w[e].y * q[e].y)};
@@ -196,7 +191,6 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
             }
             outTile[k * (B + 1) + warp] = X;
         }
-        }  // planeActive
         __syncthreads();
         // Coalesced rows of B planes per kx.
         const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.zStride + z0;
