@@ -281,13 +281,16 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
             throw Error(-2, "unsupported: tensor-core GEMM needs the padded group matrix and two data stages in "
                             "227 KB of shared memory (R=" + std::to_string(rowsOut) + ", S=" + std::to_string(inner) +
                             ")");
-        // Natural-layout FP32 matrices, one per group (a common matrix is
-        // replicated); the kernel splits them into TF32 hi/lo.
-        std::vector<float> f(groups.size() * matrixElems);
-        for (std::uint64_t gi = 0; gi < groups.size(); ++gi)
-            for (std::uint64_t e = 0; e < matrixElems; ++e)
-                f[gi * matrixElems + e] = static_cast<float>(natural[(common ? 0 : gi) * matrixElems + e]);
-        matrices_ = upload_vector(f);
+        // FP32 matrices (one, if common to all groups) -> the kernel's
+        // operand images, split into TF32 hi/lo and swizzled once here.
+        std::vector<float> f(natural.begin(), natural.end());
+        const DeviceBuffer staged = upload_vector(f);
+        const int images = static_cast<int>(groupsCount);
+        imageStride_ = common ? 0 : static_cast<long long>(tc_gemm_image_bytes(rowsOut, inner));
+        matrices_.allocate(static_cast<size_t>(images) * tc_gemm_image_bytes(rowsOut, inner));
+        check_cuda(tc_gemm_build_images(staged.get<float>(), images, rowsOut, inner, matrices_.get(), nullptr),
+                   "tensor-core GEMM operand images");
+        check_cuda(cudaStreamSynchronize(nullptr), "tensor-core GEMM operand images");
         std::vector<int> gc(groups.size()), gf(groups.size());
         for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
             gc[gi] = static_cast<int>(groups[gi].count * fields);
@@ -378,7 +381,8 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
             throw Error(-3, "the tensor-core GEMM form takes interleaved complex operands");
         const UnitTable& table = unitTables_[members - 1];
         TcGemmArgs a{};
-        a.B = matrices_.get<float>();
+        a.B = matrices_.get<unsigned char>();
+        a.imageStride = imageStride_;
         a.R = R_;
         a.S = S_;
         a.NP = (R_ + 15) / 16 * 16;

@@ -177,6 +177,7 @@ private:
     std::uint64_t members_ = 1;
     long long memberColumns_ = 0;
     DeviceBuffer matrices_, tileGroup_, tileColumn_, tileCount_;
+    long long imageStride_ = 0;  // tensor-core form: bytes between group images (0: one common image)
     // Tensor-core work units, one table per active member count 1..members.
     struct UnitTable {
         DeviceBuffer group, column, count;

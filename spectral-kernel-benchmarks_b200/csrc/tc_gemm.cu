@@ -6,24 +6,27 @@
 //     D[m][n] = sum_k Aop[m][k] * Bop[n][k]
 // with m = (column, re/im part) of the data (M = 128 rows = 64 complex
 // columns per tile), n = r (N = R padded to a multiple of 16) and k = s.  Both
-// operands are K-major: Bop is the group matrix in its natural row-major
-// [r][s] layout, Aop is the data row in[c][0..S).
+// operands are K-major: Bop is the group matrix in its row-major [r][s]
+// layout, Aop is the data row in[c][0..S).
 //
 // Split precision: x = hi + lo with hi = rna_tf32(x), lo = rna_tf32(x - hi);
 // D = Ahi*Blo + Alo*Bhi + Ahi*Bhi accumulated in FP32 in tensor memory, one
 // accumulator per 32-wide K chunk, chunk sums added in FP32 registers.  The
 // dropped lo*lo term is ~2^-22 relative.
 //
-// CTA work unit: one group and a run of up to 16 M-tiles of its (member,
-// column) list.  The group matrix is split and written once into shared
-// memory (all K chunks) and stays resident; data chunks of 32 k stream
-// through a three-stage ring filled by producer warps while one MMA lane and
-// the epilogue warps work on earlier chunks (warp specialisation below).  Operands use the canonical K-major
-// SWIZZLE_128B layout: 8-row atoms of 8 x 128 bytes, 16-byte chunk q of row
-// n stored at chunk (q xor n%8).  One elected thread issues the MMAs and
-// commits them to the stage's mbarrier; every wait is bounded and reports
-// through `error` instead of hanging.
+// Work unit: one group and a run of up to 16 M-tiles of its (member,
+// column) list; each CTA (one per SM) walks its share of the units.  The
+// group matrix, split and swizzled once at plan time into an operand image
+// (tc_gemm_build_images), is bulk-copied into shared memory and stays
+// resident for the unit; data chunks of 32 k stream through a three-stage
+// ring filled by producer warps while one MMA lane and the epilogue warps
+// work on earlier chunks (warp specialisation below).  Operands use the
+// canonical K-major SWIZZLE_128B layout: 8-row atoms of 8 x 128 bytes,
+// 16-byte chunk q of row n stored at chunk (q xor n%8).  One elected thread
+// issues the MMAs and commits them to the stage's mbarrier; every wait is
+// bounded and reports through `error` instead of hanging.
 
+#include <algorithm>
 #include <cstdint>
 
 #include "vertical.hpp"
@@ -148,6 +151,25 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// Bulk (non-tensor, single-destination) copy global -> this CTA's shared
+// memory, completing on `bar` by transaction bytes.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+// cp.async of one complex value (8 bytes); srcBytes = 0 writes zeros.
+__device__ __forceinline__ void cp_async_value(uint32_t dst, const void* src, int srcBytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(srcBytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
 // Warp roles of the pipelined kernel.
 constexpr int kProducerWarps = 8;
 constexpr int kMmaWarp = kProducerWarps;
@@ -155,13 +177,47 @@ constexpr int kEpilogueWarps = 8;
 constexpr int kPipeThreads = (kProducerWarps + 1 + kEpilogueWarps) * 32;
 constexpr int kStages = 3;
 constexpr int kAccumulators = 2;
-constexpr int kEpiStride = 17;  // floats per column row of an epilogue warp's transpose buffer
-constexpr int kEpiBytes = kEpilogueWarps * 16 * kEpiStride * 4;
+constexpr int kAhead = 2;               // data chunks each producer thread has in flight
+constexpr uint32_t kBulkPiece = 32768;  // bytes per bulk copy of a group image
 
 struct PipeState {
-    uint64_t full[kStages], empty[kStages], accFull[kAccumulators], accEmpty[kAccumulators], done;
+    uint64_t full[kStages], empty[kStages], accFull[kAccumulators], accEmpty[kAccumulators], done, unitDone, bFull;
     uint32_t tmem;
 };
+
+// Bytes of one group's operand image: hi then lo, each KCH chunks of NP
+// swizzled 128-byte rows.
+__host__ __device__ constexpr long long image_bytes(int NP, int KCH) { return 2LL * KCH * NP * 128; }
+
+// Group matrices [g][R][S] -> their shared-memory operand images: TF32 hi/lo
+// split, zero-padded to NP x KCH*32, K-major SWIZZLE_128B.  One thread per
+// (group, chunk, row, 16-byte piece).
+__global__ void tc_gemm_image_kernel(const float* __restrict__ natural, int groups, int R, int S, int NP, int KCH,
+                                     unsigned char* __restrict__ images) {
+    const long long total = static_cast<long long>(groups) * KCH * NP * 8;
+    const long long bytes = image_bytes(NP, KCH);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int q = static_cast<int>(i & 7);
+        long long rest = i >> 3;
+        const int n = static_cast<int>(rest % NP);
+        rest /= NP;
+        const int kc = static_cast<int>(rest % KCH);
+        const long long g = rest / KCH;
+        const float* m = natural + g * R * S;
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int s = kc * kChunkK + q * 4 + j;
+            v[j] = (n < R && s < S) ? m[static_cast<long long>(n) * S + s] : 0.0f;
+        }
+        const Split4 sp = split4(v[0], v[1], v[2], v[3]);
+        unsigned char* img = images + g * bytes;
+        const uint32_t off = kc * NP * 128 + sw128_offset(n, q);
+        *reinterpret_cast<float4*>(img + off) = sp.hi;
+        *reinterpret_cast<float4*>(img + bytes / 2 + off) = sp.lo;
+    }
+}
 
 // Where virtual column vc of a group lives: element offset of its first
 // value, its Hermitian partner (or -1) and whether the stored value is the
@@ -183,14 +239,40 @@ __device__ __forceinline__ ColumnRef column_ref(const TcGemmArgs& p, const BinBo
     return {__ldg(bb.cell + mode) + off, partner >= 0 ? partner + off : -1, conj};
 }
 
-// Warp-specialised split-TF32x3 grouped GEMM.
-//   producer warps 0-7: data chunk (64 columns x 32 k) -> registers -> TF32
-//       hi/lo -> swizzled A stage of a 3-deep ring; arrive full[stage].
-//   MMA warp 8 (one lane): per chunk, 3 MMAs per k-step into one of two
-//       ping-pong TMEM chunk accumulators; commit empty[stage] and accFull.
+struct Unit {
+    int g, vc0, vcN, gcols, tiles;
+    long long gfirst;
+};
+__device__ __forceinline__ Unit unit_at(const TcGemmArgs& p, int u) {
+    Unit U;
+    U.g = __ldg(p.unitGroup + u);
+    U.vc0 = __ldg(p.unitColumn + u);
+    U.vcN = __ldg(p.unitCount + u);
+    U.gcols = __ldg(p.groupColumns + U.g);
+    U.gfirst = __ldg(p.groupFirst + U.g);
+    U.tiles = (U.vcN + 63) / 64;
+    return U;
+}
+
+// Warp-specialised, persistent split-TF32x3 grouped GEMM.  Each CTA (one per
+// SM) walks the work units blockIdx.x, blockIdx.x + gridDim.x, ...; TMEM, the
+// barriers and the stage ring live across units, and every role counts chunks
+// globally so the barrier phases continue from unit to unit.
+//   producer warps 0-7: data chunks (64 columns x 32 k) stream through a
+//       3-deep ring of A stages.  Each thread copies its values of a chunk
+//       with cp.async into the stage's lo half (raw complex FP32, two chunks
+//       in flight), then the warp rewrites its own 2 KB of the stage in place
+//       as swizzled TF32 hi/lo rows and arrives full[stage].
+//   MMA warp 8 (one lane): per unit, once the previous unit's MMAs have
+//       completed, bulk-copies the group's prepared operand image (hi/lo,
+//       all K chunks) into shared memory and prefetches the next unit's into
+//       L2; per chunk, 3 MMAs per k-step into one of two ping-pong TMEM chunk
+//       accumulators; commits empty[stage] and accFull.
 //   epilogue warps 9-16: add each chunk accumulator into an FP32 running sum
 //       kept in TMEM (tcgen05.ld / tcgen05.st), release it (accEmpty), and
-//       after the tile's last chunk write the tile's outputs.
+//       after the tile's last chunk write the tile's outputs: lane pairs
+//       (the re and im rows of one column) swap halves with a shuffle so each
+//       store instruction writes 16 contiguous bytes of 16 columns.
 // NPH = NP/16: x8 column blocks per epilogue half.
 template <int NPH>
 __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArgs p) {
@@ -202,18 +284,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int KCH = p.KCH, R = p.R, S = p.S;
+    const long long imageBytes = image_bytes(NP, KCH);
     unsigned char* sBhi = base;
-    unsigned char* sBlo = sBhi + KCH * NP * 128;
-    unsigned char* sA = sBlo + KCH * NP * 128;
+    unsigned char* sBlo = sBhi + imageBytes / 2;
+    unsigned char* sA = sBhi + imageBytes;
     PipeState* st = reinterpret_cast<PipeState*>(sA + kStages * kStageBytes);
-
-    const int unit = blockIdx.x;
-    const int g = __ldg(p.unitGroup + unit);
-    const int vc0 = __ldg(p.unitColumn + unit);
-    const int vcN = __ldg(p.unitCount + unit);
-    const int gcols = __ldg(p.groupColumns + g);
-    const long long gfirst = __ldg(p.groupFirst + g);
-    const int tiles = (vcN + 63) / 64;
 
     if (tid == 0) {
         for (int i = 0; i < kStages; ++i) {
@@ -225,112 +300,134 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
             mbar_init(smem_u32(&st->accEmpty[i]), kEpilogueWarps * 32);
         }
         mbar_init(smem_u32(&st->done), 1);
+        mbar_init(smem_u32(&st->unitDone), 1);
+        mbar_init(smem_u32(&st->bFull), 1);
         fence_barrier_init();
     }
     if (warp == kMmaWarp) {
         tmem_alloc(smem_u32(&st->tmem), kTmemCols);
         tmem_relinquish();
     }
-    // L2 prefetch of one tile's data columns (S complex each), 128-byte lines.
-    auto prefetch_tile = [&](int t) {
-        const int tv0 = vc0 + t * 64;
-        const int tcount = min(64, vc0 + vcN - tv0);
-        const int lines = (S * 8 + 127) / 128 + 1;
-        for (int i = tid; i < tcount * lines; i += kProducerWarps * 32) {
-            const int cl = i / lines, l = i % lines;
-            const char* col =
-                reinterpret_cast<const char*>(p.in + column_ref(p, p.inBins, tv0 + cl, gcols, gfirst, S).base);
-            const char* line = reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(col) & ~uintptr_t(127)) + 128 * l;
-            if (line < col + S * 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
-        }
-    };
-    if (warp < kProducerWarps) prefetch_tile(0);
-    // Resident group matrix, split hi/lo, zero-padded to NP x KCH*32.
-    const float* Bg = p.B + static_cast<long long>(g) * R * S;
-    for (int item = tid; item < NP * KCH * 8; item += kPipeThreads) {
-        const int q = item & 7;
-        const int rest = item >> 3;
-        const int kc = rest % KCH;
-        const int n = rest / KCH;
-        float v[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int s = kc * kChunkK + q * 4 + j;
-            v[j] = (n < R && s < S) ? __ldg(Bg + static_cast<long long>(n) * S + s) : 0.0f;
-        }
-        const Split4 sp = split4(v[0], v[1], v[2], v[3]);
-        const uint32_t off = kc * NP * 128 + sw128_offset(n, q);
-        *reinterpret_cast<float4*>(sBhi + off) = sp.hi;
-        *reinterpret_cast<float4*>(sBlo + off) = sp.lo;
-    }
-    fence_proxy_async();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = st->tmem;
     bool failed = false;
+    // A bounded wait that expired: stop this role and make the others stop too.
+    auto fail = [&] {
+        failed = true;
+        atomicExch(p.error, 1);
+    };
 
     if (warp < kProducerWarps) {
         // ---------------------------------------------------------- producer
-        // Chunk it+1's loads are issued before chunk it is converted, so two
-        // chunks of each warp's loads are in flight.  Warp w converts columns
-        // 8w .. 8w+7 of a tile; lane = k within the chunk, so each load
-        // instruction reads one column's 32 consecutive complex values (256
-        // contiguous bytes) and each shared store fills one 128-byte row.
-        const int total = tiles * KCH;
+        // Issue cursor: unit iu, tile itT, chunk itKc of the tile.
+        int iu = blockIdx.x;
+        Unit IU{};
+        if (iu < p.units) IU = unit_at(p, iu);
+        int itT = 0, itKc = 0, curTile = -1, tileCount = 0;
         long long colBase[8];
-        unsigned conjMask = 0;  // bit c: column c of the tile is stored conjugated
-        int loadTile = -1, loadCount = 0;
-        auto load_chunk = [&](int it, float2 (&x)[8]) {
-            const int t = it / KCH, kc = it % KCH;
-            if (t != loadTile) {
-                loadTile = t;
-                const int tv0 = vc0 + t * 64;
-                loadCount = min(64, vc0 + vcN - tv0);
-                conjMask = 0;
-#pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    const int cl = warp * 8 + c;
-                    colBase[c] = 0;
-                    if (cl < loadCount) {
-                        const ColumnRef ref = column_ref(p, p.inBins, tv0 + cl, gcols, gfirst, S);
-                        colBase[c] = ref.base;
-                        conjMask |= ref.conj ? (1u << c) : 0u;
-                    }
-                }
-                // Pull the following tile's columns towards L2 meanwhile.
-                if (t + 1 < tiles) prefetch_tile(t + 1);
-            }
-            const int s = kc * kChunkK + lane;
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                x[c] = make_float2(0.f, 0.f);
-                if (warp * 8 + c < loadCount && s < S) {
-                    x[c] = __ldg(p.in + colBase[c] + s);
-                    if (conjMask & (1u << c)) x[c].y = -x[c].y;
-                }
+        unsigned tileMask = 0;  // bit c: column 8*warp+c of the tile is stored conjugated
+        int issued = 0, converted = 0, pending = 0;
+        unsigned fifo = 0;  // conjugation masks of the chunks in flight, oldest in the low byte
+        // L2 prefetch of one tile's data columns (S complex each).
+        auto prefetch_tile = [&](int t) {
+            const int tv0 = IU.vc0 + t * 64;
+            const int tcount = min(64, IU.vc0 + IU.vcN - tv0);
+            const int lines = (S * 8 + 127) / 128 + 1;
+            for (int i = tid; i < tcount * lines; i += kProducerWarps * 32) {
+                const int cl = i / lines, l = i % lines;
+                const char* col = reinterpret_cast<const char*>(
+                    p.in + column_ref(p, p.inBins, tv0 + cl, IU.gcols, IU.gfirst, S).base);
+                const char* line =
+                    reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(col) & ~uintptr_t(127)) + 128 * l;
+                if (line < col + S * 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
             }
         };
-        float2 next[8];
-        load_chunk(0, next);
-        for (int it = 0; it < total && !failed; ++it) {
-            float2 x[8];
-#pragma unroll
-            for (int c = 0; c < 8; ++c) x[c] = next[c];
-            if (it + 1 < total) load_chunk(it + 1, next);
-            const int stage = it % kStages;
-            const int round = it / kStages;
+        // Copies of the next chunk of the stream into its stage; false at the
+        // end of the stream or on an expired wait.
+        auto issue_next = [&]() -> bool {
+            if (iu >= p.units || failed) return false;
+            const int stage = issued % kStages;
+            const int round = issued / kStages;
             if (round > 0 && !mbar_wait(smem_u32(&st->empty[stage]), (round - 1) & 1, p.error)) {
-                failed = true;
-                break;
+                fail();
+                return false;
             }
+            if (itT != curTile) {
+                curTile = itT;
+                const int tv0 = IU.vc0 + itT * 64;
+                tileCount = min(64, IU.vc0 + IU.vcN - tv0);
+                tileMask = 0;
+#pragma unroll
+                for (int cc = 0; cc < 8; ++cc) {
+                    const int cl = warp * 8 + cc;
+                    colBase[cc] = 0;
+                    if (cl < tileCount) {
+                        const ColumnRef ref = column_ref(p, p.inBins, tv0 + cl, IU.gcols, IU.gfirst, S);
+                        colBase[cc] = ref.base;
+                        tileMask |= ref.conj ? (1u << cc) : 0u;
+                    }
+                }
+                if (itT + 1 < IU.tiles) prefetch_tile(itT + 1);
+            }
+            const uint32_t raw = smem_u32(sA + stage * kStageBytes + kTileRows * 128) + lane * 8;
+            const int s = itKc * kChunkK + lane;
+#pragma unroll
+            for (int cc = 0; cc < 8; ++cc) {
+                const bool ok = warp * 8 + cc < tileCount && s < S;
+                cp_async_value(raw + (warp * 8 + cc) * 256, ok ? p.in + colBase[cc] + s : p.in, ok ? 8 : 0);
+            }
+            cp_async_commit();
+            fifo |= tileMask << (8 * pending);
+            ++pending;
+            ++issued;
+            if (++itKc == KCH) {
+                itKc = 0;
+                if (++itT == IU.tiles) {
+                    itT = 0;
+                    curTile = -1;
+                    iu += gridDim.x;
+                    if (iu < p.units) {
+                        IU = unit_at(p, iu);
+                        prefetch_tile(0);
+                    }
+                }
+            }
+            return true;
+        };
+        if (iu < p.units) prefetch_tile(0);
+        for (int k = 0; k < kAhead; ++k)
+            if (!issue_next()) break;
+        while (pending > 0 && !failed) {
+            // The oldest chunk's copies have landed once at most pending-1
+            // younger groups are outstanding.
+            if (pending > 1)
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            else
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            const int stage = converted % kStages;
             unsigned char* aHi = sA + stage * kStageBytes;
             unsigned char* aLo = aHi + kTileRows * 128;
+            const unsigned m = fifo & 0xFFu;
+            fifo >>= 8;
+            --pending;
+            ++converted;
+            // This warp's columns occupy bytes [2048 warp, +2048) of the lo
+            // half both as raw values and as swizzled rows 16 warp .. +15, so
+            // the rewrite stays inside the warp once all its reads are done.
+            float2 x[8];
 #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const int cl = warp * 8 + c;
-                const float rh = tf32_rna(x[c].x), ih = tf32_rna(x[c].y);
-                const float rl = tf32_rna(x[c].x - rh), il = tf32_rna(x[c].y - ih);
+            for (int cc = 0; cc < 8; ++cc) {
+                x[cc] = *reinterpret_cast<const float2*>(aLo + (warp * 8 + cc) * 256 + lane * 8);
+                if (m & (1u << cc)) x[cc].y = -x[cc].y;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int cc = 0; cc < 8; ++cc) {
+                const int cl = warp * 8 + cc;
+                const float rh = tf32_rna(x[cc].x), ih = tf32_rna(x[cc].y);
+                const float rl = tf32_rna(x[cc].x - rh), il = tf32_rna(x[cc].y - ih);
                 const uint32_t o0 = sw128_offset(2 * cl, lane >> 2) + 4 * (lane & 3);
                 const uint32_t o1 = sw128_offset(2 * cl + 1, lane >> 2) + 4 * (lane & 3);
                 *reinterpret_cast<float*>(aHi + o0) = rh;
@@ -340,135 +437,162 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
             }
             fence_proxy_async();
             mbar_arrive(smem_u32(&st->full[stage]));
+            issue_next();
         }
+        // No copy may still be writing this CTA's shared memory at exit.
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
     } else if (warp == kMmaWarp) {
         // --------------------------------------------------------------- MMA
         if (lane == 0) {
             const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(NP >> 3) << 17) |
                                    (static_cast<uint32_t>(kTileRows >> 4) << 24);
-            int it = 0;
-            for (int t = 0; t < tiles && !failed; ++t) {
-                for (int kc = 0; kc < KCH; ++kc, ++it) {
-                    const int stage = it % kStages;
-                    const int acc = it % kAccumulators;
-                    const int accRound = it / kAccumulators;
-                    if (!mbar_wait(smem_u32(&st->full[stage]), (it / kStages) & 1, p.error) ||
-                        (accRound > 0 &&
-                         !mbar_wait(smem_u32(&st->accEmpty[acc]), (accRound - 1) & 1, p.error))) {
-                        failed = true;
+            int it = 0, loads = 0, group = -1;
+            for (int u = blockIdx.x; u < p.units && !failed; u += gridDim.x) {
+                const Unit U = unit_at(p, u);
+                if (U.g != group) {
+                    // The resident image may be replaced once every MMA that
+                    // reads it has completed.
+                    if (loads > 0) {
+                        mma_commit(smem_u32(&st->unitDone));
+                        if (!mbar_wait(smem_u32(&st->unitDone), (loads - 1) & 1, p.error)) {
+                            fail();
+                            break;
+                        }
+                    }
+                    const unsigned char* img = p.B + static_cast<long long>(U.g) * p.imageStride;
+                    mbar_expect_tx(smem_u32(&st->bFull), static_cast<uint32_t>(imageBytes));
+                    for (uint32_t o = 0; o < imageBytes; o += kBulkPiece)
+                        bulk_load(smem_u32(sBhi + o), img + o, min(kBulkPiece, static_cast<uint32_t>(imageBytes - o)),
+                                  smem_u32(&st->bFull));
+                    if (u + static_cast<int>(gridDim.x) < p.units) {
+                        const int gn = __ldg(p.unitGroup + u + gridDim.x);
+                        if (gn != U.g)
+                            bulk_prefetch_l2(p.B + static_cast<long long>(gn) * p.imageStride,
+                                             static_cast<uint32_t>(imageBytes));
+                    }
+                    if (!mbar_wait(smem_u32(&st->bFull), loads & 1, p.error)) {
+                        fail();
                         break;
                     }
-                    tc_fence_after();
-                    const uint32_t aH = smem_u32(sA + stage * kStageBytes);
-                    const uint32_t aL = aH + kTileRows * 128;
-                    const uint32_t bH = smem_u32(sBhi + kc * NP * 128), bL = smem_u32(sBlo + kc * NP * 128);
-                    const uint32_t d = tmem + static_cast<uint32_t>(acc * NP);
-                    const int ksteps = min(4, (S - kc * kChunkK + 7) / 8);
-                    for (int j = 0; j < ksteps; ++j) {
-                        const uint32_t off = j * 32;
-                        mma_tf32(d, sw128_desc(aH + off), sw128_desc(bL + off), idesc, j > 0 ? 1u : 0u);
-                        mma_tf32(d, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
-                        mma_tf32(d, sw128_desc(aH + off), sw128_desc(bH + off), idesc, 1u);
+                    ++loads;
+                    group = U.g;
+                }
+                for (int t = 0; t < U.tiles && !failed; ++t) {
+                    for (int kc = 0; kc < KCH; ++kc, ++it) {
+                        const int stage = it % kStages;
+                        const int acc = it % kAccumulators;
+                        const int accRound = it / kAccumulators;
+                        if (!mbar_wait(smem_u32(&st->full[stage]), (it / kStages) & 1, p.error) ||
+                            (accRound > 0 &&
+                             !mbar_wait(smem_u32(&st->accEmpty[acc]), (accRound - 1) & 1, p.error))) {
+                            fail();
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t aH = smem_u32(sA + stage * kStageBytes);
+                        const uint32_t aL = aH + kTileRows * 128;
+                        const uint32_t bH = smem_u32(sBhi + kc * NP * 128), bL = smem_u32(sBlo + kc * NP * 128);
+                        const uint32_t d = tmem + static_cast<uint32_t>(acc * NP);
+                        const int ksteps = min(4, (S - kc * kChunkK + 7) / 8);
+                        for (int j = 0; j < ksteps; ++j) {
+                            const uint32_t off = j * 32;
+                            mma_tf32(d, sw128_desc(aH + off), sw128_desc(bL + off), idesc, j > 0 ? 1u : 0u);
+                            mma_tf32(d, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
+                            mma_tf32(d, sw128_desc(aH + off), sw128_desc(bH + off), idesc, 1u);
+                        }
+                        mma_commit(smem_u32(&st->empty[stage]));
+                        mma_commit(smem_u32(&st->accFull[acc]));
                     }
-                    mma_commit(smem_u32(&st->empty[stage]));
-                    mma_commit(smem_u32(&st->accFull[acc]));
                 }
             }
             // Every issued MMA has completed once this commit lands.
             mma_commit(smem_u32(&st->done));
-            if (!mbar_wait(smem_u32(&st->done), 0, p.error)) failed = true;
+            if (!mbar_wait(smem_u32(&st->done), 0, p.error)) fail();
         }
         __syncwarp();
     } else {
         // ---------------------------------------------------------- epilogue
         // Running chunk sums live in a third TMEM region (columns 2*NP ..),
-        // read-added-stored eight columns at a time, so only 16 values are
-        // live per thread.  The final chunk's sum goes straight to global.
+        // read-added-stored eight columns at a time.  The final chunk's sum
+        // goes straight to global memory.  TMEM lane 32*quarter + lane is
+        // tile row 2*column + part: this lane holds the real (part 0) or
+        // imaginary (part 1) row of column 16*quarter + lane/2.
         const int quarter = warp & 3;  // TMEM lanes this warp may access
         const int half = (warp - kMmaWarp - 1) >> 2;
         const int part = lane & 1;
-        float* ebuf = reinterpret_cast<float*>(st + 1) + (warp - kMmaWarp - 1) * 16 * kEpiStride;
+        const int cl = quarter * 16 + (lane >> 1);
         const uint32_t laneBase = static_cast<uint32_t>(quarter * 32) << 16;
         const uint32_t sumBase = tmem + laneBase + static_cast<uint32_t>(kAccumulators * NP + half * HALF);
         int it = 0;
-        for (int t = 0; t < tiles && !failed; ++t) {
-            const int tv0 = vc0 + t * 64;
-            const int tcount = min(64, vc0 + vcN - tv0);
-            // The four columns this lane stores in the transposed epilogue.
-            bool storeValid[4], storeConj[4];
-            long long storeColumn[4], storePartner[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int sc = quarter * 16 + 4 * k + (lane >> 3);
-                storeValid[k] = sc < tcount;
+        for (int u = blockIdx.x; u < p.units && !failed; u += gridDim.x) {
+            const Unit U = unit_at(p, u);
+            for (int t = 0; t < U.tiles && !failed; ++t) {
+                const int tv0 = U.vc0 + t * 64;
+                const bool valid = cl < min(64, U.vc0 + U.vcN - tv0);
                 const ColumnRef ref =
-                    storeValid[k] ? column_ref(p, p.outBins, tv0 + sc, gcols, gfirst, R) : ColumnRef{0, -1, false};
-                storeColumn[k] = ref.base;
-                storePartner[k] = ref.partner;
-                storeConj[k] = ref.conj;
-            }
-            for (int kc = 0; kc < KCH; ++kc, ++it) {
-                const int acc = it % kAccumulators;
-                if (!mbar_wait(smem_u32(&st->accFull[acc]), (it / kAccumulators) & 1, p.error)) {
-                    failed = true;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t accBase = tmem + laneBase + static_cast<uint32_t>(acc * NP + half * HALF);
-                const bool first = kc == 0, last = kc == KCH - 1;
-                // Blocks of 8 accumulator columns are handled kG at a time:
-                // their TMEM loads are issued together and waited for once.
-                constexpr int kBlocks = HALF / 8, kG = 3;
+                    valid ? column_ref(p, p.outBins, tv0 + cl, U.gcols, U.gfirst, R) : ColumnRef{0, -1, false};
+                for (int kc = 0; kc < KCH; ++kc, ++it) {
+                    const int acc = it % kAccumulators;
+                    if (!mbar_wait(smem_u32(&st->accFull[acc]), (it / kAccumulators) & 1, p.error)) {
+                        fail();
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t accBase = tmem + laneBase + static_cast<uint32_t>(acc * NP + half * HALF);
+                    const bool first = kc == 0, last = kc == KCH - 1;
+                    // Blocks of 8 accumulator columns are handled kG at a
+                    // time: their TMEM loads are issued together and waited
+                    // for once.
+                    constexpr int kBlocks = HALF / 8, kG = 3;
 #pragma unroll 1
-                for (int b0 = 0; b0 < kBlocks; b0 += kG) {
-                    uint32_t a[kG][8], b[kG][8];
+                    for (int b0 = 0; b0 < kBlocks; b0 += kG) {
+                        uint32_t a[kG][8], b[kG][8];
 #pragma unroll
-                    for (int i = 0; i < kG; ++i)
-                        if (b0 + i < kBlocks) {
-                            tmem_ld_x8(accBase + (b0 + i) * 8, a[i]);
-                            if (!first) tmem_ld_x8(sumBase + (b0 + i) * 8, b[i]);
-                        }
-                    tmem_wait_ld();
+                        for (int i = 0; i < kG; ++i)
+                            if (b0 + i < kBlocks) {
+                                tmem_ld_x8(accBase + (b0 + i) * 8, a[i]);
+                                if (!first) tmem_ld_x8(sumBase + (b0 + i) * 8, b[i]);
+                            }
+                        tmem_wait_ld();
 #pragma unroll
-                    for (int i = 0; i < kG; ++i) {
-                        if (b0 + i >= kBlocks) break;
-                        const int blk = b0 + i;
-                        float x8[8];
+                        for (int i = 0; i < kG; ++i) {
+                            if (b0 + i >= kBlocks) break;
+                            const int blk = b0 + i;
+                            float x8[8];
 #pragma unroll
-                        for (int j = 0; j < 8; ++j)
-                            x8[j] = first ? __uint_as_float(a[i][j])
-                                          : __uint_as_float(b[i][j]) + __uint_as_float(a[i][j]);
-                        if (!last) {
-                            uint32_t o[8];
+                            for (int j = 0; j < 8; ++j)
+                                x8[j] = first ? __uint_as_float(a[i][j])
+                                              : __uint_as_float(b[i][j]) + __uint_as_float(a[i][j]);
+                            if (!last) {
+                                uint32_t o[8];
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) o[j] = __float_as_uint(x8[j]);
-                            tmem_st_x8(sumBase + blk * 8, o);
-                        } else {
-                            // Transpose through this warp's shared buffer so
-                            // that each store instruction writes 64 contiguous
-                            // bytes (8 complex outputs) of four columns.
+                                for (int j = 0; j < 8; ++j) o[j] = __float_as_uint(x8[j]);
+                                tmem_st_x8(sumBase + blk * 8, o);
+                            } else {
+                                // Rows n0 .. n0+7 of this column: the even lane
+                                // takes outputs n0+2k, the odd lane n0+2k+1,
+                                // each trading the other part with its partner.
+                                const int n0 = half * HALF + blk * 8;
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) ebuf[(lane >> 1) * kEpiStride + 2 * j + part] = x8[j];
-                            __syncwarp();
-                            const int n = half * HALF + blk * 8 + (lane & 7);
-#pragma unroll
-                            for (int k = 0; k < 4; ++k) {
-                                const int lc = 4 * k + (lane >> 3);
-                                if (storeValid[k] && n < R) {
-                                    const float re = ebuf[lc * kEpiStride + 2 * (lane & 7)];
-                                    const float im = ebuf[lc * kEpiStride + 2 * (lane & 7) + 1];
-                                    p.out[storeColumn[k] + n] = make_float2(re, storeConj[k] ? -im : im);
-                                    if (storePartner[k] >= 0)
-                                        p.out[storePartner[k] + n] = make_float2(re, storeConj[k] ? im : -im);
+                                for (int k = 0; k < 4; ++k) {
+                                    const float mine = part ? x8[2 * k + 1] : x8[2 * k];
+                                    const float other = __shfl_xor_sync(0xFFFFFFFFu, part ? x8[2 * k] : x8[2 * k + 1], 1);
+                                    const float re = part ? other : mine;
+                                    const float im = part ? mine : other;
+                                    const int n = n0 + 2 * k + part;
+                                    if (valid && n < R) {
+                                        p.out[ref.base + n] = make_float2(re, ref.conj ? -im : im);
+                                        if (ref.partner >= 0)
+                                            p.out[ref.partner + n] = make_float2(re, ref.conj ? im : -im);
+                                    }
                                 }
                             }
-                            __syncwarp();
                         }
                     }
+                    if (!last) tmem_wait_st();
+                    tc_fence_before();
+                    mbar_arrive(smem_u32(&st->accEmpty[acc]));
                 }
-                if (!last) tmem_wait_st();
-                tc_fence_before();
-                mbar_arrive(smem_u32(&st->accEmpty[acc]));
             }
         }
     }
@@ -483,13 +607,27 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
 size_t tc_gemm_smem_bytes(int R, int S) {
     const int NP = (R + 15) / 16 * 16;
     const int KCH = (S + kChunkK - 1) / kChunkK;
-    return 1024 + 2 * static_cast<size_t>(KCH) * NP * 128 + kStages * kStageBytes + sizeof(PipeState) + 16 +
-           kEpiBytes;
+    return 1024 + static_cast<size_t>(image_bytes(NP, KCH)) + kStages * kStageBytes + sizeof(PipeState) + 16;
 }
 
 bool tc_gemm_supported(int R, int S) {
     const int NP = (R + 15) / 16 * 16;
-    return NP >= 16 && (kAccumulators + 1) * NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
+    return NP >= 16 && NP <= 160 && (kAccumulators + 1) * NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
+}
+
+size_t tc_gemm_image_bytes(int R, int S) {
+    return static_cast<size_t>(image_bytes((R + 15) / 16 * 16, (S + kChunkK - 1) / kChunkK));
+}
+
+cudaError_t tc_gemm_build_images(const float* natural, int groups, int R, int S, void* images, cudaStream_t stream) {
+    if (groups <= 0) return cudaSuccess;
+    const int NP = (R + 15) / 16 * 16;
+    const int KCH = (S + kChunkK - 1) / kChunkK;
+    const long long items = static_cast<long long>(groups) * KCH * NP * 8;
+    const int blocks = static_cast<int>(std::min<long long>((items + 255) / 256, 148LL * 16));
+    tc_gemm_image_kernel<<<blocks, 256, 0, stream>>>(natural, groups, R, S, NP, KCH,
+                                                     static_cast<unsigned char*>(images));
+    return cudaGetLastError();
 }
 
 int tc_gemm_unit_tiles() { return 16; }
@@ -497,11 +635,20 @@ int tc_gemm_unit_tiles() { return 16; }
 namespace {
 template <int NPH>
 cudaError_t launch_np(const TcGemmArgs& args, cudaStream_t stream) {
-    const size_t bytes = tc_gemm_smem_bytes(args.R, args.S);
+    // At least half an SM's shared memory, so that two CTAs (each holding
+    // all 512 TMEM columns) never share an SM.
+    const size_t bytes = std::max<size_t>(tc_gemm_smem_bytes(args.R, args.S), 116 * 1024);
     auto kernel = tc_gemm_pipe_kernel<NPH>;
     const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (err != cudaSuccess) return err;
-    kernel<<<args.units, kPipeThreads, bytes, stream>>>(args);
+    // Persistent: one CTA per SM (or per unit, if fewer).
+    static int smCount[64] = {};
+    int device = 0;
+    cudaGetDevice(&device);
+    if (device >= 0 && device < 64 && smCount[device] == 0)
+        cudaDeviceGetAttribute(&smCount[device], cudaDevAttrMultiProcessorCount, device);
+    const int sms = (device >= 0 && device < 64 && smCount[device] > 0) ? smCount[device] : 148;
+    kernel<<<std::min(args.units, sms), kPipeThreads, bytes, stream>>>(args);
     return cudaGetLastError();
 }
 }  // namespace

@@ -53,7 +53,10 @@ struct BinBoundary {
 };
 
 struct TcGemmArgs {
-    const float* B;  // group matrices in natural layout [g][R][S], FP32
+    // Group operand images (tc_gemm_build_images), one every imageStride
+    // bytes; imageStride 0: one image shared by all groups.
+    const unsigned char* B;
+    long long imageStride;
     int R, S, NP, KCH;
     const int* unitGroup;
     const int* unitColumn;  // first virtual column of the unit
@@ -69,6 +72,12 @@ struct TcGemmArgs {
 };
 bool tc_gemm_supported(int R, int S);
 size_t tc_gemm_smem_bytes(int R, int S);
+// Bytes of one group's operand image: the group matrix split into TF32 hi/lo
+// parts, zero-padded to a multiple of 16 rows and of 32 k, in the swizzled
+// shared-memory layout the kernel's MMAs read.
+size_t tc_gemm_image_bytes(int R, int S);
+// natural [groups][R][S] FP32 (device) -> images[groups] (device).
+cudaError_t tc_gemm_build_images(const float* natural, int groups, int R, int S, void* images, cudaStream_t stream);
 int tc_gemm_unit_tiles();
 cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream);
 
