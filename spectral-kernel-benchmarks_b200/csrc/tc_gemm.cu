@@ -330,19 +330,17 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         unsigned tileMask = 0;  // bit c: column 8*warp+c of the tile is stored conjugated
         int issued = 0, converted = 0, pending = 0;
         unsigned fifo = 0;  // conjugation masks of the chunks in flight, oldest in the low byte
-        // L2 prefetch of one tile's data columns (S complex each).
-        auto prefetch_tile = [&](int t) {
-            const int tv0 = IU.vc0 + t * 64;
-            const int tcount = min(64, IU.vc0 + IU.vcN - tv0);
-            const int lines = (S * 8 + 127) / 128 + 1;
-            for (int i = tid; i < tcount * lines; i += kProducerWarps * 32) {
-                const int cl = i / lines, l = i % lines;
-                const char* col = reinterpret_cast<const char*>(
-                    p.in + column_ref(p, p.inBins, tv0 + cl, IU.gcols, IU.gfirst, S).base);
-                const char* line =
-                    reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(col) & ~uintptr_t(127)) + 128 * l;
-                if (line < col + S * 8) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
-            }
+        // L2 prefetch of column 8*warp + lane (lanes 0-7) of tile t of unit V
+        // (compact operand only: bin-array columns would first need their
+        // cells, a dependent load this warp would wait for).
+        auto prefetch_tile = [&](const Unit& V, int t) {
+            if (p.inBins.cell != nullptr || lane >= 8) return;
+            const int tv0 = V.vc0 + t * 64;
+            const int cl = warp * 8 + lane;
+            if (cl >= min(64, V.vc0 + V.vcN - tv0)) return;
+            const uintptr_t first = reinterpret_cast<uintptr_t>(p.in + column_ref(p, p.inBins, tv0 + cl, V.gcols, V.gfirst, S).base);
+            const uintptr_t a = (first + 15) & ~uintptr_t(15), b = (first + S * 8) & ~uintptr_t(15);
+            if (b > a) bulk_prefetch_l2(reinterpret_cast<const void*>(a), static_cast<uint32_t>(b - a));
         };
         // Copies of the next chunk of the stream into its stage; false at the
         // end of the stream or on an expired wait.
@@ -355,21 +353,21 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                 return false;
             }
             if (itT != curTile) {
+                // Lanes 0-7 look up one column each; the warp shares them.
                 curTile = itT;
                 const int tv0 = IU.vc0 + itT * 64;
                 tileCount = min(64, IU.vc0 + IU.vcN - tv0);
-                tileMask = 0;
+                const int cl = warp * 8 + lane;
+                ColumnRef mine{0, -1, false};
+                if (lane < 8 && cl < tileCount) mine = column_ref(p, p.inBins, tv0 + cl, IU.gcols, IU.gfirst, S);
+                tileMask = __ballot_sync(0xFFFFFFFFu, lane < 8 && mine.conj) & 0xFFu;
 #pragma unroll
-                for (int cc = 0; cc < 8; ++cc) {
-                    const int cl = warp * 8 + cc;
-                    colBase[cc] = 0;
-                    if (cl < tileCount) {
-                        const ColumnRef ref = column_ref(p, p.inBins, tv0 + cl, IU.gcols, IU.gfirst, S);
-                        colBase[cc] = ref.base;
-                        tileMask |= ref.conj ? (1u << cc) : 0u;
-                    }
+                for (int cc = 0; cc < 8; ++cc) colBase[cc] = __shfl_sync(0xFFFFFFFFu, mine.base, cc);
+                if (itT + 1 < IU.tiles) {
+                    prefetch_tile(IU, itT + 1);
+                } else if (iu + static_cast<int>(gridDim.x) < p.units) {
+                    prefetch_tile(unit_at(p, iu + gridDim.x), 0);
                 }
-                if (itT + 1 < IU.tiles) prefetch_tile(itT + 1);
             }
             const uint32_t raw = smem_u32(sA + stage * kStageBytes + kTileRows * 128) + lane * 8;
             const int s = itKc * kChunkK + lane;
@@ -388,15 +386,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                     itT = 0;
                     curTile = -1;
                     iu += gridDim.x;
-                    if (iu < p.units) {
-                        IU = unit_at(p, iu);
-                        prefetch_tile(0);
-                    }
+                    if (iu < p.units) IU = unit_at(p, iu);
                 }
             }
             return true;
         };
-        if (iu < p.units) prefetch_tile(0);
+        if (iu < p.units) prefetch_tile(IU, 0);
         for (int k = 0; k < kAhead; ++k)
             if (!issue_next()) break;
         while (pending > 0 && !failed) {
@@ -531,6 +526,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                 const bool valid = cl < min(64, U.vc0 + U.vcN - tv0);
                 const ColumnRef ref =
                     valid ? column_ref(p, p.outBins, tv0 + cl, U.gcols, U.gfirst, R) : ColumnRef{0, -1, false};
+                const float sg = ref.conj ? -1.0f : 1.0f;
+                // 16-byte stores need even element offsets (true for bin cells).
+                const bool wide = ((ref.base | (ref.partner < 0 ? 0 : ref.partner)) & 1) == 0;
                 for (int kc = 0; kc < KCH; ++kc, ++it) {
                     const int acc = it % kAccumulators;
                     if (!mbar_wait(smem_u32(&st->accFull[acc]), (it / kAccumulators) & 1, p.error)) {
@@ -569,21 +567,45 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                                 for (int j = 0; j < 8; ++j) o[j] = __float_as_uint(x8[j]);
                                 tmem_st_x8(sumBase + blk * 8, o);
                             } else {
-                                // Rows n0 .. n0+7 of this column: the even lane
-                                // takes outputs n0+2k, the odd lane n0+2k+1,
-                                // each trading the other part with its partner.
+                                // Rows n0 .. n0+7 of this column.  The even lane
+                                // stores outputs n0+{0,1} and n0+{4,5}, the odd
+                                // lane n0+{2,3} and n0+{6,7}, after trading the
+                                // other part with its partner, so each store
+                                // instruction fills whole 32-byte sectors of 16
+                                // columns.
                                 const int n0 = half * HALF + blk * 8;
+                                float o[4];
 #pragma unroll
                                 for (int k = 0; k < 4; ++k) {
-                                    const float mine = part ? x8[2 * k + 1] : x8[2 * k];
-                                    const float other = __shfl_xor_sync(0xFFFFFFFFu, part ? x8[2 * k] : x8[2 * k + 1], 1);
-                                    const float re = part ? other : mine;
-                                    const float im = part ? mine : other;
-                                    const int n = n0 + 2 * k + part;
-                                    if (valid && n < R) {
-                                        p.out[ref.base + n] = make_float2(re, ref.conj ? -im : im);
-                                        if (ref.partner >= 0)
-                                            p.out[ref.partner + n] = make_float2(re, ref.conj ? im : -im);
+                                    const int e = (k & 1) + 4 * (k >> 1);
+                                    o[k] = __shfl_xor_sync(0xFFFFFFFFu, part ? x8[e] : x8[e + 2], 1);
+                                }
+                                if (valid) {
+#pragma unroll
+                                    for (int h2 = 0; h2 < 2; ++h2) {
+                                        const int e = 4 * h2;
+                                        const int n = n0 + e + 2 * part;
+                                        const float re0 = part ? o[2 * h2] : x8[e];
+                                        const float im0 = sg * (part ? x8[e + 2] : o[2 * h2]);
+                                        const float re1 = part ? o[2 * h2 + 1] : x8[e + 1];
+                                        const float im1 = sg * (part ? x8[e + 3] : o[2 * h2 + 1]);
+                                        if (wide && n + 1 < R) {
+                                            *reinterpret_cast<float4*>(p.out + ref.base + n) =
+                                                make_float4(re0, im0, re1, im1);
+                                            if (ref.partner >= 0)
+                                                *reinterpret_cast<float4*>(p.out + ref.partner + n) =
+                                                    make_float4(re0, -im0, re1, -im1);
+                                        } else {
+                                            if (n < R) {
+                                                p.out[ref.base + n] = make_float2(re0, im0);
+                                                if (ref.partner >= 0) p.out[ref.partner + n] = make_float2(re0, -im0);
+                                            }
+                                            if (n + 1 < R) {
+                                                p.out[ref.base + n + 1] = make_float2(re1, im1);
+                                                if (ref.partner >= 0)
+                                                    p.out[ref.partner + n + 1] = make_float2(re1, -im1);
+                                            }
+                                        }
                                     }
                                 }
                             }
