@@ -189,6 +189,13 @@ struct PipeState {
 // swizzled 128-byte rows.
 __host__ __device__ constexpr long long image_bytes(int NP, int KCH) { return 2LL * KCH * NP * 128; }
 
+// k (within a 32-wide chunk) held by element e of 16-byte piece q of an
+// operand row: pieces pair k = 2q, 2q+1 with k = 2q+16, 2q+17 so that the
+// producer warps fill them with conflict-free 16-byte shared-memory accesses.
+// The MMA's k-step j (pieces 2j, 2j+1) thus covers k = 4j..4j+3 and
+// 4j+16..4j+19.
+__host__ __device__ constexpr int kperm(int q, int e) { return 2 * q + (e & 1) + 16 * (e >> 1); }
+
 // Group matrices [g][R][S] -> their shared-memory operand images: TF32 hi/lo
 // split, zero-padded to NP x KCH*32, K-major SWIZZLE_128B.  One thread per
 // (group, chunk, row, 16-byte piece).
@@ -208,7 +215,7 @@ __global__ void tc_gemm_image_kernel(const float* __restrict__ natural, int grou
         float v[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int s = kc * kChunkK + q * 4 + j;
+            const int s = kc * kChunkK + kperm(q, j);
             v[j] = (n < R && s < S) ? m[static_cast<long long>(n) * S + s] : 0.0f;
         }
         const Split4 sp = split4(v[0], v[1], v[2], v[3]);
@@ -408,27 +415,38 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
             fifo >>= 8;
             --pending;
             ++converted;
-            // This warp's columns occupy bytes [2048 warp, +2048) of the lo
-            // half both as raw values and as swizzled rows 16 warp .. +15, so
-            // the rewrite stays inside the warp once all its reads are done.
-            float2 x[8];
+            // This warp's 8 columns sit as raw complex values (column c at
+            // byte 256c, value k at 8k) in bytes [2048 warp, +2048) of the lo
+            // half, which are also the swizzled rows 16 warp .. +15 they
+            // become, so the warp rewrites them in place once all its reads
+            // are done.  In pass j a lane takes column 8 warp + 4j + lane/8
+            // and the values k = 2q, 2q+1, 2q+16, 2q+17 (q = lane % 8): two
+            // 16-byte reads 128 bytes apart, so each 8-lane phase reads 128
+            // contiguous bytes, then four 16-byte writes of piece q of the
+            // column's re and im rows (hi and lo).  Within each 16-byte piece
+            // the k order is the operand order (kperm), shared with the
+            // group images, so the MMA sums the same products.
+            const int q = lane & 7;
+            float4 v[2][2];
 #pragma unroll
-            for (int cc = 0; cc < 8; ++cc) {
-                x[cc] = *reinterpret_cast<const float2*>(aLo + (warp * 8 + cc) * 256 + lane * 8);
-                if (m & (1u << cc)) x[cc].y = -x[cc].y;
+            for (int j = 0; j < 2; ++j) {
+                const unsigned char* src = aLo + (warp * 8 + 4 * j + (lane >> 3)) * 256 + q * 16;
+                v[j][0] = *reinterpret_cast<const float4*>(src);
+                v[j][1] = *reinterpret_cast<const float4*>(src + 128);
             }
             __syncwarp();
 #pragma unroll
-            for (int cc = 0; cc < 8; ++cc) {
+            for (int j = 0; j < 2; ++j) {
+                const int cc = 4 * j + (lane >> 3);
                 const int cl = warp * 8 + cc;
-                const float rh = tf32_rna(x[cc].x), ih = tf32_rna(x[cc].y);
-                const float rl = tf32_rna(x[cc].x - rh), il = tf32_rna(x[cc].y - ih);
-                const uint32_t o0 = sw128_offset(2 * cl, lane >> 2) + 4 * (lane & 3);
-                const uint32_t o1 = sw128_offset(2 * cl + 1, lane >> 2) + 4 * (lane & 3);
-                *reinterpret_cast<float*>(aHi + o0) = rh;
-                *reinterpret_cast<float*>(aLo + o0) = rl;
-                *reinterpret_cast<float*>(aHi + o1) = ih;
-                *reinterpret_cast<float*>(aLo + o1) = il;
+                const float sgn = (m & (1u << cc)) ? -1.0f : 1.0f;
+                const Split4 re = split4(v[j][0].x, v[j][0].z, v[j][1].x, v[j][1].z);
+                const Split4 im = split4(sgn * v[j][0].y, sgn * v[j][0].w, sgn * v[j][1].y, sgn * v[j][1].w);
+                const uint32_t o0 = sw128_offset(2 * cl, q), o1 = sw128_offset(2 * cl + 1, q);
+                *reinterpret_cast<float4*>(aHi + o0) = re.hi;
+                *reinterpret_cast<float4*>(aLo + o0) = re.lo;
+                *reinterpret_cast<float4*>(aHi + o1) = im.hi;
+                *reinterpret_cast<float4*>(aLo + o1) = im.lo;
             }
             fence_proxy_async();
             mbar_arrive(smem_u32(&st->full[stage]));
@@ -488,7 +506,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                         const uint32_t aL = aH + kTileRows * 128;
                         const uint32_t bH = smem_u32(sBhi + kc * NP * 128), bL = smem_u32(sBlo + kc * NP * 128);
                         const uint32_t d = tmem + static_cast<uint32_t>(acc * NP);
-                        const int ksteps = min(4, (S - kc * kChunkK + 7) / 8);
+                        // k-steps holding any k < S (see kperm).
+                        const int left = S - kc * kChunkK;
+                        const int ksteps = left >= 16 ? 4 : (left + 3) / 4;
                         for (int j = 0; j < ksteps; ++j) {
                             const uint32_t off = j * 32;
                             mma_tf32(d, sw128_desc(aH + off), sw128_desc(bL + off), idesc, j > 0 ? 1u : 0u);
