@@ -397,6 +397,44 @@ SKB_API int skb_pipeline_profile(skb_pipeline* p, const void* real_in, void* rea
                                  uint64_t capacity, uint64_t* count);
 SKB_API void* skb_pipeline_stream(skb_pipeline* p);
 
+/* ------------------------------- constant-stratification type-I vertical */
+/* Replaces the six FFTW guru64 REDFT00/RODFT00 plans of the constant-
+ * stratification kernel (R2RPlan, src/constant_stratification.cpp:95-146),
+ * the WVM forward normalisations (normalizeForwardDct / normalizeForwardDst,
+ * 199-231) and the production call schedule (executeCompleteVerticalGraph,
+ * 359-379).  Arrays are complex [row][storage_channels][nz] with z adjacent
+ * (re/im interleaved; double for SKB_PRECISION_FP64 handles, float for FP32),
+ * transformed in place; channels first_channel .. +channels-1 of each row.
+ *   SKB_TYPE1_DCT: DCT-I over all nz points (unnormalised, FFTW REDFT00).
+ *   SKB_TYPE1_DST: DST-I over the nz-2 interior points (RODFT00); the two
+ *                  endpoints are left as they are.
+ * normalize != 0 appends the WVM forward normalisation: DCT values times
+ * 1/(nz-1) with the last point halved; DST interior times 1/(nz-1) with both
+ * endpoints set to zero.  nz >= 3. */
+#define SKB_TYPE1_DCT 0
+#define SKB_TYPE1_DST 1
+typedef struct skb_cs_vertical skb_cs_vertical;
+SKB_API int skb_cs_vertical_create(uint64_t rows, uint64_t nz, int precision, skb_cs_vertical** out);
+SKB_API int skb_cs_vertical_destroy(skb_cs_vertical* p);
+SKB_API int skb_cs_vertical_info(const skb_cs_vertical* p, skb_provider_info* info);
+/* R2RPlan::execute (+ normalisation) on a device array, stream-ordered. */
+SKB_API int skb_cs_vertical_transform_device(skb_cs_vertical* p, int kind, uint64_t storage_channels,
+                                             uint64_t first_channel, uint64_t channels, int normalize, void* data,
+                                             void* stream);
+/* The same on a host array (FP64 interleaved complex), blocking. */
+SKB_API int skb_cs_vertical_transform(skb_cs_vertical* p, int kind, uint64_t storage_channels,
+                                      uint64_t first_channel, uint64_t channels, int normalize, double* data);
+/* normalizeForwardDct / normalizeForwardDst alone, on a device array. */
+SKB_API int skb_cs_vertical_normalize_device(skb_cs_vertical* p, int kind, uint64_t storage_channels,
+                                             uint64_t first_channel, uint64_t channels, void* data, void* stream);
+/* executeCompleteVerticalGraph: 15 inverse channel transforms on arena3
+ * ([rows][3][nz]) and 4 normalised forward transforms on arena1
+ * ([rows][1][nz]).  Device arrays, stream-ordered. */
+SKB_API int skb_cs_vertical_schedule_device(skb_cs_vertical* p, void* arena3, void* arena1, void* stream);
+/* The same on host arrays (FP64 interleaved complex), blocking. */
+SKB_API int skb_cs_vertical_schedule(skb_cs_vertical* p, double* arena3, double* arena1);
+SKB_API void* skb_cs_vertical_stream(skb_cs_vertical* p);
+
 /* ------------------------------------------------------ serving loop */
 /* A continuous-batching request loop over flux size classes (no counterpart
  * in the reference, which has no serving path).  Each class gets one or more

@@ -344,3 +344,117 @@ def spectral_pipeline(w: Workload, real, family=None, workers=1):
     modal = grouped_vertical(w, family, "forward", ret) * modal_weights(w)
     back = grouped_vertical(w, family, "inverse", modal)
     return fft_c2r(w, embed_retained(w, modes, back), workers)
+
+
+# ------------------------------------------------ constant stratification
+# Type-I vertical transforms of the constant-stratification kernel
+# (src/constant_stratification.cpp).  Arrays are complex [row][channel][z]
+# (index(), 154-157).  The transforms are the FFTW r2r kinds the reference
+# plans (R2RPlan, 95-146): REDFT00 over all nz points and RODFT00 over the
+# nz-2 interior points, applied to the real and imaginary parts alike.  Here
+# they are direct sums with cosine / sine tables indexed by (k z mod 2(nz-1)),
+# so every table entry is an exactly reduced angle.
+
+def _type1_tables(nz):
+    m = nz - 1
+    kz = (np.arange(nz)[:, None] * np.arange(nz)[None, :]) % (2 * m)
+    angle = np.pi * kz.astype(np.float64) / m
+    return np.cos(angle), np.sin(angle)
+
+
+def dct1(column):
+    """REDFT00 along the last axis: Y_k = x_0 + (-1)^k x_{nz-1}
+    + 2 sum_{z=1}^{nz-2} x_z cos(pi k z / (nz-1))."""
+    x = np.asarray(column, dtype=np.complex128)
+    nz = x.shape[-1]
+    c, _ = _type1_tables(nz)
+    w = 2.0 * c
+    w[:, 0] = 1.0
+    w[:, nz - 1] = np.where(np.arange(nz) % 2 == 0, 1.0, -1.0)
+    return x @ w.T
+
+
+def dst1_interior(column):
+    """RODFT00 on the interior z = 1 .. nz-2 (endpoints returned unchanged):
+    Y_k = 2 sum_{z=1}^{nz-2} x_z sin(pi k z / (nz-1))."""
+    x = np.asarray(column, dtype=np.complex128)
+    nz = x.shape[-1]
+    _, s = _type1_tables(nz)
+    w = 2.0 * s[1:nz - 1, 1:nz - 1]
+    out = x.copy()
+    out[..., 1:nz - 1] = x[..., 1:nz - 1] @ w.T
+    return out
+
+
+def normalize_dct1(column):
+    """normalizeForwardDct (constant_stratification.cpp:199-212): every value
+    times 1/(nz-1), then the last one times 0.5."""
+    y = np.array(column, dtype=np.complex128)
+    nz = y.shape[-1]
+    y *= 1.0 / float(nz - 1)
+    y[..., nz - 1] *= 0.5
+    return y
+
+
+def normalize_dst1(column):
+    """normalizeForwardDst (214-231): endpoints zero, interior times 1/(nz-1)."""
+    y = np.array(column, dtype=np.complex128)
+    nz = y.shape[-1]
+    y[..., 1:nz - 1] *= 1.0 / float(nz - 1)
+    y[..., 0] = 0.0
+    y[..., nz - 1] = 0.0
+    return y
+
+
+def type1_transform(data, kind, storage_channels, first, channels, normalize=False):
+    """R2RPlan::execute (+ normalisation) on [row][storage_channels][nz];
+    kind 'dct' or 'dst'."""
+    a = np.array(data, dtype=np.complex128)
+    if a.ndim != 3 or a.shape[1] != storage_channels:
+        raise ValueError("type1_transform expects a [row][storage_channels][z] array")
+    sel = a[:, first:first + channels, :]
+    if kind == "dct":
+        out = dct1(sel)
+        if normalize:
+            out = normalize_dct1(out)
+    else:
+        out = dst1_interior(sel)
+        if normalize:
+            out = normalize_dst1(out)
+    a[:, first:first + channels, :] = out
+    return a
+
+
+def type1_schedule(arena3, arena1):
+    """executeCompleteVerticalGraph (constant_stratification.cpp:359-379):
+    3 x (DCT-I on channels 0-1, DST-I on channel 2) and 2 x (DST-I on
+    channels 0-1, DCT-I on channel 2) of the 3-channel arena, then 2 x
+    normalised DCT-I and 2 x normalised DST-I of the 1-channel arena."""
+    a3 = np.array(arena3, dtype=np.complex128)
+    a1 = np.array(arena1, dtype=np.complex128)
+    for _ in range(3):
+        a3 = type1_transform(a3, "dct", 3, 0, 2)
+        a3 = type1_transform(a3, "dst", 3, 2, 1)
+    for _ in range(2):
+        a3 = type1_transform(a3, "dst", 3, 0, 2)
+        a3 = type1_transform(a3, "dct", 3, 2, 1)
+    for _ in range(2):
+        a1 = type1_transform(a1, "dct", 1, 0, 1, normalize=True)
+    for _ in range(2):
+        a1 = type1_transform(a1, "dst", 1, 0, 1, normalize=True)
+    return a3, a1
+
+
+def type1_deterministic(rows, channels, nz, row_ids=None, conj=None):
+    """deterministicValue / fillFull / fillCompact (constant_stratification.cpp:
+    233-260): value(row, channel, z) = (sin a, cos 1.7a) with a = 0.017(1 +
+    row mod 97) + 0.113(1 + channel) + 0.071(1 + z).  row_ids maps each array
+    row to the row the value is taken from (the mode's storedKx + nxHalf *
+    storedKy for compact arrays); conj marks rows stored conjugated."""
+    ids = np.arange(rows) if row_ids is None else np.asarray(row_ids, np.int64)
+    a = (0.017 * (1 + ids % 97)[:, None, None] + 0.113 * (1 + np.arange(channels))[None, :, None]
+         + 0.071 * (1 + np.arange(nz))[None, None, :])
+    v = np.sin(a) + 1j * np.cos(1.7 * a)
+    if conj is not None:
+        v = np.where(np.asarray(conj, bool)[:, None, None], np.conj(v), v)
+    return v

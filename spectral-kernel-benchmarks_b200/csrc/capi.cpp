@@ -2,6 +2,7 @@
 
 #include "skb_cuda.h"
 
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -13,6 +14,7 @@
 #include "server.hpp"
 #include "pointwise.hpp"
 #include "runtime.hpp"
+#include "type1.hpp"
 #include "util.hpp"
 
 using namespace skb;
@@ -237,6 +239,19 @@ struct skb_flux {
     HostAdapter host{Precision::f64, {}};
     ~skb_flux() {
         pipeline.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct skb_cs_vertical {
+    uint64_t rows = 0, nz = 0;
+    Precision p = Precision::f64;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer tw;        // 2(nz-1) twiddles exp(-2 pi i m / (2(nz-1)))
+    DeviceBuffer arena, arena1;  // device staging of host arrays
+    HostAdapter host{Precision::f64, {}};
+    double allocation = 0.0, planning = 0.0;
+    ~skb_cs_vertical() {
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -1151,6 +1166,154 @@ int skb_pipeline_profile(skb_pipeline* p, const void* real_in, void* real_out, s
 }
 
 void* skb_pipeline_stream(skb_pipeline* p) { return p ? p->stream : nullptr; }
+
+// ------------------------------------------ constant-stratification type-I
+
+namespace {
+
+unsigned type1_mask(int kind, uint64_t channels) {
+    if (kind == SKB_TYPE1_DCT) return 0u;
+    if (kind == SKB_TYPE1_DST) return channels >= 32 ? 0xFFFFFFFFu : ((1u << channels) - 1u);
+    throw Error(SKB_ERR_INVALID_ARGUMENT, "kind must be SKB_TYPE1_DCT or SKB_TYPE1_DST");
+}
+
+void type1_check(const skb_cs_vertical* p, uint64_t storage, uint64_t first, uint64_t channels) {
+    require(p != nullptr, "handle must be non-null");
+    require(storage >= 1 && storage <= 32, "storage channels must be in [1, 32]");
+    require(channels >= 1 && first + channels <= storage,
+            "Invalid constant-stratification R2R plan shape: channels outside the storage channels.");
+}
+
+void type1_run(skb_cs_vertical* p, unsigned mask, uint64_t storage, uint64_t first, uint64_t channels,
+               bool normalize, void* data, cudaStream_t s) {
+    check_cuda(launch_type1(p->p == Precision::f64, data, static_cast<long long>(p->rows), static_cast<int>(p->nz),
+                            static_cast<int>(storage), static_cast<int>(first), static_cast<int>(channels), mask,
+                            normalize, p->tw.get(), s),
+               "type-I vertical transform kernel");
+}
+
+}  // namespace
+
+int skb_cs_vertical_create(uint64_t rows, uint64_t nz, int precision, skb_cs_vertical** out) {
+    return guard([&] {
+        require(out != nullptr, "output handle must be non-null");
+        require(rows > 0, "constant-stratification rows must be positive");
+        require(nz >= 3 && nz <= 16385, "constant-stratification Nz must be in [3, 16385]");
+        require(rows * 32 * nz < (uint64_t(1) << 62), "constant-stratification arrays too large");
+        auto p = std::make_unique<skb_cs_vertical>();
+        p->rows = rows;
+        p->nz = nz;
+        p->p = to_precision(precision);
+        p->host.p = p->p;
+        p->stream = make_stream();
+        const auto t0 = std::chrono::steady_clock::now();
+        const auto tw = twiddle_table(2 * (nz - 1));
+        if (p->p == Precision::f64) {
+            p->tw = upload_vector(tw);
+        } else {
+            p->tw = upload_vector(std::vector<float>(tw.begin(), tw.end()));
+        }
+        p->planning = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        *out = p.release();
+    });
+}
+
+int skb_cs_vertical_destroy(skb_cs_vertical* p) {
+    return guard([&] { delete p; });
+}
+
+void* skb_cs_vertical_stream(skb_cs_vertical* p) { return p ? p->stream : nullptr; }
+
+int skb_cs_vertical_info(const skb_cs_vertical* p, skb_provider_info* info) {
+    return guard([&] {
+        require(p != nullptr && info != nullptr, "handle and info must be non-null");
+        std::memset(info, 0, sizeof(*info));
+        info->planning_seconds = p->planning;
+        info->allocation_seconds = p->allocation;
+        info->persistent_bytes = p->tw.bytes();
+        info->scratch_bytes = p->arena.bytes() + p->arena1.bytes();
+        info->launches_per_execution = 1;
+        info->precision = p->p == Precision::f64 ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
+        fill_identity(info, type1_uses_fft(static_cast<int>(p->nz))
+                                ? "skb-cuda type-I vertical: warp FFT of the 2(Nz-1)-point symmetric extension"
+                                : "skb-cuda type-I vertical: direct sums");
+    });
+}
+
+int skb_cs_vertical_transform_device(skb_cs_vertical* p, int kind, uint64_t storage, uint64_t first,
+                                     uint64_t channels, int normalize, void* data, void* stream) {
+    return guard([&] {
+        type1_check(p, storage, first, channels);
+        require(data != nullptr, "data must be non-null");
+        type1_run(p, type1_mask(kind, channels), storage, first, channels, normalize != 0, data,
+                  stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    });
+}
+
+int skb_cs_vertical_normalize_device(skb_cs_vertical* p, int kind, uint64_t storage, uint64_t first,
+                                     uint64_t channels, void* data, void* stream) {
+    return guard([&] {
+        type1_check(p, storage, first, channels);
+        require(data != nullptr, "data must be non-null");
+        check_cuda(launch_type1_normalize(p->p == Precision::f64, data, static_cast<long long>(p->rows),
+                                          static_cast<int>(p->nz), static_cast<int>(storage),
+                                          static_cast<int>(first), static_cast<int>(channels),
+                                          type1_mask(kind, channels),
+                                          stream ? static_cast<cudaStream_t>(stream) : p->stream),
+                   "type-I normalisation kernel");
+    });
+}
+
+int skb_cs_vertical_transform(skb_cs_vertical* p, int kind, uint64_t storage, uint64_t first, uint64_t channels,
+                              int normalize, double* data) {
+    return guard([&] {
+        type1_check(p, storage, first, channels);
+        require(data != nullptr, "data must be non-null");
+        const unsigned mask = type1_mask(kind, channels);
+        const size_t values = 2 * p->rows * storage * p->nz;
+        if (p->arena.bytes() < values * element_bytes(p->p)) p->arena.allocate(values * element_bytes(p->p));
+        p->host.upload(p->arena.get(), data, values, p->stream);
+        type1_run(p, mask, storage, first, channels, normalize != 0, p->arena.get(), p->stream);
+        p->host.download(data, p->arena.get(), values, p->stream);
+        sync(p->stream);
+    });
+}
+
+namespace {
+// executeCompleteVerticalGraph (src/constant_stratification.cpp:359-379).
+// The reference's per-plan calls on disjoint channels of one arena (DCT-I on
+// channels 0-1 then DST-I on channel 2, and the converse) are one launch
+// each here, with the kind chosen per channel.
+void type1_schedule(skb_cs_vertical* p, void* arena3, void* arena1, cudaStream_t s) {
+    for (int g = 0; g < 3; ++g) type1_run(p, 0x4u, 3, 0, 3, false, arena3, s);  // velocity + cosine derivatives
+    for (int g = 0; g < 2; ++g) type1_run(p, 0x3u, 3, 0, 3, false, arena3, s);  // sine-family derivatives
+    for (int g = 0; g < 2; ++g) type1_run(p, 0x0u, 1, 0, 1, true, arena1, s);   // cosine flux targets
+    for (int g = 0; g < 2; ++g) type1_run(p, 0x1u, 1, 0, 1, true, arena1, s);   // sine flux targets
+}
+}  // namespace
+
+int skb_cs_vertical_schedule_device(skb_cs_vertical* p, void* arena3, void* arena1, void* stream) {
+    return guard([&] {
+        require(p != nullptr && arena3 != nullptr && arena1 != nullptr, "handle and arenas must be non-null");
+        type1_schedule(p, arena3, arena1, stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    });
+}
+
+int skb_cs_vertical_schedule(skb_cs_vertical* p, double* arena3, double* arena1) {
+    return guard([&] {
+        require(p != nullptr && arena3 != nullptr && arena1 != nullptr, "handle and arenas must be non-null");
+        const size_t v3 = 2 * p->rows * 3 * p->nz, v1 = 2 * p->rows * p->nz;
+        const size_t es = element_bytes(p->p);
+        if (p->arena.bytes() < v3 * es) p->arena.allocate(v3 * es);
+        if (p->arena1.bytes() < v1 * es) p->arena1.allocate(v1 * es);
+        p->host.upload(p->arena.get(), arena3, v3, p->stream);
+        p->host.upload(p->arena1.get(), arena1, v1, p->stream);
+        type1_schedule(p, p->arena.get(), p->arena1.get(), p->stream);
+        p->host.download(arena3, p->arena.get(), v3, p->stream);
+        p->host.download(arena1, p->arena1.get(), v1, p->stream);
+        sync(p->stream);
+    });
+}
 
 int skb_vertical_info(const skb_vertical_provider* p, skb_provider_info* info) {
     return guard([&] {

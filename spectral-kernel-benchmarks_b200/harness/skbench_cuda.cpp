@@ -3,8 +3,9 @@
 //
 // It mirrors the reference CLI (src/main.cpp:11-246): the same commands, the
 // same profiles (src/benchmark.cpp:1039-1056), kernel names `fft` (alias
-// `2d-rfft`), `pruned-horizontal`, `vertical-gemm`, `pointwise-advection` and
-// `production-lifetime-flux`, the spectral-kernel-benchmark-v1 JSON report
+// `2d-rfft`), `pruned-horizontal`, `vertical-gemm`, `pointwise-advection`,
+// `production-lifetime-flux`, `spectral-pipeline` and
+// `constant-stratification-vertical`, the spectral-kernel-benchmark-v1 JSON report
 // and nine-column CSV, and exit codes 0 (passed), 1 (a correctness check
 // failed) and 2 (bad arguments or a provider error).  Everything it runs goes
 // through the C ABI of include/skb_cuda.h; primitive timings are CUDA events
@@ -805,6 +806,245 @@ ProviderRecord run_pipeline(const Options& o, const skb_workload& w, Report& rep
     return rec;
 }
 
+// ------------------------------------- constant-stratification vertical
+// runConstantStratificationVerticalBenchmark (src/constant_stratification.cpp:
+// 481-648): the type-I vertical call graph of the constant-stratification
+// flux on the full half-spectrum rows and on the retained compact rows, with
+// the same stage names, correctness checks and record layout.
+
+namespace type1 {
+
+// deterministicValue (constant_stratification.cpp:233-239).
+cplx value(std::uint64_t row, std::uint64_t channel, std::uint64_t z) {
+    const double a = 0.017 * double(1 + row % 97) + 0.113 * double(1 + channel) + 0.071 * double(1 + z);
+    return cplx(std::sin(a), std::cos(1.7 * a));
+}
+
+std::vector<cplx> fill_full(std::uint64_t rows, std::uint64_t channels, std::uint64_t nz) {
+    std::vector<cplx> a(rows * channels * nz);
+    for (std::uint64_t r = 0; r < rows; ++r)
+        for (std::uint64_t c = 0; c < channels; ++c)
+            for (std::uint64_t z = 0; z < nz; ++z) a[(r * channels + c) * nz + z] = value(r, c, z);
+    return a;
+}
+
+std::vector<cplx> fill_compact(const std::vector<skb_retained_mode>& modes, std::uint64_t nxHalf,
+                               std::uint64_t channels, std::uint64_t nz) {
+    std::vector<cplx> a(modes.size() * channels * nz);
+    for (std::size_t m = 0; m < modes.size(); ++m) {
+        const std::uint64_t row = modes[m].stored_kx + nxHalf * modes[m].stored_ky;
+        for (std::uint64_t c = 0; c < channels; ++c)
+            for (std::uint64_t z = 0; z < nz; ++z) {
+                const cplx v = value(row, c, z);
+                a[(m * channels + c) * nz + z] = modes[m].conjugates_stored_value ? std::conj(v) : v;
+            }
+    }
+    return a;
+}
+
+// Normalised forward type-I transforms of one column in long double (the
+// reference's directForwardDct / directForwardDst, 273-311).
+std::vector<cplx> direct(const std::vector<cplx>& x, bool sine) {
+    const std::uint64_t nz = x.size(), m = nz - 1;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    std::vector<cplx> out(nz);
+    for (std::uint64_t j = 0; j < nz; ++j) {
+        if (sine && (j == 0 || j == m)) continue;
+        lcplx acc = 0;
+        if (!sine) {
+            const long double sign = j % 2 == 0 ? 1.0L : -1.0L;
+            acc = lcplx(x[0].real(), x[0].imag()) + sign * lcplx(x[m].real(), x[m].imag());
+        }
+        for (std::uint64_t z = 1; z < m; ++z) {
+            const long double angle = pi * static_cast<long double>((j * z) % (2 * m)) / static_cast<long double>(m);
+            const long double f = 2.0L * (sine ? std::sin(angle) : std::cos(angle));
+            acc += f * lcplx(x[z].real(), x[z].imag());
+        }
+        acc /= static_cast<long double>(m);
+        if (!sine && j == m) acc *= 0.5L;
+        out[j] = cplx(double(acc.real()), double(acc.imag()));
+    }
+    return out;
+}
+
+// Compact rows against their full half-spectrum rows (conjugated where the
+// mode stores its conjugate), as compactFullCorrectness (414-455).
+std::pair<double, double> compact_vs_full(const std::vector<cplx>& compact, const std::vector<cplx>& full,
+                                          const std::vector<skb_retained_mode>& modes, std::uint64_t nxHalf,
+                                          std::uint64_t channels, std::uint64_t nz) {
+    std::vector<cplx> ref(compact.size());
+    for (std::size_t m = 0; m < modes.size(); ++m) {
+        const std::uint64_t row = modes[m].stored_kx + nxHalf * modes[m].stored_ky;
+        for (std::uint64_t i = 0; i < channels * nz; ++i) {
+            const cplx v = full[row * channels * nz + i];
+            ref[m * channels * nz + i] = modes[m].conjugates_stored_value ? std::conj(v) : v;
+        }
+    }
+    return {max_relative_error(compact.data(), ref.data(), ref.size()),
+            relative_l2_error(compact.data(), ref.data(), ref.size())};
+}
+
+}  // namespace type1
+
+std::vector<ProviderRecord> run_constant_stratification(const Options& o, skb_workload& w, Report& report) {
+    if (w.nx != w.ny || w.nx % 2 != 0 || w.nz < 3)
+        throw std::invalid_argument(
+            "constant-stratification vertical benchmark requires an even square horizontal grid and Nz >= 3.");
+    w.fields = 4;
+    report.fields = 4;
+    const int prec = precision_code(o);
+    const bool f32 = prec == SKB_PRECISION_FP32;
+    const double tol = f32 ? 1e-5 : 1e-12;
+    const std::uint64_t nz = w.nz, nxHalf = w.nx / 2 + 1, fullRows = w.ny * nxHalf;
+    const auto modes = retained_modes(w);
+    const std::uint64_t compactRows = modes.size(), es = f32 ? 8 : 16;
+    report.verticalMatrixFamilyId = "wvm-constant-stratification-fftw-type1-v1";
+    report.fullSpectrumBytes = fullRows * 4 * nz * es;
+    report.retainedSpectrumBytes = compactRows * 4 * nz * es;
+    report.modalSpectrumBytes = compactRows * report.nj * 4 * es;
+
+    auto to_device = [&](const std::vector<cplx>& v, DeviceBuffer& d, void* stream) {
+        std::vector<double> flat(2 * v.size());
+        for (std::size_t i = 0; i < v.size(); ++i) {
+            flat[2 * i] = v[i].real();
+            flat[2 * i + 1] = v[i].imag();
+        }
+        if (f32) d.upload(narrow<float>(flat), stream);
+        else d.upload(flat, stream);
+    };
+    auto from_device = [&](const DeviceBuffer& d, std::uint64_t count, void* stream) {
+        return widen_complex(d, count, f32, stream);
+    };
+    auto as_used_c = [&](std::vector<cplx> v) {
+        if (f32)
+            for (auto& x : v) x = cplx(double(float(x.real())), double(float(x.imag())));
+        return v;
+    };
+
+    // Handles and arenas for both row sets.
+    struct Arena {
+        std::uint64_t rows;
+        skb_cs_vertical* h = nullptr;
+        std::unique_ptr<DeviceBuffer> a3, a1;
+    };
+    Arena full{fullRows}, compact{compactRows};
+    for (Arena* a : {&full, &compact}) {
+        ok(skb_cs_vertical_create(a->rows, nz, prec, &a->h));
+        a->a3 = std::make_unique<DeviceBuffer>(a->rows * 3 * nz * es);
+        a->a1 = std::make_unique<DeviceBuffer>(a->rows * nz * es);
+    }
+    std::unique_ptr<skb_cs_vertical, int (*)(skb_cs_vertical*)> gFull(full.h, skb_cs_vertical_destroy),
+        gCompact(compact.h, skb_cs_vertical_destroy);
+    void* sFull = skb_cs_vertical_stream(full.h);
+    void* sCompact = skb_cs_vertical_stream(compact.h);
+
+    // Correctness probes on compact row 0, channel 0 (541-556).
+    auto probe = [&](bool sine) {
+        const auto input = as_used_c(type1::fill_compact(modes, nxHalf, 1, nz));
+        to_device(input, *compact.a1, sCompact);
+        ok(skb_cs_vertical_transform_device(compact.h, sine ? SKB_TYPE1_DST : SKB_TYPE1_DCT, 1, 0, 1, 1,
+                                            compact.a1->p, sCompact));
+        const auto got = from_device(*compact.a1, nz, sCompact);
+        const std::vector<cplx> column(input.begin(), input.begin() + nz);
+        const auto want = type1::direct(column, sine);
+        return std::make_pair(max_relative_error(got.data(), want.data(), nz),
+                              relative_l2_error(got.data(), want.data(), nz));
+    };
+    const auto dctErr = probe(false);
+    const auto dstErr = probe(true);
+
+    // The call schedule on both row sets, compact against full (558-568).
+    to_device(as_used_c(type1::fill_full(fullRows, 3, nz)), *full.a3, sFull);
+    to_device(as_used_c(type1::fill_full(fullRows, 1, nz)), *full.a1, sFull);
+    to_device(as_used_c(type1::fill_compact(modes, nxHalf, 3, nz)), *compact.a3, sCompact);
+    to_device(as_used_c(type1::fill_compact(modes, nxHalf, 1, nz)), *compact.a1, sCompact);
+    ok(skb_cs_vertical_schedule_device(full.h, full.a3->p, full.a1->p, sFull));
+    ok(skb_cs_vertical_schedule_device(compact.h, compact.a3->p, compact.a1->p, sCompact));
+    const auto three = type1::compact_vs_full(from_device(*compact.a3, compactRows * 3 * nz, sCompact),
+                                              from_device(*full.a3, fullRows * 3 * nz, sFull), modes, nxHalf, 3, nz);
+    const auto oneErr = type1::compact_vs_full(from_device(*compact.a1, compactRows * nz, sCompact),
+                                            from_device(*full.a1, fullRows * nz, sFull), modes, nxHalf, 1, nz);
+
+    auto record = [&](bool isCompact) {
+        Arena& a = isCompact ? compact : full;
+        void* stream = isCompact ? sCompact : sFull;
+        ProviderRecord rec;
+        skb_provider_info info{};
+        ok(skb_cs_vertical_info(a.h, &info));
+        fill_info(rec, info);
+        rec.id = isCompact ? "cuda-wvm-type1-retained-compact" : "cuda-wvm-type1-full-half";
+        rec.algorithmId = isCompact ? "retained-rows-production-type1-call-graph"
+                                    : "wvm-full-half-production-type1-call-graph";
+        rec.nativeRepresentationId = isCompact ? "retained-radial-interleaved-complex-z-adjacent"
+                                               : "wvm-full-half-interleaved-complex-z-adjacent";
+        rec.modeOrderId = isCompact ? "logical-radial-retained-mode-order" : "wvm-half-spectrum-row-order";
+        rec.planningConfiguration = std::string(info.library_identity) + "; one launch per call-graph step";
+        rec.persistentBytes = info.persistent_bytes + a.a3->bytes + a.a1->bytes;
+        rec.forward.nativePlacement = "in-place";
+        rec.forward.adapterPlacement = "in-place";
+        rec.forward.destroysNativeInput = true;
+        rec.forward.adapterPreservesCallerInput = false;
+        rec.forward.physicalExtents = "[rows,channels,Nz] with Nz adjacent";
+        rec.forward.stridesElements = "complex: z=1, channel=Nz, row=Nz*channels; real/imag stride=1 scalar";
+        rec.forward.aliasing = "exact in-place alias";
+        rec.inverse = rec.forward;
+        to_device(as_used_c(type1::fill_full(a.rows, 3, nz)), *a.a3, stream);
+        to_device(as_used_c(type1::fill_full(a.rows, 1, nz)), *a.a1, stream);
+        const std::uint64_t one = a.rows * nz * es;
+        auto raw = [&](bool sine) {
+            return measure_device(o.warmups, o.samples, stream, [&] {
+                ok(skb_cs_vertical_transform_device(a.h, sine ? SKB_TYPE1_DST : SKB_TYPE1_DCT, 1, 0, 1, 0, a.a1->p,
+                                                    stream));
+            });
+        };
+        rec.timings.push_back(series("primitive", "raw DCT-I one complex channel", "inverse", 2 * one, raw(false)));
+        rec.timings.push_back(
+            series("primitive", "raw DST-I one complex interior channel", "inverse", 2 * one, raw(true)));
+        rec.timings.push_back(series("primitive", "raw DCT-I one complex channel", "forward", 2 * one, raw(false)));
+        rec.timings.push_back(
+            series("primitive", "raw DST-I one complex interior channel", "forward", 2 * one, raw(true)));
+        auto norm = [&](bool sine) {
+            return measure_device(o.warmups, o.samples, stream, [&] {
+                ok(skb_cs_vertical_normalize_device(a.h, sine ? SKB_TYPE1_DST : SKB_TYPE1_DCT, 1, 0, 1, a.a1->p,
+                                                    stream));
+            });
+        };
+        rec.timings.push_back(
+            series("adapter-component", "WVM forward DCT-I normalization", "forward", 2 * one, norm(false)));
+        rec.timings.push_back(series("adapter-component", "WVM forward DST-I normalization and endpoints", "forward",
+                                     2 * one, norm(true)));
+        rec.timings.push_back(series(
+            "uninstrumented-total",
+            "production nonlinear-flux vertical transform schedule (15 inverse + 4 forward complex channels)",
+            "complete", 38 * one, measure_device(o.warmups, o.samples, stream, [&] {
+                ok(skb_cs_vertical_schedule_device(a.h, a.a3->p, a.a1->p, stream));
+            })));
+        rec.ledger = {
+            {"setup/planning", StageState::setupOnly, "twiddles of the 2(Nz-1)-point symmetric extension"},
+            {"raw inverse vertical transforms", StageState::executed,
+             "15 complex channels in 5 launches (DCT-I and DST-I channels of one arena share a launch)"},
+            {"raw forward vertical transforms", StageState::executed, "four complex flux-target projections"},
+            {"forward normalization", StageState::fused,
+             "exact WVM type-I endpoint and 1/(Nz-1) scaling, in the forward transform's store"},
+            {"horizontal retained transforms", StageState::unsupported,
+             "isolated vertical call-graph benchmark; composed horizontal timing is deferred"},
+            {"coefficient assembly and pointwise products", StageState::unsupported,
+             "not part of this attributable vertical component benchmark"}};
+        rec.correctness.push_back(
+            metric("WVM normalized DCT-I versus direct oracle", dctErr.first, dctErr.second, tol));
+        rec.correctness.push_back(
+            metric("WVM normalized DST-I versus direct oracle", dstErr.first, dstErr.second, tol));
+        if (isCompact) {
+            rec.correctness.push_back(metric("retained three-channel vertical call schedule versus full-half control",
+                                             three.first, three.second, tol));
+            rec.correctness.push_back(metric("retained one-channel projection schedule versus full-half control",
+                                             oneErr.first, oneErr.second, tol));
+        }
+        return rec;
+    };
+    return {record(false), record(true)};
+}
+
 int flux_mode(const std::string& m) {
     if (m == "fp64-plain") return SKB_FLUX_FP64_PLAIN;
     if (m == "fp32") return SKB_FLUX_FP32;
@@ -1120,7 +1360,8 @@ void usage(std::ostream& out) {
         << "  skbench-cuda list\n"
         << "  skbench-cuda validate [--profile NAME]\n"
         << "  skbench-cuda run [--kernel fft|2d-rfft|pruned-horizontal|vertical-gemm|pointwise-advection|"
-           "production-lifetime-flux|spectral-pipeline] [--profile NAME] [--providers cuda]\n"
+           "production-lifetime-flux|spectral-pipeline|constant-stratification-vertical] [--profile NAME]\n"
+           "              [--providers cuda]\n"
         << "              [--precision fp64|fp32] [--vertical-gemm-family common|k2-grouped]\n"
         << "              [--vertical-gemm-precision fp64|fp32|tf32x3] [--flux-mode fp64-plain|fp32|split-tf32x3]\n"
         << "              [--members N] [--targets 3|4] [--nx N --ny N --nz N --fields N]\n"
@@ -1135,7 +1376,7 @@ void list() {
                   << "\n    " << p.purpose << '\n';
     std::cout << "providers:\n  cuda: " << skb_version() << "\n"
               << "kernels:\n  fft (alias 2d-rfft)\n  pruned-horizontal\n  vertical-gemm\n  pointwise-advection\n"
-              << "  production-lifetime-flux\n  spectral-pipeline\n"
+              << "  production-lifetime-flux\n  spectral-pipeline\n  constant-stratification-vertical\n"
               << "precisions:\n  fp64\n  fp32\n"
               << "vertical GEMM precisions:\n  fp64\n  fp32\n  tf32x3\n"
               << "vertical GEMM matrix families:\n  common\n  k2-grouped\n"
@@ -1187,8 +1428,10 @@ int run(int argc, char** argv) {
     if (!o.samplesSet) o.samples = prof.samples;
     if (o.samples == 0) throw std::invalid_argument("samples must be positive.");
     Report report = base_report(o, prof, w);
+    std::vector<ProviderRecord> records;
     ProviderRecord rec;
-    if (o.kernel == "fft") rec = run_fft(o, w, report);
+    if (o.kernel == "constant-stratification-vertical") records = run_constant_stratification(o, w, report);
+    else if (o.kernel == "fft") rec = run_fft(o, w, report);
     else if (o.kernel == "pruned-horizontal") rec = run_pruned(o, w, report);
     else if (o.kernel == "vertical-gemm") rec = run_vertical(o, w, report);
     else if (o.kernel == "pointwise-advection") rec = run_pointwise(o, w, report);
@@ -1197,12 +1440,15 @@ int run(int argc, char** argv) {
     else
         throw std::invalid_argument(
             "kernel must be 'fft', '2d-rfft', 'pruned-horizontal', 'vertical-gemm', 'pointwise-advection', "
-            "'production-lifetime-flux' or 'spectral-pipeline'.");
-    rec.compilerFlags = "nvcc -gencode arch=compute_100a,code=sm_100a -O3";
-    rec.sourceIdentity = std::string("libskb_cuda ") + skb_version();
-    for (const auto& m : rec.correctness)
-        if (!m.passed) report.status = "failed";
-    report.providers.push_back(rec);
+            "'production-lifetime-flux', 'spectral-pipeline' or 'constant-stratification-vertical'.");
+    if (records.empty()) records.push_back(rec);
+    for (auto& r : records) {
+        r.compilerFlags = "nvcc -gencode arch=compute_100a,code=sm_100a -O3";
+        r.sourceIdentity = std::string("libskb_cuda ") + skb_version();
+        for (const auto& m : r.correctness)
+            if (!m.passed) report.status = "failed";
+        report.providers.push_back(r);
+    }
 
     std::filesystem::path json = o.output.empty() ? std::filesystem::path("results/local") / (report.runId + ".json")
                                                   : std::filesystem::path(o.output);
@@ -1223,14 +1469,16 @@ int run(int argc, char** argv) {
               << " workload=" << w.nx << 'x' << w.ny << " Nz=" << w.nz << " fields=" << w.fields
               << " Nkl=" << report.nkl << '\n';
     std::cout << "provider\tscope\tstage\tdirection\tmedian_ms\n";
-    for (const auto& t : rec.timings) {
-        if (t.seconds.empty()) continue;
-        std::cout << rec.id << '\t' << t.scope << '\t' << t.stage << '\t' << t.direction << '\t' << std::fixed
-                  << std::setprecision(6) << 1000.0 * median(t.seconds) << '\n';
-    }
-    for (const auto& m : rec.correctness)
-        std::cout << rec.id << " correctness " << m.name << '=' << std::scientific << m.maximumRelativeError
-                  << " passed=" << (m.passed ? "true" : "false") << '\n';
+    for (const auto& r : report.providers)
+        for (const auto& t : r.timings) {
+            if (t.seconds.empty()) continue;
+            std::cout << r.id << '\t' << t.scope << '\t' << t.stage << '\t' << t.direction << '\t' << std::fixed
+                      << std::setprecision(6) << 1000.0 * median(t.seconds) << '\n';
+        }
+    for (const auto& r : report.providers)
+        for (const auto& m : r.correctness)
+            std::cout << r.id << " correctness " << m.name << '=' << std::scientific << m.maximumRelativeError
+                      << " passed=" << (m.passed ? "true" : "false") << '\n';
     std::cout << "json=" << std::filesystem::absolute(json).string() << '\n';
     std::cout << "csv=" << std::filesystem::absolute(csv).string() << '\n';
     return report.status == "passed" ? 0 : 1;

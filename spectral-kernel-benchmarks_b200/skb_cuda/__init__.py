@@ -9,6 +9,10 @@ numpy arrays on the host side:
     VerticalGemmProvider      VerticalGemmProvider       (skbench.hpp:152-218)
     PointwiseAdvectionExecutor PointwiseAdvectionExecutor (pointwise_advection.hpp:18-43)
     Flux                      the 15 -> 4 executeAll composition (benchmark.cpp:4405-4424)
+    ConstantStratificationVertical
+                              the type-I (REDFT00 / RODFT00) vertical plans of the
+                              constant-stratification kernel
+                              (constant_stratification.cpp:95-379)
 
 Errors map to the reference's exception classes: ValueError for
 std::invalid_argument, RuntimeError for std::runtime_error, LogicError for
@@ -38,6 +42,7 @@ GEMM_FP64, GEMM_FP32, GEMM_TF32X3, GEMM_BF16X3 = 0, 1, 2, 3
 INTERLEAVED, SPLIT = 0, 1
 BIDIRECTIONAL, FORWARD_ONLY, INVERSE_ONLY = 0, 1, 2
 FAMILY_COMMON_DCT2, FAMILY_K2_ROTATION, FAMILY_STURM_LIOUVILLE = 0, 1, 2
+TYPE1_DCT, TYPE1_DST = 0, 1
 FLUX_FP64_PLAIN, FLUX_FP32, FLUX_SPLIT_TF32X3, FLUX_SPLIT_BF16X3 = 0, 1, 2, 3
 FIXTURES = ("impulse", "sinusoid", "random", "dc", "nyquist")
 
@@ -134,7 +139,7 @@ def library():
         lib.skb_last_error.restype = ctypes.c_char_p
         lib.skb_version.restype = ctypes.c_char_p
         for name in ("skb_fft_stream", "skb_pruned_stream", "skb_vertical_stream", "skb_pointwise_stream",
-                     "skb_flux_stream", "skb_vertical_wvm_stream", "skb_pipeline_stream"):
+                     "skb_flux_stream", "skb_vertical_wvm_stream", "skb_pipeline_stream", "skb_cs_vertical_stream"):
             getattr(lib, name).restype = ctypes.c_void_p
             getattr(lib, name).argtypes = [ctypes.c_void_p]
         _LIB = lib
@@ -733,6 +738,84 @@ class SpectralPipeline:
     def close(self):
         if self.h:
             check(library().skb_pipeline_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ConstantStratificationVertical:
+    """Type-I vertical transforms of the constant-stratification kernel, in
+    place on complex [row][storage_channels][nz] arrays (z adjacent).
+
+    transform(..., kind=TYPE1_DCT) is FFTW's REDFT00 over all nz points,
+    kind=TYPE1_DST its RODFT00 over the nz-2 interior points (endpoints left
+    as they are); normalize=True appends the WVM forward normalisation
+    (normalizeForwardDct / normalizeForwardDst).  schedule() is the
+    production call graph executeCompleteVerticalGraph: 15 inverse channel
+    transforms on a 3-channel arena and 4 normalised forward transforms on a
+    1-channel arena."""
+
+    def __init__(self, rows, nz, precision=FP64):
+        self.rows = int(rows)
+        self.nz = int(nz)
+        self.precision = precision
+        h = ctypes.c_void_p()
+        check(library().skb_cs_vertical_create(_u64(rows), _u64(nz), ctypes.c_int(precision), ctypes.byref(h)))
+        self.h = h
+
+    @property
+    def stream(self):
+        return library().skb_cs_vertical_stream(self.h)
+
+    @property
+    def device_dtype(self):
+        return np.float64 if self.precision == FP64 else np.float32
+
+    def info(self):
+        return _info(library().skb_cs_vertical_info, self.h)
+
+    def _host(self, data, storage):
+        x = np.ascontiguousarray(data, dtype=np.complex128).copy()
+        assert x.size == self.rows * storage * self.nz
+        return x
+
+    def transform(self, data, kind, storage_channels, first_channel, channels, normalize=False):
+        """Host array in, transformed copy out (complex128)."""
+        x = self._host(data, storage_channels)
+        check(library().skb_cs_vertical_transform(self.h, ctypes.c_int(kind), _u64(storage_channels),
+                                                  _u64(first_channel), _u64(channels), ctypes.c_int(int(normalize)),
+                                                  _p(x)))
+        return x
+
+    def transform_device(self, ptr, kind, storage_channels, first_channel, channels, normalize=False, stream=None):
+        check(library().skb_cs_vertical_transform_device(self.h, ctypes.c_int(kind), _u64(storage_channels),
+                                                         _u64(first_channel), _u64(channels),
+                                                         ctypes.c_int(int(normalize)), ctypes.c_void_p(ptr),
+                                                         ctypes.c_void_p(stream)))
+
+    def normalize_device(self, ptr, kind, storage_channels, first_channel, channels, stream=None):
+        check(library().skb_cs_vertical_normalize_device(self.h, ctypes.c_int(kind), _u64(storage_channels),
+                                                         _u64(first_channel), _u64(channels), ctypes.c_void_p(ptr),
+                                                         ctypes.c_void_p(stream)))
+
+    def schedule(self, arena3, arena1):
+        """Host arrays in, (arena3, arena1) after the production schedule out."""
+        a3 = self._host(arena3, 3)
+        a1 = self._host(arena1, 1)
+        check(library().skb_cs_vertical_schedule(self.h, _p(a3), _p(a1)))
+        return a3, a1
+
+    def schedule_device(self, arena3_ptr, arena1_ptr, stream=None):
+        check(library().skb_cs_vertical_schedule_device(self.h, ctypes.c_void_p(arena3_ptr),
+                                                        ctypes.c_void_p(arena1_ptr), ctypes.c_void_p(stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().skb_cs_vertical_destroy(self.h)
             self.h = None
 
     def __del__(self):

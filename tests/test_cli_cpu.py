@@ -25,7 +25,7 @@ def test_list_names_the_reference_profiles_and_kernels():
                  "wvm-historical-512-nz129-f4: 512x512, Nz=129, fields=4", "wvm-large-1024-nz129-f4"):
         assert name in out.stdout
     for kernel in ("fft (alias 2d-rfft)", "pruned-horizontal", "vertical-gemm", "pointwise-advection",
-                   "production-lifetime-flux", "spectral-pipeline"):
+                   "production-lifetime-flux", "spectral-pipeline", "constant-stratification-vertical"):
         assert kernel in out.stdout
 
 

@@ -67,6 +67,35 @@ def test_run_writes_the_reference_schema(tmp_path, args):
     assert len(rows) > 1 and all(len(r) == 9 for r in rows)
 
 
+@pytest.mark.parametrize("args", [
+    ("--profile", "smoke"),
+    ("--profile", "smoke", "--precision", "fp32"),
+    ("--profile", "quick", "--samples", "3", "--warmups", "1"),
+    ("--profile", "wvm-historical-512-nz129-f4", "--samples", "3", "--warmups", "1"),
+], ids=lambda a: "-".join(a[1::2]))
+def test_constant_stratification_vertical_records(tmp_path, args):
+    """runConstantStratificationVerticalBenchmark's report shape
+    (src/constant_stratification.cpp:481-648): a full-half and a retained
+    compact record, seven timings each, two direct-oracle checks on both and
+    the two compact-versus-full schedule checks on the compact one."""
+    report, rows = run(tmp_path, "--kernel", "constant-stratification-vertical", *args)
+    with open(os.path.join(GOLDEN, "reference_report.json")) as fh:
+        keys_match(json.load(fh), report)
+    assert report["status"] == "passed"
+    assert report["workload"]["fields"] == 4
+    full, compact = report["providers"]
+    assert full["id"] == "cuda-wvm-type1-full-half" and compact["id"] == "cuda-wvm-type1-retained-compact"
+    for p, checks in ((full, 2), (compact, 4)):
+        assert len(p["correctness"]) == checks and all(m["passed"] for m in p["correctness"])
+        stages = {(t["scope"], t["stage"], t["direction"]) for t in p["timings"]}
+        assert ("primitive", "raw DCT-I one complex channel", "inverse") in stages
+        assert ("primitive", "raw DST-I one complex interior channel", "forward") in stages
+        assert ("adapter-component", "WVM forward DST-I normalization and endpoints", "forward") in stages
+        total = [t for t in p["timings"] if t["scope"] == "uninstrumented-total"]
+        assert len(total) == 1 and total[0]["medianSeconds"] > 0
+    assert len(rows) > 1 and all(len(r) == 9 for r in rows)
+
+
 def test_validate_passes():
     proc = subprocess.run([CLI, "validate"], capture_output=True, text=True, timeout=600)
     assert proc.returncode == 0, proc.stdout + proc.stderr

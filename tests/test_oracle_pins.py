@@ -157,3 +157,46 @@ def test_spectral_pipeline_restatement_matches_reference(golden_vectors):
     assert np.array_equal(orc.make_fixture(w, 2, 129), g["pipeline_in"])
     out = orc.spectral_pipeline(w, g["pipeline_in"])
     assert orc.max_rel_error(out, g["pipeline_out"]) <= 1e-12
+
+
+@pytest.mark.parametrize("nz", [3, 4, 7, 9, 33, 65, 129, 130, 257])
+def test_type1_restatement_matches_pocketfft(nz):
+    """The constant-stratification transforms are FFTW REDFT00 / RODFT00
+    (src/constant_stratification.cpp:95-146); the reference's FFTW is absent
+    here, so the oracle's direct sums are pinned to scipy's pocketfft, which
+    defines DCT / DST type 1 (norm=None) identically."""
+    import scipy.fft as sf
+
+    rng = np.random.default_rng(nz)
+    x = rng.standard_normal((6, nz)) + 1j * rng.standard_normal((6, nz))
+    want_dct = sf.dct(x.real, type=1, axis=-1) + 1j * sf.dct(x.imag, type=1, axis=-1)
+    assert orc.max_rel_error(orc.dct1(x), want_dct) <= 1e-14
+    want_dst = x.copy()
+    want_dst[:, 1:-1] = sf.dst(x.real[:, 1:-1], type=1, axis=-1) + 1j * sf.dst(x.imag[:, 1:-1], type=1, axis=-1)
+    assert orc.max_rel_error(orc.dst1_interior(x), want_dst) <= 1e-14
+    # The reference's own direct forward oracles (directForwardDct /
+    # directForwardDst, constant_stratification.cpp:273-311) are the
+    # normalised transforms of one column.
+    col = x[0]
+    m = nz - 1
+    ref_dct = np.array([(col[0] + (-1) ** j * col[-1] + sum(2 * np.cos(np.pi * ((j * z) % (2 * m)) / m) * col[z]
+                                                           for z in range(1, m))) / m for j in range(nz)])
+    ref_dct[-1] *= 0.5
+    assert orc.max_rel_error(orc.normalize_dct1(orc.dct1(col)), ref_dct) <= 1e-13
+    ref_dst = np.zeros(nz, complex)
+    for j in range(1, m):
+        ref_dst[j] = sum(2 * np.sin(np.pi * ((j * z) % (2 * m)) / m) * col[z] for z in range(1, m)) / m
+    assert orc.max_rel_error(orc.normalize_dst1(orc.dst1_interior(col)), ref_dst) <= 1e-13
+
+
+def test_type1_deterministic_fill_compact_equals_full():
+    """fillCompact takes each mode's value from its stored full-half row,
+    conjugated where the mode stores its conjugate (constant_stratification.cpp:243-260)."""
+    n, nz = 16, 9
+    modes = orc.retained_modes(n, n)
+    ids = modes.kx + (n // 2 + 1) * modes.ky
+    full = orc.type1_deterministic(n * (n // 2 + 1), 3, nz)
+    comp = orc.type1_deterministic(len(modes), 3, nz, ids, modes.conj)
+    want = np.where(modes.conj[:, None, None], np.conj(full[ids]), full[ids])
+    assert np.array_equal(comp, want)
+    assert full[0, 0, 0] == np.sin(0.017 + 0.113 + 0.071) + 1j * np.cos(1.7 * (0.017 + 0.113 + 0.071))
