@@ -4,12 +4,13 @@
 // of the column's even extension e (e_z = e_{L-z} = x_z); a DST-I of the
 // interior is i times the DFT of the odd extension (o_z = -o_{L-z} = x_z,
 // o_0 = o_{nz-1} = 0).  Both hold for complex columns because the transform
-// matrices are real.  One warp owns one (row, channel) column: it reads the
-// nz contiguous values, writes the extension into its shared-memory slot,
-// runs warp_fft, and writes the nz results back over the column (all reads
-// finish before the first write, so the transform is in place).  Columns are
-// contiguous in HBM, so each warp moves whole sectors; the kernel is bound by
-// HBM traffic (one read and one write of every transformed value).
+// matrices are real.  Each warp walks (row, channel) columns with a grid
+// stride: it holds the next column's values in registers while it writes the
+// current one's extension into its shared-memory slot, runs warp_fft and
+// writes the nz results back over the column (all reads of a column finish
+// before its first write, so the transform is in place).  Columns are
+// contiguous in HBM, so each warp moves whole sectors; the bound is HBM
+// traffic (one read and one write of every transformed value).
 
 #include <algorithm>
 
@@ -46,27 +47,61 @@ __global__ void __launch_bounds__(kWarps * 32) type1_fft_kernel(cx<T>* __restric
     constexpr int M = L / 2;
     constexpr int nz = M + 1;
     constexpr int kSlots = L + L / 16;  // pad16(L - 1) + 1
+    constexpr int kPer = (nz + 31) / 32;  // column values per lane
+    // Up to five values per lane are held for the next column while the
+    // current one is transformed, so its loads overlap the FFT.
+    constexpr bool kPrefetch = kPer <= 5;
     extern __shared__ unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long seq = static_cast<long long>(blockIdx.x) * kWarps + warp;
-    if (seq >= seqs) return;  // whole warps leave; only __syncwarp() follows
-    const long long row = seq / channels;
-    const int c = static_cast<int>(seq - row * channels);
-    const bool sine = (dstMask >> c) & 1u;
+    const long long stride = static_cast<long long>(gridDim.x) * kWarps;
     V* x = reinterpret_cast<V*>(smem_raw) + warp * kSlots;
-    V* col = data + (row * storage + first + c) * nz;
-    for (int i = lane; i < nz; i += 32) {
-        V v = col[i];
-        if (sine && (i == 0 || i == M)) v = V{T(0), T(0)};
-        x[pad16(i)] = v;
-        if (i > 0 && i < M) x[pad16(L - i)] = sine ? V{-v.x, -v.y} : v;
+    auto column = [&](long long sq) {
+        const long long row = sq / channels;
+        return data + (row * storage + first + (sq - row * channels)) * nz;
+    };
+    auto load = [&](long long sq, V* v) {
+        const V* col = column(sq);
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int i = lane + 32 * q;
+            v[q] = i < nz ? col[i] : V{T(0), T(0)};
+        }
+    };
+    long long seq = static_cast<long long>(blockIdx.x) * kWarps + warp;
+    V cur[kPrefetch ? kPer : 1];
+    if constexpr (kPrefetch) {
+        if (seq < seqs) load(seq, cur);
     }
-    __syncwarp();
-    warp_fft<T, L, -1>(x, tw, lane);
-    for (int k = lane; k < nz; k += 32) {
-        V y = x[pad16(k)];
-        if (sine) y = V{-y.y, y.x};  // i * X_k
-        store_result<T>(col, k, y, M, sine, normalize);
+    // Warp-uniform loop; only __syncwarp() is used inside.
+    for (; seq < seqs; seq += stride) {
+        V* col = column(seq);
+        const bool sine = (dstMask >> static_cast<int>(seq % channels)) & 1u;
+        V nxt[kPrefetch ? kPer : 1];
+        auto extend = [&](int i, V v) {
+            if (sine && (i == 0 || i == M)) v = V{T(0), T(0)};
+            x[pad16(i)] = v;
+            if (i > 0 && i < M) x[pad16(L - i)] = sine ? V{-v.x, -v.y} : v;
+        };
+        if constexpr (kPrefetch) {
+            if (seq + stride < seqs) load(seq + stride, nxt);
+#pragma unroll
+            for (int q = 0; q < kPer; ++q)
+                if (lane + 32 * q < nz) extend(lane + 32 * q, cur[q]);
+        } else {
+            for (int i = lane; i < nz; i += 32) extend(i, col[i]);
+        }
+        __syncwarp();
+        warp_fft<T, L, -1>(x, tw, lane);
+        for (int k = lane; k < nz; k += 32) {
+            V y = x[pad16(k)];
+            if (sine) y = V{-y.y, y.x};  // i * X_k
+            store_result<T>(col, k, y, M, sine, normalize);
+        }
+        __syncwarp();  // the slot is rewritten by the next column
+        if constexpr (kPrefetch) {
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) cur[q] = nxt[q];
+        }
     }
 }
 
@@ -138,12 +173,25 @@ cudaError_t launch_fft(cx<T>* data, long long seqs, int storage, int first, int 
                        const cx<T>* tw, cudaStream_t s) {
     const size_t bytes = static_cast<size_t>(kWarps) * (L + L / 16) * sizeof(cx<T>);
     auto kernel = type1_fft_kernel<T, L>;
-    if (bytes > 48 * 1024) {
-        const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    // Resident blocks per SM and SM count, per device (each instantiation).
+    static int cachedDevice = -1, cachedBlocks = 0;
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) return err;
+    if (device != cachedDevice) {
+        if (bytes > 48 * 1024) {
+            err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+            if (err != cudaSuccess) return err;
+        }
+        int perSm = 0, sms = 0;
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kWarps * 32, bytes);
         if (err != cudaSuccess) return err;
+        err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (err != cudaSuccess) return err;
+        cachedBlocks = std::max(1, perSm) * std::max(1, sms);
+        cachedDevice = device;
     }
-    const long long blocks = (seqs + kWarps - 1) / kWarps;
-    if (blocks > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
+    const long long blocks = std::min<long long>((seqs + kWarps - 1) / kWarps, cachedBlocks);
     kernel<<<static_cast<unsigned>(blocks), kWarps * 32, bytes, s>>>(data, seqs, storage, first, channels, mask, norm,
                                                                      tw);
     return cudaGetLastError();
