@@ -373,6 +373,31 @@ SKB_API int skb_flux_check_device(skb_flux* p);
 SKB_API int skb_flux_capture_graph(skb_flux* p, const void* modal_input, void* modal_output);
 SKB_API int skb_flux_replay_graph(skb_flux* p, void* stream);
 
+/* ---------------------------------------------------------- autotuner */
+/* The project autotuner picks the fused flux path's launch shapes (work-unit
+ * size of each tensor-core GEMM: 4, 8, 16 or 32 M-tiles; kernel form of each
+ * 512-point band column stage: direct or warp-per-plane) by timing every
+ * candidate with CUDA events on the caller's device buffers.  Choices are
+ * cached per (stage shape, device) for the process and, when the environment
+ * variable SKB_TUNE_CACHE names a file, in that file (one "<value> <ms> <key>"
+ * line per choice); every flux handle created afterwards with the same shape
+ * starts with them.  skb_flux_autotune measures what is not cached yet,
+ * applies the choices, leaves the flux of modal_input in modal_output, drops
+ * any captured graph (capture again afterwards), adds the time to the
+ * handle's planning seconds, and writes "key = value (ms)" lines to summary
+ * (NUL-terminated, truncated to capacity; may be NULL).  The staged FP64 and
+ * FP32 modes have no tuned shapes (an empty summary). */
+SKB_API int skb_flux_autotune(skb_flux* p, const void* modal_input, void* modal_output, char* summary,
+                              uint64_t capacity);
+/* Host-side access to the cache (no GPU needed). */
+SKB_API int skb_tune_cache_size(uint64_t* count);
+SKB_API int skb_tune_cache_entry(uint64_t index, char* key, uint64_t key_capacity, int* value, double* ms);
+SKB_API int skb_tune_cache_store(const char* key, int value, double ms);
+SKB_API int skb_tune_cache_lookup(const char* key, int* value, int* found);
+SKB_API int skb_tune_cache_clear(void);
+SKB_API int skb_tune_cache_load(const char* path, uint64_t* count);
+SKB_API int skb_tune_cache_save(const char* path, uint64_t* count);
+
 /* ---------------------------------------------- spectral-pipeline round trip */
 /* The spectral-pipeline kernel of skbench (runSpectralPipelineBenchmark,
  * src/benchmark.cpp:2978-3956; reference order 3072-3110): r2c with radial 2/3

@@ -2,12 +2,15 @@
 
 #include "skb_cuda.h"
 
+#include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <new>
 #include <string>
 
+#include "autotune.hpp"
 #include "flux.hpp"
 #include "noalloc.hpp"
 #include "pipeline.hpp"
@@ -1657,6 +1660,86 @@ int skb_flux_replay_graph(skb_flux* p, void* stream) {
     return guard([&] {
         require(p != nullptr, "handle must be non-null");
         p->pipeline->replay(stream ? static_cast<cudaStream_t>(stream) : p->stream);
+    });
+}
+
+// --------------------------------------------------------------- autotuner
+
+namespace {
+void copy_string(const std::string& text, char* out, uint64_t capacity) {
+    if (out == nullptr || capacity == 0) return;
+    const size_t n = std::min<size_t>(text.size(), static_cast<size_t>(capacity - 1));
+    std::memcpy(out, text.data(), n);
+    out[n] = '\0';
+}
+}  // namespace
+
+int skb_flux_autotune(skb_flux* p, const void* in, void* out, char* summary, uint64_t capacity) {
+    return guard([&] {
+        require(p && in && out, "handle and buffers must be non-null");
+        const auto chosen = p->pipeline->autotune(in, out, p->stream);
+        std::string text;
+        for (const auto& c : chosen) {
+            char ms[32];
+            std::snprintf(ms, sizeof ms, "%.4f", c.ms);
+            text += c.key + " = " + std::to_string(c.value) + " (" + ms + " ms)\n";
+        }
+        copy_string(text, summary, capacity);
+    });
+}
+
+int skb_tune_cache_size(uint64_t* count) {
+    return guard([&] {
+        require(count != nullptr, "count must be non-null");
+        *count = tune_entries().size();
+    });
+}
+
+int skb_tune_cache_entry(uint64_t index, char* key, uint64_t key_capacity, int* value, double* ms) {
+    return guard([&] {
+        const auto entries = tune_entries();
+        require(index < entries.size(), "tuning cache index out of range");
+        copy_string(entries[index].key, key, key_capacity);
+        if (value != nullptr) *value = entries[index].value;
+        if (ms != nullptr) *ms = entries[index].ms;
+    });
+}
+
+int skb_tune_cache_store(const char* key, int value, double ms) {
+    return guard([&] {
+        require(key != nullptr && *key != '\0', "key must be non-empty");
+        const std::string k(key);
+        require(k.find('\n') == std::string::npos, "key must be one line");
+        tune_store(k, value, ms);
+    });
+}
+
+int skb_tune_cache_lookup(const char* key, int* value, int* found) {
+    return guard([&] {
+        require(key != nullptr && found != nullptr, "key and found must be non-null");
+        int v = 0;
+        *found = tune_lookup(key, v) ? 1 : 0;
+        if (value != nullptr && *found) *value = v;
+    });
+}
+
+int skb_tune_cache_clear(void) {
+    return guard([&] { tune_clear(); });
+}
+
+int skb_tune_cache_load(const char* path, uint64_t* count) {
+    return guard([&] {
+        require(path != nullptr, "path must be non-null");
+        const int n = tune_load(path);
+        if (count != nullptr) *count = static_cast<uint64_t>(n);
+    });
+}
+
+int skb_tune_cache_save(const char* path, uint64_t* count) {
+    return guard([&] {
+        require(path != nullptr, "path must be non-null");
+        const int n = tune_save(path);
+        if (count != nullptr) *count = static_cast<uint64_t>(n);
     });
 }
 

@@ -550,11 +550,11 @@ __global__ void __launch_bounds__(32 * B, 4) columns_forward_band_warp_kernel(in
 
 template <int N>
 cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, const void* tw,
-                           cudaStream_t s) {
+                           bool warpForm, cudaStream_t s) {
     constexpr int B = 8;
     const int zChunks = (nz + B - 1) / B;
     const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
-    if constexpr (N == kDirectN) {
+    if (N == kDirectN && !warpForm) {
         cudaError_t err = prepare(columns_inverse_band_kernel, kDirectSmem);
         if (err != cudaSuccess) return err;
         columns_inverse_band_kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band,
@@ -571,11 +571,11 @@ cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBin
 
 template <int N>
 cudaError_t forward_band_n(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, double scale,
-                           const void* tw, cudaStream_t s) {
+                           const void* tw, bool warpForm, cudaStream_t s) {
     constexpr int B = 8;
     const int zChunks = (nz + B - 1) / B;
     const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
-    if constexpr (N == kDirectN) {
+    if (N == kDirectN && !warpForm) {
         cudaError_t err = prepare(columns_forward_band_kernel, kDirectSmem);
         if (err != cudaSuccess) return err;
         columns_forward_band_kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band, float(scale),
@@ -639,27 +639,29 @@ cudaError_t launch_columns_gather_warp(int ny, int nz, int zStride, int columns,
 namespace skb {
 
 cudaError_t launch_columns_inverse_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
-                                        const int* band, const void* tw, cudaStream_t s) {
+                                        const int* band, const void* tw, int form, cudaStream_t s) {
+    const bool w = form == kBandWarp;
     if (slots <= 0 || columns <= 0) return cudaSuccess;
     switch (ny) {
-        case 32: return inverse_band_n<32>(nz, zStride, slots, columns, bins, band, tw, s);
-        case 64: return inverse_band_n<64>(nz, zStride, slots, columns, bins, band, tw, s);
-        case 128: return inverse_band_n<128>(nz, zStride, slots, columns, bins, band, tw, s);
-        case 256: return inverse_band_n<256>(nz, zStride, slots, columns, bins, band, tw, s);
-        case 512: return inverse_band_n<512>(nz, zStride, slots, columns, bins, band, tw, s);
+        case 32: return inverse_band_n<32>(nz, zStride, slots, columns, bins, band, tw, w, s);
+        case 64: return inverse_band_n<64>(nz, zStride, slots, columns, bins, band, tw, w, s);
+        case 128: return inverse_band_n<128>(nz, zStride, slots, columns, bins, band, tw, w, s);
+        case 256: return inverse_band_n<256>(nz, zStride, slots, columns, bins, band, tw, w, s);
+        case 512: return inverse_band_n<512>(nz, zStride, slots, columns, bins, band, tw, w, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_columns_forward_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
-                                        const int* band, double scale, const void* tw, cudaStream_t s) {
+                                        const int* band, double scale, const void* tw, int form, cudaStream_t s) {
+    const bool w = form == kBandWarp;
     if (slots <= 0 || columns <= 0) return cudaSuccess;
     switch (ny) {
-        case 32: return forward_band_n<32>(nz, zStride, slots, columns, bins, band, scale, tw, s);
-        case 64: return forward_band_n<64>(nz, zStride, slots, columns, bins, band, scale, tw, s);
-        case 128: return forward_band_n<128>(nz, zStride, slots, columns, bins, band, scale, tw, s);
-        case 256: return forward_band_n<256>(nz, zStride, slots, columns, bins, band, scale, tw, s);
-        case 512: return forward_band_n<512>(nz, zStride, slots, columns, bins, band, scale, tw, s);
+        case 32: return forward_band_n<32>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
+        case 64: return forward_band_n<64>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
+        case 128: return forward_band_n<128>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
+        case 256: return forward_band_n<256>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
+        case 512: return forward_band_n<512>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -22,9 +22,14 @@ cudaError_t launch_columns_gather_warp(int ny, int nz, int zStride, int columns,
 // f: f * zStride + z): band[kx] bounds the retained cells of column kx
 // (min(ky, Ny - ky) <= band[kx]).  Inverse: band cells in, whole column out.
 // Forward: whole column in, band cells (times scale) out.
+// Band kernel forms: kBandDefault is the direct three-pass kernel at Ny = 512
+// and the warp-per-plane kernel below; kBandWarp selects the warp-per-plane
+// kernel at every size (an autotuner candidate at 512).
+constexpr int kBandDefault = 0;
+constexpr int kBandWarp = 1;
 cudaError_t launch_columns_inverse_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
-                                        const int* band, const void* tw, cudaStream_t s);
+                                        const int* band, const void* tw, int form, cudaStream_t s);
 cudaError_t launch_columns_forward_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
-                                        const int* band, double scale, const void* tw, cudaStream_t s);
+                                        const int* band, double scale, const void* tw, int form, cudaStream_t s);
 
 }  // namespace skb

@@ -1,5 +1,10 @@
 #include "flux.hpp"
 
+#include <chrono>
+#include <functional>
+
+#include "autotune.hpp"
+#include "columns_warp.hpp"
 #include "flux_rows.hpp"
 #include "pointwise.hpp"
 
@@ -96,6 +101,103 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
     // Staged: 2 GEMMs, 2 launches per inverse / forward horizontal, members pointwise per target.
     // Fused: GEMM, embed+columns, fused rows, columns+retention, GEMM.
     launches_ = fused_ ? 5 : 2 + 2 + cfg.targets * (2 + cfg.members + 2);
+    apply_tuned(nullptr, nullptr, nullptr, nullptr);
+}
+
+// Tuned launch shapes of the fused path (autotune.hpp):
+//   work-unit size (M-tiles per unit) of each tensor-core GEMM, 4 / 8 / 16 / 32;
+//   kernel form of each 512-point band column stage, direct / warp-per-plane.
+// With buffers, missing choices are measured on them (tune_pick); without,
+// only cached choices are applied.  Returns the choices in force.
+std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* modalOut, cudaStream_t s,
+                                                 double* seconds) {
+    std::vector<TuneEntry> chosen;
+    if (!fused_ || !dense_) return chosen;
+    const auto start = std::chrono::steady_clock::now();
+    const bool measure = modalIn != nullptr;
+    const std::string dev = " | " + device_tag();
+    const std::uint64_t M = cfg_.members, T = cfg_.targets;
+    const std::string shape = " n=" + std::to_string(cfg_.n) + " nz=" + std::to_string(cfg_.nz) +
+                              " targets=" + std::to_string(T) + " members=" + std::to_string(M);
+    const long long keep = horizontal_->keep();
+    const long long inStored = static_cast<long long>(M * fieldsIn_ * zStride_);
+    const long long outStored = static_cast<long long>(M * T * zStride_);
+    const DenseBins binsIn{binsIn_.get(), inStored, keep};
+    const DenseBins binsOut{binsOut_.get(), outStored, keep};
+    const BinBoundary gemmOut{cellIn_.get<long long>(), partnerIn_.get<long long>(), modeConj_.get<unsigned char>(),
+                              static_cast<int>(fieldsIn_), static_cast<int>(zStride_)};
+    const BinBoundary gemmIn{cellOut_.get<long long>(), nullptr, modeConj_.get<unsigned char>(), static_cast<int>(T),
+                             static_cast<int>(zStride_)};
+    auto pick = [&](const std::string& key, const std::vector<int>& candidates, const std::function<void(int)>& apply,
+                    const std::function<void()>& run) {
+        int value = 0;
+        double ms = 0.0;
+        if (measure) {
+            value = tune_pick(key, candidates, [&](int c) {
+                apply(c);
+                run();
+            }, s, 1, 3, &ms);
+        } else if (!tune_lookup(key, value)) {
+            return;
+        }
+        apply(value);
+        chosen.push_back({key, value, ms});
+    };
+    auto unitTiles = [&](VerticalPlan& g) {
+        return [&g, s](int c) {
+            if (g.unit_tiles() == c) return;
+            // The unit tables are replaced: no launch may still read them.
+            if (s != nullptr) check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+            g.set_unit_tiles(c);
+        };
+    };
+    auto gemmKey = [&](const char* dir, const VerticalPlan& g) {
+        return std::string("flux.tc_gemm.unit_tiles ") + dir + shape + " R=" + std::to_string(g.rows_out()) +
+               " S=" + std::to_string(g.inner()) + " groups=" + std::to_string(g.groups()) + dev;
+    };
+    const std::vector<int> tileCandidates{4, 8, 16, 32};
+    pick(gemmKey("inverse", *inverseGemm_), tileCandidates, unitTiles(*inverseGemm_), [&] {
+        inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {binsIn_.get(), nullptr}, s, M, nullptr,
+                              &gemmOut);
+    });
+    pick(gemmKey("forward", *forwardGemm_), tileCandidates, unitTiles(*forwardGemm_), [&] {
+        forwardGemm_->execute({binsOut_.get(), nullptr}, {modalOut, nullptr}, s, M, &gemmIn, nullptr);
+    });
+    if (cfg_.n == 512) {
+        // Both forms run in place on the bin arrays; repeated runs leave values
+        // the final execution below overwrites.
+        const std::vector<int> forms{kBandDefault, kBandWarp};
+        pick("flux.columns_band.form inverse" + shape + dev, forms,
+             [&](int c) { horizontal_->set_band_forms(c, horizontal_->band_form_forward()); },
+             [&] { horizontal_->inverse_columns_band(binsIn, static_cast<int>(M * fieldsIn_), static_cast<int>(zStride_), s); });
+        pick("flux.columns_band.form forward" + shape + dev, forms,
+             [&](int c) { horizontal_->set_band_forms(horizontal_->band_form_inverse(), c); },
+             [&] {
+                 horizontal_->forward_columns_band(binsOut, static_cast<int>(M * T), 1.0, static_cast<int>(zStride_), s);
+             });
+    }
+    if (measure) run(modalIn, modalOut, s, nullptr, M);
+    if (seconds != nullptr) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+    return chosen;
+}
+
+std::vector<TuneEntry> FluxPipeline::autotune(const void* modalIn, void* modalOut, cudaStream_t s) {
+    if (modalIn == nullptr || modalOut == nullptr) throw Error(-1, "autotune needs the input and output buffers");
+    // A captured graph holds the old launch shapes.
+    if (graphExec_ != nullptr) {
+        cudaGraphExecDestroy(graphExec_);
+        graphExec_ = nullptr;
+    }
+    if (graph_ != nullptr) {
+        cudaGraphDestroy(graph_);
+        graph_ = nullptr;
+    }
+    double seconds = 0.0;
+    auto chosen = apply_tuned(modalIn, modalOut, s, &seconds);
+    check_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    planningSeconds += seconds;
+    tunedSeconds = seconds;
+    return chosen;
 }
 
 FluxPipeline::~FluxPipeline() {

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "autotune.hpp"
 #include "runtime.hpp"
 
 namespace skb {
@@ -52,6 +53,13 @@ public:
     };
     std::vector<StageTime> profile(const void* modalIn, void* modalOut, cudaStream_t s);
     void capture(const void* modalIn, void* modalOut, cudaStream_t s);
+    // Project autotuner: measures every missing launch-shape choice of the
+    // fused path on these buffers (the input is read; the output receives the
+    // flux), applies and caches them (autotune.hpp), and drops any captured
+    // graph (capture again after tuning).  Cached choices are already applied
+    // when a pipeline is created.  Returns the choices in force.
+    std::vector<TuneEntry> autotune(const void* modalIn, void* modalOut, cudaStream_t s);
+    double tunedSeconds = 0.0;
     // Raises if a bounded device wait inside a tensor-core kernel expired.
     void check_device_errors() const;
     void replay(cudaStream_t s);
@@ -90,6 +98,7 @@ private:
     std::uint64_t launches_ = 0;
     struct Recorder;
     void runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
+    std::vector<TuneEntry> apply_tuned(const void* modalIn, void* modalOut, cudaStream_t s, double* seconds);
     void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graphExec_ = nullptr;

@@ -182,7 +182,7 @@ void HorizontalPlan::inverse_columns_band(DenseBins bins, int slots, int zStride
     if (!bandExact_ || p_ != Precision::f32 || !columns_warp_supported(static_cast<long long>(w_.ny)))
         throw Error(-3, "band column stage needs FP32, an exact retained band and Ny in [32, 512]");
     check_cuda(launch_columns_inverse_band(static_cast<int>(w_.ny), static_cast<int>(w_.nz), zStride, slots, keep_,
-                                           bins, band_.get<int>(), twCol_.get(), s),
+                                           bins, band_.get<int>(), twCol_.get(), bandFormInverse_, s),
                "band inverse column kernel");
 }
 
@@ -190,7 +190,7 @@ void HorizontalPlan::forward_columns_band(DenseBins bins, int slots, double scal
     if (!bandExact_ || p_ != Precision::f32 || !columns_warp_supported(static_cast<long long>(w_.ny)))
         throw Error(-3, "band column stage needs FP32, an exact retained band and Ny in [32, 512]");
     check_cuda(launch_columns_forward_band(static_cast<int>(w_.ny), static_cast<int>(w_.nz), zStride, slots, keep_,
-                                           bins, band_.get<int>(), scale, twCol_.get(), s),
+                                           bins, band_.get<int>(), scale, twCol_.get(), bandFormForward_, s),
                "band forward column kernel");
 }
 
@@ -296,35 +296,8 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
             gc[gi] = static_cast<int>(groups[gi].count * fields);
             gf[gi] = static_cast<int>(groups[gi].first * fields);
         }
-        // Units: runs of up to unit_tiles * 64 virtual (member, column) pairs of
-        // one group, largest first so the long units start early.  One table
-        // per active member count so partial batches launch only their units.
-        struct Unit {
-            int g, col, count;
-        };
-        const int span = tc_gemm_unit_tiles() * 64;
-        for (std::uint64_t active = 1; active <= members; ++active) {
-            std::vector<Unit> units;
-            for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
-                const int total = static_cast<int>(active) * gc[gi];
-                for (int c = 0; c < total; c += span)
-                    units.push_back({static_cast<int>(gi), c, std::min(span, total - c)});
-            }
-            std::stable_sort(units.begin(), units.end(),
-                             [](const Unit& a, const Unit& b) { return a.count > b.count; });
-            std::vector<int> ug, uc, un;
-            for (const auto& u : units) {
-                ug.push_back(u.g);
-                uc.push_back(u.col);
-                un.push_back(u.count);
-            }
-            UnitTable table;
-            table.units = static_cast<int>(ug.size());
-            table.group = upload_vector(ug);
-            table.column = upload_vector(uc);
-            table.count = upload_vector(un);
-            unitTables_.push_back(std::move(table));
-        }
+        groupColumnsHost_ = gc;
+        build_units(tc_gemm_unit_tiles());
         groupColumns_ = upload_vector(gc);
         groupFirst_ = upload_vector(gf);
         error_.allocate(sizeof(int));
@@ -363,6 +336,46 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
     tileGroup_ = upload_vector(tg);
     tileColumn_ = upload_vector(tc);
     tileCount_ = upload_vector(tn);
+}
+
+// Units: runs of up to tiles * 64 virtual (member, column) pairs of one
+// group, largest first so the long units start early.  One table per active
+// member count so partial batches launch only their units.
+void VerticalPlan::build_units(int tiles) {
+    if (tiles < 1) throw Error(-1, "work units need at least one tile");
+    struct Unit {
+        int g, col, count;
+    };
+    const int span = tiles * 64;
+    std::vector<UnitTable> tables;
+    for (std::uint64_t active = 1; active <= members_; ++active) {
+        std::vector<Unit> units;
+        for (std::size_t gi = 0; gi < groupColumnsHost_.size(); ++gi) {
+            const int total = static_cast<int>(active) * groupColumnsHost_[gi];
+            for (int c = 0; c < total; c += span)
+                units.push_back({static_cast<int>(gi), c, std::min(span, total - c)});
+        }
+        std::stable_sort(units.begin(), units.end(), [](const Unit& a, const Unit& b) { return a.count > b.count; });
+        std::vector<int> ug, uc, un;
+        for (const auto& u : units) {
+            ug.push_back(u.g);
+            uc.push_back(u.col);
+            un.push_back(u.count);
+        }
+        UnitTable table;
+        table.units = static_cast<int>(ug.size());
+        table.group = upload_vector(ug);
+        table.column = upload_vector(uc);
+        table.count = upload_vector(un);
+        tables.push_back(std::move(table));
+    }
+    unitTables_ = std::move(tables);
+    unitTiles_ = tiles;
+}
+
+void VerticalPlan::set_unit_tiles(int tiles) {
+    if (p_ != GemmPrecision::tf32x3) throw Error(-3, "work-unit size applies to the tensor-core form only");
+    if (tiles != unitTiles_) build_units(tiles);
 }
 
 std::uint64_t VerticalPlan::persistentBytes() const {

@@ -126,6 +126,13 @@ public:
     bool band_exact() const { return bandExact_; }
     void inverse_columns_band(DenseBins bins, int slots, int zStride, cudaStream_t s) const;
     void forward_columns_band(DenseBins bins, int slots, double scale, int zStride, cudaStream_t s) const;
+    // Kernel form of each band stage (kBandDefault / kBandWarp, columns_warp.hpp).
+    void set_band_forms(int inverseForm, int forwardForm) {
+        bandFormInverse_ = inverseForm;
+        bandFormForward_ = forwardForm;
+    }
+    int band_form_inverse() const { return bandFormInverse_; }
+    int band_form_forward() const { return bandFormForward_; }
     const void* twiddlesHalf() const { return twHalf_.get(); }
     const void* twiddlesFull() const { return twFull_.get(); }
     void embed_dense(const ViewSet& views, void* wvm, std::uint64_t planes, cudaStream_t s) const;
@@ -144,6 +151,7 @@ private:
     DeviceBuffer bins_;
     DeviceBuffer band_;
     bool bandExact_ = false;
+    int bandFormInverse_ = 0, bandFormForward_ = 0;
 };
 
 // Vertical plan for one direction: the group matrices prepared for the chosen
@@ -168,8 +176,16 @@ public:
     std::uint64_t matrixBytes() const { return matrices_.bytes(); }
     std::uint64_t persistentBytes() const;
     int launches() const { return 1; }
+    // Tensor-core form: M-tiles (64 columns) per work unit; the unit tables are
+    // rebuilt for a new size (device work must not be in flight on them).
+    void set_unit_tiles(int tiles);
+    int unit_tiles() const { return unitTiles_; }
+    int rows_out() const { return R_; }
+    int inner() const { return S_; }
+    std::uint64_t groups() const { return groupColumnsHost_.size(); }
 
 private:
+    void build_units(int tiles);
     GemmPrecision p_;
     int R_, S_;
     std::uint64_t columns_ = 0;
@@ -184,6 +200,8 @@ private:
         int units = 0;
     };
     std::vector<UnitTable> unitTables_;
+    std::vector<int> groupColumnsHost_;  // complex columns per member in each group
+    int unitTiles_ = 0;
     DeviceBuffer groupColumns_, groupFirst_, error_;
 };
 

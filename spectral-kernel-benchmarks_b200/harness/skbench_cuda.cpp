@@ -199,7 +199,7 @@ struct Options {
     std::string kernel = "fft", profile = "smoke", providers = "cuda", precision = "fp64";
     std::string gemm = "fp64", family = "k2-grouped", fluxMode = "split-tf32x3", output;
     std::uint64_t members = 1, targets = 4, warmups = 0, samples = 0, seed = 129;
-    bool warmupsSet = false, samplesSet = false;
+    bool warmupsSet = false, samplesSet = false, autotune = false;
     std::uint64_t nx = 0, ny = 0, nz = 0, fields = 0;
 };
 
@@ -1110,6 +1110,27 @@ ProviderRecord run_flux(const Options& o, const skb_workload& w, Report& report)
     if (f64) dIn.upload(x, stream);
     else dIn.upload(narrow<float>(x), stream);
     const std::uint64_t bytes = (inN + outN) * 2 * s;
+    if (o.autotune) {
+        // Launch shapes from the project autotuner, measured on these buffers
+        // before any timing; the tuning time counts as planning.
+        std::vector<char> summary(8192);
+        ok(skb_flux_autotune(h, dIn.p, dOut.p, summary.data(), summary.size()));
+        ok(skb_flux_info(h, &info));
+        rec.planningSeconds = info.planning_seconds;
+        std::string choices;
+        for (const char* line = summary.data(); *line;) {
+            const char* end = std::strchr(line, '\n');
+            std::string entry(line, end ? end : line + std::strlen(line));
+            const auto bar = entry.find(" | ");
+            const auto eq = entry.find(" = ");
+            if (bar != std::string::npos && eq != std::string::npos)
+                entry = entry.substr(0, bar) + entry.substr(eq);
+            choices += (choices.empty() ? "" : "; ") + entry;
+            if (!end) break;
+            line = end + 1;
+        }
+        rec.planningConfiguration += "; autotuned: " + (choices.empty() ? std::string("no tuned shapes") : choices);
+    }
     rec.timings.push_back(series("primitive", "production-lifetime streamed four-target spectral-flux composition",
                                  "forward", bytes, measure_device(o.warmups, o.samples, stream, [&] {
                                      ok(skb_flux_execute_device(h, dIn.p, dOut.p, stream));
@@ -1132,6 +1153,8 @@ ProviderRecord run_flux(const Options& o, const skb_workload& w, Report& report)
                    mode == SKB_FLUX_SPLIT_TF32X3 ? "inside the row kernel" : "separate kernel"},
                   {"forward horizontal and retention", StageState::executed, "per target"},
                   {"forward vertical GEMM", StageState::executed, "all targets in one launch"}};
+    if (o.autotune)
+        rec.ledger.push_back({"autotune", StageState::setupOnly, "launch shapes measured on the run's own buffers"});
     ok(skb_flux_check_device(h));
 
     // Correctness.  FP64-plain: member 0 against the direct host composition
@@ -1364,7 +1387,7 @@ void usage(std::ostream& out) {
            "              [--providers cuda]\n"
         << "              [--precision fp64|fp32] [--vertical-gemm-family common|k2-grouped]\n"
         << "              [--vertical-gemm-precision fp64|fp32|tf32x3] [--flux-mode fp64-plain|fp32|split-tf32x3]\n"
-        << "              [--members N] [--targets 3|4] [--nx N --ny N --nz N --fields N]\n"
+        << "              [--members N] [--targets 3|4] [--autotune] [--nx N --ny N --nz N --fields N]\n"
         << "              [--warmups N] [--samples N] [--seed N] [--output PATH]\n"
         << "  skbench-cuda compare --input SAMPLES.csv\n";
 }
@@ -1413,6 +1436,7 @@ int run(int argc, char** argv) {
             o.samplesSet = true;
         } else if (k == "--seed") o.seed = std::stoull(value(argc, argv, i));
         else if (k == "--output") o.output = value(argc, argv, i);
+        else if (k == "--autotune") o.autotune = true;
         else throw std::invalid_argument("Unknown run option: " + std::string(k));
     }
     if (o.kernel == "2d-rfft") o.kernel = "fft";

@@ -747,6 +747,49 @@ class SpectralPipeline:
             pass
 
 
+def tune_cache():
+    """The autotuner's cache: {key: (value, ms)}."""
+    lib = library()
+    n = ctypes.c_uint64()
+    check(lib.skb_tune_cache_size(ctypes.byref(n)))
+    out = {}
+    key = ctypes.create_string_buffer(1024)
+    value = ctypes.c_int()
+    ms = ctypes.c_double()
+    for i in range(n.value):
+        check(lib.skb_tune_cache_entry(_u64(i), key, _u64(len(key)), ctypes.byref(value), ctypes.byref(ms)))
+        out[key.value.decode()] = (value.value, ms.value)
+    return out
+
+
+def tune_cache_store(key, value, ms=0.0):
+    check(library().skb_tune_cache_store(key.encode(), ctypes.c_int(value), ctypes.c_double(ms)))
+
+
+def tune_cache_lookup(key):
+    """The cached value for key, or None."""
+    value = ctypes.c_int()
+    found = ctypes.c_int()
+    check(library().skb_tune_cache_lookup(key.encode(), ctypes.byref(value), ctypes.byref(found)))
+    return value.value if found.value else None
+
+
+def tune_cache_clear():
+    check(library().skb_tune_cache_clear())
+
+
+def tune_cache_load(path):
+    n = ctypes.c_uint64()
+    check(library().skb_tune_cache_load(os.fsencode(path), ctypes.byref(n)))
+    return n.value
+
+
+def tune_cache_save(path):
+    n = ctypes.c_uint64()
+    check(library().skb_tune_cache_save(os.fsencode(path), ctypes.byref(n)))
+    return n.value
+
+
 class ConstantStratificationVertical:
     """Type-I vertical transforms of the constant-stratification kernel, in
     place on complex [row][storage_channels][nz] arrays (z adjacent).
@@ -922,6 +965,21 @@ class Flux:
 
     def capture_graph(self, in_ptr, out_ptr):
         check(library().skb_flux_capture_graph(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr)))
+
+    def autotune(self, in_ptr, out_ptr):
+        """Project autotuner: measure the fused path's launch shapes on these
+        device buffers (cached per shape and device), apply them and leave the
+        flux in out_ptr.  Returns {key: (value, ms)}; a captured graph is
+        dropped (capture again afterwards)."""
+        buf = ctypes.create_string_buffer(8192)
+        check(library().skb_flux_autotune(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), buf,
+                                          _u64(len(buf))))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            key, _, rest = line.rpartition(" = ")
+            value, _, ms = rest.partition(" (")
+            out[key] = (int(value), float(ms.split(" ")[0]))
+        return out
 
     def replay_graph(self, stream=None):
         check(library().skb_flux_replay_graph(self.h, ctypes.c_void_p(stream)))

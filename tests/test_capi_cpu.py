@@ -117,3 +117,42 @@ def skb_cuda_has_device():
         return skb_cuda.device_count() > 0
     except RuntimeError:
         return False
+
+
+def test_tuning_cache_round_trip(tmp_path):
+    """The autotuner's cache on the host: store / lookup / save / clear / load,
+    one "<value> <ms> <key>" line per entry."""
+    skb_cuda.tune_cache_clear()
+    key = "flux.tc_gemm.unit_tiles inverse n=64 nz=17 targets=4 members=2 R=17 S=10 groups=40 | test-device/1"
+    skb_cuda.tune_cache_store(key, 8, 0.125)
+    assert skb_cuda.tune_cache_lookup(key) == 8
+    assert skb_cuda.tune_cache_lookup(key + " other") is None
+    path = tmp_path / "tune.txt"
+    assert skb_cuda.tune_cache_save(str(path)) == 1
+    assert path.read_text() == "8 0.125 " + key + "\n"
+    skb_cuda.tune_cache_clear()
+    assert skb_cuda.tune_cache() == {}
+    path.write_text(path.read_text() + "not a line\n16 2.5 second key | test-device/1\n")
+    assert skb_cuda.tune_cache_load(str(path)) == 2
+    assert skb_cuda.tune_cache() == {key: (8, 0.125), "second key | test-device/1": (16, 2.5)}
+    with pytest.raises(ValueError):
+        skb_cuda.tune_cache_store("two\nlines", 1)
+    skb_cuda.tune_cache_clear()
+
+
+def test_tuning_cache_file_from_the_environment(tmp_path):
+    """SKB_TUNE_CACHE: a new process starts with the file's choices and appends
+    the ones it makes."""
+    import subprocess
+    import sys
+
+    path = tmp_path / "env_tune.txt"
+    path.write_text("32 1.5 stage A | test-device/1\n")
+    code = ("import sys; sys.path.insert(0, %r); import skb_cuda as S; "
+            "print(S.tune_cache_lookup('stage A | test-device/1')); S.tune_cache_store('stage B | test-device/1', 4, 0.5)"
+            % os.path.join(ROOT, "spectral-kernel-benchmarks_b200"))
+    env = dict(os.environ, SKB_TUNE_CACHE=str(path))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == "32"
+    assert path.read_text().splitlines() == ["32 1.5 stage A | test-device/1", "4 0.5 stage B | test-device/1"]

@@ -1,0 +1,93 @@
+"""The project autotuner on the GPU: tuned launch shapes keep the split flux
+within its tolerance (1e-6 relative L2 against the FP64-plain path), choices
+are cached per shape and reused by later handles, and every band-column form
+the tuner may pick at 512 points is correct."""
+
+import numpy as np
+import pytest
+
+import skb_cuda
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _inputs(flux, seed):
+    rng = np.random.default_rng(seed)
+    n = flux.input_elements
+    return (rng.uniform(-0.125, 0.125, n) + 1j * rng.uniform(-0.125, 0.125, n)).astype(np.complex64)
+
+
+def _run(flux, x):
+    d_in = skb_cuda.DeviceArray.from_numpy(x)
+    d_out = skb_cuda.DeviceArray(flux.output_elements * 8)
+    flux.execute_device(d_in.ptr, d_out.ptr)
+    skb_cuda.synchronize()
+    return d_out.download(np.complex64, flux.output_elements)
+
+
+def _fp64(n, nz, members, x):
+    ref = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_FP64_PLAIN)
+    return ref.execute(x.astype(np.complex128))
+
+
+def test_autotune_keeps_parity_and_caches():
+    skb_cuda.tune_cache_clear()
+    n, nz, members = 64, 17, 2
+    flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    x = _inputs(flux, 5)
+    d_in = skb_cuda.DeviceArray.from_numpy(x)
+    d_out = skb_cuda.DeviceArray(flux.output_elements * 8)
+    flux.capture_graph(d_in.ptr, d_out.ptr)
+    chosen = flux.autotune(d_in.ptr, d_out.ptr)
+    kinds = sorted(k.split(" ")[0] + " " + k.split(" ")[1] for k in chosen)
+    assert kinds == ["flux.tc_gemm.unit_tiles forward", "flux.tc_gemm.unit_tiles inverse"]
+    assert all(v in (4, 8, 16, 32) and ms > 0 for v, ms in chosen.values())
+    tuned_out = d_out.download(np.complex64, flux.output_elements)
+    want = _fp64(n, nz, members, x)
+    assert orc.rel_l2_error(tuned_out, want) <= 1e-6
+    # The captured graph held the old shapes and was dropped.
+    with pytest.raises(skb_cuda.LogicError):
+        flux.replay_graph()
+    # Cached: a new handle starts with the choices and re-tuning measures nothing.
+    for key, (value, _) in chosen.items():
+        assert skb_cuda.tune_cache_lookup(key) == value
+    again = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    assert {k: v[0] for k, v in again.autotune(d_in.ptr, d_out.ptr).items()} == {k: v[0] for k, v in chosen.items()}
+    assert orc.rel_l2_error(_run(again, x), want) <= 1e-6
+
+
+@pytest.mark.parametrize("tiles", [4, 32])
+def test_every_unit_size_is_correct(tiles):
+    """A cached choice is applied when a handle is created: force each extreme."""
+    n, nz, members = 64, 17, 3
+    probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    x = _inputs(probe, 11)
+    d_in = skb_cuda.DeviceArray.from_numpy(x)
+    d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
+    keys = list(probe.autotune(d_in.ptr, d_out.ptr))
+    for key in keys:
+        skb_cuda.tune_cache_store(key, tiles, 0.0)
+    flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    assert orc.rel_l2_error(_run(flux, x), _fp64(n, nz, members, x)) <= 1e-6
+    skb_cuda.tune_cache_clear()
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_band_forms_at_512(form):
+    """Both 512-point band-column kernel forms (direct, warp-per-plane) the
+    tuner chooses between give the split flux within 1e-6 of FP64."""
+    skb_cuda.tune_cache_clear()
+    n, nz, members = 512, 9, 1
+    probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    x = _inputs(probe, 23)
+    d_in = skb_cuda.DeviceArray.from_numpy(x)
+    d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
+    chosen = probe.autotune(d_in.ptr, d_out.ptr)
+    band = [k for k in chosen if k.startswith("flux.columns_band.form")]
+    assert len(band) == 2
+    for key in band:
+        skb_cuda.tune_cache_store(key, form, 0.0)
+    flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    assert orc.rel_l2_error(_run(flux, x), _fp64(n, nz, members, x)) <= 1e-6
+    skb_cuda.tune_cache_clear()

@@ -50,11 +50,19 @@ def run(tmp_path, *args):
     ("--kernel", "production-lifetime-flux", "--flux-mode", "fp64-plain", "--nx", "32", "--ny", "32", "--nz", "9"),
     ("--kernel", "production-lifetime-flux", "--flux-mode", "split-tf32x3", "--nx", "64", "--ny", "64", "--nz",
      "17", "--members", "2"),
+    ("--kernel", "production-lifetime-flux", "--flux-mode", "split-tf32x3", "--nx", "64", "--ny", "64", "--nz",
+     "17", "--members", "2", "--autotune", "on"),
     ("--kernel", "spectral-pipeline", "--nx", "32", "--ny", "32", "--nz", "9"),
     ("--kernel", "spectral-pipeline", "--precision", "fp32", "--nx", "32", "--ny", "32", "--nz", "9"),
 ], ids=lambda a: "-".join(a[1::2]))
 def test_run_writes_the_reference_schema(tmp_path, args):
+    autotune = "--autotune" in args
+    if autotune:
+        args = tuple(a for a in args if a != "on")
     report, rows = run(tmp_path, "--profile", "smoke", *args)
+    if autotune:
+        cfg = report["providers"][0]["planning"]["configuration"]
+        assert "autotuned: flux.tc_gemm.unit_tiles inverse" in cfg, cfg
     with open(os.path.join(GOLDEN, "reference_report.json")) as fh:
         keys_match(json.load(fh), report)
     assert report["status"] == "passed"
