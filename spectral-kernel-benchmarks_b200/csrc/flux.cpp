@@ -106,6 +106,7 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
 
 // Tuned launch shapes of the fused path (autotune.hpp):
 //   work-unit size (M-tiles per unit) of each tensor-core GEMM, 4 / 8 / 16 / 32;
+//   z-planes (warps) per CTA of the fused row kernel, 4 / 8 / 16;
 //   kernel form of each 512-point band column stage, direct / warp-per-plane.
 // With buffers, missing choices are measured on them (tune_pick); without,
 // only cached choices are applied.  Returns the choices in force.
@@ -163,6 +164,8 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
     pick(gemmKey("forward", *forwardGemm_), tileCandidates, unitTiles(*forwardGemm_), [&] {
         forwardGemm_->execute({binsOut_.get(), nullptr}, {modalOut, nullptr}, s, M, &gemmIn, nullptr);
     });
+    pick("flux.rows.planes_per_cta" + shape + dev, {4, 8, 16}, [&](int c) { rowsPlanes_ = c; },
+         [&] { check_cuda(launch_rows_flux(row_args(M), s), "fused row flux kernel"); });
     if (cfg_.n == 512) {
         // Both forms run in place on the bin arrays; repeated runs leave values
         // the final execution below overwrites.
@@ -262,6 +265,27 @@ std::vector<FluxPipeline::StageTime> FluxPipeline::profile(const void* modalIn, 
     return rec.finish();
 }
 
+RowFluxArgs FluxPipeline::row_args(std::uint64_t members) const {
+    const double n = static_cast<double>(cfg_.n);
+    const long long keep = horizontal_->keep();
+    RowFluxArgs a{};
+    a.nx = static_cast<int>(cfg_.n);
+    a.ny = static_cast<int>(cfg_.n);
+    a.nz = static_cast<int>(cfg_.nz);
+    a.zStride = static_cast<int>(zStride_);
+    a.keep = static_cast<int>(keep);
+    a.members = static_cast<int>(members);
+    a.fieldsIn = static_cast<int>(fieldsIn_);
+    a.targets = static_cast<int>(cfg_.targets);
+    a.scale = static_cast<float>(1.0 / (n * n * n * n));
+    a.binsIn = {binsIn_.get(), static_cast<long long>(cfg_.members * fieldsIn_ * zStride_), keep};
+    a.binsOut = {binsOut_.get(), static_cast<long long>(cfg_.members * cfg_.targets * zStride_), keep};
+    a.twHalf = horizontal_->twiddlesHalf();
+    a.twFull = horizontal_->twiddlesFull();
+    a.planes = rowsPlanes_;
+    return a;
+}
+
 void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec,
                             std::uint64_t members) {
     const auto H = modes_, nz = cfg_.nz, T = cfg_.targets, M = members;
@@ -301,20 +325,7 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
         if (rec) rec->end("columns_inverse_embed", 1, double(inPlanes) * (compactPlane + binsPlane), 0.0);
     }
 
-    RowFluxArgs a{};
-    a.nx = static_cast<int>(cfg_.n);
-    a.ny = static_cast<int>(cfg_.n);
-    a.nz = static_cast<int>(nz);
-    a.zStride = static_cast<int>(zStride_);
-    a.keep = static_cast<int>(keep);
-    a.members = static_cast<int>(M);
-    a.fieldsIn = static_cast<int>(fieldsIn_);
-    a.targets = static_cast<int>(T);
-    a.scale = static_cast<float>(1.0 / (n * n * n * n));
-    a.binsIn = binsIn;
-    a.binsOut = binsOutArr;
-    a.twHalf = horizontal_->twiddlesHalf();
-    a.twFull = horizontal_->twiddlesFull();
+    const RowFluxArgs a = row_args(M);
     check_cuda(launch_rows_flux(a, s), "fused row flux kernel");
     if (rec) rec->end("rows_flux_fused", 1, double(inPlanes + outPlanes) * binsPlane, 0.0);
 

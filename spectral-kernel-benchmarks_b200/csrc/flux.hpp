@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "autotune.hpp"
+#include "flux_rows.hpp"
 #include "runtime.hpp"
 
 namespace skb {
@@ -99,6 +100,8 @@ private:
     struct Recorder;
     void runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     std::vector<TuneEntry> apply_tuned(const void* modalIn, void* modalOut, cudaStream_t s, double* seconds);
+    RowFluxArgs row_args(std::uint64_t members) const;
+    int rowsPlanes_ = 8;  // z-planes per CTA of the fused row kernel
     void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graphExec_ = nullptr;

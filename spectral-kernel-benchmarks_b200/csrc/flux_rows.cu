@@ -33,8 +33,10 @@ constexpr int region() {
     return M + M / 16 + 8;
 }
 
+// Launch bounds keep 128 registers per thread whatever the CTA width:
+// 16 / B CTAs of 32 * B threads fill 512 threads' worth of the register file.
 template <int M, int B>
-__global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
+__global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a) {
     using V = float2;
     constexpr int NT = 32 * B;
     constexpr int PER = M / 32;  // elements of its plane each lane keeps in registers
@@ -206,9 +208,10 @@ __global__ void __launch_bounds__(32 * B, 2) rows_flux_kernel(RowFluxArgs a) {
 
 }  // namespace
 
-template <int M>
-cudaError_t launch_m(const RowFluxArgs& a, dim3 grid, cudaStream_t stream) {
-    constexpr int B = 8;
+template <int M, int B>
+cudaError_t launch_m(const RowFluxArgs& a, cudaStream_t stream) {
+    const int zChunks = (a.nz + B - 1) / B;
+    const dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
     auto kernel = rows_flux_kernel<M, B>;
     const size_t bytes =
         sizeof(float2) * (size_t(B) * region<M>() + 2 * size_t(B) * (a.keep | 1) + size_t(a.keep) * (B + 1));
@@ -220,17 +223,24 @@ cudaError_t launch_m(const RowFluxArgs& a, dim3 grid, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+template <int M>
+cudaError_t launch_planes(const RowFluxArgs& a, cudaStream_t stream) {
+    switch (a.planes) {
+        case 4: return launch_m<M, 4>(a, stream);
+        case 8: return launch_m<M, 8>(a, stream);
+        case 16: return launch_m<M, 16>(a, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
     const int M = a.nx / 2;
-    constexpr int B = 8;
     if (a.keep < 1 || a.keep > M + 1 || a.fieldsIn != 3 + 3 * a.targets || a.zStride < a.nz) return cudaErrorInvalidValue;
-    const int zChunks = (a.nz + B - 1) / B;
-    dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
     switch (M) {
-        case 32: return launch_m<32>(a, grid, stream);
-        case 64: return launch_m<64>(a, grid, stream);
-        case 128: return launch_m<128>(a, grid, stream);
-        case 256: return launch_m<256>(a, grid, stream);
+        case 32: return launch_planes<32>(a, stream);
+        case 64: return launch_planes<64>(a, stream);
+        case 128: return launch_planes<128>(a, stream);
+        case 256: return launch_planes<256>(a, stream);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -16,6 +16,7 @@ struct RowFluxArgs {
     DenseBins binsOut;    // target bins, plane (member*targets + t)*zStride + z
     const void* twHalf;   // exp(-2 pi i k/(nx/2)), float2
     const void* twFull;   // exp(-2 pi i k/nx), float2
+    int planes = 8;       // z-planes (warps) per CTA: 4, 8 or 16 (an autotuner choice)
 };
 
 bool rows_flux_supported(long long nx);

@@ -40,9 +40,12 @@ def test_autotune_keeps_parity_and_caches():
     d_out = skb_cuda.DeviceArray(flux.output_elements * 8)
     flux.capture_graph(d_in.ptr, d_out.ptr)
     chosen = flux.autotune(d_in.ptr, d_out.ptr)
-    kinds = sorted(k.split(" ")[0] + " " + k.split(" ")[1] for k in chosen)
-    assert kinds == ["flux.tc_gemm.unit_tiles forward", "flux.tc_gemm.unit_tiles inverse"]
-    assert all(v in (4, 8, 16, 32) and ms > 0 for v, ms in chosen.values())
+    kinds = sorted(" ".join(k.split(" ")[:2]) for k in chosen)
+    assert kinds == ["flux.rows.planes_per_cta n=64", "flux.tc_gemm.unit_tiles forward",
+                     "flux.tc_gemm.unit_tiles inverse"]
+    for key, (value, ms) in chosen.items():
+        allowed = (4, 8, 16) if key.startswith("flux.rows") else (4, 8, 16, 32)
+        assert value in allowed and ms > 0
     tuned_out = d_out.download(np.complex64, flux.output_elements)
     want = _fp64(n, nz, members, x)
     assert orc.rel_l2_error(tuned_out, want) <= 1e-6
@@ -65,7 +68,8 @@ def test_every_unit_size_is_correct(tiles):
     x = _inputs(probe, 11)
     d_in = skb_cuda.DeviceArray.from_numpy(x)
     d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
-    keys = list(probe.autotune(d_in.ptr, d_out.ptr))
+    keys = [k for k in probe.autotune(d_in.ptr, d_out.ptr) if k.startswith("flux.tc_gemm.unit_tiles")]
+    assert len(keys) == 2
     for key in keys:
         skb_cuda.tune_cache_store(key, tiles, 0.0)
     flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
@@ -88,6 +92,24 @@ def test_band_forms_at_512(form):
     assert len(band) == 2
     for key in band:
         skb_cuda.tune_cache_store(key, form, 0.0)
+    flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    assert orc.rel_l2_error(_run(flux, x), _fp64(n, nz, members, x)) <= 1e-6
+    skb_cuda.tune_cache_clear()
+
+
+@pytest.mark.parametrize("n,planes", [(64, 4), (64, 16), (512, 4), (512, 16)])
+def test_every_row_kernel_width_is_correct(n, planes):
+    """The fused row kernel with 4, 8 or 16 z-planes per CTA (the tuner's
+    candidates; 8 is covered by every other flux test)."""
+    skb_cuda.tune_cache_clear()
+    nz, members = 17, 2
+    probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    x = _inputs(probe, 31)
+    d_in = skb_cuda.DeviceArray.from_numpy(x)
+    d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
+    keys = [k for k in probe.autotune(d_in.ptr, d_out.ptr) if k.startswith("flux.rows.planes_per_cta")]
+    assert len(keys) == 1
+    skb_cuda.tune_cache_store(keys[0], planes, 0.0)
     flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
     assert orc.rel_l2_error(_run(flux, x), _fp64(n, nz, members, x)) <= 1e-6
     skb_cuda.tune_cache_clear()
