@@ -240,8 +240,17 @@ struct skb_flux {
     cudaStream_t stream = nullptr;
     DeviceBuffer in, out;
     HostAdapter host{Precision::f64, {}};
+    // Host-array path: copy streams, FP64 staging of the FP32 forms, and one
+    // pair of events per member (input landed / result ready).
+    cudaStream_t copyIn = nullptr, copyOut = nullptr;
+    DeviceBuffer stageIn, stageOut;
+    std::vector<cudaEvent_t> landed, ready;
     ~skb_flux() {
         pipeline.reset();
+        for (auto e : landed) cudaEventDestroy(e);
+        for (auto e : ready) cudaEventDestroy(e);
+        if (copyIn) cudaStreamDestroy(copyIn);
+        if (copyOut) cudaStreamDestroy(copyOut);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -1603,20 +1612,72 @@ int skb_flux_execute_device_members(skb_flux* p, const void* in, void* out, uint
     });
 }
 
+// Host arrays: the members are pipelined so the link never waits on the
+// device.  Member m's input is uploaded on copyIn while member m-1 is computed
+// on the handle's stream and member m-2's result is downloaded on copyOut
+// (PCIe moves both directions at once); each member runs as a one-member flux
+// on its slice of the device buffers, with the FP64 <-> FP32 conversions of
+// reduced-precision handles on the compute stream.
 int skb_flux_execute(skb_flux* p, const skb_complex* in, skb_complex* out) {
     return guard([&] {
         require(p && in && out, "handle and buffers must be non-null");
         auto& f = *p->pipeline;
-        const size_t es = f.f64() ? sizeof(double) : sizeof(float);
+        const bool f64 = f.f64();
+        const size_t es = f64 ? sizeof(double) : sizeof(float);
+        const std::uint64_t members = f.config().members;
+        const std::uint64_t inPer = 2 * f.inputElements() / members, outPer = 2 * f.outputElements() / members;
         if (p->in.bytes() == 0) {
-            p->in.allocate(2 * es * f.inputElements());
-            p->out.allocate(2 * es * f.outputElements());
+            p->in.allocate(es * inPer * members);
+            p->out.allocate(es * outPer * members);
         }
-        p->host.p = f.f64() ? Precision::f64 : Precision::f32;
-        p->host.ensure(2 * std::max(f.inputElements(), f.outputElements()));
-        p->host.upload(p->in.get(), reinterpret_cast<const double*>(in), 2 * f.inputElements(), p->stream);
-        f.execute(p->in.get(), p->out.get(), p->stream);
-        p->host.download(reinterpret_cast<double*>(out), p->out.get(), 2 * f.outputElements(), p->stream);
+        if (p->copyIn == nullptr) {
+            p->copyIn = make_stream();
+            p->copyOut = make_stream();
+            for (std::uint64_t m = 0; m < members; ++m) {
+                cudaEvent_t a = nullptr, b = nullptr;
+                check_cuda(cudaEventCreateWithFlags(&a, cudaEventDisableTiming), "cudaEventCreate");
+                p->landed.push_back(a);
+                check_cuda(cudaEventCreateWithFlags(&b, cudaEventDisableTiming), "cudaEventCreate");
+                p->ready.push_back(b);
+            }
+            if (!f64) {
+                p->stageIn.allocate(sizeof(double) * inPer * members);
+                p->stageOut.allocate(sizeof(double) * outPer * members);
+            }
+        }
+        const auto* src = reinterpret_cast<const double*>(in);
+        auto* dst = reinterpret_cast<double*>(out);
+        // The previous call's downloads have finished (it synchronised), so
+        // the staging buffers are free; the compute stream orders after them.
+        for (std::uint64_t m = 0; m < members; ++m) {
+            void* upTarget = f64 ? static_cast<void*>(p->in.get<double>() + m * inPer)
+                                 : static_cast<void*>(p->stageIn.get<double>() + m * inPer);
+            copy_in(upTarget, src + m * inPer, sizeof(double) * inPer, p->copyIn);
+            check_cuda(cudaEventRecord(p->landed[m], p->copyIn), "cudaEventRecord");
+        }
+        for (std::uint64_t m = 0; m < members; ++m) {
+            check_cuda(cudaStreamWaitEvent(p->stream, p->landed[m], 0), "cudaStreamWaitEvent");
+            unsigned char* dIn = p->in.get<unsigned char>() + es * m * inPer;
+            unsigned char* dOut = p->out.get<unsigned char>() + es * m * outPer;
+            if (!f64)
+                check_cuda(launch_convert_f64_to_f32(p->stageIn.get<double>() + m * inPer, reinterpret_cast<float*>(dIn),
+                                                     static_cast<long long>(inPer), p->stream),
+                           "convert kernel");
+            f.execute(dIn, dOut, p->stream, 1);
+            if (!f64)
+                check_cuda(launch_convert_f32_to_f64(reinterpret_cast<const float*>(dOut),
+                                                     p->stageOut.get<double>() + m * outPer,
+                                                     static_cast<long long>(outPer), p->stream),
+                           "convert kernel");
+            check_cuda(cudaEventRecord(p->ready[m], p->stream), "cudaEventRecord");
+        }
+        for (std::uint64_t m = 0; m < members; ++m) {
+            check_cuda(cudaStreamWaitEvent(p->copyOut, p->ready[m], 0), "cudaStreamWaitEvent");
+            const void* downSource = f64 ? static_cast<const void*>(p->out.get<double>() + m * outPer)
+                                         : static_cast<const void*>(p->stageOut.get<double>() + m * outPer);
+            copy_out(dst + m * outPer, downSource, sizeof(double) * outPer, p->copyOut);
+        }
+        sync(p->copyOut);
         sync(p->stream);
         f.check_device_errors();
     });
