@@ -12,6 +12,8 @@
 // and conjugated where the mode stores its partner, into the view.
 
 #include "columns_warp.hpp"
+
+#include <algorithm>
 #include "async_copy.cuh"
 #include "fft_device.cuh"
 
@@ -466,6 +468,104 @@ __global__ void __launch_bounds__(256, 3) columns_forward_band_kernel(int nz, in
     }
 }
 
+// Persistent forms of the two direct band kernels: two CTAs per SM walk the
+// (kx, slot, z-chunk) tiles in the launch order of the kernels above, and each
+// thread issues the next tile's sixteen loads before running the current
+// tile's three passes, so the next tile's HBM reads overlap this tile's
+// shared-memory passes and stores.  Tile t is (kx, slot, z-chunk) =
+// (t / (zChunks * slots), (t % (zChunks * slots)) / zChunks, t % zChunks).
+template <int SIGN>
+__global__ void __launch_bounds__(256, 2) columns_band_persist_kernel(int nz, int zStride, int slots, int columns,
+                                                                       DenseBins bins, const int* __restrict__ bandOf,
+                                                                       float scale, const float2* __restrict__ tw) {
+    // SIGN = +1: inverse (read the band, write every row);
+    // SIGN = -1: forward (read every row, write the band, times scale).
+    constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int b = tid & 7;
+    const int zChunks = (nz + B - 1) / B;
+    const long long perColumn = static_cast<long long>(zChunks) * slots;
+    const long long tiles = perColumn * columns;
+    const long long rowStride = bins.planes * bins.kxStride;
+    struct Tile {
+        int kx, z0, band;
+        float2* col;
+    };
+    auto tile_at = [&](long long t) {
+        Tile T;
+        T.kx = static_cast<int>(t / perColumn);
+        const int x = static_cast<int>(t - T.kx * perColumn);
+        const int f = x / zChunks;
+        T.z0 = (x - f * zChunks) * B;
+        T.band = __ldg(bandOf + T.kx);
+        T.col = static_cast<float2*>(bins.data) + static_cast<long long>(f) * zStride + T.z0 + b + bins.planes * T.kx;
+        return T;
+    };
+    auto load = [&](const Tile& T, float2 (&v)[2][8]) {
+        const bool inRange = T.z0 + b < nz;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = pass1_butterfly(tid, q);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int ky = j + 64 * r;
+                const bool have = inRange && (SIGN < 0 || in_band(ky, N, T.band));
+                v[q][r] = have ? T.col[rowStride * ky] : make_float2(0.f, 0.f);
+            }
+        }
+    };
+    long long t = blockIdx.x;
+    if (t >= tiles) return;  // whole CTA; no barrier has been reached
+    Tile cur = tile_at(t);
+    float2 v[2][8];
+    load(cur, v);
+    for (; t < tiles; t += gridDim.x) {
+        // Pass 1 of this tile from registers.
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = pass1_butterfly(tid, q);
+            dft8<SIGN>(v[q]);
+            float2* o = xs + b * XP + 8 * j + (j >> 1);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) o[r] = v[q][r];
+        }
+        // The next tile's loads, in flight during passes 2 and 3.
+        const long long tn = t + gridDim.x;
+        Tile next = cur;
+        if (tn < tiles) {
+            next = tile_at(tn);
+            load(next, v);
+        }
+        __syncthreads();
+        if (cur.z0 + warp < nz) direct_middle_pass<SIGN>(xs, tw, warp, lane);  // planes beyond Nz stay idle
+        __syncthreads();
+        if (cur.z0 + b < nz) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int j = (tid >> 3) + 32 * q;
+                float2 w[8];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) w[r] = xs[b * XP + j + (j >> 4) + 68 * r];
+#pragma unroll
+                for (int r = 1; r < 8; ++r) w[r] = cmul(w[r], twiddle<SIGN>(tw, j * r));
+                dft8<SIGN>(w);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const int ky = j + 64 * r;
+                    if (SIGN > 0)
+                        cur.col[rowStride * ky] = w[r];
+                    else if (in_band(ky, N, cur.band))
+                        cur.col[rowStride * ky] = make_float2(scale * w[r].x, scale * w[r].y);
+                }
+            }
+        }
+        __syncthreads();  // this tile's reads of xs precede the next tile's pass 1
+        cur = next;
+    }
+}
+
 // Generic-N band forms (warp per plane, cp.async staging).
 template <int N, int B>
 __global__ void __launch_bounds__(32 * B, 4) columns_inverse_band_warp_kernel(int nz, int zStride, DenseBins bins,
@@ -548,13 +648,41 @@ __global__ void __launch_bounds__(32 * B, 4) columns_forward_band_warp_kernel(in
     }
 }
 
+template <int SIGN>
+cudaError_t launch_band_persist(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band,
+                                float scale, const void* tw, cudaStream_t s) {
+    auto kernel = columns_band_persist_kernel<SIGN>;
+    cudaError_t err = prepare(kernel, kDirectSmem);
+    if (err != cudaSuccess) return err;
+    static int cachedDevice = -1, cachedBlocks = 0;
+    int device = 0;
+    err = cudaGetDevice(&device);
+    if (err != cudaSuccess) return err;
+    if (device != cachedDevice) {
+        int perSm = 0, sms = 0;
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, 256, kDirectSmem);
+        if (err != cudaSuccess) return err;
+        err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (err != cudaSuccess) return err;
+        cachedBlocks = std::max(1, perSm) * std::max(1, sms);
+        cachedDevice = device;
+    }
+    const long long tiles = static_cast<long long>((nz + 7) / 8) * slots * columns;
+    const int blocks = static_cast<int>(std::min<long long>(tiles, cachedBlocks));
+    kernel<<<blocks, 256, kDirectSmem, s>>>(nz, zStride, slots, columns, bins, band, scale,
+                                            static_cast<const float2*>(tw));
+    return cudaGetLastError();
+}
+
 template <int N>
 cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, const void* tw,
-                           bool warpForm, cudaStream_t s) {
+                           int form, cudaStream_t s) {
     constexpr int B = 8;
     const int zChunks = (nz + B - 1) / B;
     const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
-    if (N == kDirectN && !warpForm) {
+    if (N == kDirectN && form == kBandPersist)
+        return launch_band_persist<+1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
+    if (N == kDirectN && form != kBandWarp) {
         cudaError_t err = prepare(columns_inverse_band_kernel, kDirectSmem);
         if (err != cudaSuccess) return err;
         columns_inverse_band_kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band,
@@ -571,11 +699,13 @@ cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBin
 
 template <int N>
 cudaError_t forward_band_n(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, double scale,
-                           const void* tw, bool warpForm, cudaStream_t s) {
+                           const void* tw, int form, cudaStream_t s) {
     constexpr int B = 8;
     const int zChunks = (nz + B - 1) / B;
     const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
-    if (N == kDirectN && !warpForm) {
+    if (N == kDirectN && form == kBandPersist)
+        return launch_band_persist<-1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
+    if (N == kDirectN && form != kBandWarp) {
         cudaError_t err = prepare(columns_forward_band_kernel, kDirectSmem);
         if (err != cudaSuccess) return err;
         columns_forward_band_kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band, float(scale),
@@ -640,28 +770,26 @@ namespace skb {
 
 cudaError_t launch_columns_inverse_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
                                         const int* band, const void* tw, int form, cudaStream_t s) {
-    const bool w = form == kBandWarp;
     if (slots <= 0 || columns <= 0) return cudaSuccess;
     switch (ny) {
-        case 32: return inverse_band_n<32>(nz, zStride, slots, columns, bins, band, tw, w, s);
-        case 64: return inverse_band_n<64>(nz, zStride, slots, columns, bins, band, tw, w, s);
-        case 128: return inverse_band_n<128>(nz, zStride, slots, columns, bins, band, tw, w, s);
-        case 256: return inverse_band_n<256>(nz, zStride, slots, columns, bins, band, tw, w, s);
-        case 512: return inverse_band_n<512>(nz, zStride, slots, columns, bins, band, tw, w, s);
+        case 32: return inverse_band_n<32>(nz, zStride, slots, columns, bins, band, tw, form, s);
+        case 64: return inverse_band_n<64>(nz, zStride, slots, columns, bins, band, tw, form, s);
+        case 128: return inverse_band_n<128>(nz, zStride, slots, columns, bins, band, tw, form, s);
+        case 256: return inverse_band_n<256>(nz, zStride, slots, columns, bins, band, tw, form, s);
+        case 512: return inverse_band_n<512>(nz, zStride, slots, columns, bins, band, tw, form, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_columns_forward_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
                                         const int* band, double scale, const void* tw, int form, cudaStream_t s) {
-    const bool w = form == kBandWarp;
     if (slots <= 0 || columns <= 0) return cudaSuccess;
     switch (ny) {
-        case 32: return forward_band_n<32>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
-        case 64: return forward_band_n<64>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
-        case 128: return forward_band_n<128>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
-        case 256: return forward_band_n<256>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
-        case 512: return forward_band_n<512>(nz, zStride, slots, columns, bins, band, scale, tw, w, s);
+        case 32: return forward_band_n<32>(nz, zStride, slots, columns, bins, band, scale, tw, form, s);
+        case 64: return forward_band_n<64>(nz, zStride, slots, columns, bins, band, scale, tw, form, s);
+        case 128: return forward_band_n<128>(nz, zStride, slots, columns, bins, band, scale, tw, form, s);
+        case 256: return forward_band_n<256>(nz, zStride, slots, columns, bins, band, scale, tw, form, s);
+        case 512: return forward_band_n<512>(nz, zStride, slots, columns, bins, band, scale, tw, form, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -107,7 +107,8 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
 // Tuned launch shapes of the fused path (autotune.hpp):
 //   work-unit size (M-tiles per unit) of each tensor-core GEMM, 4 / 8 / 16 / 32;
 //   z-planes (warps) per CTA of the fused row kernel, 4 / 8 / 16;
-//   kernel form of each 512-point band column stage, direct / warp-per-plane.
+//   kernel form of each 512-point band column stage, direct / warp-per-plane /
+//   persistent direct.
 // With buffers, missing choices are measured on them (tune_pick); without,
 // only cached choices are applied.  Returns the choices in force.
 std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* modalOut, cudaStream_t s,
@@ -169,7 +170,7 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
     if (cfg_.n == 512) {
         // Both forms run in place on the bin arrays; repeated runs leave values
         // the final execution below overwrites.
-        const std::vector<int> forms{kBandDefault, kBandWarp};
+        const std::vector<int> forms{kBandDefault, kBandWarp, kBandPersist};
         pick("flux.columns_band.form inverse" + shape + dev, forms,
              [&](int c) { horizontal_->set_band_forms(c, horizontal_->band_form_forward()); },
              [&] { horizontal_->inverse_columns_band(binsIn, static_cast<int>(M * fieldsIn_), static_cast<int>(zStride_), s); });

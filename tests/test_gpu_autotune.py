@@ -77,9 +77,10 @@ def test_every_unit_size_is_correct(tiles):
     skb_cuda.tune_cache_clear()
 
 
-@pytest.mark.parametrize("form", [0, 1])
+@pytest.mark.parametrize("form", [0, 1, 2])
 def test_band_forms_at_512(form):
-    """Both 512-point band-column kernel forms (direct, warp-per-plane) the
+    """Every 512-point band-column kernel form (direct, warp-per-plane,
+    persistent direct) the
     tuner chooses between give the split flux within 1e-6 of FP64."""
     skb_cuda.tune_cache_clear()
     n, nz, members = 512, 9, 1
