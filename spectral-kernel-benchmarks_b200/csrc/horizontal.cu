@@ -42,8 +42,12 @@ __global__ void __launch_bounds__(cta_threads<T, M>()) rows_forward_kernel(
     const int y = blockIdx.y;
     constexpr int NX = 2 * M;
     constexpr int LD = B + 1;  // padded so the walk along x below is conflict-free
-    // Consecutive threads take consecutive x-pairs of one row: full-line loads.
-    for (int idx = tid; idx < M * B; idx += NT) {
+    // Consecutive threads take consecutive x-pairs of one row: full-line loads,
+    // all of a thread's loads issued before the first shared store.
+    static_assert((M * B) % NT == 0, "whole load rounds");
+#pragma unroll
+    for (int it = 0; it < (M * B) / NT; ++it) {
+        const int idx = tid + it * NT;
         const int m = idx % M;
         const int b = idx / M;
         const long long p = p0 + b;
@@ -106,7 +110,12 @@ __global__ void __launch_bounds__(cta_threads<T, M>()) rows_inverse_kernel(
     };
     // Pairs (k, M-k) for k in [0, M/2]; k = 0 pairs with the Nyquist bin M.
     constexpr int pairs = M / 2 + 1;
-    for (int idx = tid; idx < pairs * B; idx += NT) {
+    // FP64 issues all of a thread's loads first; FP32 measured faster rolled.
+    constexpr int kUnroll = sizeof(T) == 8 ? (pairs * B + NT - 1) / NT : 1;
+#pragma unroll kUnroll
+    for (int it = 0; it < (pairs * B + NT - 1) / NT; ++it) {
+        const int idx = tid + it * NT;
+        if (idx >= pairs * B) break;
         const int b = idx % B;
         const int k = idx / B;
         if (k == 0) {
@@ -134,7 +143,9 @@ __global__ void __launch_bounds__(cta_threads<T, M>()) rows_inverse_kernel(
     __syncthreads();
     fft_smem<T, M, B, +1, LD>(data, twHalf, tid, true);
     // Consecutive threads write consecutive x-pairs of one row.
-    for (int idx = tid; idx < M * B; idx += NT) {
+#pragma unroll
+    for (int it = 0; it < (M * B) / NT; ++it) {
+        const int idx = tid + it * NT;
         const int m = idx % M;
         const int b = idx / M;
         const long long p = p0 + b;
@@ -198,7 +209,10 @@ __global__ void __launch_bounds__(cta_threads<T, N>()) columns_dense_kernel(long
     const long long p0 = (long long)blockIdx.x * B;
     const long long kx = blockIdx.y;
     const V* src = reinterpret_cast<const V*>(in.data);
-    for (int idx = tid; idx < N * B; idx += NT) {
+    static_assert((N * B) % NT == 0, "whole load rounds");
+#pragma unroll
+    for (int it = 0; it < (N * B) / NT; ++it) {
+        const int idx = tid + it * NT;
         const int b = idx % B;
         const int ky = idx / B;
         const long long p = p0 + b;
@@ -209,7 +223,9 @@ __global__ void __launch_bounds__(cta_threads<T, N>()) columns_dense_kernel(long
     __syncthreads();
     fft_smem<T, N, B, SIGN>(data, tw, tid, true);
     V* dst = reinterpret_cast<V*>(out.data);
-    for (int idx = tid; idx < N * B; idx += NT) {
+#pragma unroll
+    for (int it = 0; it < (N * B) / NT; ++it) {
+        const int idx = tid + it * NT;
         const int b = idx % B;
         const int ky = idx / B;
         const long long p = p0 + b;
@@ -235,7 +251,12 @@ __global__ void __launch_bounds__(cta_threads<T, N>()) columns_embed_kernel(int 
     const int kx = blockIdx.y;
     const FieldView view = views.v[f];
     const int* map = tables.cellMap + (long long)kx * N;
-    for (int idx = tid; idx < N * B; idx += NT) {
+    static_assert((N * B) % NT == 0, "whole load rounds");
+    // FP64 issues all of a thread's loads first; FP32 measured faster rolled.
+    constexpr int kUnroll = sizeof(T) == 8 ? (N * B) / NT : 1;
+#pragma unroll kUnroll
+    for (int it = 0; it < (N * B) / NT; ++it) {
+        const int idx = tid + it * NT;
         const int b = idx % B;
         const int ky = idx / B;
         const int z = z0 + b;
@@ -251,7 +272,9 @@ __global__ void __launch_bounds__(cta_threads<T, N>()) columns_embed_kernel(int 
     fft_smem<T, N, B, +1>(data, tw, tid, true);
     V* dst = reinterpret_cast<V*>(out.data);
     const long long pBase = (long long)f * nz;
-    for (int idx = tid; idx < N * B; idx += NT) {
+#pragma unroll
+    for (int it = 0; it < (N * B) / NT; ++it) {
+        const int idx = tid + it * NT;
         const int b = idx % B;
         const int ky = idx / B;
         const int z = z0 + b;
@@ -276,7 +299,10 @@ __global__ void __launch_bounds__(cta_threads<T, N>()) columns_gather_kernel(int
     const int kx = blockIdx.y;
     const V* src = reinterpret_cast<const V*>(in.data);
     const long long pBase = (long long)f * nz;
-    for (int idx = tid; idx < N * B; idx += NT) {
+    static_assert((N * B) % NT == 0, "whole load rounds");
+#pragma unroll
+    for (int it = 0; it < (N * B) / NT; ++it) {
+        const int idx = tid + it * NT;
         const int b = idx % B;
         const int ky = idx / B;
         const int z = z0 + b;
