@@ -341,6 +341,24 @@ typedef struct skb_flux_options {
 
 typedef struct skb_flux skb_flux;
 SKB_API int skb_flux_create(const skb_flux_options* options, skb_flux** out);
+/* The authoritative WVM form (runAuthoritativeProductionLifetimeFluxBenchmark,
+ * src/authoritative_spectral_flux.cpp:1409-1571; loadPreparedSpectralFluxFixture,
+ * src/spectral_flux_fixture.cpp:150-411): the same 15 -> 4 composition with
+ * the vertical operators of two families (wave-f = 0, wave-g = 1) given by the
+ * caller over explicit operator groups (contiguous runs of the retained modes
+ * in retainedHorizontalModes order; one matrix per group and family, groups
+ * may share a K^2 key), each input slot and target using its family's
+ * matrices.  options->family is ignored; targets must be 4. */
+typedef struct skb_flux_families {
+    uint64_t groups;              /* operator groups */
+    const uint64_t* group_modes;  /* modes in each group, in order; sum = retained modes */
+    const double* forward[2];     /* family f: [group][j][z], groups*Nj*Nz doubles */
+    const double* inverse[2];     /* family f: [group][z][j] */
+    uint32_t input_family[15];    /* family of each input slot */
+    uint32_t target_family[4];    /* family of each target */
+} skb_flux_families;
+SKB_API int skb_flux_create_families(const skb_flux_options* options, const skb_flux_families* families,
+                                     skb_flux** out);
 SKB_API int skb_flux_destroy(skb_flux* p);
 SKB_API int skb_flux_info(const skb_flux* p, skb_provider_info* info);
 /* Sizes in complex elements for all members. */

@@ -249,13 +249,31 @@ def pointwise(volume, scale, shared, derivative, workers=1):
     return out
 
 
-def flux(n, nz, modal_in, targets=4, family=None, modes=None, workers=1):
+def family_vertical(families, direction, data, fields, rows_in, rows_out, field_family):
+    """Per operator group and field, the field's family matrix (the
+    authoritative WVM form: VerticalGemmProvider calls partitioned by family,
+    authoritative_spectral_flux.cpp:1409-1571).  families: 'group_modes',
+    'forward' / 'inverse' per family [group][j][z] / [group][z][j]."""
+    counts = np.asarray(families["group_modes"], np.int64)
+    first = np.r_[0, np.cumsum(counts)[:-1]]
+    H = int(counts.sum())
+    mats = families["forward" if direction == "forward" else "inverse"]
+    x = np.asarray(data, dtype=np.complex128).reshape(H, fields, rows_in)
+    out = np.empty((H, fields, rows_out), np.complex128)
+    for g, (f0, c) in enumerate(zip(first, counts)):
+        for f in range(fields):
+            out[f0:f0 + c, f] = x[f0:f0 + c, f] @ np.asarray(mats[field_family[f]][g]).T
+    return out.reshape(-1)
+
+
+def flux(n, nz, modal_in, targets=4, family=None, modes=None, workers=1, families=None):
     """The 15 -> 4 streamed flux of runProductionLifetimeFluxBenchmark
     (benchmark.cpp:4182-4241 oracle order, 4405-4424 executeAll): inverse
     vertical GEMM of all input fields, inverse horizontal of [U,V,W] once, then per
     target the inverse of its derivative triple, pointwise advection with
     scale 1/(Nx*Ny)^2, forward horizontal + retention, and finally the forward
-    vertical GEMM of the targets.  ``targets`` = 3 gives the 12 -> 3 variant.
+    vertical GEMM of the targets.  ``targets`` = 3 gives the 12 -> 3 variant;
+    ``families`` (see family_vertical) gives the authoritative two-family form.
     Returns modal [mode][target][j]."""
     fields_in = 3 + 3 * targets
     w_in = Workload(n, n, nz, fields_in)
@@ -263,9 +281,13 @@ def flux(n, nz, modal_in, targets=4, family=None, modes=None, workers=1):
     w3 = Workload(n, n, nz, 3)
     w1 = Workload(n, n, nz, 1)
     modes = modes or retained_modes(n, n)
-    family = family or k2_family(w_out)
     H = len(modes)
-    phys = grouped_vertical(w_in, family, "inverse", modal_in).reshape(H, fields_in, nz)
+    if families is not None:
+        phys = family_vertical(families, "inverse", modal_in, fields_in, w_in.nj, nz,
+                               families["input_family"]).reshape(H, fields_in, nz)
+    else:
+        family = family or k2_family(w_out)
+        phys = grouped_vertical(w_in, family, "inverse", modal_in).reshape(H, fields_in, nz)
     scale = 1.0 / float((n * n) ** 2)
     shared = fft_c2r(w3, embed_retained(w3, modes, phys[:, 0:3, :].reshape(-1)), workers)
     phys_out = np.empty((H, targets, nz), np.complex128)
@@ -274,6 +296,9 @@ def flux(n, nz, modal_in, targets=4, family=None, modes=None, workers=1):
         deriv = fft_c2r(w3, embed_retained(w3, modes, trip), workers)
         target = pointwise(n * n * nz, scale, shared, deriv, workers)
         phys_out[:, t, :] = gather_retained(w1, modes, fft_r2c(w1, target, workers)).reshape(H, nz)
+    if families is not None:
+        return family_vertical(families, "forward", phys_out.reshape(-1), targets, nz, w_out.nj,
+                               families["target_family"])
     return grouped_vertical(w_out, family, "forward", phys_out.reshape(-1))
 
 

@@ -1565,6 +1565,42 @@ int skb_flux_create(const skb_flux_options* o, skb_flux** out) {
     });
 }
 
+int skb_flux_create_families(const skb_flux_options* o, const skb_flux_families* fam, skb_flux** out) {
+    return guard([&] {
+        require(o != nullptr && fam != nullptr && out != nullptr, "options, families and handle must be non-null");
+        require(o->mode >= SKB_FLUX_FP64_PLAIN && o->mode <= SKB_FLUX_SPLIT_BF16X3, "unknown flux mode");
+        require(o->targets == 4, "operator families are defined for the 15 -> 4 flux");
+        require(fam->groups > 0 && fam->group_modes != nullptr, "families need their operator groups");
+        const uint64_t nj = o->nz < 2 ? 0 : 2 * (o->nz - 1) / 3;
+        auto F = std::make_shared<FluxFamilies>();
+        std::uint64_t first = 0;
+        for (uint64_t g = 0; g < fam->groups; ++g) {
+            require(fam->group_modes[g] > 0, "operator groups must be nonempty");
+            F->groups.push_back({0, first, fam->group_modes[g]});
+            first += fam->group_modes[g];
+        }
+        const size_t matrix = static_cast<size_t>(fam->groups * nj * o->nz);
+        for (int f = 0; f < 2; ++f) {
+            require(fam->forward[f] != nullptr && fam->inverse[f] != nullptr, "both families need both directions");
+            F->forward[f].assign(fam->forward[f], fam->forward[f] + matrix);
+            F->inverse[f].assign(fam->inverse[f], fam->inverse[f] + matrix);
+        }
+        F->inputFamily.assign(fam->input_family, fam->input_family + 15);
+        F->targetFamily.assign(fam->target_family, fam->target_family + 4);
+        FluxConfig cfg;
+        cfg.n = o->n;
+        cfg.nz = o->nz;
+        cfg.targets = o->targets;
+        cfg.members = o->members;
+        cfg.mode = static_cast<FluxMode>(o->mode);
+        cfg.families = std::move(F);
+        auto p = std::make_unique<skb_flux>();
+        p->pipeline = std::make_unique<FluxPipeline>(cfg);
+        p->stream = make_stream();
+        *out = p.release();
+    });
+}
+
 int skb_flux_destroy(skb_flux* p) {
     return guard([&] { delete p; });
 }

@@ -22,13 +22,37 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
     wOut_ = Workload{cfg.n, cfg.n, cfg.nz, cfg.targets, 1.0, 1.0, true};
     fieldsIn_ = 3 + 3 * cfg.targets;
     const auto modes = retained_modes(wOut_);
-    const auto groups = squared_wavenumber_groups(modes);
     modes_ = modes.size();
     nj_ = wOut_.nj();
     volume_ = cfg.n * cfg.n * cfg.nz;
-    VerticalFamily fam = cfg.family == 2 ? sturm_liouville_family(wOut_, groups, cfg.familySeed)
-                                         : k2_rotation_family(wOut_, groups);
-    familyId = fam.id;
+    families_ = cfg.families != nullptr;
+    const auto groups = families_ ? cfg.families->groups : squared_wavenumber_groups(modes);
+    VerticalFamily fam;
+    if (families_) {
+        const FluxFamilies& F = *cfg.families;
+        if (cfg.targets != 4) throw Error(-1, "operator families are defined for the 15 -> 4 flux");
+        std::uint64_t next = 0;
+        for (const auto& g : groups) {
+            if (g.first != next || g.count == 0) throw Error(-1, "operator groups must be contiguous runs of modes");
+            next += g.count;
+        }
+        if (next != modes_) throw Error(-1, "operator groups must cover every retained mode");
+        const std::uint64_t matrix = groups.size() * nj_ * cfg.nz;
+        for (int f = 0; f < 2; ++f)
+            if (F.forward[f].size() != matrix || F.inverse[f].size() != matrix)
+                throw Error(-1, "operator family matrices must be groups x Nj x Nz");
+        if (F.inputFamily.size() != fieldsIn_ || F.targetFamily.size() != cfg.targets)
+            throw Error(-1, "the family map needs one entry per input slot and per target");
+        for (const int v : F.inputFamily)
+            if (v != 0 && v != 1) throw Error(-1, "family indices must be 0 (wave-f) or 1 (wave-g)");
+        for (const int v : F.targetFamily)
+            if (v != 0 && v != 1) throw Error(-1, "family indices must be 0 (wave-f) or 1 (wave-g)");
+        familyId = "external wave-f + wave-g operator families";
+    } else {
+        fam = cfg.family == 2 ? sturm_liouville_family(wOut_, groups, cfg.familySeed)
+                              : k2_rotation_family(wOut_, groups);
+        familyId = fam.id;
+    }
     planningSeconds = seconds_since(planStart);
 
     const auto allocStart = Clock::now();
@@ -51,10 +75,44 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
                             std::to_string(freeBytes) + " are free");
     horizontal_ = std::make_unique<HorizontalPlan>(Workload{cfg.n, cfg.n, cfg.nz, 3, 1.0, 1.0, true}, hp, true,
                                                    maxPlanes);
-    inverseGemm_ = std::make_unique<VerticalPlan>(gp, static_cast<int>(cfg.nz), static_cast<int>(nj_), groups,
-                                                  fieldsIn_, cfg.members, fam.inverse);
-    forwardGemm_ = std::make_unique<VerticalPlan>(gp, static_cast<int>(nj_), static_cast<int>(cfg.nz), groups,
-                                                  cfg.targets, cfg.members, fam.forward);
+    if (!families_) {
+        inverseGemm_ = std::make_unique<VerticalPlan>(gp, static_cast<int>(cfg.nz), static_cast<int>(nj_), groups,
+                                                      fieldsIn_, cfg.members, fam.inverse);
+        forwardGemm_ = std::make_unique<VerticalPlan>(gp, static_cast<int>(nj_), static_cast<int>(cfg.nz), groups,
+                                                      cfg.targets, cfg.members, fam.forward);
+    } else {
+        const FluxFamilies& F = *cfg.families;
+        for (int f = 0; f < 2; ++f) {
+            std::vector<int> in, out;
+            for (std::uint64_t i = 0; i < fieldsIn_; ++i)
+                if (F.inputFamily[i] == f) in.push_back(static_cast<int>(i));
+            for (std::uint64_t t = 0; t < cfg.targets; ++t)
+                if (F.targetFamily[t] == f) out.push_back(static_cast<int>(t));
+            if (!in.empty()) {
+                inverseFamily_[f].plan = std::make_unique<VerticalPlan>(
+                    gp, static_cast<int>(cfg.nz), static_cast<int>(nj_), groups, in.size(), cfg.members, F.inverse[f]);
+                inverseFamily_[f].fieldMap = upload_vector(in);
+                inverseFamily_[f].fields = static_cast<int>(in.size());
+            }
+            if (!out.empty()) {
+                forwardFamily_[f].plan = std::make_unique<VerticalPlan>(
+                    gp, static_cast<int>(nj_), static_cast<int>(cfg.nz), groups, out.size(), cfg.members, F.forward[f]);
+                forwardFamily_[f].fieldMap = upload_vector(out);
+                forwardFamily_[f].fields = static_cast<int>(out.size());
+            }
+        }
+        std::vector<long long> mi(modes_), mo(modes_), pi(modes_), po(modes_);
+        for (std::uint64_t m = 0; m < modes_; ++m) {
+            mi[m] = static_cast<long long>(m * fieldsIn_ * nj_);
+            mo[m] = static_cast<long long>(m * cfg.targets * nj_);
+            pi[m] = static_cast<long long>(m * fieldsIn_ * cfg.nz);
+            po[m] = static_cast<long long>(m * cfg.targets * cfg.nz);
+        }
+        cellModalIn_ = upload_vector(mi);
+        cellModalOut_ = upload_vector(mo);
+        cellPhysIn_ = upload_vector(pi);
+        cellPhysOut_ = upload_vector(po);
+    }
     dense_ = fused_ && horizontal_->band_exact();
     if (!dense_) {
         physIn_.allocate(2 * es * cfg.members * modes_ * fieldsIn_ * cfg.nz);
@@ -95,12 +153,15 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
     }
     allocationSeconds = seconds_since(allocStart) + horizontal_->allocationSeconds;
     planningSeconds += horizontal_->planningSeconds;
-    persistentBytes = horizontal_->persistentBytes + inverseGemm_->persistentBytes() + forwardGemm_->persistentBytes();
+    persistentBytes = horizontal_->persistentBytes + cellModalIn_.bytes() + cellModalOut_.bytes() +
+                      cellPhysIn_.bytes() + cellPhysOut_.bytes();
+    for (const VerticalPlan* g : gemm_plans()) persistentBytes += g->persistentBytes();
     scratchBytes = horizontal_->scratchBytes + physIn_.bytes() + physOut_.bytes() + shared_.bytes() +
                    deriv_.bytes() + target_.bytes() + binsIn_.bytes() + binsOut_.bytes();
     // Staged: 2 GEMMs, 2 launches per inverse / forward horizontal, members pointwise per target.
-    // Fused: GEMM, embed+columns, fused rows, columns+retention, GEMM.
-    launches_ = fused_ ? 5 : 2 + 2 + cfg.targets * (2 + cfg.members + 2);
+    // Fused: GEMM, embed+columns, fused rows, columns+retention, GEMM.  With
+    // operator families each GEMM is one launch per family.
+    launches_ = (fused_ ? 5 : 2 + 2 + cfg.targets * (2 + cfg.members + 2)) + (families_ ? 2 : 0);
     apply_tuned(nullptr, nullptr, nullptr, nullptr);
 }
 
@@ -158,11 +219,11 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
                " S=" + std::to_string(g.inner()) + " groups=" + std::to_string(g.groups()) + dev;
     };
     const std::vector<int> tileCandidates{4, 8, 16, 32};
-    pick(gemmKey("inverse", *inverseGemm_), tileCandidates, unitTiles(*inverseGemm_), [&] {
+    if (!families_) pick(gemmKey("inverse", *inverseGemm_), tileCandidates, unitTiles(*inverseGemm_), [&] {
         inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {binsIn_.get(), nullptr}, s, M, nullptr,
                               &gemmOut);
     });
-    pick(gemmKey("forward", *forwardGemm_), tileCandidates, unitTiles(*forwardGemm_), [&] {
+    if (!families_) pick(gemmKey("forward", *forwardGemm_), tileCandidates, unitTiles(*forwardGemm_), [&] {
         forwardGemm_->execute({binsOut_.get(), nullptr}, {modalOut, nullptr}, s, M, &gemmIn, nullptr);
     });
     pick("flux.rows.planes_per_cta" + shape + dev, {4, 8, 16}, [&](int c) { rowsPlanes_ = c; },
@@ -296,8 +357,8 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
     auto* physIn = physIn_.get<unsigned char>();
     auto* physOut = physOut_.get<unsigned char>();
     const double binsPlane = n * keep * ces, compactPlane = double(H) * ces;
-    const double gemmIn = double(M) * H * fieldsIn_ * (nj_ + nz) * ces + inverseGemm_->matrixBytes();
-    const double gemmOut = double(M) * H * T * (nj_ + nz) * ces + forwardGemm_->matrixBytes();
+    const double gemmIn = double(M) * H * fieldsIn_ * (nj_ + nz) * ces + matrix_bytes(true);
+    const double gemmOut = double(M) * H * T * (nj_ + nz) * ces + matrix_bytes(false);
     const long long inPlanes = static_cast<long long>(M * fieldsIn_ * nz);
     const long long outPlanes = static_cast<long long>(M * T * nz);
     // Stored planes (stride between kx in the bin arrays) include the z-padding.
@@ -307,14 +368,12 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
     const DenseBins binsOutArr{binsOut_.get(), outStored, keep};
     if (dense_) {
         // GEMM -> retained cells of binsIn -> in-place inverse columns.
-        BinBoundary out{cellIn_.get<long long>(), partnerIn_.get<long long>(), modeConj_.get<unsigned char>(),
-                        static_cast<int>(fieldsIn_), static_cast<int>(zStride_)};
-        inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {binsIn_.get(), nullptr}, s, M, nullptr, &out);
+        gemm_inverse(modalIn, s, M, true);
         if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
         horizontal_->inverse_columns_band(binsIn, static_cast<int>(M * fieldsIn_), static_cast<int>(zStride_), s);
         if (rec) rec->end("columns_inverse_embed", 1, double(inPlanes) * (compactPlane + binsPlane), 0.0);
     } else {
-        inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s, M);
+        gemm_inverse(modalIn, s, M, false);
         if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
         ViewSet inViews{};
         inViews.count = static_cast<int>(M * fieldsIn_);
@@ -334,9 +393,7 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
         // In-place forward columns keep the retained cells; the GEMM reads them there.
         horizontal_->forward_columns_band(binsOutArr, static_cast<int>(M * T), 1.0, static_cast<int>(zStride_), s);
         if (rec) rec->end("columns_forward_gather", 1, double(outPlanes) * (binsPlane + compactPlane), 0.0);
-        BinBoundary in{cellOut_.get<long long>(), nullptr, modeConj_.get<unsigned char>(), static_cast<int>(T),
-                       static_cast<int>(zStride_)};
-        forwardGemm_->execute({binsOut_.get(), nullptr}, {modalOut, nullptr}, s, M, &in, nullptr);
+        gemm_forward(modalOut, s, M, true);
         if (rec) rec->end("gemm_forward_tf32x3", 1, gemmOut, 3.0 * 4.0 * nz * nj_ * double(M) * H * T);
         return;
     }
@@ -348,7 +405,7 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
     horizontal_->forward_columns_from(a.binsOut, outViews, 1.0, s, static_cast<int>(zStride_));
     if (rec) rec->end("columns_forward_gather", 1, double(outPlanes) * (binsPlane + compactPlane), 0.0);
 
-    forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s, M);
+    gemm_forward(modalOut, s, M, false);
     if (rec) rec->end("gemm_forward_tf32x3", 1, gemmOut, 3.0 * 4.0 * nz * nj_ * double(M) * H * T);
 }
 
@@ -366,10 +423,10 @@ void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Reco
     auto* physOut = physOut_.get<unsigned char>();
     // Algorithmic bytes of one plane through each horizontal stage.
     const double binsPlane = n * keep * ces, realPlane = n * n * es, compactPlane = double(H) * ces;
-    const double gemmIn = double(M) * H * fieldsIn_ * (nj_ + nz) * ces + inverseGemm_->matrixBytes();
-    const double gemmOut = double(M) * H * T * (nj_ + nz) * ces + forwardGemm_->matrixBytes();
+    const double gemmIn = double(M) * H * fieldsIn_ * (nj_ + nz) * ces + matrix_bytes(true);
+    const double gemmOut = double(M) * H * T * (nj_ + nz) * ces + matrix_bytes(false);
 
-    inverseGemm_->execute({const_cast<void*>(modalIn), nullptr}, {physIn_.get(), nullptr}, s, M);
+    gemm_inverse(modalIn, s, M, false);
     if (rec) rec->end("gemm_inverse", 1, gemmIn, 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
 
     auto triple = [&](std::uint64_t firstField) {
@@ -411,13 +468,86 @@ void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Reco
         horizontal_->forward_columns(out, 1.0, s);
         if (rec) rec->end("columns_forward_gather", 1, double(M) * nz * (binsPlane + compactPlane), 0.0);
     }
-    forwardGemm_->execute({physOut_.get(), nullptr}, {modalOut, nullptr}, s, M);
+    gemm_forward(modalOut, s, M, false);
     if (rec) rec->end("gemm_forward", 1, gemmOut, 4.0 * nz * nj_ * double(M) * H * T);
 }
 
+std::vector<const VerticalPlan*> FluxPipeline::gemm_plans() const {
+    std::vector<const VerticalPlan*> out;
+    if (inverseGemm_) out.push_back(inverseGemm_.get());
+    if (forwardGemm_) out.push_back(forwardGemm_.get());
+    for (int f = 0; f < 2; ++f) {
+        if (inverseFamily_[f].plan) out.push_back(inverseFamily_[f].plan.get());
+        if (forwardFamily_[f].plan) out.push_back(forwardFamily_[f].plan.get());
+    }
+    return out;
+}
+
+double FluxPipeline::matrix_bytes(bool inverse) const {
+    if (!families_) return static_cast<double>(inverse ? inverseGemm_->matrixBytes() : forwardGemm_->matrixBytes());
+    double bytes = 0.0;
+    for (const auto& f : inverse ? inverseFamily_ : forwardFamily_)
+        if (f.plan) bytes += static_cast<double>(f.plan->matrixBytes());
+    return bytes;
+}
+
+void FluxPipeline::gemm_inverse(const void* modalIn, cudaStream_t s, std::uint64_t M, bool dense) {
+    const ComplexOperand in{const_cast<void*>(modalIn), nullptr};
+    const ComplexOperand out{dense ? binsIn_.get() : physIn_.get(), nullptr};
+    if (!families_) {
+        if (!dense) {
+            inverseGemm_->execute(in, out, s, M);
+            return;
+        }
+        const BinBoundary bins{cellIn_.get<long long>(), partnerIn_.get<long long>(), modeConj_.get<unsigned char>(),
+                               static_cast<int>(fieldsIn_), static_cast<int>(zStride_)};
+        inverseGemm_->execute(in, out, s, M, nullptr, &bins);
+        return;
+    }
+    for (const auto& f : inverseFamily_) {
+        if (!f.plan) continue;
+        const int* map = f.fieldMap.get<int>();
+        const BinBoundary modal{cellModalIn_.get<long long>(), nullptr, nullptr, f.fields, static_cast<int>(nj_),
+                                static_cast<long long>(modes_ * fieldsIn_ * nj_), map};
+        const BinBoundary target =
+            dense ? BinBoundary{cellIn_.get<long long>(), partnerIn_.get<long long>(), modeConj_.get<unsigned char>(),
+                                f.fields, static_cast<int>(zStride_), static_cast<long long>(fieldsIn_ * zStride_), map}
+                  : BinBoundary{cellPhysIn_.get<long long>(), nullptr, nullptr, f.fields, static_cast<int>(cfg_.nz),
+                                static_cast<long long>(modes_ * fieldsIn_ * cfg_.nz), map};
+        f.plan->execute(in, out, s, M, &modal, &target);
+    }
+}
+
+void FluxPipeline::gemm_forward(void* modalOut, cudaStream_t s, std::uint64_t M, bool dense) {
+    const ComplexOperand in{dense ? binsOut_.get() : physOut_.get(), nullptr};
+    const ComplexOperand out{modalOut, nullptr};
+    const std::uint64_t T = cfg_.targets;
+    if (!families_) {
+        if (!dense) {
+            forwardGemm_->execute(in, out, s, M);
+            return;
+        }
+        const BinBoundary bins{cellOut_.get<long long>(), nullptr, modeConj_.get<unsigned char>(), static_cast<int>(T),
+                               static_cast<int>(zStride_)};
+        forwardGemm_->execute(in, out, s, M, &bins, nullptr);
+        return;
+    }
+    for (const auto& f : forwardFamily_) {
+        if (!f.plan) continue;
+        const int* map = f.fieldMap.get<int>();
+        const BinBoundary source =
+            dense ? BinBoundary{cellOut_.get<long long>(), nullptr, modeConj_.get<unsigned char>(), f.fields,
+                                static_cast<int>(zStride_), static_cast<long long>(T * zStride_), map}
+                  : BinBoundary{cellPhysOut_.get<long long>(), nullptr, nullptr, f.fields, static_cast<int>(cfg_.nz),
+                                static_cast<long long>(modes_ * T * cfg_.nz), map};
+        const BinBoundary modal{cellModalOut_.get<long long>(), nullptr, nullptr, f.fields, static_cast<int>(nj_),
+                                static_cast<long long>(modes_ * T * nj_), map};
+        f.plan->execute(in, out, s, M, &source, &modal);
+    }
+}
+
 void FluxPipeline::check_device_errors() const {
-    inverseGemm_->check_device_error();
-    forwardGemm_->check_device_error();
+    for (const VerticalPlan* g : gemm_plans()) g->check_device_error();
 }
 
 void FluxPipeline::capture(const void* modalIn, void* modalOut, cudaStream_t s) {

@@ -12,6 +12,7 @@
 
 #pragma once
 
+#include <array>
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -25,11 +26,24 @@ namespace skb {
 
 enum class FluxMode { fp64_plain = 0, fp32 = 1, split_tf32x3 = 2, split_bf16x3 = 3 };
 
+// Externally supplied vertical operators (the authoritative WVM path,
+// src/authoritative_spectral_flux.cpp and src/spectral_flux_fixture.cpp of
+// the reference): two families (wave-f = 0, wave-g = 1) over explicit operator
+// groups, and the family each input slot and each target uses.
+struct FluxFamilies {
+    std::vector<ModeGroup> groups;               // contiguous runs of the retained modes, in order
+    std::array<std::vector<double>, 2> forward;  // family: [group][j][z]
+    std::array<std::vector<double>, 2> inverse;  // family: [group][z][j]
+    std::vector<int> inputFamily;                // per input slot: 0 or 1
+    std::vector<int> targetFamily;               // per target: 0 or 1
+};
+
 struct FluxConfig {
     std::uint64_t n = 0, nz = 0, targets = 4, members = 1;
     FluxMode mode = FluxMode::fp64_plain;
     int family = 1;  // SKB_FAMILY_K2_ROTATION or SKB_FAMILY_STURM_LIOUVILLE
     std::uint64_t familySeed = 0;
+    std::shared_ptr<const FluxFamilies> families;  // overrides `family` when set
 };
 
 class FluxPipeline {
@@ -101,6 +115,22 @@ private:
     void runFused(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     std::vector<TuneEntry> apply_tuned(const void* modalIn, void* modalOut, cudaStream_t s, double* seconds);
     RowFluxArgs row_args(std::uint64_t members) const;
+    // The vertical GEMMs of both directions: one plan, or with external
+    // families one plan per family over that family's fields.  `dense`:
+    // the bin arrays of the fused path, else the compact physical buffers.
+    void gemm_inverse(const void* modalIn, cudaStream_t s, std::uint64_t members, bool dense);
+    void gemm_forward(void* modalOut, cudaStream_t s, std::uint64_t members, bool dense);
+    struct FamilyPlan {
+        std::unique_ptr<VerticalPlan> plan;
+        DeviceBuffer fieldMap;  // plan field -> input slot or target
+        int fields = 0;
+    };
+    std::vector<const VerticalPlan*> gemm_plans() const;
+    double matrix_bytes(bool inverse) const;
+    bool families_ = false;
+    std::array<FamilyPlan, 2> inverseFamily_, forwardFamily_;
+    // Per mode: element offset of (member 0, field 0) in the compact arrays.
+    DeviceBuffer cellModalIn_, cellModalOut_, cellPhysIn_, cellPhysOut_;
     int rowsPlanes_ = 8;  // z-planes per CTA of the fused row kernel
     void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     cudaGraph_t graph_ = nullptr;

@@ -415,12 +415,22 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
         check_cuda(launch_tc_gemm(a, s), "tensor-core grouped vertical GEMM kernel");
         return;
     }
-    if ((inBins != nullptr || outBins != nullptr) && members_ != 1)
-        throw Error(-3, "bin-array operands of the SIMT GEMM need a single-member plan");
     // SIMT tiles are member-major: the first members' tiles form a prefix.
+    // Cell-addressed operands decompose a tile's global column index into
+    // (member, mode, field) with the plan's columns per member.
     const int tiles = static_cast<int>(static_cast<std::uint64_t>(tiles_) / members_ * members);
     const GroupTiles t{tileGroup_.get<int>(), tileColumn_.get<int>(), tileCount_.get<int>(), tiles};
-    check_cuda(launch_grouped_gemm(p_, R_, S_, matrices_.get(), t, in, out, s, inBins, outBins),
+    BinBoundary ib, ob;
+    if (inBins != nullptr) {
+        ib = *inBins;
+        ib.memberColumns = memberColumns_;
+    }
+    if (outBins != nullptr) {
+        ob = *outBins;
+        ob.memberColumns = memberColumns_;
+    }
+    check_cuda(launch_grouped_gemm(p_, R_, S_, matrices_.get(), t, in, out, s, inBins ? &ib : nullptr,
+                                   outBins ? &ob : nullptr),
                "grouped vertical GEMM kernel");
 }
 

@@ -239,8 +239,11 @@ __device__ __forceinline__ ColumnRef column_ref(const TcGemmArgs& p, const BinBo
     const int c = static_cast<int>(gfirst) + (vc - member * gcols);  // column within the member (< 2^31)
     if (bb.cell == nullptr) return {(static_cast<long long>(member) * p.memberColumns + c) * len, -1, false};
     const int mode = c / bb.fields;
-    const int field = c - mode * bb.fields;
-    const long long off = (static_cast<long long>(member) * bb.fields + field) * bb.zStride;
+    const int sub = c - mode * bb.fields;
+    const int field = bb.fieldMap != nullptr ? __ldg(bb.fieldMap + sub) : sub;
+    const long long memberStride =
+        bb.memberStride != 0 ? bb.memberStride : static_cast<long long>(bb.fields) * bb.zStride;
+    const long long off = member * memberStride + static_cast<long long>(field) * bb.zStride;
     const long long partner = bb.partner != nullptr ? __ldg(bb.partner + mode) : -1;
     const bool conj = bb.conj != nullptr && __ldg(bb.conj + mode) != 0;
     return {__ldg(bb.cell + mode) + off, partner >= 0 ? partner + off : -1, conj};

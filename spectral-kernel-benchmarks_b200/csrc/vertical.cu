@@ -53,9 +53,19 @@ __device__ __forceinline__ void cp_async_wait() {
 // field) in a bin-array operand, with its partner (or -1) and conjugation.
 __device__ __forceinline__ void bin_column(const BinBoundary& bb, int col, long long& base, long long& partner,
                                            bool& conj) {
-    const int mode = col / bb.fields;
-    const int field = col - mode * bb.fields;
-    const long long off = static_cast<long long>(field) * bb.zStride;
+    // Plan column = member * memberColumns + mode * fields + plan field.
+    long long member = 0;
+    int rest = col;
+    if (bb.memberColumns > 0) {
+        member = col / bb.memberColumns;
+        rest = static_cast<int>(col - member * bb.memberColumns);
+    }
+    const int mode = rest / bb.fields;
+    const int sub = rest - mode * bb.fields;
+    const int field = bb.fieldMap != nullptr ? __ldg(bb.fieldMap + sub) : sub;
+    const long long memberStride =
+        bb.memberStride != 0 ? bb.memberStride : static_cast<long long>(bb.fields) * bb.zStride;
+    const long long off = member * memberStride + static_cast<long long>(field) * bb.zStride;
     base = __ldg(bb.cell + mode) + off;
     const long long p = bb.partner != nullptr ? __ldg(bb.partner + mode) : -1;
     partner = p >= 0 ? p + off : -1;

@@ -38,18 +38,23 @@ int gemm_tile_columns(GemmPrecision p);
 // (member, column) list of one group: virtual column v of group g is member
 // v / groupColumns[g], column groupFirst[g] + v % groupColumns[g] of that
 // member, i.e. global complex column member*memberColumns + ...
-// Optional operand in the dense bin array of the fused flux instead of the
-// compact [column][len] layout: complex column (member, mode, field) lives at
-// element cell[mode] + (member * fields + field) * zStride + i (i along Nz).
-// conj[mode] != 0 where the cell holds the conjugate of the retained value;
-// partner[mode] >= 0 (output side) is a second cell, the kx = 0 Hermitian
-// partner, that receives the conjugate of the cell value.
+// Optional cell-addressed operand instead of the compact [column][len] array
+// (the fused flux's dense bin arrays, full WVM-order spectra, or a field
+// subset of a compact array).  Plan column (member, mode, f) lives at element
+//   cell[mode] + member * memberStride + field * zStride + i   (i along the column)
+// with field = fieldMap[f] (f itself without a map) and memberStride =
+// fields * zStride when left 0.  conj[mode] != 0 where the cell holds the
+// conjugate of the value; partner[mode] >= 0 (output side) is a second cell,
+// the kx = 0 Hermitian partner, that receives the conjugate of the value.
 struct BinBoundary {
     const long long* cell = nullptr;  // nullptr: compact operand
     const long long* partner = nullptr;
     const unsigned char* conj = nullptr;
-    int fields = 1;
-    int zStride = 0;
+    int fields = 1;              // plan fields per mode
+    int zStride = 0;             // elements between consecutive stored fields
+    long long memberStride = 0;  // elements between members (0: fields * zStride)
+    const int* fieldMap = nullptr;  // plan field -> stored field (nullptr: identity)
+    long long memberColumns = 0;    // plan columns per member (the SIMT form sets it)
 };
 
 struct TcGemmArgs {

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "direct.hpp"
+#include "fixture.hpp"
 #include "report.hpp"
 #include "skb_cuda.h"
 
@@ -197,7 +198,7 @@ Environment environment() {
 
 struct Options {
     std::string kernel = "fft", profile = "smoke", providers = "cuda", precision = "fp64";
-    std::string gemm = "fp64", family = "k2-grouped", fluxMode = "split-tf32x3", output;
+    std::string gemm = "fp64", family = "k2-grouped", fluxMode = "split-tf32x3", output, fluxFixture;
     std::uint64_t members = 1, targets = 4, warmups = 0, samples = 0, seed = 129;
     bool warmupsSet = false, samplesSet = false, autotune = false;
     std::uint64_t nx = 0, ny = 0, nz = 0, fields = 0;
@@ -1052,6 +1053,101 @@ int flux_mode(const std::string& m) {
     throw std::invalid_argument("flux-mode must be 'fp64-plain', 'fp32' or 'split-tf32x3'.");
 }
 
+// runAuthoritativeProductionLifetimeFluxBenchmark (src/authoritative_spectral_flux.cpp:
+// 1409-1571): the 15 -> 4 flux with the prepared fixture's wave-f / wave-g
+// operators over its floating groups, checked against the fixture's expected
+// modal targets (1e-12 FP64-plain, 1e-6 split).  Loading and reordering stay
+// outside every timed region.
+ProviderRecord run_flux_fixture(const Options& o, const skb_workload& w, Report& report) {
+    const auto modes = retained_modes(w);
+    const auto loadStart = std::chrono::steady_clock::now();
+    const PreparedFixture fx = load_prepared_fixture(o.fluxFixture, modes);
+    const double loadSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - loadStart).count();
+    if (fx.nx != w.nx || fx.ny != w.ny || fx.nz != w.nz)
+        throw std::invalid_argument("Prepared spectral-flux fixture dimensions do not match the selected profile.");
+    const int mode = flux_mode(o.fluxMode);
+    const bool f64 = mode == SKB_FLUX_FP64_PLAIN;
+    skb_flux_options fo{w.nx, w.nz, 4, 1, mode, SKB_FAMILY_K2_ROTATION, 0};
+    skb_flux_families fam{};
+    fam.groups = fx.groupModes.size();
+    fam.group_modes = fx.groupModes.data();
+    for (int f = 0; f < 2; ++f) {
+        fam.forward[f] = fx.forward[f].data();
+        fam.inverse[f] = fx.inverse[f].data();
+    }
+    for (int i = 0; i < 15; ++i) fam.input_family[i] = fx.inputFamily[i];
+    for (int i = 0; i < 4; ++i) fam.target_family[i] = fx.targetFamily[i];
+    skb_flux* h = nullptr;
+    ok(skb_flux_create_families(&fo, &fam, &h));
+    std::unique_ptr<skb_flux, int (*)(skb_flux*)> guard(h, skb_flux_destroy);
+    void* stream = skb_flux_stream(h);
+    std::uint64_t nModes = 0, nj = 0, inN = 0, outN = 0;
+    ok(skb_flux_sizes(h, &nModes, &nj, &inN, &outN));
+    skb_provider_info info{};
+    ok(skb_flux_info(h, &info));
+    ProviderRecord rec;
+    fill_info(rec, info);
+    rec.otherSetupSeconds += loadSeconds;
+    rec.algorithmId = std::string(f64 ? "staged" : "split-TF32x3") +
+                      " flux with wave-f / wave-g operators: one GEMM launch per family and direction";
+    rec.nativeRepresentationId = "modal [mode][field][j] interleaved";
+    rec.modeOrderId = "radial-two-thirds-sorted(radius,k,l); floating K^2 operator groups";
+    rec.planningConfiguration = o.fluxMode + "; fixture " + fx.fixtureId + " (" + fx.fixtureHash + "); " +
+                                std::to_string(fx.groupModes.size()) + " operator groups from " +
+                                std::to_string(fx.sourceGroups) + " fixture groups";
+    rec.gemmCallsPerExecution = 4;
+    rec.forward.nativePlacement = "out-of-place device arrays";
+    rec.forward.adapterPlacement = "out-of-place host arrays";
+    rec.inverse.nativePlacement = rec.inverse.adapterPlacement = "unsupported";
+    rec.inverse.physicalExtents = "the composition exposes one 15-to-4 forward flux boundary only";
+    report.verticalMatrixFamilyId = "wvm-wave-f+wave-g-floating-k2-exact";
+    report.verticalGroupCount = fx.groupModes.size();
+    report.fields = 4;
+
+    const std::uint64_t s = f64 ? 8 : 4;
+    std::vector<double> x(2 * inN);
+    for (std::uint64_t i = 0; i < inN; ++i) {
+        x[2 * i] = fx.modalInputs[i].real();
+        x[2 * i + 1] = fx.modalInputs[i].imag();
+    }
+    DeviceBuffer dIn(inN * 2 * s), dOut(outN * 2 * s);
+    if (f64) dIn.upload(x, stream);
+    else dIn.upload(narrow<float>(x), stream);
+    const std::uint64_t bytes = (inN + outN) * 2 * s;
+    rec.timings.push_back(series("primitive", "authoritative production-lifetime four-target spectral-flux composition",
+                                 "forward", bytes, measure_device(o.warmups, o.samples, stream, [&] {
+                                     ok(skb_flux_execute_device(h, dIn.p, dOut.p, stream));
+                                 })));
+    ok(skb_flux_capture_graph(h, dIn.p, dOut.p));
+    rec.timings.push_back(series("uninstrumented-total",
+                                 "authoritative production-lifetime four-target spectral-flux composition (CUDA graph)",
+                                 "forward", bytes, measure_device(o.warmups, o.samples, stream, [&] {
+                                     ok(skb_flux_replay_graph(h, stream));
+                                 })));
+    std::vector<double> got(2 * outN);
+    rec.timings.push_back(series("adapter-total", "authoritative spectral-flux composition (host arrays)", "forward",
+                                 bytes, measure_host(o.warmups, o.samples, [&] {
+                                     ok(skb_flux_execute(h, reinterpret_cast<const skb_complex*>(x.data()),
+                                                         reinterpret_cast<skb_complex*>(got.data())));
+                                 })));
+    ok(skb_flux_check_device(h));
+    std::vector<cplx> actual(outN), expected(outN);
+    for (std::uint64_t i = 0; i < outN; ++i) {
+        actual[i] = cplx(got[2 * i], got[2 * i + 1]);
+        expected[i] = fx.expectedTargets[i];
+    }
+    const double tol = f64 ? 1e-12 : 1e-6;
+    rec.correctness.push_back(metric("four modal targets versus the fixture's expected outputs",
+                                     max_relative_error(actual.data(), expected.data(), outN),
+                                     relative_l2_error(actual.data(), expected.data(), outN), tol));
+    rec.ledger = {{"fixture load and validation", StageState::setupOnly, "outside every timed region"},
+                  {"vertical inverse", StageState::executed, "one launch per operator family"},
+                  {"vertical forward", StageState::executed, "one launch per operator family"}};
+    (void)nModes;
+    (void)nj;
+    return rec;
+}
+
 // Modal inputs as the reference's production-lifetime fixture draws them:
 // uniform in [-1/8, 1/8], the DC mode's imaginary part zero.
 std::vector<double> flux_inputs(const std::vector<skb_retained_mode>& modes, std::uint64_t fieldsIn, std::uint64_t nj,
@@ -1388,6 +1484,7 @@ void usage(std::ostream& out) {
         << "              [--precision fp64|fp32] [--vertical-gemm-family common|k2-grouped]\n"
         << "              [--vertical-gemm-precision fp64|fp32|tf32x3] [--flux-mode fp64-plain|fp32|split-tf32x3]\n"
         << "              [--members N] [--targets 3|4] [--autotune] [--nx N --ny N --nz N --fields N]\n"
+        << "              [--spectral-flux-fixture PREPARED.bin]\n"
         << "              [--warmups N] [--samples N] [--seed N] [--output PATH]\n"
         << "  skbench-cuda compare --input SAMPLES.csv\n";
 }
@@ -1437,9 +1534,12 @@ int run(int argc, char** argv) {
         } else if (k == "--seed") o.seed = std::stoull(value(argc, argv, i));
         else if (k == "--output") o.output = value(argc, argv, i);
         else if (k == "--autotune") o.autotune = true;
+        else if (k == "--spectral-flux-fixture") o.fluxFixture = value(argc, argv, i);
         else throw std::invalid_argument("Unknown run option: " + std::string(k));
     }
     if (o.kernel == "2d-rfft") o.kernel = "fft";
+    if (!o.fluxFixture.empty() && o.kernel != "production-lifetime-flux")
+        throw std::invalid_argument("--spectral-flux-fixture is valid only for production-lifetime-flux.");
     if (o.providers != "cuda" && o.providers != "both")
         throw std::invalid_argument("providers must be 'cuda' (this build provides no other).");
     const auto prof = profile_named(o.profile);
@@ -1459,6 +1559,7 @@ int run(int argc, char** argv) {
     else if (o.kernel == "pruned-horizontal") rec = run_pruned(o, w, report);
     else if (o.kernel == "vertical-gemm") rec = run_vertical(o, w, report);
     else if (o.kernel == "pointwise-advection") rec = run_pointwise(o, w, report);
+    else if (o.kernel == "production-lifetime-flux" && !o.fluxFixture.empty()) rec = run_flux_fixture(o, w, report);
     else if (o.kernel == "production-lifetime-flux") rec = run_flux(o, w, report);
     else if (o.kernel == "spectral-pipeline") rec = run_pipeline(o, w, report);
     else

@@ -908,13 +908,40 @@ class PointwiseAdvectionExecutor:
 
 # ------------------------------------------------------------------- flux
 
-class Flux:
-    """The composed 15 -> 4 (targets=4) or 12 -> 3 (targets=3) flux."""
+class FluxFamilies(ctypes.Structure):
+    _fields_ = [("groups", ctypes.c_uint64), ("group_modes", ctypes.POINTER(ctypes.c_uint64)),
+                ("forward", ctypes.POINTER(ctypes.c_double) * 2), ("inverse", ctypes.POINTER(ctypes.c_double) * 2),
+                ("input_family", ctypes.c_uint32 * 15), ("target_family", ctypes.c_uint32 * 4)]
 
-    def __init__(self, n, nz, targets=4, members=1, mode=FLUX_FP64_PLAIN, family=FAMILY_K2_ROTATION, family_seed=0):
+
+class Flux:
+    """The composed 15 -> 4 (targets=4) or 12 -> 3 (targets=3) flux.
+
+    `families` (the authoritative WVM form): a dict with 'group_modes' (modes
+    per operator group, retained-mode order), 'forward' / 'inverse' (per family
+    [group][j][z] / [group][z][j]), 'input_family' (15) and 'target_family' (4),
+    e.g. from skb_cuda.fixture.load; `family` is then ignored."""
+
+    def __init__(self, n, nz, targets=4, members=1, mode=FLUX_FP64_PLAIN, family=FAMILY_K2_ROTATION, family_seed=0,
+                 families=None):
         opts = FluxOptions(n, nz, targets, members, mode, family, family_seed)
         h = ctypes.c_void_p()
-        check(library().skb_flux_create(ctypes.byref(opts), ctypes.byref(h)))
+        if families is None:
+            check(library().skb_flux_create(ctypes.byref(opts), ctypes.byref(h)))
+        else:
+            keep = [np.ascontiguousarray(families["group_modes"], dtype=np.uint64)]
+            for name in ("forward", "inverse"):
+                for f in range(2):
+                    keep.append(np.ascontiguousarray(families[name][f], dtype=np.float64))
+            fam = FluxFamilies()
+            fam.groups = len(keep[0])
+            fam.group_modes = keep[0].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+            for f in range(2):
+                fam.forward[f] = keep[1 + f].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+                fam.inverse[f] = keep[3 + f].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            fam.input_family[:] = [int(v) for v in families["input_family"]]
+            fam.target_family[:] = [int(v) for v in families["target_family"]]
+            check(library().skb_flux_create_families(ctypes.byref(opts), ctypes.byref(fam), ctypes.byref(h)))
         self.h = h
         self.n, self.nz, self.targets, self.members, self.mode = n, nz, targets, members, mode
         m, nj, i, o = (ctypes.c_uint64() for _ in range(4))

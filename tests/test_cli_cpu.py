@@ -44,3 +44,14 @@ def test_compare_reads_the_reference_csv():
     lines = out.stdout.strip().splitlines()
     assert lines[0] == "provider\tscope\tstage\tdirection\tmedian_ms\tsamples"
     assert lines[1].split("\t") == ["sample", "primitive", "stage", "forward", "1500.000000", "2"]
+
+
+def test_bad_fixture_exits_2(tmp_path):
+    """The prepared fixture is validated before any device work."""
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"SKFXP002" + bytes(64))
+    out = cli("run", "--kernel", "production-lifetime-flux", "--spectral-flux-fixture", str(bad))
+    assert out.returncode == 2
+    assert "wrong magic" in out.stderr
+    out = cli("run", "--kernel", "fft", "--spectral-flux-fixture", str(bad))
+    assert out.returncode == 2 and "valid only for production-lifetime-flux" in out.stderr

@@ -1,0 +1,92 @@
+"""The prepared spectral-flux fixture format (the authoritative WVM boundary)
+on CPU: loader round trip, the reference's validation rules, and the oracle's
+two-family flux against its one-family form."""
+
+import struct
+
+import numpy as np
+import pytest
+
+import skb_cuda.fixture as fx
+from oracle import oracle as orc
+from synthetic_fixture import families_canonical, make
+
+
+def test_round_trip(tmp_path):
+    path = tmp_path / "f.bin"
+    fam, inputs, expected = make(path, 16, 9)
+    f = fx.load(path)
+    assert (f.nx, f.ny, f.nz, f.nj) == (16, 16, 9, 5)
+    assert np.array_equal(f.group_modes, fam["group_modes"])
+    for d in ("forward", "inverse"):
+        for k in range(2):
+            assert np.array_equal(getattr(f, d)[k], fam[d][k])
+    assert np.array_equal(f.modal_inputs, inputs)
+    assert np.array_equal(f.expected_targets, expected)
+    assert f.input_family == fx.INPUT_FAMILIES and f.target_family == fx.TARGET_FAMILIES
+    assert f.pointwise_scale == 1.0 / 16.0 ** 4
+
+
+def _corrupt(tmp_path, edit):
+    path = tmp_path / "f.bin"
+    make(path, 8, 7)
+    data = bytearray(path.read_bytes())
+    edit(data)
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(bytes(data))
+    return bad
+
+
+@pytest.mark.parametrize("edit,message", [
+    (lambda d: d.__setitem__(slice(0, 8), b"SKFXP002"), "wrong magic"),
+    (lambda d: d.__setitem__(slice(16, 20), struct.pack("<I", 0)), "not authoritative"),
+    (lambda d: d.extend(b"\0"), "trailing bytes"),
+    (lambda d: d.__delitem__(slice(len(d) - 16, len(d))), "truncated"),
+])
+def test_validation_rejects(tmp_path, edit, message):
+    with pytest.raises(fx.FixtureError, match=message):
+        fx.load(_corrupt(tmp_path, edit))
+
+
+def test_validation_rejects_a_wrong_family_map(tmp_path):
+    modes, fam, keys = families_canonical(8, 7, 3)
+    H = len(modes)
+    path = tmp_path / "f.bin"
+    group_of = np.repeat(np.arange(len(fam["group_modes"])), fam["group_modes"].astype(np.int64))
+    inputs = np.zeros((H, 15, 4), complex)
+    wrong = list(fx.INPUT_FAMILIES)
+    wrong[0] = 1
+    fx.write(path, 8, 7, np.stack([modes.k, modes.l], 1), group_of, keys, fam["forward"], fam["inverse"], inputs,
+             np.zeros((H, 4, 4), complex), input_family=wrong)
+    with pytest.raises(fx.FixtureError, match="input field-to-operator map"):
+        fx.load(path)
+
+
+def test_validation_rejects_a_missing_mode(tmp_path):
+    modes, fam, keys = families_canonical(8, 7, 3)
+    H = len(modes)
+    k = np.stack([modes.k, modes.l], 1).copy()
+    k[-1] = (99, 99)  # not a retained mode (also breaks its group key)
+    group_of = np.repeat(np.arange(len(fam["group_modes"])), fam["group_modes"].astype(np.int64))
+    path = tmp_path / "f.bin"
+    fx.write(path, 8, 7, k, group_of, keys, fam["forward"], fam["inverse"], np.zeros((H, 15, 4), complex),
+             np.zeros((H, 4, 4), complex))
+    with pytest.raises(fx.FixtureError, match="missing a retained horizontal mode key"):
+        fx.load(path)
+
+
+def test_two_family_oracle_reduces_to_the_one_family_flux():
+    """With both families equal to the K^2 family over the K^2 groups, the
+    two-family flux is the production flux."""
+    n, nz = 16, 9
+    w = orc.Workload(n, n, nz, 4)
+    fwd, inv = orc.k2_family(w)
+    _, _, counts = orc.k2_groups(n, n)
+    fam = {"group_modes": counts, "forward": [fwd, fwd], "inverse": [inv, inv],
+           "input_family": fx.INPUT_FAMILIES, "target_family": fx.TARGET_FAMILIES}
+    rng = np.random.default_rng(2)
+    H = len(orc.retained_modes(n, n))
+    x = rng.uniform(-0.125, 0.125, H * 15 * 5) + 1j * rng.uniform(-0.125, 0.125, H * 15 * 5)
+    a = orc.flux(n, nz, x, families=fam)
+    b = orc.flux(n, nz, x)
+    assert orc.max_rel_error(a, b) <= 1e-14

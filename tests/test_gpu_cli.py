@@ -110,3 +110,22 @@ def test_validate_passes():
     assert "validation passed" in proc.stdout
     assert proc.stdout.count("cuda/") == 10 and proc.stdout.count("cuda-pruned/") == 10
     assert "cuda-flux/split-tf32x3/32x32x9" in proc.stdout
+
+
+@pytest.mark.parametrize("mode", ["fp64-plain", "split-tf32x3"])
+def test_authoritative_fixture_run(tmp_path, mode):
+    """--spectral-flux-fixture: the two-family flux against the fixture's
+    expected targets (a synthetic fixture in the prepared format)."""
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from synthetic_fixture import make
+
+    path = tmp_path / "fixture.bin"
+    make(path, 16, 9)
+    report, rows = run(tmp_path, "--kernel", "production-lifetime-flux", "--profile", "smoke", "--nx", "16", "--ny",
+                       "16", "--nz", "9", "--flux-mode", mode, "--spectral-flux-fixture", str(path))
+    assert report["status"] == "passed"
+    provider = report["providers"][0]
+    assert len(provider["correctness"]) == 1 and provider["correctness"][0]["passed"]
+    assert "synthetic" in provider["planning"]["configuration"]
