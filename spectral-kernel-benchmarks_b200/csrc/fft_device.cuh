@@ -355,8 +355,41 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
 // radix 8 for 512, both with Ns = 64) writes straight back to v (butterfly j
 // produces elements j + 64r = lane + 32(q + 2r)), so only the middle pass
 // round-trips through the padded shared region x.
+//
+// Twiddles come from a table in the order the lanes read them (rr_fill_table
+// copies them out of the length-N table, so the values are identical):
+//   pass 2:  t[8(r-1) + m]       = tw[(N/64) m r],  m = j mod 8, r = 1..7
+//   pass 3:  t[56 + 64(r-1) + j] = tw[j r],         j < 64,      r = 1..N/64-1
+// A pass-2 read is eight adjacent entries (one wavefront, broadcast), a pass-3
+// read 32 adjacent ones, where the strided reads of tw touched up to eight
+// lines each.  The table may live in shared or global memory (plain loads).
+template <int N>
+constexpr int rr_table_size() {
+    return 56 + (N / 64 - 1) * 64;
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void rr_fill_table(cx<T>* t, const cx<T>* __restrict__ tw, int tid, int nt) {
+    for (int i = tid; i < rr_table_size<N>(); i += nt) {
+        int idx;
+        if (i < 56) {
+            idx = (N / 64) * (i % 8) * (i / 8 + 1);
+        } else {
+            const int ii = i - 56;
+            idx = (ii % 64) * (ii / 64 + 1);
+        }
+        t[i] = tw[idx];
+    }
+}
+
+template <int SIGN, typename V>
+__device__ __forceinline__ V twiddle_plain(const V* t, int k) {
+    const V w = t[k];
+    return SIGN < 0 ? w : cconj(w);
+}
+
 template <typename T, int N, int SIGN>
-__device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const cx<T>* __restrict__ tw, int lane) {
+__device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const cx<T>* t, int lane) {
     using V = cx<T>;
     static_assert(N == 256 || N == 512, "warp_fft_rr handles N = 256 and N = 512");
     constexpr int Q = N / 256;  // radix-8 butterflies per lane in the first / middle passes
@@ -387,9 +420,9 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
             const V* in = x + j + (j >> 4);
 #pragma unroll
             for (int r = 0; r < 8; ++r) b[q][r] = in[(N / 8 + N / 128) * r];
-            const int step = (j % 8) * (N / 64);
+            const V* t2 = t + (j % 8);
 #pragma unroll
-            for (int r = 1; r < 8; ++r) b[q][r] = cmul(b[q][r], twiddle<SIGN>(tw, step * r));
+            for (int r = 1; r < 8; ++r) b[q][r] = cmul(b[q][r], twiddle_plain<SIGN>(t2, 8 * (r - 1)));
             dft8<SIGN>(b[q]);
         }
         __syncwarp();
@@ -412,7 +445,7 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
 #pragma unroll
         for (int r = 0; r < R3; ++r) b[r] = in[68 * r];
 #pragma unroll
-        for (int r = 1; r < R3; ++r) b[r] = cmul(b[r], twiddle<SIGN>(tw, j * r));
+        for (int r = 1; r < R3; ++r) b[r] = cmul(b[r], twiddle_plain<SIGN>(t + 56 + j, 64 * (r - 1)));
         if constexpr (R3 == 4) {
             dft4<SIGN>(b[0], b[1], b[2], b[3]);
         } else {

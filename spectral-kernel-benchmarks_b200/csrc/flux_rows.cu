@@ -18,6 +18,10 @@
 // The 3+3T slots are consumed in order, so the bins of slot f+1 are copied
 // into a second shared stage with cp.async while slot f is transformed; the
 // only CTA-wide barriers are one per slot and one per target.
+// Each stage row holds kx = 0..M and is zero beyond keep (written once, never
+// copied over), so the c2r pre-processing reads bins k and M-k without range
+// tests; the r2c twiddles and the 512-point FFT's lane-ordered twiddle table
+// are copied into shared memory once per CTA.
 
 #include "flux_rows.hpp"
 
@@ -32,6 +36,24 @@ template <int M>
 constexpr int region() {
     return M + M / 16 + 8;
 }
+// Stage row stride: kx = 0..M, odd so the B planes of one kx hit distinct banks.
+template <int M>
+constexpr int stage_row() {
+    return (M + 1) | 1;
+}
+// Entries of the lane-ordered FFT twiddle table (512-point rows only).
+template <int M>
+constexpr int rr_entries() {
+    if constexpr (M == 256) {
+        return rr_table_size<M>();
+    } else {
+        return 0;
+    }
+}
+template <int M, int B>
+constexpr size_t rows_smem_words(int keep) {
+    return size_t(B) * region<M>() + 2 * size_t(B) * stage_row<M>() + size_t(keep) * (B + 1) + M + rr_entries<M>();
+}
 
 // Launch bounds keep 128 registers per thread whatever the CTA width:
 // 16 / B CTAs of 32 * B threads fill 512 threads' worth of the register file.
@@ -42,12 +64,14 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
     constexpr int PER = M / 32;  // elements of its plane each lane keeps in registers
     constexpr int XP = region<M>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int KP = stage_row<M>();
     const int keep = a.keep;
-    const int KP = keep | 1;  // odd stage row stride: the 8 planes of one kx hit distinct banks
     V* xs = reinterpret_cast<V*>(smem_raw);
     V* stage0 = xs + B * XP;
     V* stage1 = stage0 + B * KP;
     V* outTile = stage1 + B * KP;  // [k][b], row stride B + 1
+    V* tf = outTile + keep * (B + 1);  // twFull[0..M)
+    V* tt = tf + M;                    // warp_fft_rr table (M = 256)
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int zChunks = (a.nz + B - 1) / B;
@@ -62,19 +86,26 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
     const long long outRow = a.binsOut.planes;
     V* x = xs + warp * XP;  // this warp's plane
 
+    for (int i = tid; i < M; i += NT) tf[i] = twFull[i];
+    if constexpr (rr_entries<M>() > 0) rr_fill_table<float, M>(tt, twHalf, tid, NT);
+    for (int i = tid; i < 2 * B * (KP - keep); i += NT) {
+        const int row = i / (KP - keep);
+        stage0[row * KP + keep + i % (KP - keep)] = V{0.f, 0.f};
+    }
+
     // Asynchronous copy of slot f's bins of this row into a plane-major stage
     // [b][k]; consecutive threads read consecutive planes of one kx (the
-    // planes-innermost global rows), planes beyond Nz are zero-filled.
+    // planes-innermost global rows), planes beyond Nz are zero-filled.  NT is a
+    // multiple of B, so a thread keeps its plane cb and steps kx by NT / B.
+    constexpr int KSTEP = NT / B;
+    const int cb = tid % B;
+    const int ck = tid / B;
+    const bool cok = z0 + cb < a.nz;
     auto issue = [&](int f, V* stage) {
-        const long long pBase = (static_cast<long long>(member) * a.fieldsIn + f) * a.zStride + z0;
-        const long long rowBase = a.binsIn.kxStride * y;
-        for (int idx = tid; idx < keep * B; idx += NT) {
-            const int b = idx % B;
-            const int k = idx / B;
-            const bool ok = z0 + b < a.nz;
-            const V* src = ok ? in + pBase + b + inRow * (static_cast<long long>(k) + rowBase) : in;
-            cp_async8(stage + b * KP + k, src, ok ? 8 : 0);
-        }
+        const long long plane = (static_cast<long long>(member) * a.fieldsIn + f) * a.zStride + z0 + cb;
+        const V* src = in + plane + inRow * (a.binsIn.kxStride * y + ck);
+        V* dst = stage + cb * KP + ck;
+        for (int k = ck; k < keep; k += KSTEP, src += inRow * KSTEP, dst += KSTEP) cp_async8(dst, cok ? src : in, cok ? 8 : 0);
         cp_async_commit();
     };
 
@@ -93,24 +124,26 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
         };
         if constexpr (M == 256) {
             // Pre-processed half-length spectrum straight into registers
-            // (element k = lane + 32e), then the register-ended FFT.
+            // (element k = lane + 32e), then the register-ended FFT.  At k = 0
+            // (lane 0, e = 0) the bins 0 and M are real, and the general form
+            // reduces to {X0 + XM, X0 - XM} since tf[0] = 1.
+            const V* stk = st + lane;
+            const V* stm = st + (M - lane);
+            const V* tfk = tf + lane;
 #pragma unroll
             for (int e = 0; e < PER; ++e) {
-                const int k = lane + 32 * e;
-                if (k == 0) {
-                    const V x0 = load(0);
-                    const V xm = load(M);
-                    r[e] = {x0.x + xm.x, x0.x - xm.x};
-                } else {
-                    const V xk = load(k);
-                    const V xm = load(M - k);
-                    const V s = cadd(xk, cconj(xm));
-                    const V d = csub(xk, cconj(xm));
-                    const V t = cmulc(d, __ldg(twFull + k));
-                    r[e] = {s.x - t.y, s.y + t.x};
+                V xk = stk[32 * e];
+                V xm = stm[-32 * e];
+                if (e == 0 && lane == 0) {
+                    xk.y = 0.f;
+                    xm.y = 0.f;
                 }
+                const V s = cadd(xk, cconj(xm));
+                const V d = csub(xk, cconj(xm));
+                const V t = cmulc(d, tfk[32 * e]);
+                r[e] = {s.x - t.y, s.y + t.x};
             }
-            warp_fft_rr<float, M, +1>(r, x, twHalf, lane);
+            warp_fft_rr<float, M, +1>(r, x, tt, lane);
         } else {
             constexpr int pairs = M / 2 + 1;
             for (int k = lane; k < pairs; k += 32) {
@@ -126,13 +159,13 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
                 {
                     const V s = cadd(xk, cconj(xm));
                     const V d = csub(xk, cconj(xm));
-                    const V t = cmulc(d, __ldg(twFull + k));
+                    const V t = cmulc(d, tf[k]);
                     x[pad16(k)] = {s.x - t.y, s.y + t.x};
                 }
                 if (kk != k) {
                     const V s = cadd(xm, cconj(xk));
                     const V d = csub(xm, cconj(xk));
-                    const V t = cmulc(d, __ldg(twFull + kk));
+                    const V t = cmulc(d, tf[kk]);
                     x[pad16(kk)] = {s.x - t.y, s.y + t.x};
                 }
             }
@@ -163,7 +196,7 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
         for (int e = 0; e < PER; ++e)
             acc[e] = {-scale * (acc[e].x + w[e].x * q[e].x), -scale * (acc[e].y + w[e].y * q[e].y)};
         if constexpr (M == 256) {
-            warp_fft_rr<float, M, -1>(acc, x, twHalf, lane);
+            warp_fft_rr<float, M, -1>(acc, x, tt, lane);
             // pad16(lane + 32e) = lane + lane/16 + 34e
             V* o = x + lane + (lane >> 4);
 #pragma unroll
@@ -189,18 +222,17 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
                 const V ev = cscale(cadd(zk, zm), 0.5f);
                 const V d = csub(zk, zm);
                 const V o = {0.5f * d.y, -0.5f * d.x};
-                X = cadd(ev, cmul(__ldg(twFull + k), o));
+                X = cadd(ev, cmul(tf[k], o));
             }
             outTile[k * (B + 1) + warp] = X;
         }
         __syncthreads();
         // Coalesced rows of B planes per kx.
-        const long long pOut = (static_cast<long long>(member) * a.targets + t) * a.zStride + z0;
-        for (int idx = tid; idx < keep * B; idx += NT) {
-            const int b = idx % B;
-            const int k = idx / B;
-            if (z0 + b < a.nz)
-                out[pOut + b + outRow * (static_cast<long long>(k) + a.binsOut.kxStride * y)] = outTile[k * (B + 1) + b];
+        if (cok) {
+            const long long plane = (static_cast<long long>(member) * a.targets + t) * a.zStride + z0 + cb;
+            V* dst = out + plane + outRow * (a.binsOut.kxStride * y + ck);
+            const V* src = outTile + ck * (B + 1) + cb;
+            for (int k = ck; k < keep; k += KSTEP, dst += outRow * KSTEP, src += KSTEP * (B + 1)) *dst = *src;
         }
         // The next outTile write happens after the next inverse_row's barrier.
     }
@@ -213,8 +245,7 @@ cudaError_t launch_m(const RowFluxArgs& a, cudaStream_t stream) {
     const int zChunks = (a.nz + B - 1) / B;
     const dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
     auto kernel = rows_flux_kernel<M, B>;
-    const size_t bytes =
-        sizeof(float2) * (size_t(B) * region<M>() + 2 * size_t(B) * (a.keep | 1) + size_t(a.keep) * (B + 1));
+    const size_t bytes = sizeof(float2) * rows_smem_words<M, B>(a.keep);
     if (bytes > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (err != cudaSuccess) return err;
