@@ -149,24 +149,50 @@ __global__ void __launch_bounds__(32 * B, 4) columns_gather_warp_kernel(int nz, 
 // ky.  Pass 2 is warp-per-plane in shared memory.  Pass 3 is again thread
 // (b, j): its outputs are ky = j + 64r of plane b, stored straight to global
 // memory with the same coalescing.  Each element touches shared memory four
-// times instead of eight.  The butterfly-to-thread maps are chosen so that,
-// with a plane region of 2 mod 4 elements, the pass-1 stores and pass-3 loads
-// are free of bank conflicts: in a half-warp the two butterflies of pass 1
-// differ by 2 and those of pass 3 by 1.
+// times instead of eight.
+// Two layouts share a plane's region: pass 1 writes element e at pad16(e),
+// pass 2 reads that and writes element e at e + 8(e/64), which pass 3 reads.
+// With a plane region of 2 mod 16 elements every access is free of bank
+// conflicts: in a half-warp the two butterflies of pass 1 differ by 2 and
+// those of pass 3 by 1 (planes b = 0..7 then fill the other residues), and
+// the pass-2 stores of butterflies j and j + 8 land 72 = 8 (mod 16) apart.
+// Twiddles of passes 2 and 3 come from the lane-ordered table of
+// rr_fill_table, copied into shared memory once per CTA.
 constexpr int kDirectN = 512;
-constexpr int kDirectRegion = 546;  // >= pad16(511) + 1, and 546 % 4 == 2
-static_assert(kDirectRegion % 4 == 2 && kDirectRegion > 542, "direct plane region");
+constexpr int kDirectRegion = 578;  // > 511 + 8 * 7, and 578 % 16 == 2
+static_assert(kDirectRegion % 16 == 2 && kDirectRegion > 567, "direct plane region");
+constexpr int kDirectTable = rr_table_size<kDirectN>();
+
+// The CTA's twiddle table, after the eight plane regions; filled by all 256
+// threads, read after the CTA's next barrier.
+__device__ __forceinline__ const float2* direct_table(float2* xs, const float2* __restrict__ tw, int tid) {
+    float2* tt = xs + 8 * kDirectRegion;
+    rr_fill_table<float, kDirectN>(tt, tw, tid, 256);
+    return tt;
+}
+
+// Pass-3 inputs of butterfly j (< 64) of plane b: elements j + 64r in the
+// pass-2 layout, times their twiddles.
+template <int SIGN>
+__device__ __forceinline__ void direct_last_inputs(const float2* xs, const float2* tt, int b, int j, float2 (&v)[8]) {
+    const float2* in = xs + b * kDirectRegion + j;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = in[72 * r];
+#pragma unroll
+    for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle_plain<SIGN>(tt + 56 + j, 64 * (r - 1)));
+}
 
 __device__ __forceinline__ int pass1_butterfly(int t, int q) {
     const int h = t >> 4;
     return 4 * (h >> 1) + (h & 1) + 2 * ((t >> 3) & 1) + 32 * q;
 }
 
-// Padded addresses of the passes as per-lane bases plus compile-time offsets
-// (j < 64): pad16(8j + r) = 8j + j/2 + r, pad16(j + 64r) = j + j/16 + 68r,
-// pad16(64(j/8) + j%8 + 8r) = 68(j/8) + j%8 + 8r + r/2.
+// Addresses of the passes as per-lane bases plus compile-time offsets
+// (j < 64): pass-1 stores pad16(8j + r) = 8j + j/2 + r, pass-2 loads
+// pad16(j + 64r) = j + j/16 + 68r, pass-2 stores of element 64(j/8) + j%8 + 8r
+// at 72(j/8) + j%8 + 8r, pass-3 loads of element j + 64r at j + 72r.
 template <int SIGN>
-__device__ __forceinline__ void direct_middle_pass(float2* xs, const float2* __restrict__ tw, int warp, int lane) {
+__device__ __forceinline__ void direct_middle_pass(float2* xs, const float2* tt, int warp, int lane) {
     float2* x = xs + warp * kDirectRegion;
     float2 v[2][8];
 #pragma unroll
@@ -175,18 +201,18 @@ __device__ __forceinline__ void direct_middle_pass(float2* xs, const float2* __r
         const float2* in = x + j + (j >> 4);
 #pragma unroll
         for (int r = 0; r < 8; ++r) v[q][r] = in[68 * r];
-        const int step = (j % 8) * 8;
+        const float2* t2 = tt + (j % 8);
 #pragma unroll
-        for (int r = 1; r < 8; ++r) v[q][r] = cmul(v[q][r], twiddle<SIGN>(tw, step * r));
+        for (int r = 1; r < 8; ++r) v[q][r] = cmul(v[q][r], twiddle_plain<SIGN>(t2, 8 * (r - 1)));
         dft8<SIGN>(v[q]);
     }
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int j = lane + 32 * q;
-        float2* o = x + 68 * (j / 8) + (j % 8);
+        float2* o = x + 72 * (j / 8) + (j % 8);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) o[8 * r + (r >> 1)] = v[q][r];
+        for (int r = 0; r < 8; ++r) o[8 * r] = v[q][r];
     }
 }
 
@@ -196,6 +222,7 @@ __global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, in
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* xs = reinterpret_cast<float2*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const float2* tt = direct_table(xs, tw, tid);
     const int zChunks = (nz + B - 1) / B;
     const int f = blockIdx.x / zChunks;
     const int z0 = (blockIdx.x % zChunks) * B;
@@ -234,7 +261,7 @@ __global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, in
         }
     }
     __syncthreads();
-    if (z0 + warp < nz) direct_middle_pass<+1>(xs, tw, warp, lane);  // planes beyond Nz stay idle
+    if (z0 + warp < nz) direct_middle_pass<+1>(xs, tt, warp, lane);  // planes beyond Nz stay idle
     __syncthreads();
     if (!inRange) return;
     float2* dst = static_cast<float2*>(out.data) + static_cast<long long>(f) * zStride + z + out.planes * kx;
@@ -243,10 +270,7 @@ __global__ void __launch_bounds__(256, 3) columns_embed_direct_kernel(int nz, in
     for (int q = 0; q < 2; ++q) {
         const int j = (tid >> 3) + 32 * q;
         float2 v[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + j + (j >> 4) + 68 * r];
-#pragma unroll
-        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<+1>(tw, j * r));
+        direct_last_inputs<+1>(xs, tt, b, j, v);
         dft8<+1>(v);
 #pragma unroll
         for (int r = 0; r < 8; ++r) dst[rowStride * (j + 64 * r)] = v[r];
@@ -260,6 +284,7 @@ __global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, i
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* xs = reinterpret_cast<float2*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const float2* tt = direct_table(xs, tw, tid);
     const int zChunks = (nz + B - 1) / B;
     const int f = blockIdx.x / zChunks;
     const int z0 = (blockIdx.x % zChunks) * B;
@@ -283,7 +308,7 @@ __global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, i
         }
     }
     __syncthreads();
-    if (z0 + warp < nz) direct_middle_pass<-1>(xs, tw, warp, lane);
+    if (z0 + warp < nz) direct_middle_pass<-1>(xs, tt, warp, lane);
     __syncthreads();
     if (!inRange) return;
     const FieldView view = views.v[f];
@@ -295,10 +320,7 @@ __global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, i
 #pragma unroll
         for (int r = 0; r < 8; ++r) e[r] = __ldg(map + j + 64 * r);
         float2 v[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + j + (j >> 4) + 68 * r];
-#pragma unroll
-        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<-1>(tw, j * r));
+        direct_last_inputs<-1>(xs, tt, b, j, v);
         dft8<-1>(v);
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
@@ -317,7 +339,7 @@ __global__ void __launch_bounds__(256, 3) columns_gather_direct_kernel(int nz, i
     }
 }
 
-constexpr size_t kDirectSmem = sizeof(float2) * 8 * kDirectRegion;
+constexpr size_t kDirectSmem = sizeof(float2) * (8 * kDirectRegion + kDirectTable);
 
 constexpr int kPlanes = 8;
 
@@ -377,6 +399,7 @@ __global__ void __launch_bounds__(256, 3) columns_inverse_band_kernel(int nz, in
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* xs = reinterpret_cast<float2*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const float2* tt = direct_table(xs, tw, tid);
     const int zChunks = (nz + B - 1) / B;
     const int f = blockIdx.x / zChunks;
     const int z0 = (blockIdx.x % zChunks) * B;
@@ -402,17 +425,14 @@ __global__ void __launch_bounds__(256, 3) columns_inverse_band_kernel(int nz, in
         for (int r = 0; r < 8; ++r) o[r] = v[r];
     }
     __syncthreads();
-    if (z0 + warp < nz) direct_middle_pass<+1>(xs, tw, warp, lane);  // planes beyond Nz stay idle
+    if (z0 + warp < nz) direct_middle_pass<+1>(xs, tt, warp, lane);  // planes beyond Nz stay idle
     __syncthreads();
     if (!inRange) return;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int j = (tid >> 3) + 32 * q;
         float2 v[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + j + (j >> 4) + 68 * r];
-#pragma unroll
-        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<+1>(tw, j * r));
+        direct_last_inputs<+1>(xs, tt, b, j, v);
         dft8<+1>(v);
 #pragma unroll
         for (int r = 0; r < 8; ++r) col[rowStride * (j + 64 * r)] = v[r];
@@ -426,6 +446,7 @@ __global__ void __launch_bounds__(256, 3) columns_forward_band_kernel(int nz, in
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* xs = reinterpret_cast<float2*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const float2* tt = direct_table(xs, tw, tid);
     const int zChunks = (nz + B - 1) / B;
     const int f = blockIdx.x / zChunks;
     const int z0 = (blockIdx.x % zChunks) * B;
@@ -447,7 +468,7 @@ __global__ void __launch_bounds__(256, 3) columns_forward_band_kernel(int nz, in
         for (int r = 0; r < 8; ++r) o[r] = v[r];
     }
     __syncthreads();
-    if (z0 + warp < nz) direct_middle_pass<-1>(xs, tw, warp, lane);
+    if (z0 + warp < nz) direct_middle_pass<-1>(xs, tt, warp, lane);
     __syncthreads();
     if (!inRange) return;
     const int band = __ldg(bandOf + kx);
@@ -455,10 +476,7 @@ __global__ void __launch_bounds__(256, 3) columns_forward_band_kernel(int nz, in
     for (int q = 0; q < 2; ++q) {
         const int j = (tid >> 3) + 32 * q;
         float2 v[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = xs[b * XP + j + (j >> 4) + 68 * r];
-#pragma unroll
-        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle<-1>(tw, j * r));
+        direct_last_inputs<-1>(xs, tt, b, j, v);
         dft8<-1>(v);
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
@@ -484,6 +502,7 @@ __global__ void __launch_bounds__(256, 2) columns_band_persist_kernel(int nz, in
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* xs = reinterpret_cast<float2*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const float2* tt = direct_table(xs, tw, tid);
     const int b = tid & 7;
     const int zChunks = (nz + B - 1) / B;
     const long long perColumn = static_cast<long long>(zChunks) * slots;
@@ -539,17 +558,14 @@ __global__ void __launch_bounds__(256, 2) columns_band_persist_kernel(int nz, in
             load(next, v);
         }
         __syncthreads();
-        if (cur.z0 + warp < nz) direct_middle_pass<SIGN>(xs, tw, warp, lane);  // planes beyond Nz stay idle
+        if (cur.z0 + warp < nz) direct_middle_pass<SIGN>(xs, tt, warp, lane);  // planes beyond Nz stay idle
         __syncthreads();
         if (cur.z0 + b < nz) {
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int j = (tid >> 3) + 32 * q;
                 float2 w[8];
-#pragma unroll
-                for (int r = 0; r < 8; ++r) w[r] = xs[b * XP + j + (j >> 4) + 68 * r];
-#pragma unroll
-                for (int r = 1; r < 8; ++r) w[r] = cmul(w[r], twiddle<SIGN>(tw, j * r));
+                direct_last_inputs<SIGN>(xs, tt, b, j, w);
                 dft8<SIGN>(w);
 #pragma unroll
                 for (int r = 0; r < 8; ++r) {
