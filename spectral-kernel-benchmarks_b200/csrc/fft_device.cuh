@@ -354,7 +354,11 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
 // elements j + (N/8)r = lane + 32(q + Qr)), the last pass (radix 4 for 256,
 // radix 8 for 512, both with Ns = 64) writes straight back to v (butterfly j
 // produces elements j + 64r = lane + 32(q + 2r)), so only the middle pass
-// round-trips through the padded shared region x.
+// round-trips through the shared region x.  Pass 1 writes element e at
+// pad16(e); pass 2 writes element e at e + 8(e/64), so that its stores (the
+// butterflies j and j + 8 of a half-warp land 72 = 8 mod 16 words apart) and
+// the pass-3 loads (consecutive j) are both free of bank conflicts.  x must
+// hold rr_region_min<N>() elements.
 //
 // Twiddles come from a table in the order the lanes read them (rr_fill_table
 // copies them out of the length-N table, so the values are identical):
@@ -366,6 +370,11 @@ __device__ __forceinline__ void warp_fft(cx<T>* x, const cx<T>* __restrict__ tw,
 template <int N>
 constexpr int rr_table_size() {
     return 56 + (N / 64 - 1) * 64;
+}
+
+template <int N>
+constexpr int rr_region_min() {
+    return N + 8 * (N / 64 - 1);
 }
 
 template <typename T, int N>
@@ -393,11 +402,12 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
     using V = cx<T>;
     static_assert(N == 256 || N == 512, "warp_fft_rr handles N = 256 and N = 512");
     constexpr int Q = N / 256;  // radix-8 butterflies per lane in the first / middle passes
-    // Padded addresses as per-lane bases plus compile-time offsets (j < 64,
-    // BF = N/8 a multiple of 16):
-    //   pad16(8j + r)                = 8j + j/2 + r
-    //   pad16(j + BF r)              = j + j/16 + (BF + BF/16) r
-    //   pad16(64(j/8) + j%8 + 8r)    = 68(j/8) + j%8 + 8r + r/2
+    // Addresses as per-lane bases plus compile-time offsets (j < 64, BF = N/8
+    // a multiple of 16):
+    //   pass-1 stores  pad16(8j + r)   = 8j + j/2 + r
+    //   pass-2 loads   pad16(j + BF r) = j + j/16 + (BF + BF/16) r
+    //   pass-2 stores  element 64(j/8) + j%8 + 8r at 72(j/8) + j%8 + 8r
+    //   pass-3 loads   element j + 64r at j + 72r
     // Pass 1: Ns = 1, radix 8, registers -> x.
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -429,9 +439,9 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = lane + 32 * q;
-            V* o = x + 68 * (j / 8) + (j % 8);
+            V* o = x + 72 * (j / 8) + (j % 8);
 #pragma unroll
-            for (int r = 0; r < 8; ++r) o[8 * r + (r >> 1)] = b[q][r];
+            for (int r = 0; r < 8; ++r) o[8 * r] = b[q][r];
         }
         __syncwarp();
     }
@@ -440,10 +450,10 @@ __device__ __forceinline__ void warp_fft_rr(cx<T> (&v)[N / 32], cx<T>* x, const 
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int j = lane + 32 * q;
-        const V* in = x + j + (j >> 4);
+        const V* in = x + j;
         V b[R3];
 #pragma unroll
-        for (int r = 0; r < R3; ++r) b[r] = in[68 * r];
+        for (int r = 0; r < R3; ++r) b[r] = in[72 * r];
 #pragma unroll
         for (int r = 1; r < R3; ++r) b[r] = cmul(b[r], twiddle_plain<SIGN>(t + 56 + j, 64 * (r - 1)));
         if constexpr (R3 == 4) {

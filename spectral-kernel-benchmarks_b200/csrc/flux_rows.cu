@@ -36,10 +36,20 @@ template <int M>
 constexpr int region() {
     return M + M / 16 + 8;
 }
-// Stage row stride: kx = 0..M, odd so the B planes of one kx hit distinct banks.
-template <int M>
+// Stage row stride: kx = 0..M, and a residue mod 16 (in 8-byte words) that
+// spreads one cp.async instruction's B planes x 32/B consecutive kx over the
+// 16 bank pairs exactly twice (4 for B = 4 and 8, 1 for B = 16).
+template <int M, int B>
 constexpr int stage_row() {
-    return (M + 1) | 1;
+    constexpr int want = B == 16 ? 1 : 4;
+    return M + 1 + ((want - (M + 1) % 16) + 16) % 16;
+}
+// Output tile [k][b], row stride B, plane b of row k at b ^ swz(k): a warp's
+// 16 consecutive kx of one plane and a copy-out instruction's B planes x 32/B
+// consecutive kx both touch every bank pair equally often.
+template <int B>
+__device__ __forceinline__ int out_slot(int k, int b) {
+    return k * B + (b ^ ((k / (16 / B)) & (B - 1)));
 }
 // Entries of the lane-ordered FFT twiddle table (512-point rows only).
 template <int M>
@@ -52,7 +62,7 @@ constexpr int rr_entries() {
 }
 template <int M, int B>
 constexpr size_t rows_smem_words(int keep) {
-    return size_t(B) * region<M>() + 2 * size_t(B) * stage_row<M>() + size_t(keep) * (B + 1) + M + rr_entries<M>();
+    return size_t(B) * region<M>() + 2 * size_t(B) * stage_row<M, B>() + size_t(keep) * B + M + rr_entries<M>();
 }
 
 // Launch bounds keep 128 registers per thread whatever the CTA width:
@@ -64,13 +74,14 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
     constexpr int PER = M / 32;  // elements of its plane each lane keeps in registers
     constexpr int XP = region<M>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int KP = stage_row<M>();
+    constexpr int KP = stage_row<M, B>();
+    static_assert(M != 256 || XP >= rr_region_min<256>(), "plane region too small for warp_fft_rr");
     const int keep = a.keep;
     V* xs = reinterpret_cast<V*>(smem_raw);
     V* stage0 = xs + B * XP;
     V* stage1 = stage0 + B * KP;
-    V* outTile = stage1 + B * KP;  // [k][b], row stride B + 1
-    V* tf = outTile + keep * (B + 1);  // twFull[0..M)
+    V* outTile = stage1 + B * KP;  // [k][b] at out_slot(k, b)
+    V* tf = outTile + keep * B;        // twFull[0..M)
     V* tt = tf + M;                    // warp_fft_rr table (M = 256)
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -224,15 +235,14 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
                 const V o = {0.5f * d.y, -0.5f * d.x};
                 X = cadd(ev, cmul(tf[k], o));
             }
-            outTile[k * (B + 1) + warp] = X;
+            outTile[out_slot<B>(k, warp)] = X;
         }
         __syncthreads();
         // Coalesced rows of B planes per kx.
         if (cok) {
             const long long plane = (static_cast<long long>(member) * a.targets + t) * a.zStride + z0 + cb;
             V* dst = out + plane + outRow * (a.binsOut.kxStride * y + ck);
-            const V* src = outTile + ck * (B + 1) + cb;
-            for (int k = ck; k < keep; k += KSTEP, dst += outRow * KSTEP, src += KSTEP * (B + 1)) *dst = *src;
+            for (int k = ck; k < keep; k += KSTEP, dst += outRow * KSTEP) *dst = outTile[out_slot<B>(k, cb)];
         }
         // The next outTile write happens after the next inverse_row's barrier.
     }
