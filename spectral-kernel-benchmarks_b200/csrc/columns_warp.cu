@@ -392,7 +392,10 @@ cudaError_t gather_n(int nz, int zStride, int columns, DenseBins in, const ViewS
 // at plane f * zStride.
 __device__ __forceinline__ bool in_band(int ky, int n, int band) { return min(ky, n - ky) <= band; }
 
-__global__ void __launch_bounds__(256, 3) columns_inverse_band_kernel(int nz, int zStride, DenseBins bins,
+// MINB: CTAs per SM the register allocation must allow (3, or 4 for the
+// kBandDirect4 form, which trades registers for loads in flight).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) columns_inverse_band_kernel(int nz, int zStride, DenseBins bins,
                                                                       const int* __restrict__ bandOf,
                                                                       const float2* __restrict__ tw) {
     constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
@@ -439,7 +442,8 @@ __global__ void __launch_bounds__(256, 3) columns_inverse_band_kernel(int nz, in
     }
 }
 
-__global__ void __launch_bounds__(256, 3) columns_forward_band_kernel(int nz, int zStride, DenseBins bins,
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) columns_forward_band_kernel(int nz, int zStride, DenseBins bins,
                                                                       const int* __restrict__ bandOf, float scale,
                                                                       const float2* __restrict__ tw) {
     constexpr int B = 8, N = kDirectN, XP = kDirectRegion;
@@ -699,10 +703,10 @@ cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBin
     if (N == kDirectN && form == kBandPersist)
         return launch_band_persist<+1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
     if (N == kDirectN && form != kBandWarp) {
-        cudaError_t err = prepare(columns_inverse_band_kernel, kDirectSmem);
+        auto kernel = form == kBandDirect4 ? columns_inverse_band_kernel<4> : columns_inverse_band_kernel<3>;
+        cudaError_t err = prepare(kernel, kDirectSmem);
         if (err != cudaSuccess) return err;
-        columns_inverse_band_kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band,
-                                                                    static_cast<const float2*>(tw));
+        kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band, static_cast<const float2*>(tw));
     } else {
         auto kernel = columns_inverse_band_warp_kernel<N, B>;
         const size_t bytes = sizeof(float2) * size_t(B) * plane_region<N>();
@@ -722,10 +726,10 @@ cudaError_t forward_band_n(int nz, int zStride, int slots, int columns, DenseBin
     if (N == kDirectN && form == kBandPersist)
         return launch_band_persist<-1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
     if (N == kDirectN && form != kBandWarp) {
-        cudaError_t err = prepare(columns_forward_band_kernel, kDirectSmem);
+        auto kernel = form == kBandDirect4 ? columns_forward_band_kernel<4> : columns_forward_band_kernel<3>;
+        cudaError_t err = prepare(kernel, kDirectSmem);
         if (err != cudaSuccess) return err;
-        columns_forward_band_kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band, float(scale),
-                                                                    static_cast<const float2*>(tw));
+        kernel<<<grid, 256, kDirectSmem, s>>>(nz, zStride, bins, band, float(scale), static_cast<const float2*>(tw));
     } else {
         auto kernel = columns_forward_band_warp_kernel<N, B>;
         const size_t bytes = sizeof(float2) * size_t(B) * plane_region<N>();

@@ -25,11 +25,14 @@ cudaError_t launch_columns_gather_warp(int ny, int nz, int zStride, int columns,
 // Band kernel forms: kBandDefault is the direct three-pass kernel at Ny = 512
 // and the warp-per-plane kernel below; kBandWarp selects the warp-per-plane
 // kernel at every size; kBandPersist the persistent direct kernel (Ny = 512
-// only), which loads the next tile during the current one's passes.  The
-// forms at 512 are autotuner candidates.
+// only), which loads the next tile during the current one's passes;
+// kBandDirect4 the direct kernel compiled for four resident CTAs per SM
+// instead of three (at most 64 registers a thread), for more loads in flight.
+// The forms at 512 are autotuner candidates.
 constexpr int kBandDefault = 0;
 constexpr int kBandWarp = 1;
 constexpr int kBandPersist = 2;
+constexpr int kBandDirect4 = 3;
 cudaError_t launch_columns_inverse_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
                                         const int* band, const void* tw, int form, cudaStream_t s);
 cudaError_t launch_columns_forward_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
