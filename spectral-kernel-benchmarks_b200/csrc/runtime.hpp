@@ -189,10 +189,18 @@ private:
     GemmPrecision p_;
     int R_, S_;
     std::uint64_t columns_ = 0;
-    int tiles_ = 0;
     std::uint64_t members_ = 1;
     long long memberColumns_ = 0;
-    DeviceBuffer matrices_, tileGroup_, tileColumn_, tileCount_;
+    long long matrixStride_ = 0;  // SIMT form: elements between group matrices (0: one common matrix)
+    DeviceBuffer matrices_;
+    // SIMT tiles over each group's member-concatenated columns, one table per
+    // active member count 1..members.
+    struct TileTable {
+        DeviceBuffer group, column, count, per, first;
+        int tiles = 0;
+    };
+    std::vector<TileTable> tileTables_;
+    bool virtualTiles_ = false;  // SIMT tile numbering (GroupTiles::virtualColumns)
     long long imageStride_ = 0;  // tensor-core form: bytes between group images (0: one common image)
     // Tensor-core work units, one table per active member count 1..members.
     struct UnitTable {

@@ -49,8 +49,9 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Element offset of column `col` (single member, column = mode * fields +
-// field) in a bin-array operand, with its partner (or -1) and conjugation.
+// Element offset of plan column `col` (member * memberColumns + mode * fields
+// + field) in a cell-addressed operand, with its partner (or -1) and
+// conjugation.
 __device__ __forceinline__ void bin_column(const BinBoundary& bb, int col, long long& base, long long& partner,
                                            bool& conj) {
     // Plan column = member * memberColumns + mode * fields + plan field.
@@ -72,7 +73,7 @@ __device__ __forceinline__ void bin_column(const BinBoundary& bb, int col, long 
     conj = bb.conj != nullptr && __ldg(bb.conj + mode) != 0;
 }
 
-template <typename T, int KR, bool SPLIT, bool BINS>
+template <typename T, int KR, bool SPLIT, bool BINS, bool VIRT>
 __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, const T* __restrict__ At,
                                                                 GroupTiles tiles, ComplexOperand in,
                                                                 ComplexOperand out, BinBoundary inBins,
@@ -88,11 +89,11 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
     __shared__ signed char conjIn[kTileCols], conjOut[kTileCols];
     const int tile = blockIdx.x;
     const int g = __ldg(tiles.tileGroup + tile);
-    const int c0 = __ldg(tiles.tileColumn + tile);
+    const int c0 = __ldg(tiles.tileColumn + tile);  // first global (member tiles) or virtual column
     const int ncols = __ldg(tiles.tileCount + tile);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    if (BINS && threadIdx.x < kTileCols) {
+    if (!VIRT && BINS && threadIdx.x < kTileCols) {
         const int c = threadIdx.x;
         long long base = static_cast<long long>(c0 + c) * S, partner = -1;
         bool conj = false;
@@ -107,8 +108,35 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
         colPartner[c] = partner;
         conjOut[c] = conj ? 1 : 0;
     }
-    if (BINS) __syncthreads();
-    const T* A = At + (long long)g * R * S;
+    if (!VIRT && BINS) __syncthreads();
+    // Virtual tiles: warp w copies, multiplies and stores the tile columns
+    // w + 8m (m < 4), so its lanes 0..3 resolve exactly those and a warp
+    // barrier suffices.
+    if (VIRT && lane < kTileCols / 8) {
+        const int per = __ldg(tiles.tilePer + tile);
+        const int first = __ldg(tiles.tileFirst + tile);
+        // Virtual column c0 + c of group g -> global plan column.
+        const int c = warp + 8 * lane;
+        long long inBase = 0, outBase = 0, partner = -1;
+        bool cIn = false, cOut = false;
+        if (c < ncols) {
+            const int v = c0 + c;
+            const int member = v / per;
+            const long long col = member * tiles.memberColumns + first + (v - member * per);
+            inBase = col * S;
+            outBase = col * R;
+            long long unused = -1;
+            if (BINS && inBins.cell != nullptr) bin_column(inBins, static_cast<int>(col), inBase, unused, cIn);
+            if (BINS && outBins.cell != nullptr) bin_column(outBins, static_cast<int>(col), outBase, partner, cOut);
+        }
+        colIn[c] = inBase;
+        conjIn[c] = cIn ? 1 : 0;
+        colOut[c] = outBase;
+        colPartner[c] = partner;
+        conjOut[c] = cOut ? 1 : 0;
+    }
+    if (VIRT) __syncwarp();
+    const T* A = At + g * tiles.matrixStride;
     const int chunks = (S + kChunk - 1) / kChunk;
 
     auto stageX = [&](int b) { return reinterpret_cast<V(*)[kChunk + 1]>(smem_raw + b * (xBytes + aBytes)); };
@@ -128,7 +156,7 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
         for (int i = threadIdx.x; i < kTileCols * kChunk; i += kThreads) {
             const int c = i / kChunk, s = i % kChunk;
             const bool ok = c < ncols && s0 + s < S;
-            const long long idx = ok ? (BINS ? colIn[c] : (long long)(c0 + c) * S) + s0 + s : 0;
+            const long long idx = ok ? ((VIRT || BINS) ? colIn[c] : (long long)(c0 + c) * S) + s0 + s : 0;
             if (SPLIT) {
                 // Split operands: two scalar copies into the complex slot.
                 T* slot = reinterpret_cast<T*>(&sX[c][s]);
@@ -187,7 +215,7 @@ __global__ void __launch_bounds__(kThreads) grouped_gemm_kernel(int R, int S, co
             // The matrices are real, so a conjugated input column gives the
             // conjugate product: both flags are applied here, once.
             V v = acc[k][m];
-            if (!BINS) {
+            if (!VIRT && !BINS) {
                 store_operand<T, SPLIT>(out, (long long)(c0 + c) * R + r, v);
                 continue;
             }
@@ -205,8 +233,14 @@ cudaError_t launch_kr(int R, int S, const void* At, const GroupTiles& tiles, Com
     if (split != (out.im != nullptr)) return cudaErrorInvalidValue;
     const size_t bytes = 2 * (sizeof(cx<T>) * kTileCols * (kChunk + 1) + sizeof(T) * kChunk * 32 * KR);
     const bool bins = inBins.cell != nullptr || outBins.cell != nullptr;
-    auto kernel = split ? (bins ? grouped_gemm_kernel<T, KR, true, true> : grouped_gemm_kernel<T, KR, true, false>)
-                        : (bins ? grouped_gemm_kernel<T, KR, false, true> : grouped_gemm_kernel<T, KR, false, false>);
+    using K = void (*)(int, int, const T*, GroupTiles, ComplexOperand, ComplexOperand, BinBoundary, BinBoundary);
+    // [split][bins][virtual]
+    const K kernels[2][2][2] = {
+        {{grouped_gemm_kernel<T, KR, false, false, false>, grouped_gemm_kernel<T, KR, false, false, true>},
+         {grouped_gemm_kernel<T, KR, false, true, false>, grouped_gemm_kernel<T, KR, false, true, true>}},
+        {{grouped_gemm_kernel<T, KR, true, false, false>, grouped_gemm_kernel<T, KR, true, false, true>},
+         {grouped_gemm_kernel<T, KR, true, true, false>, grouped_gemm_kernel<T, KR, true, true, true>}}};
+    const K kernel = kernels[split][bins][tiles.virtualColumns];
     if (bytes > 48 * 1024) {
         const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (err != cudaSuccess) return err;

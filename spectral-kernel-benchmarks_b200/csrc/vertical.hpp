@@ -18,11 +18,27 @@ namespace skb {
 
 enum class GemmPrecision { f64 = 0, f32 = 1, tf32x3 = 2, bf16x3 = 3 };
 
+// SIMT tiles, in one of two numberings.
+// Member tiles (virtual == false): a tile is up to the tile width of one
+// member's columns of one group; tileColumn is its first global complex
+// column (member * memberColumns + column within the member).
+// Virtual tiles (virtual == true): runs of the (member, column) list of one
+// group, numbered like the tensor-core work units below: virtual column v of
+// group g is member v / groupColumns[g], complex column
+// groupFirst[g] + v % groupColumns[g] of that member.  Concatenating the
+// members keeps a group's tiles full when it has few columns per member (a
+// field subset, small groups); each tile carries its group's groupColumns /
+// groupFirst so that a CTA's first loads do not wait on a dependent read.
 struct GroupTiles {
-    const int* tileGroup;   // matrix (K^2 group) of each CTA tile
-    const int* tileColumn;  // first complex column of each tile
-    const int* tileCount;   // complex columns in each tile (<= tile width)
+    const int* tileGroup;     // K^2 group of each CTA tile
+    const int* tileColumn;    // first global (member tiles) or virtual column of each tile
+    const int* tileCount;     // columns in each tile (<= tile width)
+    const int* tilePer;       // virtual tiles: groupColumns of the tile's group
+    const int* tileFirst;     // virtual tiles: groupFirst of the tile's group
     int tiles;
+    long long memberColumns;  // complex columns per member
+    long long matrixStride;   // elements between group matrices (0: one matrix for all groups)
+    bool virtualColumns;      // the numbering of tileColumn
 };
 
 // Operand element: complex interleaved (im == nullptr) or split re/im arrays.
@@ -86,8 +102,8 @@ cudaError_t tc_gemm_build_images(const float* natural, int groups, int R, int S,
 int tc_gemm_unit_tiles();
 cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream);
 
-// inBins / outBins (optional): operands in a bin array; the SIMT form
-// supports them for a single ensemble member (column = mode * fields + field).
+// inBins / outBins (optional): cell-addressed operands (BinBoundary) instead of
+// the compact [column][len] arrays.
 cudaError_t launch_grouped_gemm(GemmPrecision p, int R, int S, const void* matrices, const GroupTiles& tiles,
                                 ComplexOperand in, ComplexOperand out, cudaStream_t stream,
                                 const BinBoundary* inBins = nullptr, const BinBoundary* outBins = nullptr);
