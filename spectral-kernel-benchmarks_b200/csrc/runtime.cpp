@@ -333,11 +333,17 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
         padded += (static_cast<std::uint64_t>(n) + width - 1) / width * width;
     }
     virtualTiles_ = members > 1 && used < 0.9 * static_cast<double>(padded);
-    tileTables_.resize(members);
-    for (std::uint64_t m = 1; m <= members; ++m) {
-        // Launch order member-major (by the member of a tile's first column,
-        // then group), as consecutive CTAs then stream through one member's
-        // operands; virtual tiles of a group still run on across members.
+    // Launch order member-major (by the member of a tile's first column, then
+    // group), as consecutive CTAs then stream through one member's operands;
+    // virtual tiles of a group still run on across members.  The member tiles
+    // of the first m members are then a prefix of the full table, so one table
+    // with per-count prefix lengths serves every member count; virtual tiles
+    // need a table per count.
+    const std::uint64_t tables = virtualTiles_ ? members : 1;
+    tileTables_.resize(tables);
+    tilePrefix_.assign(members, 0);
+    for (std::uint64_t ti = 0; ti < tables; ++ti) {
+        const std::uint64_t m = virtualTiles_ ? ti + 1 : members;
         std::vector<std::array<std::uint64_t, 3>> order;  // (member, group, first column in the group's list)
         for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
             const std::uint64_t per = static_cast<std::uint64_t>(gc[gi]);
@@ -365,13 +371,19 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
             tp.push_back(gc[gi]);
             tf.push_back(gf[gi]);
         }
-        TileTable& t = tileTables_[m - 1];
+        TileTable& t = tileTables_[ti];
         t.group = upload_vector(tg);
         t.column = upload_vector(tc);
         t.count = upload_vector(tn);
         t.per = upload_vector(tp);
         t.first = upload_vector(tf);
         t.tiles = static_cast<int>(tg.size());
+        if (virtualTiles_) {
+            tilePrefix_[m - 1] = t.tiles;
+        } else {
+            for (const auto& o : order) ++tilePrefix_[o[0]];
+            for (std::uint64_t mm = 1; mm < members; ++mm) tilePrefix_[mm] += tilePrefix_[mm - 1];
+        }
     }
     matrixStride_ = common ? 0 : static_cast<long long>(matrixElems);
     if (p == GemmPrecision::f64) {
@@ -466,9 +478,10 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
     // SIMT tiles of the table for this member count; cell-addressed operands
     // decompose a tile column's global plan column into (member, mode, field)
     // with the plan's columns per member.
-    const TileTable& table = tileTables_[members - 1];
+    const TileTable& table = tileTables_[virtualTiles_ ? members - 1 : 0];
     const GroupTiles t{table.group.get<int>(), table.column.get<int>(), table.count.get<int>(), table.per.get<int>(),
-                       table.first.get<int>(), table.tiles, memberColumns_, matrixStride_, virtualTiles_};
+                       table.first.get<int>(), tilePrefix_[members - 1], memberColumns_, matrixStride_,
+                       virtualTiles_};
     BinBoundary ib, ob;
     if (inBins != nullptr) {
         ib = *inBins;

@@ -193,14 +193,15 @@ private:
     long long memberColumns_ = 0;
     long long matrixStride_ = 0;  // SIMT form: elements between group matrices (0: one common matrix)
     DeviceBuffer matrices_;
-    // SIMT tiles over each group's member-concatenated columns, one table per
-    // active member count 1..members.
+    // SIMT tiles: one member-major table whose first tilePrefix_[m - 1] tiles
+    // cover m members, or (virtual numbering) one table per member count.
     struct TileTable {
         DeviceBuffer group, column, count, per, first;
         int tiles = 0;
     };
     std::vector<TileTable> tileTables_;
-    bool virtualTiles_ = false;  // SIMT tile numbering (GroupTiles::virtualColumns)
+    std::vector<int> tilePrefix_;  // tiles launched for 1..members members
+    bool virtualTiles_ = false;    // SIMT tile numbering (GroupTiles::virtualColumns)
     long long imageStride_ = 0;  // tensor-core form: bytes between group images (0: one common image)
     // Tensor-core work units, one table per active member count 1..members.
     struct UnitTable {
