@@ -1,6 +1,7 @@
 #include "runtime.hpp"
 
 #include "columns_warp.hpp"
+#include "simt_tiles.hpp"
 
 #include <algorithm>
 #include <array>
@@ -320,70 +321,28 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
         gf[gi] = static_cast<int>(groups[gi].first * fields);
     }
     groupColumnsHost_ = gc;
-    // Member tiles unless they would run less than 90 % full and the plan has
-    // several members; then virtual tiles over each group's member-concatenated
-    // columns (measured at 512²,
-    // Nz 129, 8 members, FP64: forward 6.1 -> 4.5 ms with 4 targets, the
-    // two-family GEMMs 23.2 / 11.3 -> 21.5 / 4.5 ms; the 15-field inverse,
-    // 93 % full as member tiles, ran 17.0 ms as member tiles and 20.4 as
-    // virtual ones).
-    std::uint64_t used = 0, padded = 0;
-    for (const int n : gc) {
-        used += static_cast<std::uint64_t>(n);
-        padded += (static_cast<std::uint64_t>(n) + width - 1) / width * width;
-    }
-    virtualTiles_ = members > 1 && used < 0.9 * static_cast<double>(padded);
-    // Launch order member-major (by the member of a tile's first column, then
-    // group), as consecutive CTAs then stream through one member's operands;
-    // virtual tiles of a group still run on across members.  The member tiles
-    // of the first m members are then a prefix of the full table, so one table
-    // with per-count prefix lengths serves every member count; virtual tiles
-    // need a table per count.
+    // Member tiles unless they would run under 90 % full in a plan of several
+    // members; then virtual tiles over each group's member-concatenated columns
+    // (measured at 512², Nz 129, 8 members, FP64: forward 6.1 -> 4.5 ms with 4
+    // targets, the two-family GEMMs 23.2 / 11.3 -> 21.9 / 4.6 ms; the 15-field
+    // inverse, 94 % full as member tiles, ran 17.0 ms as member tiles and 20.4
+    // as virtual ones).  Member tiles: one table whose prefixes serve smaller
+    // member counts; virtual tiles: one table per member count.
+    virtualTiles_ = simt_virtual_tiles(gc, members, width);
     const std::uint64_t tables = virtualTiles_ ? members : 1;
     tileTables_.resize(tables);
     tilePrefix_.assign(members, 0);
     for (std::uint64_t ti = 0; ti < tables; ++ti) {
         const std::uint64_t m = virtualTiles_ ? ti + 1 : members;
-        std::vector<std::array<std::uint64_t, 3>> order;  // (member, group, first column in the group's list)
-        for (std::uint64_t gi = 0; gi < groups.size(); ++gi) {
-            const std::uint64_t per = static_cast<std::uint64_t>(gc[gi]);
-            if (virtualTiles_) {
-                for (std::uint64_t c = 0; c < m * per; c += width) order.push_back({c / per, gi, c});
-            } else {
-                for (std::uint64_t mm = 0; mm < m; ++mm)
-                    for (std::uint64_t c = 0; c < per; c += width) order.push_back({mm, gi, mm * per + c});
-            }
-        }
-        std::sort(order.begin(), order.end());
-        std::vector<int> tg, tc, tn, tp, tf;
-        for (const auto& o : order) {
-            const std::uint64_t mm = o[0], gi = o[1], c = o[2];
-            const std::uint64_t per = static_cast<std::uint64_t>(gc[gi]);
-            tg.push_back(static_cast<int>(gi));
-            if (virtualTiles_) {
-                tc.push_back(static_cast<int>(c));
-                tn.push_back(static_cast<int>(std::min<std::uint64_t>(width, m * per - c)));
-            } else {
-                const std::uint64_t within = c - mm * per;
-                tc.push_back(static_cast<int>(mm * perMember + static_cast<std::uint64_t>(gf[gi]) + within));
-                tn.push_back(static_cast<int>(std::min<std::uint64_t>(width, per - within)));
-            }
-            tp.push_back(gc[gi]);
-            tf.push_back(gf[gi]);
-        }
+        const SimtTileTable h = simt_tiles(gc, gf, perMember, m, width, virtualTiles_, &tilePrefix_);
         TileTable& t = tileTables_[ti];
-        t.group = upload_vector(tg);
-        t.column = upload_vector(tc);
-        t.count = upload_vector(tn);
-        t.per = upload_vector(tp);
-        t.first = upload_vector(tf);
-        t.tiles = static_cast<int>(tg.size());
-        if (virtualTiles_) {
-            tilePrefix_[m - 1] = t.tiles;
-        } else {
-            for (const auto& o : order) ++tilePrefix_[o[0]];
-            for (std::uint64_t mm = 1; mm < members; ++mm) tilePrefix_[mm] += tilePrefix_[mm - 1];
-        }
+        t.group = upload_vector(h.group);
+        t.column = upload_vector(h.column);
+        t.count = upload_vector(h.count);
+        t.per = upload_vector(h.per);
+        t.first = upload_vector(h.first);
+        t.tiles = static_cast<int>(h.group.size());
+        if (virtualTiles_) tilePrefix_[m - 1] = t.tiles;
     }
     matrixStride_ = common ? 0 : static_cast<long long>(matrixElems);
     if (p == GemmPrecision::f64) {
