@@ -393,9 +393,11 @@ SKB_API int skb_flux_replay_graph(skb_flux* p, void* stream);
 
 /* ---------------------------------------------------------- autotuner */
 /* The project autotuner picks the fused flux path's launch shapes (work-unit
- * size of each tensor-core GEMM: 4, 8, 16 or 32 M-tiles; kernel form of each
- * 512-point band column stage: direct or warp-per-plane) by timing every
- * candidate with CUDA events on the caller's device buffers.  Choices are
+ * size of each tensor-core GEMM: 4, 8, 16 or 32 M-tiles; z-planes per CTA of
+ * the fused row kernel: 4, 8 or 16; kernel form of each 512-point band column
+ * stage: direct, warp-per-plane, persistent direct, or direct at four CTAs
+ * per SM) by timing every candidate with CUDA events on the caller's device
+ * buffers.  Choices are
  * cached per (stage shape, device) for the process and, when the environment
  * variable SKB_TUNE_CACHE names a file, in that file (one "<value> <ms> <key>"
  * line per choice); every flux handle created afterwards with the same shape
