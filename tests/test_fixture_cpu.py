@@ -2,7 +2,9 @@
 on CPU: loader round trip, the reference's validation rules, and the oracle's
 two-family flux against its one-family form."""
 
+import os
 import struct
+import subprocess
 
 import numpy as np
 import pytest
@@ -73,6 +75,52 @@ def test_validation_rejects_a_missing_mode(tmp_path):
              np.zeros((H, 4, 4), complex))
     with pytest.raises(fx.FixtureError, match="missing a retained horizontal mode key"):
         fx.load(path)
+
+
+CLI = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "spectral-kernel-benchmarks_b200",
+                   "skbench-cuda")
+
+
+def _cli_rejects(path, message):
+    out = subprocess.run([CLI, "run", "--kernel", "production-lifetime-flux", "--spectral-flux-fixture", str(path)],
+                         capture_output=True, text=True, timeout=60)
+    assert out.returncode == 2, out.stdout + out.stderr
+    assert message in out.stderr
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="skbench-cuda is not built")
+@pytest.mark.parametrize("edit,message", [
+    (lambda d: d.__setitem__(slice(0, 8), b"SKFXP002"), "wrong magic"),
+    (lambda d: d.__setitem__(slice(16, 20), struct.pack("<I", 0)), "not authoritative"),
+    (lambda d: d.extend(b"\0"), "trailing bytes"),
+    (lambda d: d.__delitem__(slice(len(d) - 16, len(d))), "truncated"),
+])
+def test_cli_loader_rejects_like_the_python_one(tmp_path, edit, message):
+    """The command line's C++ reader (harness/fixture.cpp) applies the same
+    checks, before any device work, with the same reasons."""
+    bad = _corrupt(tmp_path, edit)
+    with pytest.raises(fx.FixtureError, match=message):
+        fx.load(bad)
+    _cli_rejects(bad, message)
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="skbench-cuda is not built")
+def test_cli_loader_rejects_a_wrong_family_map_and_a_missing_mode(tmp_path):
+    modes, fam, keys = families_canonical(8, 7, 3)
+    H = len(modes)
+    group_of = np.repeat(np.arange(len(fam["group_modes"])), fam["group_modes"].astype(np.int64))
+    wrong = list(fx.INPUT_FAMILIES)
+    wrong[0] = 1
+    path = tmp_path / "map.bin"
+    fx.write(path, 8, 7, np.stack([modes.k, modes.l], 1), group_of, keys, fam["forward"], fam["inverse"],
+             np.zeros((H, 15, 4), complex), np.zeros((H, 4, 4), complex), input_family=wrong)
+    _cli_rejects(path, "input field-to-operator map")
+    k = np.stack([modes.k, modes.l], 1).copy()
+    k[-1] = (99, 99)
+    path = tmp_path / "mode.bin"
+    fx.write(path, 8, 7, k, group_of, keys, fam["forward"], fam["inverse"], np.zeros((H, 15, 4), complex),
+             np.zeros((H, 4, 4), complex))
+    _cli_rejects(path, "missing a retained horizontal mode key")
 
 
 def test_two_family_oracle_reduces_to_the_one_family_flux():
