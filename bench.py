@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--skip-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes instead of the autotuner's choices")
+    p.add_argument("--families", action="store_true",
+                   help="the authoritative two-family flux (wave-f / wave-g operators) with seeded stand-in "
+                        "matrices over the K^2 groups")
     p.add_argument("--serve", action="store_true",
                    help="serving benchmark: Poisson arrivals over mixed grid sizes with resident states")
     p.add_argument("--serve-requests", type=int, default=600)
@@ -203,12 +206,31 @@ def ncu_traffic(kernel_stage):
 
 # ---------------------------------------------------------------- CUDA arm
 
+def synthetic_families(n, nz, seed=5):
+    """Seeded stand-ins for the WVM wave-f / wave-g operator families (the
+    prepared WVM exports are not available): over the grid's K^2 groups, per
+    family and group, Gaussian forward [j][z] and inverse [z][j] matrices
+    scaled by 1/sqrt(inner size), with the reference's field-to-family maps."""
+    import skb_cuda as S
+    import skb_cuda.fixture as fx
+
+    w = S.Workload(n, n, nz, 1)
+    counts = np.array([g.mode_count for g in S.squared_wavenumber_groups(w)], dtype=np.uint64)
+    rng = np.random.default_rng(seed)
+    groups, nj = len(counts), w.nj
+    return {"group_modes": counts,
+            "forward": [rng.standard_normal((groups, nj, nz)) / np.sqrt(nz) for _ in range(2)],
+            "inverse": [rng.standard_normal((groups, nz, nj)) / np.sqrt(nj) for _ in range(2)],
+            "input_family": fx.INPUT_FAMILIES, "target_family": fx.TARGET_FAMILIES}
+
+
 def cuda_arm(args, dist):
     import skb_cuda as S
 
     S.set_device(dist.local)
     mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
-    flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode)
+    families = synthetic_families(args.n, args.nz) if args.families else None
+    flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode, families=families)
     mode_name = {"split": "split-tf32x3"}.get(args.mode, args.mode)
     dtype = flux.device_dtype
     x = power_law_inputs(args.n, args.nz, args.members, seed=129 + dist.rank)
@@ -252,7 +274,8 @@ def cuda_arm(args, dist):
     rel_err = None
     if mode != S.FLUX_FP64_PLAIN:
         out = dout.download(dtype, flux.output_elements).astype(np.complex128)
-        ref_flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=S.FLUX_FP64_PLAIN)
+        ref_flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=S.FLUX_FP64_PLAIN,
+                          families=families)
         ref = ref_flux.execute(x)
         num = float(np.linalg.norm(out - ref))
         den = float(np.linalg.norm(ref))
@@ -304,9 +327,11 @@ def cuda_arm(args, dist):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64" if mode == S.FLUX_FP64_PLAIN else ("f32" if mode == S.FLUX_FP32 else "tf32x3+f32"),
-        "data": "synthetic (seeded k^-3 power-law modal spectra, K^2 pair-rotation vertical family)",
-        "config": {"workload": f"15->4 flux {args.n}x{args.n}, Nz={args.nz}, 4 targets, {args.members} members "
-                               "per launch, CUDA graph replay",
+        "data": "synthetic (seeded k^-3 power-law modal spectra, "
+                + ("seeded Gaussian wave-f / wave-g operator families over the K^2 groups)" if families else
+                   "K^2 pair-rotation vertical family)"),
+        "config": {"workload": f"15->4 {'two-family ' if families else ''}flux {args.n}x{args.n}, Nz={args.nz}, "
+                               f"4 targets, {args.members} members per launch, CUDA graph replay",
                    "n": args.n, "nz": args.nz, "targets": 4, "members_per_gpu": args.members, "mode": mode_name,
                    "evals_per_step_per_gpu": args.members, "l2": "inputs larger than L2 (%.2f GB modal input)"
                    % (din.nbytes / 1e9), "parallelism": f"replicas x{dist.world}",
