@@ -138,3 +138,21 @@ def test_two_family_oracle_reduces_to_the_one_family_flux():
     a = orc.flux(n, nz, x, families=fam)
     b = orc.flux(n, nz, x)
     assert orc.max_rel_error(a, b) <= 1e-14
+
+
+@pytest.mark.parametrize("change,message", [
+    (lambda fam, o: o.update(targets=3), "15 -> 4"),
+    (lambda fam, o: fam.update(group_modes=np.concatenate([[0], fam["group_modes"]]).astype(np.uint64)),
+     "nonempty"),
+    (lambda fam, o: fam.update(group_modes=np.zeros(0, np.uint64)), "operator groups"),
+])
+def test_family_flux_arguments_are_refused_before_device_work(change, message):
+    """skb_flux_create_families checks its arguments (the reference's
+    std::invalid_argument cases) before it allocates anything on a device."""
+    import skb_cuda
+
+    _, fam, _ = families_canonical(8, 7, 3)
+    opts = {"targets": 4}
+    change(fam, opts)
+    with pytest.raises(ValueError, match=message):
+        skb_cuda.Flux(8, 7, targets=opts["targets"], members=1, mode=skb_cuda.FLUX_FP64_PLAIN, families=fam)
