@@ -105,6 +105,14 @@ def test_invalid_arguments_raise_value_error():
         skb_cuda.make_fixture(skb_cuda.Workload(8, 8, 0, 2), 2, 1)
 
 
+def test_type1_handle_arguments_are_refused_before_device_work():
+    """skb_cs_vertical_create: rows > 0 and Nz in [3, 16385] (a DCT-I needs
+    two intervals), checked before any stream or allocation."""
+    for rows, nz in ((4, 2), (0, 9), (4, 16386)):
+        with pytest.raises(ValueError):
+            skb_cuda.ConstantStratificationVertical(rows, nz)
+
+
 def test_gpu_calls_fail_loudly_without_a_device():
     if skb_cuda_has_device():
         pytest.skip("a CUDA device is present")
