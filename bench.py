@@ -9,6 +9,13 @@ flux evaluations per second (one evaluation = one member's 15 -> 4 flux).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--mode split|fp32|fp64]
     python bench.py --impl reference ...     # CPU arm, rank 0 only
+    python bench.py --serve [--serve-rate R]  # serving benchmark on its own line
+    python bench.py --profile-run --members 2 --repeat 1   # device path for a kernel profiler
+
+The default line also times the FP64-plain flux on the same inputs (the
+ratio's denominator) and runs a short serving pass: the same seeded Poisson
+stream of mixed requests through the split and the FP64-plain paths, whose
+p50 / p99 latencies it reports.
 
 Under torchrun every rank runs an independent replica (the path shards over
 members with no exchange); a gloo barrier brackets the timed region and the
@@ -48,9 +55,18 @@ def parse():
     p.add_argument("--n", type=int, default=512)
     p.add_argument("--nz", type=int, default=129)
     p.add_argument("--members", type=int, default=8)
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--skip-cpu-baseline", action="store_true")
     p.add_argument("--skip-e2e", action="store_true")
+    p.add_argument("--skip-fp64", action="store_true",
+                   help="do not time the FP64-plain flux beside the split one")
+    p.add_argument("--skip-serve-pass", action="store_true",
+                   help="do not run the short same-stream serving pass (split and FP64-plain)")
+    p.add_argument("--profile-run", action="store_true",
+                   help="for a kernel profiler: run the device path (no graph) --repeat times, print the "
+                        "per-stage event timing of one more run as JSON, and exit")
+    p.add_argument("--repeat", type=int, default=1)
+    p.add_argument("--no-stage-times", action="store_true", help="with --profile-run: skip the extra timed run")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes instead of the autotuner's choices")
     p.add_argument("--families", action="store_true",
@@ -62,6 +78,9 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=400.0, help="mean arrivals per second")
     p.add_argument("--serve-batch", type=int, default=8)
     p.add_argument("--serve-states", type=int, default=8, help="resident member states per size class")
+    p.add_argument("--serve-pass-rate", type=float, default=150.0,
+                   help="arrival rate of the serving pass that runs with the default benchmark")
+    p.add_argument("--serve-pass-requests", type=int, default=300)
     return p.parse_args()
 
 
@@ -224,6 +243,65 @@ def synthetic_families(n, nz, seed=5):
             "input_family": fx.INPUT_FAMILIES, "target_family": fx.TARGET_FAMILIES}
 
 
+def timed_replays(S, flux, steps, dist):
+    """Device time of `steps` graph replays on the flux's stream (CUDA events),
+    bracketed by a barrier and a device synchronisation; max over ranks."""
+    stream = flux.stream
+    timer = S.Timer()
+    dist.barrier()
+    S.synchronize()
+    timer.start(stream)
+    for _ in range(steps):
+        flux.replay_graph()
+    timer.stop(stream)
+    S.synchronize()
+    dist.barrier()
+    return dist.max(timer.elapsed_ms() / steps)
+
+
+def fp64_plain_leg(S, args, x, families, dist):
+    """The FP64-plain flux (the north-star denominator) on the same inputs, by
+    the same method as the split line: graph capture, warm-up, `steps` timed
+    replays.  Returns (evals/s, ms per step, its output)."""
+    ref_flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=S.FLUX_FP64_PLAIN, families=families)
+    din = S.DeviceArray.from_numpy(np.ascontiguousarray(x, dtype=np.complex128))
+    dout = S.DeviceArray(ref_flux.output_elements * 16)
+    ref_flux.execute_device(din.ptr, dout.ptr)
+    ref_flux.capture_graph(din.ptr, dout.ptr)
+    for _ in range(args.warmup):
+        ref_flux.replay_graph()
+    S.synchronize()
+    ms = timed_replays(S, ref_flux, args.steps, dist)
+    ref_flux.check_device()
+    out = dout.download(np.complex128, ref_flux.output_elements)
+    ref_flux.close()
+    din.free()
+    dout.free()
+    return dist.world * args.members * 1000.0 / ms, ms, out
+
+
+def profile_run(args, dist):
+    """Device-path executions for a kernel profiler (no graph, so each launch
+    is visible), then the per-stage event timing of one more execution."""
+    import skb_cuda as S
+
+    S.set_device(dist.local)
+    mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
+    families = synthetic_families(args.n, args.nz) if args.families else None
+    flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode, families=families)
+    x = power_law_inputs(args.n, args.nz, args.members, seed=129 + dist.rank)
+    din = S.DeviceArray.from_numpy(x.astype(flux.device_dtype))
+    dout = S.DeviceArray(flux.output_elements * np.dtype(flux.device_dtype).itemsize)
+    for _ in range(args.repeat):
+        flux.execute_device(din.ptr, dout.ptr)
+    S.synchronize()
+    flux.check_device()
+    if args.no_stage_times or dist.rank != 0:
+        return None
+    return {"profile_run": {"n": args.n, "nz": args.nz, "members": args.members, "mode": args.mode,
+                            "repeat": args.repeat}, "stages": flux.profile(din.ptr, dout.ptr)}
+
+
 def cuda_arm(args, dist):
     import skb_cuda as S
 
@@ -236,7 +314,6 @@ def cuda_arm(args, dist):
     x = power_law_inputs(args.n, args.nz, args.members, seed=129 + dist.rank)
     din = S.DeviceArray.from_numpy(x.astype(dtype))
     dout = S.DeviceArray(flux.output_elements * np.dtype(dtype).itemsize)
-    stream = flux.stream
 
     # Launch shapes from the project autotuner (measured on these buffers,
     # outside the timed region), then warm-up through the graph path
@@ -252,35 +329,37 @@ def cuda_arm(args, dist):
         flux.replay_graph()
     S.synchronize()
 
-    timer = S.Timer()
     with ClockSampler(dist.local) as clocks:
-        dist.barrier()
-        S.synchronize()
-        timer.start(stream)
-        for _ in range(args.steps):
-            flux.replay_graph()
-        timer.stop(stream)
-        S.synchronize()
-        dist.barrier()
-    ms = timer.elapsed_ms() / args.steps
+        ms_max = timed_replays(S, flux, args.steps, dist)
     flux.check_device()
-    ms_max = dist.max(ms)
     value = dist.world * args.members * 1000.0 / ms_max
 
     stages = flux.profile(din.ptr, dout.ptr)
     info = flux.info()
 
-    # Accuracy of this run's mode against the FP64-plain CUDA path on the same inputs.
-    rel_err = None
+    # The FP64-plain flux on the same inputs, timed the same way (the ratio's
+    # denominator), and this run's error against it.
+    rel_err, fp64 = None, None
     if mode != S.FLUX_FP64_PLAIN:
+        flux.replay_graph()
+        S.synchronize()
         out = dout.download(dtype, flux.output_elements).astype(np.complex128)
-        ref_flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=S.FLUX_FP64_PLAIN,
-                          families=families)
-        ref = ref_flux.execute(x)
+        if args.skip_fp64:
+            ref_flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=S.FLUX_FP64_PLAIN,
+                              families=families)
+            ref = ref_flux.execute(x)
+            ref_flux.close()
+        else:
+            with ClockSampler(dist.local) as fp64_clocks:
+                fp64_value, fp64_ms, ref = fp64_plain_leg(S, args, x, families, dist)
+            fp64 = {"evals_per_s": fp64_value, "ms_per_step": fp64_ms, "steps": args.steps,
+                    "warmup": args.warmup, "dtype": "f64", "clocks": fp64_clocks.summary()}
         num = float(np.linalg.norm(out - ref))
         den = float(np.linalg.norm(ref))
         rel_err = num / den if den else num
-        del ref_flux
+        if fp64 is not None:
+            fp64["split_rel_l2_err"] = rel_err
+            fp64["split_max_rel_err"] = float(np.max(np.abs(out - ref)) / max(1.0, float(np.max(np.abs(ref)))))
 
     # End to end through the public host API: pinned FP64 host arrays, H2D,
     # compute, D2H every step.
@@ -302,6 +381,20 @@ def cuda_arm(args, dist):
                "ms_per_step": e2e_ms, "steps": args.e2e_steps}
         hin.free()
         hout.free()
+
+    # Serving: the same seeded Poisson stream of mixed requests through the
+    # split and the FP64-plain paths (p50 / p99 latency of the metric).
+    serving = None
+    if not args.skip_serve_pass and not args.families:
+        flux.close()
+        din.free()
+        dout.free()
+        serving = {"arrival_rate_per_s": args.serve_pass_rate, "requests": args.serve_pass_requests,
+                   "mix": "40% 128x128xNz33 12->3, 40% 256x256xNz65 12->3, 20% 512x512xNz129 15->4",
+                   "max_batch": args.serve_batch, "resident_states_per_class": 2}
+        for name, m in (("split", S.FLUX_SPLIT_TF32X3), ("fp64", S.FLUX_FP64_PLAIN)):
+            r = serving_run(S, m, args.serve_pass_rate, args.serve_pass_requests, args.serve_batch, 2, dist)
+            serving[name] = {k: r[k] for k in ("p50_ms", "p99_ms", "throughput_evals_per_s", "classes", "batches")}
 
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.skip_cpu_baseline:
@@ -338,6 +431,10 @@ def cuda_arm(args, dist):
                    "autotune": {"seconds": round(tune_s, 3),
                                 "choices": {k.split(" | ")[0]: v[0] for k, v in tuned.items()}}},
         "rel_err_vs_fp64": rel_err,
+        "fp64_plain": fp64,
+        "split_over_fp64": (value / fp64["evals_per_s"]) if fp64 else None,
+        "p99_ms": serving["split"]["p99_ms"] if serving else None,
+        "serving": serving,
         "roofline": {"bound": "hbm", "kernel": dominant["name"], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": ncu_traffic(dominant["name"]),
@@ -360,27 +457,25 @@ def cuda_arm(args, dist):
 SERVE_CLASSES = [(128, 33, 3, 0.4), (256, 65, 3, 0.4), (512, 129, 4, 0.2)]
 
 
-def serve_arm(args, dist):
-    """Requests with seeded exponential inter-arrival times pick a size class
-    by the mix above and a resident member state of that class; the server
-    batches what queues per class.  Latency = submit -> result in host memory."""
-    import skb_cuda as S
-
-    S.set_device(dist.local)
-    mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
-    classes = [(n, nz, t, args.serve_batch, mode) for n, nz, t, _ in SERVE_CLASSES]
+def serving_run(S, mode, rate, requests, batch, states_per_class, dist, classes_mix=None):
+    """Requests with seeded exponential inter-arrival times (`rate` per second)
+    pick a size class by the mix and a resident member state of that class; the
+    server batches what queues per class.  Latency = submit -> result in host
+    memory.  The stream (classes, gaps, states) depends only on the seeds, so
+    two modes see the same requests at the same times."""
+    mix = classes_mix or SERVE_CLASSES
+    classes = [(n, nz, t, batch, mode) for n, nz, t, _ in mix]
     server = S.Server(classes, hbm_budget_bytes=64 << 30, max_slots_per_class=2)
     states = []
-    for c, (n, nz, t, _) in enumerate(SERVE_CLASSES):
+    for c, (n, nz, t, _) in enumerate(mix):
         states.append([server.load_state(c, power_law_inputs(n, nz, 1, targets=t, seed=1000 * c + i + 977 * dist.rank))
-                       for i in range(args.serve_states)])
+                       for i in range(states_per_class)])
     rng = np.random.default_rng(7 + dist.rank)
-    picks = rng.choice(len(SERVE_CLASSES), size=args.serve_requests, p=[c[3] for c in SERVE_CLASSES])
-    gaps = rng.exponential(1.0 / args.serve_rate, size=args.serve_requests)
-    outputs = [S.PinnedArray(np.complex128, server.sizes[c][1]) for c in range(len(SERVE_CLASSES))
-               for _ in range(2)]
+    picks = rng.choice(len(mix), size=requests, p=[c[3] for c in mix])
+    gaps = rng.exponential(1.0 / rate, size=requests)
+    outputs = [S.PinnedArray(np.complex128, server.sizes[c][1]) for c in range(len(mix)) for _ in range(2)]
     # Warm-up: every class once, alone.
-    for c in range(len(SERVE_CLASSES)):
+    for c in range(len(mix)):
         server.wait(server.submit_state(states[c][0], outputs[2 * c].array), timeout=300)
     base = server.stats()
     dist.barrier()
@@ -398,29 +493,44 @@ def serve_arm(args, dist):
                     time.sleep(due - now - 1e-4)
             # Two pinned result buffers per class, reused: the results of
             # this benchmark are not read, only their arrival times.
-            tickets.append((c, server.submit_state(states[c][i % args.serve_states], outputs[2 * c + i % 2].array)))
+            tickets.append((c, server.submit_state(states[c][i % states_per_class], outputs[2 * c + i % 2].array)))
         lat = [(c, server.wait(t, timeout=600)[1]) for c, t in tickets]
         t1 = time.perf_counter()
     stats = server.stats()
     server.close()
     for o in outputs:
         o.free()
-    if dist.rank != 0:
-        return None
     all_ms = np.array([x for _, x in lat])
     span = t1 - t0
     per_class = {}
-    for c, (n, nz, t, share) in enumerate(SERVE_CLASSES):
+    for c, (n, nz, t, share) in enumerate(mix):
         v = np.array([x for k, x in lat if k == c])
         per_class[f"{n}x{n}xNz{nz}_f{t}"] = {
             "requests": int(v.size), "p50_ms": float(np.percentile(v, 50)) if v.size else None,
             "p99_ms": float(np.percentile(v, 99)) if v.size else None,
             "evals_per_s": float(v.size / span)}
+    return {"p50_ms": float(np.percentile(all_ms, 50)), "p99_ms": float(np.percentile(all_ms, 99)),
+            "mean_ms": float(np.mean(all_ms)), "throughput_evals_per_s": float(len(all_ms) / span),
+            "classes": per_class, "batches": stats["batches"] - base["batches"],
+            "server": {"batches": stats["batches"] - base["batches"], "slots": stats["slots"],
+                       "slot_bytes": stats["slot_bytes"], "state_bytes": stats["state_bytes"]},
+            "clocks": clocks.summary()}
+
+
+def serve_arm(args, dist):
+    """The serving benchmark on its own line (p99 latency as the value)."""
+    import skb_cuda as S
+
+    S.set_device(dist.local)
+    mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
+    r = serving_run(S, mode, args.serve_rate, args.serve_requests, args.serve_batch, args.serve_states, dist)
+    if dist.rank != 0:
+        return None
     mode_name = {"split": "split-tf32x3"}.get(args.mode, args.mode)
     return {
         "metric": "serving p99 latency, mixed flux requests (40% 128²×33 f3, 40% 256²×65 f3, 20% 512²×129 f4)",
-        "value": float(np.percentile(all_ms, 99)), "unit": "ms", "n_gpus": dist.world,
-        "steps": args.serve_requests, "warmup": len(SERVE_CLASSES), "ms_per_step": float(np.mean(all_ms)),
+        "value": r["p99_ms"], "unit": "ms", "n_gpus": dist.world,
+        "steps": args.serve_requests, "warmup": len(SERVE_CLASSES), "ms_per_step": r["mean_ms"],
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if mode == S.FLUX_FP64_PLAIN else ("f32" if mode == S.FLUX_FP32 else "tf32x3+f32"),
         "data": "synthetic (seeded k^-3 power-law resident states, seeded Poisson arrivals)",
@@ -428,11 +538,9 @@ def serve_arm(args, dist):
                    "arrival_rate_per_s": args.serve_rate, "requests": args.serve_requests,
                    "max_batch": args.serve_batch, "resident_states_per_class": args.serve_states,
                    "parallelism": f"replicas x{dist.world}"},
-        "p50_ms": float(np.percentile(all_ms, 50)), "p99_ms": float(np.percentile(all_ms, 99)),
-        "throughput_evals_per_s": float(len(all_ms) / span), "classes": per_class,
-        "server": {"batches": stats["batches"] - base["batches"], "slots": stats["slots"],
-                   "slot_bytes": stats["slot_bytes"], "state_bytes": stats["state_bytes"]},
-        "clocks": clocks.summary(),
+        "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
+        "throughput_evals_per_s": r["throughput_evals_per_s"], "classes": r["classes"],
+        "server": r["server"], "clocks": r["clocks"],
     }
 
 
@@ -496,6 +604,8 @@ def main():
             line = reference_arm(args, dist)
         elif args.serve:
             line = serve_arm(args, dist)
+        elif args.profile_run:
+            line = profile_run(args, dist)
         else:
             line = cuda_arm(args, dist)
         if line is not None and dist.rank == 0:

@@ -191,14 +191,20 @@ SKB_API int skb_fft_embed_retained_device(skb_fft_provider* p, const skb_field_v
  * they run: a host that enforces its own device-memory budget through its own
  * allocator, or a plugin whose host forbids cudaMalloc / cudaFree inside its
  * compute callbacks (an allocation can fail once the budget is reserved, and
- * cudaFree stalls every stream on the device).  The result is that of
- * skb_fft_inverse_device for the same workload and precision; the spectrum is
- * preserved.  The scratch (twiddle tables and the column-transformed
+ * cudaFree stalls every stream on the device).  The result equals that of
+ * skb_fft_inverse_device for the same workload and precision to within
+ * rounding, not bit for bit: the twiddle tables here are computed on the
+ * device with sincospi, the handle's are built on the host (both are tested
+ * against the CPU oracle at 1e-12 relative for FP64 and 1e-5 for FP32).  The
+ * spectrum is preserved.  The scratch (twiddle tables and the column-transformed
  * spectrum) is a fixed 64 MiB device array inside this library, which every
  * GPU that loads the library holds until the process exits; a workload that
  * needs more is refused with SKB_ERR_INVALID_ARGUMENT.  The first call on each
  * device looks the array's address up and may make the driver load the
- * library's device code, so make that call before any stream capture begins.
+ * library's device code, so make that call before any stream capture begins;
+ * the address kept belongs to the device's current context, so after a
+ * cudaDeviceReset of that device the entry point must not be called on it again
+ * in the same process.
  * Each call writes everything it later reads, so nothing has to start at zero,
  * but all calls share the one array: calls whose GPU work overlaps (other
  * streams, other threads) race and corrupt each other; serialise them.

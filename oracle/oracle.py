@@ -223,6 +223,41 @@ def k2_family(w: Workload):
     return fwd.reshape(len(keys), nj, nz), inv.reshape(len(keys), nz, nj)
 
 
+def sturm_liouville_family(w: Workload, seed):
+    """The build-side seeded Sturm-Liouville vertical family (the perf-realistic
+    dense operators; the reference has none): per K^2 group, the lowest Nj
+    eigenvectors of the tridiagonal discretisation of -d/dz (1/N^2 d/dz) + 1e-3
+    K^2/N^2 on a unit-depth grid of Nz cells with Neumann ends, where
+    1/N^2 = exp(-(z_i - 1)/h) at cell interfaces z_i = i/Nz and h is the seeded
+    scale height.  Eigenvectors from LAPACK (scipy eigh_tridiagonal), ordered
+    by eigenvalue, signed so their first entry above 1e-12 in magnitude is
+    positive.  Returns (forward[g][j][z], inverse[g][z][j])."""
+    from scipy.linalg import eigh_tridiagonal
+
+    h = ctypes.c_double()
+    _check(library().oracle_sl_scale_height(U64(seed), ctypes.byref(h)))
+    keys, _, _ = k2_groups(w.nx, w.ny)
+    nz, nj = w.nz, w.nj
+    dz = 1.0 / nz
+    inv = np.exp(-(np.arange(nz + 1) * dz - 1.0) / h.value)
+    up = np.where(np.arange(nz) + 1 < nz, inv[1:], 0.0)
+    dn = np.where(np.arange(nz) > 0, inv[:-1], 0.0)
+    base = (up + dn) / (dz * dz)
+    mid = 0.5 * (inv[:-1] + inv[1:])
+    off = -inv[1:nz] / (dz * dz)
+    fwd = np.empty((len(keys), nj, nz))
+    for g, key in enumerate(keys):
+        k2 = 4.0 * np.pi * np.pi * float(key)
+        vals, vecs = eigh_tridiagonal(base + 1e-3 * k2 * mid, off)
+        vecs = vecs[:, np.argsort(vals, kind="stable")[:nj]].T
+        for j in range(nj):
+            first = np.flatnonzero(np.abs(vecs[j]) > 1e-12)
+            if first.size and vecs[j, first[0]] < 0:
+                vecs[j] = -vecs[j]
+        fwd[g] = vecs
+    return fwd, np.ascontiguousarray(fwd.transpose(0, 2, 1))
+
+
 def grouped_vertical(w: Workload, family, direction, data):
     """Per-group vertical projection (model.cpp:567-605 applied per K^2 group, as
     VerticalGemmProvider does, vertical_gemm.cpp:534-596).  forward: retained

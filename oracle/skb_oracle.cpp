@@ -397,4 +397,17 @@ int oracle_k2_vertical_family(std::uint64_t nz, std::uint64_t nj, const std::uin
     });
 }
 
+// The build-side Sturm-Liouville family (no counterpart in the reference)
+// draws its exponential N^2 scale height as the first value of
+// std::uniform_real_distribution<double>(0.1, 0.3) over std::mt19937_64(seed).
+// Only that draw needs the C++ library; the operator and its eigenvectors are
+// restated in oracle.py with LAPACK.
+int oracle_sl_scale_height(std::uint64_t seed, double* h) {
+    return guarded([&] {
+        std::mt19937_64 gen(seed);
+        std::uniform_real_distribution<double> dist(0.1, 0.3);
+        *h = dist(gen);
+    });
+}
+
 }  // extern "C"

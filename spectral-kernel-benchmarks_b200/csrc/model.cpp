@@ -7,6 +7,7 @@
 #include <random>
 #include <set>
 #include <stdexcept>
+#include <thread>
 
 namespace skb {
 namespace {
@@ -55,8 +56,8 @@ struct Fnv {
 
 void validate_workload(const Workload& w) {
     if (w.nx < 2 || w.ny < 2 || w.nz < 1 || w.fields < 1)
-        throw std::invalid_argument("Nx and Ny must be at least two; Nz and fields must be positive.");
-    if (!(w.lx > 0.0) || !(w.ly > 0.0)) throw std::invalid_argument("Horizontal domain lengths must be positive.");
+        throw std::invalid_argument("workload: need Nx >= 2, Ny >= 2, Nz >= 1 and fields >= 1");
+    if (!(w.lx > 0.0) || !(w.ly > 0.0)) throw std::invalid_argument("workload: Lx and Ly must be greater than zero");
 }
 
 std::vector<RetainedMode> retained_modes(const Workload& w) {
@@ -103,7 +104,7 @@ std::vector<RetainedMode> retained_modes(const Workload& w) {
 }
 
 std::vector<ModeGroup> squared_wavenumber_groups(const std::vector<RetainedMode>& modes) {
-    if (modes.empty()) throw std::invalid_argument("Squared-wavenumber grouping requires retained modes.");
+    if (modes.empty()) throw std::invalid_argument("K^2 grouping: the retained-mode list is empty");
     std::vector<ModeGroup> groups;
     std::set<std::uint64_t> closed;
     for (std::uint64_t i = 0; i < modes.size(); ++i) {
@@ -112,7 +113,7 @@ std::vector<ModeGroup> squared_wavenumber_groups(const std::vector<RetainedMode>
         const auto key = k * k + l * l;
         if (groups.empty() || groups.back().key != key) {
             if (closed.count(key))
-                throw std::invalid_argument("Equal squared-wavenumber modes are not contiguous in the retained order.");
+                throw std::invalid_argument("K^2 grouping: a K^2 key reappears after its group closed (modes with one key must be adjacent)");
             if (!groups.empty()) closed.insert(groups.back().key);
             groups.push_back({key, i, 1});
         } else {
@@ -299,40 +300,57 @@ VerticalFamily sturm_liouville_family(const Workload& w, const std::vector<ModeG
     const double dz = 1.0 / static_cast<double>(nz);
     std::vector<double> inv(nz + 1);  // 1/N^2 at cell interfaces
     for (int i = 0; i <= nz; ++i) inv[i] = std::exp(-(static_cast<double>(i) * dz - 1.0) / h);
-    for (std::uint64_t g = 0; g < fam.groups; ++g) {
-        const double k2 = 4.0 * kPi * kPi * static_cast<double>(groups[g].key);
-        std::vector<double> d(nz), e(nz, 0.0), z(static_cast<std::size_t>(nz) * nz, 0.0);
-        for (int i = 0; i < nz; ++i) {
-            const double up = i + 1 < nz ? inv[i + 1] : 0.0;  // Neumann top
-            const double dn = i > 0 ? inv[i] : 0.0;           // Neumann bottom
-            // K^2 enters weighted by 1/N^2, so the eigenvectors depend on the group.
-            d[i] = (up + dn) / (dz * dz) + 1e-3 * k2 * 0.5 * (inv[i] + inv[i + 1]);
-            if (i > 0) e[i] = -inv[i] / (dz * dz);
-            z[static_cast<std::size_t>(i) * nz + i] = 1.0;
-        }
-        tridiagonal_eigen(d, e, z, nz);
-        std::vector<int> order(nz);
-        for (int i = 0; i < nz; ++i) order[i] = i;
-        std::sort(order.begin(), order.end(), [&](int a, int b) { return d[a] < d[b]; });
-        double* F = fam.forward.data() + g * elems;
-        double* I = fam.inverse.data() + g * elems;
-        for (std::uint64_t j = 0; j < nj; ++j) {
-            const int col = order[j];
-            // Sign convention: first nonzero entry positive.
-            double sign = 1.0;
-            for (int r = 0; r < nz; ++r) {
-                if (std::fabs(z[static_cast<std::size_t>(r) * nz + col]) > 1e-12) {
-                    sign = z[static_cast<std::size_t>(r) * nz + col] < 0 ? -1.0 : 1.0;
-                    break;
+    // Groups are independent: split them over the host threads (set-up time
+    // only; 7,486 groups of Nz = 129 take about 30 s on one thread).
+    auto group_range = [&](std::uint64_t g0, std::uint64_t g1) {
+        for (std::uint64_t g = g0; g < g1; ++g) {
+            const double k2 = 4.0 * kPi * kPi * static_cast<double>(groups[g].key);
+            std::vector<double> d(nz), e(nz, 0.0), z(static_cast<std::size_t>(nz) * nz, 0.0);
+            for (int i = 0; i < nz; ++i) {
+                const double up = i + 1 < nz ? inv[i + 1] : 0.0;  // Neumann top
+                const double dn = i > 0 ? inv[i] : 0.0;           // Neumann bottom
+                // K^2 enters weighted by 1/N^2, so the eigenvectors depend on the group.
+                d[i] = (up + dn) / (dz * dz) + 1e-3 * k2 * 0.5 * (inv[i] + inv[i + 1]);
+                if (i > 0) e[i] = -inv[i] / (dz * dz);
+                z[static_cast<std::size_t>(i) * nz + i] = 1.0;
+            }
+            tridiagonal_eigen(d, e, z, nz);
+            std::vector<int> order(nz);
+            for (int i = 0; i < nz; ++i) order[i] = i;
+            std::sort(order.begin(), order.end(), [&](int a, int b) { return d[a] < d[b]; });
+            double* F = fam.forward.data() + g * elems;
+            double* I = fam.inverse.data() + g * elems;
+            for (std::uint64_t j = 0; j < nj; ++j) {
+                const int col = order[j];
+                // Sign convention: first nonzero entry positive.
+                double sign = 1.0;
+                for (int r = 0; r < nz; ++r) {
+                    if (std::fabs(z[static_cast<std::size_t>(r) * nz + col]) > 1e-12) {
+                        sign = z[static_cast<std::size_t>(r) * nz + col] < 0 ? -1.0 : 1.0;
+                        break;
+                    }
+                }
+                for (int r = 0; r < nz; ++r) {
+                    const double v = sign * z[static_cast<std::size_t>(r) * nz + col];
+                    F[j * fam.nz + r] = v;
+                    I[r * fam.nj + j] = v;
                 }
             }
-            for (int r = 0; r < nz; ++r) {
-                const double v = sign * z[static_cast<std::size_t>(r) * nz + col];
-                F[j * fam.nz + r] = v;
-                I[r * fam.nj + j] = v;
-            }
         }
+    };
+    const std::uint64_t threads =
+        std::min<std::uint64_t>(std::max(1u, std::thread::hardware_concurrency()), (fam.groups + 63) / 64);
+    if (threads <= 1) {
+        group_range(0, fam.groups);
+        return fam;
     }
+    std::vector<std::thread> pool;
+    const std::uint64_t per = (fam.groups + threads - 1) / threads;
+    for (std::uint64_t t = 0; t < threads; ++t) {
+        const std::uint64_t g0 = t * per, g1 = std::min(fam.groups, g0 + per);
+        if (g0 < g1) pool.emplace_back(group_range, g0, g1);
+    }
+    for (auto& th : pool) th.join();
     return fam;
 }
 

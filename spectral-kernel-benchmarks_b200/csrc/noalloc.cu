@@ -17,7 +17,10 @@
 // host it names a stand-in object), so the first call on each device, with
 // that device current, looks the address up with cudaGetSymbolAddress and
 // keeps it; that first call may also make the CUDA driver load this file's
-// device code, so make it before any stream capture begins.
+// device code, so make it before any stream capture begins.  The kept address
+// belongs to the device's current context: a host that calls cudaDeviceReset
+// on a device ends that context, and this entry point must not be called on
+// that device again in the same process.
 //
 // Each call writes, in stream order, the three twiddle tables and then every
 // entry of the intermediate column spectrum it reads, so nothing in the array
@@ -65,7 +68,20 @@ void* scratch_address() {
     return g_scratchAddress[device];
 }
 
-std::size_t round_up(std::size_t bytes) { return (bytes + 255) & ~std::size_t(255); }
+// Byte counts saturate at SIZE_MAX instead of wrapping, so a workload whose
+// Nz * fields (both unbounded) overflows the product is refused like any other
+// workload that needs more than the array holds.
+std::size_t mul_sat(std::size_t a, std::size_t b) {
+    std::size_t r = 0;
+    return __builtin_mul_overflow(a, b, &r) ? SIZE_MAX : r;
+}
+
+std::size_t add_sat(std::size_t a, std::size_t b) {
+    std::size_t r = 0;
+    return __builtin_add_overflow(a, b, &r) ? SIZE_MAX : r;
+}
+
+std::size_t round_up(std::size_t bytes) { return bytes > SIZE_MAX - 255 ? SIZE_MAX : (bytes + 255) & ~std::size_t(255); }
 
 // tw[k] = exp(-2 pi i k / n) for k in [0, n), the table layout the transform
 // kernels read.  sincospi of the exact dyadic argument 2k/n, rounded to T.
@@ -96,8 +112,12 @@ std::size_t static_inverse_scratch_limit() { return kScratchBytes; }
 std::size_t static_inverse_scratch_bytes(const Workload& w, Precision p) {
     const std::size_t complexBytes = 2 * element_bytes(p);
     const std::size_t half = std::max<std::uint64_t>(1, w.nx / 2);
-    return round_up(complexBytes * half) + round_up(complexBytes * w.nx) + round_up(complexBytes * w.ny) +
-           round_up(complexBytes * w.ny * w.nxHalf() * w.planes());
+    const std::size_t planes = mul_sat(w.nz, w.fields);
+    const std::size_t columns = mul_sat(mul_sat(mul_sat(complexBytes, w.ny), w.nxHalf()), planes);
+    std::size_t total = round_up(mul_sat(complexBytes, half));
+    total = add_sat(total, round_up(mul_sat(complexBytes, w.nx)));
+    total = add_sat(total, round_up(mul_sat(complexBytes, w.ny)));
+    return add_sat(total, round_up(columns));
 }
 
 void inverse_dense_static(const Workload& w, Precision p, const void* wvm, void* real, cudaStream_t s) {

@@ -70,7 +70,7 @@ HorizontalPlan::HorizontalPlan(const Workload& w, Precision p, bool pruned, std:
     const auto planStart = Clock::now();
     const auto modes = retained_modes(w);
     modeCount_ = modes.size();
-    if (pruned && modes.empty()) throw Error(-1, "The pruned provider requires retained modes.");
+    if (pruned && modes.empty()) throw Error(-1, "pruned provider: the workload retains no modes");
     keep_ = static_cast<int>(pruned ? active_columns(modes) : w.nxHalf());
     const auto columnsForTables = pruned ? static_cast<std::uint64_t>(keep_) : w.nxHalf();
     const auto tables = column_tables(w, modes, columnsForTables);

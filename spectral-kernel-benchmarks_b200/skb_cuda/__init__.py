@@ -929,10 +929,25 @@ class Flux:
         if families is None:
             check(library().skb_flux_create(ctypes.byref(opts), ctypes.byref(h)))
         else:
-            keep = [np.ascontiguousarray(families["group_modes"], dtype=np.uint64)]
+            keep = [np.ascontiguousarray(families["group_modes"], dtype=np.uint64).reshape(-1)]
+            groups, nj = len(keep[0]), (2 * (nz - 1) // 3 if nz >= 2 else 0)
+            # The C ABI copies groups * Nj * Nz values from each matrix pointer:
+            # refuse arrays of another shape here, before C reads past them.
+            expect = {"forward": (groups, nj, nz), "inverse": (groups, nz, nj)}
             for name in ("forward", "inverse"):
+                if len(families[name]) != 2:
+                    raise ValueError(f"families['{name}'] must hold the wave-f and wave-g matrices (2 entries)")
                 for f in range(2):
-                    keep.append(np.ascontiguousarray(families[name][f], dtype=np.float64))
+                    a = np.ascontiguousarray(families[name][f], dtype=np.float64)
+                    if a.size != int(np.prod(expect[name])) or (a.ndim == 3 and a.shape != expect[name]):
+                        raise ValueError(f"families['{name}'][{f}] has shape {a.shape}; expected {expect[name]} "
+                                         f"([group][{'j][z' if name == 'forward' else 'z][j'}] for {groups} groups, "
+                                         f"Nz={nz}, Nj={nj})")
+                    keep.append(a)
+            for name, count in (("input_family", 15), ("target_family", 4)):
+                if len(families[name]) != count:
+                    raise ValueError(f"families['{name}'] must map {count} slots to a family; got "
+                                     f"{len(families[name])}")
             fam = FluxFamilies()
             fam.groups = len(keep[0])
             fam.group_modes = keep[0].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))

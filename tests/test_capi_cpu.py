@@ -98,6 +98,18 @@ def test_sturm_liouville_family_is_orthonormal_and_group_dependent():
     assert not np.allclose(F[1], F[-1])
 
 
+@pytest.mark.parametrize("shape,seed", [((32, 32, 17, 3), 129), ((128, 128, 33, 3), 7)])
+def test_sturm_liouville_family_matches_lapack_restatement(shape, seed):
+    # The library's QL iteration against LAPACK's tridiagonal eigensolver on the
+    # same seeded operator: eigenvectors agree to rounding (the spectrum is
+    # simple, so the vectors are unique up to the fixed sign convention).
+    w = skb_cuda.Workload(*shape)
+    fwd, inv, _ = skb_cuda.vertical_family(w, skb_cuda.FAMILY_STURM_LIOUVILLE, seed=seed)
+    ofwd, oinv = orc.sturm_liouville_family(orc.Workload(*shape), seed)
+    assert np.max(np.abs(fwd.reshape(ofwd.shape) - ofwd)) <= 1e-10
+    assert np.max(np.abs(inv.reshape(oinv.shape) - oinv)) <= 1e-10
+
+
 def test_invalid_arguments_raise_value_error():
     with pytest.raises(ValueError):
         skb_cuda.retained_modes(skb_cuda.Workload(1, 8, 7, 2))
@@ -111,6 +123,17 @@ def test_type1_handle_arguments_are_refused_before_device_work():
     for rows, nz in ((4, 2), (0, 9), (4, 16386)):
         with pytest.raises(ValueError):
             skb_cuda.ConstantStratificationVertical(rows, nz)
+
+
+def test_allocation_free_inverse_refuses_an_overflowing_workload():
+    # Nz * fields wraps a 64-bit product (2^62 * 8 = 2^65); the scratch size
+    # saturates instead, so the call is refused before any device work.
+    lib = skb_cuda.library()
+    for w in (skb_cuda.Workload(64, 64, 1 << 62, 8), skb_cuda.Workload(1024, 1024, (1 << 64) - 1, 3)):
+        with pytest.raises(ValueError, match="bytes of scratch"):
+            skb_cuda.check(lib.skb_fft_inverse_device_noalloc(ctypes.byref(w), ctypes.c_int(skb_cuda.FP64),
+                                                              ctypes.c_void_p(16), ctypes.c_void_p(16),
+                                                              ctypes.c_void_p(None)))
 
 
 def test_gpu_calls_fail_loudly_without_a_device():

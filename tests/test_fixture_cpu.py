@@ -142,9 +142,21 @@ def test_two_family_oracle_reduces_to_the_one_family_flux():
 
 @pytest.mark.parametrize("change,message", [
     (lambda fam, o: o.update(targets=3), "15 -> 4"),
-    (lambda fam, o: fam.update(group_modes=np.concatenate([[0], fam["group_modes"]]).astype(np.uint64)),
+    # (matrices padded or emptied to the changed group count, so the C ABI's own
+    # checks are the ones that refuse)
+    (lambda fam, o: fam.update(group_modes=np.concatenate([[0], fam["group_modes"]]).astype(np.uint64),
+                               forward=[np.concatenate([f[:1], f]) for f in fam["forward"]],
+                               inverse=[np.concatenate([i[:1], i]) for i in fam["inverse"]]),
      "nonempty"),
-    (lambda fam, o: fam.update(group_modes=np.zeros(0, np.uint64)), "operator groups"),
+    (lambda fam, o: fam.update(group_modes=np.zeros(0, np.uint64), forward=[f[:0] for f in fam["forward"]],
+                               inverse=[i[:0] for i in fam["inverse"]]), "operator groups"),
+    # Matrices shaped for another Nz or group count, and short family maps, are
+    # refused by the binding before the C ABI copies groups * Nj * Nz values.
+    (lambda fam, o: fam.update(forward=[f[:, :, :-1] for f in fam["forward"]]), "expected"),
+    (lambda fam, o: fam.update(inverse=[i[:-1] for i in fam["inverse"]]), "expected"),
+    (lambda fam, o: fam.update(forward=fam["forward"][:1]), "wave-f and wave-g"),
+    (lambda fam, o: fam.update(input_family=list(fam["input_family"])[:14]), "15 slots"),
+    (lambda fam, o: fam.update(target_family=list(fam["target_family"]) + [0]), "4 slots"),
 ])
 def test_family_flux_arguments_are_refused_before_device_work(change, message):
     """skb_flux_create_families checks its arguments (the reference's

@@ -1,0 +1,170 @@
+"""GPU parity at the shapes the benchmark is quoted on, against the CPU oracle.
+
+* The 15 -> 4 flux at 512 x 512, Nz = 129, one member, with the reference's
+  modal-input generator (uniform [-0.125, 0.125], real DC): FP64-plain within
+  1e-12 (the reference's own FP64 tolerance) and split TF32x3 within 1e-6 (the
+  split-precision bound), both max-relative and relative-L2.  The same split
+  check on the benchmark's own k^-3 power-law inputs.
+* The build-side Sturm-Liouville vertical family (dense, group-dependent
+  operators, the realistic case for split-precision error): through the
+  grouped GEMM at 256 x 256, Nz = 65, 3 fields in every precision, and through
+  the flux at 512 x 512, Nz = 129.
+* The serving mix's three size classes (128^2 x 33 12 -> 3, 256^2 x 65 12 -> 3,
+  512^2 x 129 15 -> 4) in both modes: every result of a mixed stream equals the
+  same request computed alone, and matches the oracle.
+
+One oracle flux at 512^2 x 129 takes a few seconds on the host's cores; each is
+computed once per module.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+import skb_cuda
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+N, NZ = 512, 129
+NJ = 2 * (NZ - 1) // 3
+WORKERS = os.cpu_count() or 1
+SL_SEED = 3
+
+
+@pytest.fixture(scope="module")
+def modes512():
+    return orc.retained_modes(N, N)
+
+
+@pytest.fixture(scope="module")
+def reference_case(modes512):
+    x = orc.flux_inputs(modes512, 15, NJ, 129)
+    return x, orc.flux(N, NZ, x, modes=modes512, workers=WORKERS)
+
+
+@pytest.fixture(scope="module")
+def sl_family():
+    fwd, inv, ident = skb_cuda.vertical_family(skb_cuda.Workload(N, N, NZ, 4), skb_cuda.FAMILY_STURM_LIOUVILLE,
+                                               SL_SEED)
+    assert ident.startswith("seeded-sturm-liouville")
+    return fwd.reshape(-1, NJ, NZ), inv.reshape(-1, NZ, NJ)
+
+
+def _errors(out, ref):
+    return orc.max_rel_error(out, ref), orc.rel_l2_error(out, ref)
+
+
+def test_flux_fp64_plain_full_size_matches_oracle(reference_case):
+    x, ref = reference_case
+    flux = skb_cuda.Flux(N, NZ)
+    out = flux.execute(x)
+    flux.check_device()
+    max_rel, l2 = _errors(out, ref)
+    assert max_rel <= 1e-12 and l2 <= 1e-12, (max_rel, l2)
+
+
+def test_flux_split_full_size_matches_oracle(reference_case):
+    x, ref = reference_case
+    flux = skb_cuda.Flux(N, NZ, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    out = flux.execute(x)
+    flux.check_device()
+    max_rel, l2 = _errors(out, ref)
+    assert max_rel <= 1e-6 and l2 <= 1e-6, (max_rel, l2)
+
+
+def test_flux_split_power_law_inputs_match_oracle(modes512):
+    # The benchmark's k^-3 power-law inputs (amplitude (1 + |k|^2)^-1.5, random
+    # phase, real DC), one member, against the oracle.
+    k = modes512.k.astype(np.float64)
+    l = modes512.l.astype(np.float64)
+    rng = np.random.default_rng(129)
+    shape = (len(k), 15, NJ)
+    amp = (1.0 + k * k + l * l) ** -1.5
+    x = amp[:, None, None] * rng.uniform(0.5, 1.5, shape) * np.exp(1j * rng.uniform(0.0, 2.0 * np.pi, shape))
+    x[(k == 0) & (l == 0)] = x[(k == 0) & (l == 0)].real
+    x = x.reshape(-1)
+    ref = orc.flux(N, NZ, x, modes=modes512, workers=WORKERS)
+    out = skb_cuda.Flux(N, NZ, mode=skb_cuda.FLUX_SPLIT_TF32X3).execute(x)
+    assert orc.rel_l2_error(out, ref) <= 1e-6
+
+
+@pytest.mark.parametrize("precision,tol", [(skb_cuda.GEMM_FP64, 1e-12), (skb_cuda.GEMM_FP32, 1e-6),
+                                           (skb_cuda.GEMM_TF32X3, 1e-6)])
+def test_sturm_liouville_grouped_gemm_matches_oracle(precision, tol):
+    shape = (256, 256, 65, 3)
+    w = skb_cuda.Workload(*shape)
+    o = orc.Workload(*shape)
+    fwd, inv, _ = skb_cuda.vertical_family(w, skb_cuda.FAMILY_STURM_LIOUVILLE, SL_SEED)
+    fam = (fwd.reshape(-1, w.nj, w.nz), inv.reshape(-1, w.nz, w.nj))
+    H = len(orc.retained_modes(w.nx, w.ny))
+    rng = np.random.default_rng(21)
+    phys = rng.uniform(-1, 1, H * w.fields * w.nz) + 1j * rng.uniform(-1, 1, H * w.fields * w.nz)
+    modal = rng.uniform(-1, 1, H * w.fields * w.nj) + 1j * rng.uniform(-1, 1, H * w.fields * w.nj)
+    vp = skb_cuda.VerticalGemmProvider(w, skb_cuda.squared_wavenumber_groups(w), fwd, inv,
+                                       gemm_precision=precision)
+    vp.load_physical_input(phys)
+    vp.execute_forward()
+    max_rel, l2 = _errors(vp.copy_forward_output(), orc.grouped_vertical(o, fam, "forward", phys))
+    assert max_rel <= tol and l2 <= tol, (max_rel, l2)
+    vp.load_modal_input(modal)
+    vp.execute_inverse()
+    max_rel, l2 = _errors(vp.copy_inverse_output(), orc.grouped_vertical(o, fam, "inverse", modal))
+    assert max_rel <= tol and l2 <= tol, (max_rel, l2)
+
+
+def test_sturm_liouville_flux_full_size_matches_oracle(modes512, sl_family):
+    x = orc.flux_inputs(modes512, 15, NJ, 131)
+    ref = orc.flux(N, NZ, x, family=sl_family, modes=modes512, workers=WORKERS)
+    for mode, tol in ((skb_cuda.FLUX_FP64_PLAIN, 1e-12), (skb_cuda.FLUX_SPLIT_TF32X3, 1e-6)):
+        flux = skb_cuda.Flux(N, NZ, mode=mode, family=skb_cuda.FAMILY_STURM_LIOUVILLE, family_seed=SL_SEED)
+        out = flux.execute(x)
+        flux.check_device()
+        max_rel, l2 = _errors(out, ref)
+        assert max_rel <= tol and l2 <= tol, (mode, max_rel, l2)
+        flux.close()
+
+
+# Serving mix of the benchmark's stream: (n, Nz, targets); 3 targets is the
+# 12 -> 3 flux, 4 the full 15 -> 4 one.
+SERVE = [(128, 33, 3), (256, 65, 3), (512, 129, 4)]
+
+
+def test_serving_mix_classes_alone_equals_mixed_and_matches_oracle(reference_case, modes512):
+    skb_cuda.tune_cache_clear()
+    modes_of = {128: orc.retained_modes(128, 128), 256: orc.retained_modes(256, 256), 512: modes512}
+    classes = [(n, nz, t, 2, mode) for mode in (skb_cuda.FLUX_SPLIT_TF32X3, skb_cuda.FLUX_FP64_PLAIN)
+               for n, nz, t in SERVE]
+    server = skb_cuda.Server(classes, hbm_budget_bytes=48 << 30, max_slots_per_class=1)
+    order = [0, 3, 1, 4, 2, 5, 0, 1, 3, 4, 2, 5]
+    xs = []
+    for i, c in enumerate(order):
+        n, nz, t = classes[c][:3]
+        if n == N and i < 6:
+            xs.append(reference_case[0])   # the first 512^2 request of each mode reuses the oracle case
+        else:
+            xs.append(orc.flux_inputs(modes_of[n], 3 + 3 * t, 2 * (nz - 1) // 3, 500 + i))
+    tickets = [server.submit(c, x) for c, x in zip(order, xs)]
+    results = [server.wait(t, timeout=600)[0] for t in tickets]
+    stats = server.stats()
+    assert stats["completed"] == len(order)
+    server.close()
+    alone_cache = {}
+    for i, (c, x, out) in enumerate(zip(order, xs, results)):
+        n, nz, t, _, mode = classes[c]
+        if c not in alone_cache:
+            alone_cache[c] = skb_cuda.Flux(n, nz, targets=t, mode=mode)
+        assert np.array_equal(out, alone_cache[c].execute(x)), (i, classes[c])
+        if n == N:
+            if x is reference_case[0]:
+                ref = reference_case[1]
+            else:
+                continue            # one oracle per 512^2 mode is enough
+        else:
+            ref = orc.flux(n, nz, x, targets=t, modes=modes_of[n], workers=WORKERS)
+        tol = 1e-12 if mode == skb_cuda.FLUX_FP64_PLAIN else 1e-6
+        max_rel, l2 = _errors(out, ref)
+        assert max_rel <= tol and l2 <= tol, (classes[c], max_rel, l2)
+    for f in alone_cache.values():
+        f.close()

@@ -77,3 +77,26 @@ def test_oversized_workload_is_refused():
     d = skb_cuda.DeviceArray(16)
     with pytest.raises(ValueError, match="bytes of scratch"):
         _noalloc(w, skb_cuda.FP64, d.ptr, d.ptr)
+
+
+@pytest.mark.parametrize("precision", [skb_cuda.FP64, skb_cuda.FP32])
+def test_matches_the_oracle_inverse(precision):
+    # Against the CPU oracle's c2r (pocketfft in float64 with FFTW's
+    # half-spectrum semantics), on a spectrum that is not Hermitian-consistent,
+    # so the kx = 0 and Nyquist handling is exercised as well.
+    from oracle import oracle as orc
+
+    real_t, complex_t = DTYPES[precision]
+    for shape, seed in (((64, 32, 9, 2), 31), ((256, 256, 5, 2), 32)):
+        w = skb_cuda.Workload(*shape)
+        rng = np.random.default_rng(seed)
+        n = w.spectrum_elements
+        spectrum = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(complex_t)
+        d_spec = skb_cuda.DeviceArray.from_numpy(spectrum)
+        d_real = skb_cuda.DeviceArray(w.real_elements * np.dtype(real_t).itemsize)
+        _noalloc(w, precision, d_spec.ptr, d_real.ptr)
+        skb_cuda.synchronize()
+        got = d_real.download(real_t, w.real_elements)
+        ref = orc.fft_c2r(orc.Workload(*shape), spectrum.astype(np.complex128))
+        assert orc.rel_l2_error(got, ref) <= TOL[precision]
+        assert orc.max_rel_error(got, ref) <= TOL[precision]
