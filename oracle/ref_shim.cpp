@@ -1,7 +1,8 @@
 // Test infrastructure only: a C shim over the reference's own CPU functions.
 //
 // This file is compiled together with the reference sources where they lie
-// (src/model.cpp, src/pointwise_advection.cpp, src/json.cpp of
+// (src/model.cpp, src/pointwise_advection.cpp, src/json.cpp and
+// src/spectral_flux_fixture.cpp of
 // JeffreyEarly/spectral-kernel-benchmarks) by oracle/Makefile into
 // oracle/_ref/libskbref.so.  Nothing in the product links it.  It exists so
 // that tests/golden/make_golden.py can pin the oracle restatement
@@ -352,6 +353,152 @@ int skbref_flux_direct(std::uint64_t n, std::uint64_t nz, std::uint64_t seed, do
             const auto first = family.groups[g].firstMode;
             skbench::verticalForward(out, family.groups[g].modeCount, ops, physicalOut.data() + first * 4 * nz,
                                      result + first * 4 * nj);
+        }
+    });
+}
+
+// A prepared spectral-flux fixture (SKFXP001) read by the reference's own loader,
+// loadPreparedSpectralFluxFixture (spectral_flux_fixture.cpp:150-411), reported
+// in the loader's order: modes as retainedHorizontalModes orders them, operator
+// groups (first mode, mode count, key, matrix source group) of family 0 (both
+// families share them), matrices per family and source group as the loader
+// stores them (forward [j][z], inverse [z][j]), modal inputs [mode][15][j] and
+// the file's expected targets [mode][4][j].  dims receives Nx, Nz, modes, Nj,
+// operator groups and source groups; with null arrays only dims is written.
+int skbref_load_flux_fixture(const char* path, std::uint64_t* dims, std::int64_t* k, std::int64_t* l,
+                             std::uint64_t* groupFirst, std::uint64_t* groupCount, std::uint64_t* groupKey,
+                             std::uint64_t* matrixSource, double* forward, double* inverse, double* modalIn,
+                             double* expected) {
+    return guarded([&] {
+        const auto fixture = skbench::loadPreparedSpectralFluxFixture(path);
+        const auto& fam0 = fixture.operatorFamilies[0];
+        const std::size_t sources = fixture.groupKeys.size();
+        dims[0] = fixture.workload.nx;
+        dims[1] = fixture.workload.nz;
+        dims[2] = fixture.modes.size();
+        dims[3] = fam0.nj;
+        dims[4] = fam0.groups.size();
+        dims[5] = sources;
+        if (k == nullptr) return;
+        for (std::size_t m = 0; m < fixture.modes.size(); ++m) {
+            k[m] = fixture.modes[m].k;
+            l[m] = fixture.modes[m].l;
+        }
+        for (std::size_t g = 0; g < fam0.groups.size(); ++g) {
+            groupFirst[g] = fam0.groups[g].firstMode;
+            groupCount[g] = fam0.groups[g].modeCount;
+            groupKey[g] = fam0.groups[g].squaredModeKey;
+            matrixSource[g] = fam0.matrixSourceGroups[g];
+        }
+        const std::size_t per = fam0.nz * fam0.nj * sources;
+        for (std::size_t f = 0; f < 2; ++f) {
+            std::memcpy(forward + f * per, fixture.operatorFamilies[f].forward.data(), per * sizeof(double));
+            std::memcpy(inverse + f * per, fixture.operatorFamilies[f].inverse.data(), per * sizeof(double));
+        }
+        std::memcpy(modalIn, fixture.modalInputs.data(), fixture.modalInputs.size() * sizeof(skbench::Complex));
+        std::memcpy(expected, fixture.expectedModalTargets.data(),
+                    fixture.expectedModalTargets.size() * sizeof(skbench::Complex));
+    });
+}
+
+// The authoritative two-family 15 -> 4 flux of a prepared fixture, composed from
+// the reference's own functions: the fixture read by its loader, each input slot
+// and target taken through verticalInverse / verticalForward (model.cpp:567-605)
+// with the operator matrices of its family (the fixture's field-to-family maps,
+// authoritative_spectral_flux.cpp:193-216, 340-440) and operator group, then the
+// streamed order of skbref_flux_direct: embedRetained + directC2R of U,V,W, per
+// target the derivative triple, PointwiseAdvectionExecutor with the fixture's
+// pointwise scale, directR2C + gatherRetained.  The direct DFTs stand in for the
+// FFTW plans (same unnormalised transforms), so keep Nx small.  modalOut holds
+// modes*4*nj complex in the loader's mode order.
+int skbref_two_family_flux_direct(const char* path, double* modalOut) {
+    return guarded([&] {
+        using skbench::Complex;
+        const auto fixture = skbench::loadPreparedSpectralFluxFixture(path);
+        const auto n = fixture.workload.nx, nz = fixture.workload.nz;
+        skbench::Workload out = fixture.workload;
+        out.fields = 4;
+        skbench::Workload in = fixture.workload;
+        in.fields = 15;
+        skbench::Workload triple = fixture.workload;
+        triple.fields = 3;
+        skbench::Workload single = fixture.workload;
+        single.fields = 1;
+        const auto& modes = fixture.modes;
+        const auto H = modes.size();
+        const auto nj = out.retainedVerticalModes();
+        const auto volume = n * n * nz;
+        auto slice = [&](std::size_t family, std::size_t group) {
+            const auto& ops = fixture.operatorFamilies[family];
+            return groupSlice(ops, ops.matrixSourceGroups[group]);
+        };
+        const auto& groups = fixture.operatorFamilies[0].groups;
+
+        // Inverse vertical transform, one slot at a time with its family's matrices.
+        std::vector<Complex> physicalIn(H * nz * 15);
+        for (std::size_t f = 0; f < 15; ++f) {
+            const auto family = fixture.inputFieldFamilies[f];
+            for (std::size_t g = 0; g < groups.size(); ++g) {
+                const auto first = groups[g].firstMode, count = groups[g].modeCount;
+                std::vector<Complex> modal(count * nj), phys(count * nz);
+                for (std::size_t m = 0; m < count; ++m)
+                    for (std::size_t j = 0; j < nj; ++j)
+                        modal[skbench::modalSpectrumIndex(single, m, j, 0)] =
+                            fixture.modalInputs[skbench::modalSpectrumIndex(in, first + m, j, f)];
+                skbench::verticalInverse(single, count, slice(family, g), modal.data(), phys.data());
+                for (std::size_t m = 0; m < count; ++m)
+                    for (std::size_t z = 0; z < nz; ++z)
+                        physicalIn[skbench::retainedSpectrumIndex(in, first + m, z, f)] =
+                            phys[skbench::retainedSpectrumIndex(single, m, z, 0)];
+            }
+        }
+
+        std::vector<Complex> compactTriple(H * nz * 3), compactTarget(H * nz), physicalOut(H * nz * 4);
+        std::vector<Complex> tripleSpectrum(triple.spectrumElements()), targetSpectrum(single.spectrumElements());
+        std::vector<double> shared(triple.realElements()), derivative(triple.realElements()),
+            targetVolume(single.realElements());
+        auto copyTriple = [&](std::size_t firstField) {
+            for (std::size_t m = 0; m < H; ++m)
+                for (std::size_t f = 0; f < 3; ++f)
+                    for (std::size_t z = 0; z < nz; ++z)
+                        compactTriple[skbench::retainedSpectrumIndex(triple, m, z, f)] =
+                            physicalIn[skbench::retainedSpectrumIndex(in, m, z, firstField + f)];
+        };
+        copyTriple(0);
+        skbench::embedRetained(triple, modes, compactTriple.data(), tripleSpectrum.data());
+        skbench::directC2R(triple, tripleSpectrum.data(), shared.data());
+        skbench::PointwiseAdvectionExecutor pointwise(skbench::PointwiseAdvectionPolicy::serial, 1, volume,
+                                                      fixture.pointwiseScale);
+        for (std::size_t t = 0; t < 4; ++t) {
+            copyTriple(3 + 3 * t);
+            skbench::embedRetained(triple, modes, compactTriple.data(), tripleSpectrum.data());
+            skbench::directC2R(triple, tripleSpectrum.data(), derivative.data());
+            pointwise.execute(shared.data(), derivative.data(), targetVolume.data());
+            skbench::directR2C(single, targetVolume.data(), targetSpectrum.data());
+            skbench::gatherRetained(single, modes, targetSpectrum.data(), compactTarget.data());
+            for (std::size_t m = 0; m < H; ++m)
+                for (std::size_t z = 0; z < nz; ++z)
+                    physicalOut[skbench::retainedSpectrumIndex(out, m, z, t)] =
+                        compactTarget[skbench::retainedSpectrumIndex(single, m, z, 0)];
+        }
+
+        // Forward vertical transform, one target at a time with its family's matrices.
+        auto* result = reinterpret_cast<Complex*>(modalOut);
+        for (std::size_t t = 0; t < 4; ++t) {
+            const auto family = fixture.targetFieldFamilies[t];
+            for (std::size_t g = 0; g < groups.size(); ++g) {
+                const auto first = groups[g].firstMode, count = groups[g].modeCount;
+                std::vector<Complex> phys(count * nz), modal(count * nj);
+                for (std::size_t m = 0; m < count; ++m)
+                    for (std::size_t z = 0; z < nz; ++z)
+                        phys[skbench::retainedSpectrumIndex(single, m, z, 0)] =
+                            physicalOut[skbench::retainedSpectrumIndex(out, first + m, z, t)];
+                skbench::verticalForward(single, count, slice(family, g), phys.data(), modal.data());
+                for (std::size_t m = 0; m < count; ++m)
+                    for (std::size_t j = 0; j < nj; ++j)
+                        result[skbench::modalSpectrumIndex(out, first + m, j, t)] =
+                            modal[skbench::modalSpectrumIndex(single, m, j, 0)];
+            }
         }
     });
 }

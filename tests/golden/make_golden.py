@@ -6,8 +6,10 @@ Run in a container where the reference tree exists (it is compiled in place by
     python tests/golden/make_golden.py
 
 Every number written here comes from the reference's functions
-(src/model.cpp, src/pointwise_advection.cpp, src/json.cpp) through the thin
-shim oracle/ref_shim.cpp.  The fixtures are small (tens of KB) so that the
+(src/model.cpp, src/pointwise_advection.cpp, src/json.cpp,
+src/spectral_flux_fixture.cpp) through the thin shim oracle/ref_shim.cpp
+(the two-family fixture's inputs and matrices are seeded data; its expected
+targets come from the reference's functions).  The fixtures are small (tens of KB) so that the
 tests can pin the oracle restatement and the CUDA provider without the
 reference tree, which is absent on the GPU host.
 """
@@ -33,7 +35,8 @@ def p(a):
 
 
 def load():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    ref = os.environ.get("REF", "/root/reference")
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref], check=True)
     lib = ctypes.CDLL(REF_LIB)
     lib.skbref_last_error.restype = ctypes.c_char_p
     lib.skbref_max_rel_error_complex.restype = ctypes.c_double
@@ -91,6 +94,65 @@ def direct_c2r(lib, n, nz, fields, spec):
     s = np.ascontiguousarray(spec).view(np.float64)
     check(lib, lib.skbref_direct_c2r(U64(n), U64(n), U64(nz), U64(fields), p(s), p(out)))
     return out
+
+
+def two_family_fixture(lib, n=16, nz=7, seed=11):
+    """The authoritative two-family flux, pinned to the reference: a synthetic
+    prepared fixture (SKFXP001; seeded floating K^2 groups, wave-f / wave-g
+    matrices, modal inputs, modes stored in the file in reverse order within each
+    group) is written, read by the reference's own loader
+    (loadPreparedSpectralFluxFixture), and its expected targets are the flux that
+    oracle/ref_shim.cpp composes from the reference's functions with the
+    fixture's family maps.  The file (with those targets) is kept beside this
+    script as two_family_16x7.skfxp; the loader's view of it goes into the
+    returned arrays (two_family_*)."""
+    for path in (ROOT, os.path.join(ROOT, "tests"), os.path.join(ROOT, "spectral-kernel-benchmarks_b200")):
+        if path not in sys.path:
+            sys.path.insert(0, path)
+    import skb_cuda.fixture as fx
+    from synthetic_fixture import families_canonical
+
+    modes, fam, group_keys = families_canonical(n, nz, seed)
+    H = len(modes.k)
+    nj = 2 * (nz - 1) // 3
+    rng = np.random.default_rng(seed + 1)
+    inputs = rng.uniform(-0.125, 0.125, (H, 15, nj)) + 1j * rng.uniform(-0.125, 0.125, (H, 15, nj))
+    inputs[0].imag = 0.0
+    counts = fam["group_modes"].astype(np.int64)
+    first = np.r_[0, np.cumsum(counts)[:-1]]
+    order = np.concatenate([np.arange(f0 + c - 1, f0 - 1, -1) for f0, c in zip(first, counts)])
+    group_of = np.repeat(np.arange(len(counts)), counts)
+    keys = np.stack([modes.k, modes.l], axis=1)
+    path = os.path.join(HERE, "two_family_16x7.skfxp")
+    meta = {"fixture_id": "synthetic-two-family-16x7", "generator": "tests/golden/make_golden.py"}
+
+    def write(targets):
+        fx.write(path, n, nz, keys[order], group_of, group_keys, fam["forward"], fam["inverse"], inputs[order],
+                 targets[order], meta=meta)
+
+    write(np.zeros((H, 4, nj), np.complex128))
+    targets = np.zeros(2 * H * 4 * nj)
+    check(lib, lib.skbref_two_family_flux_direct(path.encode(), p(targets)))
+    targets = targets.view(np.complex128).reshape(H, 4, nj)
+    write(targets)
+
+    dims = np.zeros(6, np.uint64)
+    check(lib, lib.skbref_load_flux_fixture(path.encode(), p(dims), *([None] * 10)))
+    _, _, nkl, nj2, ngroups, nsource = (int(v) for v in dims)
+    k = np.zeros(nkl, np.int64)
+    l = np.zeros(nkl, np.int64)
+    gfirst, gcount, gkey, gsource = (np.zeros(ngroups, np.uint64) for _ in range(4))
+    fwd = np.zeros(2 * nsource * nj2 * nz)
+    inv = np.zeros(2 * nsource * nj2 * nz)
+    modal_in = np.zeros(2 * nkl * 15 * nj2)
+    expected = np.zeros(2 * nkl * 4 * nj2)
+    check(lib, lib.skbref_load_flux_fixture(path.encode(), p(dims), p(k), p(l), p(gfirst), p(gcount), p(gkey),
+                                            p(gsource), p(fwd), p(inv), p(modal_in), p(expected)))
+    return {"two_family_k": k, "two_family_l": l, "two_family_group_first": gfirst,
+            "two_family_group_count": gcount, "two_family_group_key": gkey, "two_family_matrix_source": gsource,
+            "two_family_forward": fwd.reshape(2, nsource, nj2, nz), "two_family_inverse": inv.reshape(2, nsource, nz, nj2),
+            "two_family_inputs": modal_in.view(np.complex128).reshape(nkl, 15, nj2),
+            "two_family_targets": expected.view(np.complex128).reshape(nkl, 4, nj2)}
 
 
 def main():
@@ -218,6 +280,8 @@ def main():
     pout = np.zeros(n * n * nz * f)
     check(lib, lib.skbref_spectral_pipeline(U64(n), U64(nz), U64(f), U64(129), p(pin), p(pw), p(pout)))
     arrays.update(pipeline_in=pin, pipeline_weights=pw, pipeline_out=pout)
+
+    arrays.update(two_family_fixture(lib))
 
     np.savez_compressed(os.path.join(HERE, "reference_vectors.npz"), **arrays)
 

@@ -168,3 +168,43 @@ def test_family_flux_arguments_are_refused_before_device_work(change, message):
     change(fam, opts)
     with pytest.raises(ValueError, match=message):
         skb_cuda.Flux(8, 7, targets=opts["targets"], members=1, mode=skb_cuda.FLUX_FP64_PLAIN, families=fam)
+
+
+GOLDEN_FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "two_family_16x7.skfxp")
+
+
+def test_loader_matches_the_reference_loader(golden_vectors):
+    """The golden two-family fixture as this library's loader returns it equals,
+    bit for bit, what the reference's loadPreparedSpectralFluxFixture made of
+    the same file (mode order, operator groups, each group's matrices through
+    its source group, inputs and targets)."""
+    g = golden_vectors
+    f = fx.load(GOLDEN_FIXTURE)
+    import skb_cuda
+
+    mine = skb_cuda.retained_modes(skb_cuda.Workload(f.nx, f.ny, f.nz, 4))
+    assert [m.k for m in mine] == list(g["two_family_k"])
+    assert [m.l for m in mine] == list(g["two_family_l"])
+    assert np.array_equal(f.group_modes, g["two_family_group_count"])
+    assert np.array_equal(np.r_[0, np.cumsum(f.group_modes)[:-1]], g["two_family_group_first"])
+    assert np.array_equal(f.group_keys, g["two_family_group_key"])
+    source = g["two_family_matrix_source"].astype(np.int64)
+    for fam in range(2):
+        assert np.array_equal(f.forward[fam], g["two_family_forward"][fam][source])
+        assert np.array_equal(f.inverse[fam], g["two_family_inverse"][fam][source])
+    assert np.array_equal(f.modal_inputs, g["two_family_inputs"])
+    assert np.array_equal(f.expected_targets, g["two_family_targets"])
+
+
+def test_two_family_oracle_matches_the_reference_composition(golden_vectors):
+    """The oracle's two-family flux against the one composed from the
+    reference's own functions (loader, verticalInverse / verticalForward with
+    the family maps, direct DFTs, PointwiseAdvectionExecutor) at the
+    reference's FP64 tolerance."""
+    f = fx.load(GOLDEN_FIXTURE)
+    fam = {"group_modes": f.group_modes, "forward": f.forward, "inverse": f.inverse,
+           "input_family": f.input_family, "target_family": f.target_family}
+    got = orc.flux(f.nx, f.nz, f.modal_inputs.reshape(-1), families=fam)
+    ref = golden_vectors["two_family_targets"].reshape(-1)
+    assert orc.max_rel_error(got, ref) <= 1e-12
+    assert orc.rel_l2_error(got, ref) <= 1e-12

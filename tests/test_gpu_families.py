@@ -59,3 +59,23 @@ def test_bad_families_are_refused():
         skb_cuda.Flux(16, 9, families={"group_modes": np.array([1], np.uint64), "forward": [np.zeros(45)] * 2,
                                        "inverse": [np.zeros(45)] * 2, "input_family": fx.INPUT_FAMILIES,
                                        "target_family": fx.TARGET_FAMILIES})
+
+
+@pytest.mark.parametrize("mode,tol", [(skb_cuda.FLUX_FP64_PLAIN, 1e-12), (skb_cuda.FLUX_SPLIT_TF32X3, 1e-6)])
+def test_golden_fixture_matches_the_reference_composition(golden_vectors, mode, tol):
+    """The golden prepared fixture (read by the reference's own loader when it
+    was made) against the two-family flux composed from the reference's
+    functions: FP64-plain at the reference's 1e-12, split TF32x3 at 1e-6."""
+    import os
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "two_family_16x7.skfxp")
+    f = fx.load(path)
+    ref = golden_vectors["two_family_targets"]
+    for members in (1, 2):
+        flux = skb_cuda.Flux(f.nx, f.nz, members=members, mode=mode, families=_families(f))
+        x = np.concatenate([f.modal_inputs.reshape(-1)] * members)
+        got = flux.execute(x).reshape(members, *ref.shape)
+        for m in range(members):
+            assert orc.max_rel_error(got[m], ref) <= tol
+            assert orc.rel_l2_error(got[m], ref) <= tol
+        flux.close()
