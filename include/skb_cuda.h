@@ -280,6 +280,16 @@ SKB_API int skb_vertical_forward_device(skb_vertical_provider* p, const void* in
 SKB_API int skb_vertical_inverse_device(skb_vertical_provider* p, const void* in_real, const void* in_imag, void* out_real,
                                 void* out_imag, void* stream);
 
+/* Test of the failure path (no counterpart in the reference; the reference's
+ * CPU GEMMs cannot wait on a device).  With enable != 0, every later launch of
+ * this tensor-core (SKB_GEMM_TF32X3) provider makes its MMA lane wait first on
+ * a device barrier that nothing signals.  That wait is bounded like every wait
+ * of the kernel, so it runs out: the kernel records the expiry, every role of
+ * every CTA stops, outstanding copies are drained and TMEM is freed, and the
+ * next host-array call reports SKB_ERR_RUNTIME ("a bounded device wait
+ * expired").  The handle stays in that state; the CUDA context stays usable. */
+SKB_API int skb_vertical_expire_wait_for_test(skb_vertical_provider* p, int enable);
+
 /* ------------------------------------ WVM-direct vertical GEMM provider */
 /* Replaces WvmDirectVerticalGemmProvider (skbench.hpp:220-257,
  * src/vertical_gemm.cpp:935-1169): per retained mode, the group matrix times

@@ -1425,6 +1425,15 @@ int skb_vertical_load_modal_input_split(skb_vertical_provider* p, const double* 
     });
 }
 
+int skb_vertical_expire_wait_for_test(skb_vertical_provider* p, int enable) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        require(p->gp == GemmPrecision::tf32x3, "the expired-wait test applies to the tensor-core GEMM form");
+        for (auto* plan : {p->forward.get(), p->inverse.get()})
+            if (plan) plan->set_expire_wait_for_test(enable != 0);
+    });
+}
+
 int skb_vertical_execute_forward(skb_vertical_provider* p) {
     return guard([&] {
         require(p != nullptr, "handle must be non-null");

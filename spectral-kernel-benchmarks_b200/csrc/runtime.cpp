@@ -429,6 +429,7 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
         a.in = static_cast<const float2*>(in.re);
         a.out = static_cast<float2*>(out.re);
         a.error = error_.get<int>();
+        a.expireWaitForTest = expireWaitForTest_ ? 1 : 0;
         if (inBins != nullptr) a.inBins = *inBins;
         if (outBins != nullptr) a.outBins = *outBins;
         check_cuda(launch_tc_gemm(a, s), "tensor-core grouped vertical GEMM kernel");

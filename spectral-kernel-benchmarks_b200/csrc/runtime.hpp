@@ -171,6 +171,9 @@ public:
                  const BinBoundary* inBins = nullptr, const BinBoundary* outBins = nullptr) const;
     // Raises if a bounded device wait of the tensor-core form expired.
     void check_device_error() const;
+    // Tensor-core form: the next launches wait on a device barrier that
+    // nothing signals, so their bounded wait expires (tests the error path).
+    void set_expire_wait_for_test(bool on) { expireWaitForTest_ = on; }
     GemmPrecision precision() const { return p_; }
     std::uint64_t columns() const { return columns_; }
     std::uint64_t matrixBytes() const { return matrices_.bytes(); }
@@ -212,6 +215,7 @@ private:
     std::vector<int> groupColumnsHost_;  // complex columns per member in each group
     int unitTiles_ = 0;
     DeviceBuffer groupColumns_, groupFirst_, error_;
+    bool expireWaitForTest_ = false;
 };
 
 }  // namespace skb

@@ -39,6 +39,7 @@ constexpr int kChunkK = 32;       // tf32 elements per 128-byte row
 constexpr int kTmemCols = 512;  // two chunk accumulators + the running sum, NP columns each
 constexpr int kStageBytes = 2 * kTileRows * 128;  // hi + lo
 constexpr long long kWaitLimit = 1LL << 22;
+constexpr long long kTestWaitLimit = 1LL << 14;  // the expired-wait test's wait (expireWaitForTest)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -62,8 +63,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 
 // Bounded wait for the phase with the given parity to complete.
 // Gives up early once any CTA of the launch has reported an expired wait.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const int* error) {
-    for (long long i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const int* error,
+                                          long long limit = kWaitLimit) {
+    for (long long i = 0; i < limit; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((i & 1023) == 1023 && *reinterpret_cast<const volatile int*>(error) != 0) return false;
     }
@@ -182,6 +184,7 @@ constexpr uint32_t kBulkPiece = 32768;  // bytes per bulk copy of a group image
 
 struct PipeState {
     uint64_t full[kStages], empty[kStages], accFull[kAccumulators], accEmpty[kAccumulators], done, unitDone, bFull;
+    uint64_t never;  // no thread or copy ever arrives on it (expired-wait test)
     uint32_t tmem;
 };
 
@@ -312,6 +315,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         mbar_init(smem_u32(&st->done), 1);
         mbar_init(smem_u32(&st->unitDone), 1);
         mbar_init(smem_u32(&st->bFull), 1);
+        mbar_init(smem_u32(&st->never), 1);
         fence_barrier_init();
     }
     if (warp == kMmaWarp) {
@@ -463,6 +467,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
             const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(NP >> 3) << 17) |
                                    (static_cast<uint32_t>(kTileRows >> 4) << 24);
             int it = 0, loads = 0, group = -1;
+            // Expired-wait test: before this lane has issued any copy or MMA,
+            // a bounded wait on a barrier nothing arrives on runs out and takes
+            // the same path as any expired wait (error word, every role stops,
+            // copies drained, TMEM freed, SKB_ERR_RUNTIME on the host).
+            if (p.expireWaitForTest != 0 && !mbar_wait(smem_u32(&st->never), 0, p.error, kTestWaitLimit)) fail();
             for (int u = blockIdx.x; u < p.units && !failed; u += gridDim.x) {
                 const Unit U = unit_at(p, u);
                 if (U.g != group) {

@@ -90,6 +90,9 @@ struct TcGemmArgs {
     float2* out;       // [column][R] complex FP32 (or the bin array, see outBins)
     int* error;        // set to nonzero if a bounded wait expired
     BinBoundary inBins, outBins;
+    // Test of the expired-wait path: the MMA lane of every CTA first waits on
+    // a barrier that nothing arrives on, so that bounded wait runs out.
+    int expireWaitForTest;
 };
 bool tc_gemm_supported(int R, int S);
 size_t tc_gemm_smem_bytes(int R, int S);

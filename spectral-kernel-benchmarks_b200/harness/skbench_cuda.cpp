@@ -15,6 +15,7 @@
 #include <sys/utsname.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -202,7 +203,44 @@ struct Options {
     std::uint64_t members = 1, targets = 4, warmups = 0, samples = 0, seed = 129;
     bool warmupsSet = false, samplesSet = false, autotune = false;
     std::uint64_t nx = 0, ny = 0, nz = 0, fields = 0;
+    // The reference's streaming-provider knobs (RunOptions boundaryPolicy,
+    // streamingTileWidth, streamingInversePolicy; skbench.hpp:522-532, 952-954):
+    // checked as the reference checks them and recorded, with no effect here.
+    std::string boundaryPolicy, inversePolicy = "full-zero";
+    std::uint64_t tileWidth = 1;
 };
+
+// Checks the streaming-provider knobs against the values the reference accepts
+// for the kernel (benchmark.cpp:2978-2985, 3962-3970, 5398-5403;
+// pruned_fftw_provider.cpp:626-643; authoritative_spectral_flux.cpp:333-338).
+void check_streaming_options(const Options& o) {
+    const std::vector<std::string> inverse{"full-zero", "active-reset", "compact-preserved", "full-preserved"};
+    if (std::find(inverse.begin(), inverse.end(), o.inversePolicy) == inverse.end())
+        throw std::invalid_argument("--streaming-inverse-policy: expected full-zero, active-reset, compact-preserved "
+                                    "or full-preserved; got '" + o.inversePolicy + "'.");
+    if (o.inversePolicy != "full-zero") {
+        if (o.kernel != "production-lifetime-flux")
+            throw std::invalid_argument("--streaming-inverse-policy other than full-zero applies to "
+                                        "production-lifetime-flux only.");
+        if (o.fluxFixture.empty())
+            throw std::invalid_argument("--streaming-inverse-policy other than full-zero needs a prepared fixture "
+                                        "(--spectral-flux-fixture).");
+    }
+    if (!o.fluxFixture.empty() && o.tileWidth != 1 && o.tileWidth != 16)
+        throw std::invalid_argument("--streaming-tile-width: the authoritative flux graph runs with 16-plane tiles; "
+                                    "got " + std::to_string(o.tileWidth) + ".");
+    if (o.boundaryPolicy.empty()) return;
+    std::vector<std::string> allowed;
+    if (o.kernel == "production-lifetime-flux") allowed = {"wvm-direct", "streaming-pruned-compact-split"};
+    if (o.kernel == "spectral-pipeline")
+        allowed = {"wvm-direct", "plane-major-fused-split", "streaming-pruned-compact-split"};
+    if (!allowed.empty() && std::find(allowed.begin(), allowed.end(), o.boundaryPolicy) == allowed.end()) {
+        std::string list;
+        for (const auto& a : allowed) list += (list.empty() ? "" : ", ") + a;
+        throw std::invalid_argument("--boundary-policy for " + o.kernel + ": expected one of " + list + "; got '" +
+                                    o.boundaryPolicy + "'.");
+    }
+}
 
 std::vector<skb_retained_mode> retained_modes(const skb_workload& w) {
     std::uint64_t count = 0;
@@ -1485,6 +1523,7 @@ void usage(std::ostream& out) {
         << "              [--vertical-gemm-precision fp64|fp32|tf32x3] [--flux-mode fp64-plain|fp32|split-tf32x3]\n"
         << "              [--members N] [--targets 3|4] [--autotune] [--nx N --ny N --nz N --fields N]\n"
         << "              [--spectral-flux-fixture PREPARED.bin]\n"
+        << "              [--boundary-policy NAME] [--streaming-tile-width N] [--streaming-inverse-policy NAME]\n"
         << "              [--warmups N] [--samples N] [--seed N] [--output PATH]\n"
         << "  skbench-cuda compare --input SAMPLES.csv\n";
 }
@@ -1535,9 +1574,13 @@ int run(int argc, char** argv) {
         else if (k == "--output") o.output = value(argc, argv, i);
         else if (k == "--autotune") o.autotune = true;
         else if (k == "--spectral-flux-fixture") o.fluxFixture = value(argc, argv, i);
+        else if (k == "--boundary-policy") o.boundaryPolicy = value(argc, argv, i);
+        else if (k == "--streaming-tile-width") o.tileWidth = std::stoull(value(argc, argv, i));
+        else if (k == "--streaming-inverse-policy") o.inversePolicy = value(argc, argv, i);
         else throw std::invalid_argument("Unknown run option: " + std::string(k));
     }
     if (o.kernel == "2d-rfft") o.kernel = "fft";
+    check_streaming_options(o);
     if (!o.fluxFixture.empty() && o.kernel != "production-lifetime-flux")
         throw std::invalid_argument("--spectral-flux-fixture is valid only for production-lifetime-flux.");
     if (o.providers != "cuda" && o.providers != "both")
@@ -1567,6 +1610,15 @@ int run(int argc, char** argv) {
             "kernel must be 'fft', '2d-rfft', 'pruned-horizontal', 'vertical-gemm', 'pointwise-advection', "
             "'production-lifetime-flux', 'spectral-pipeline' or 'constant-stratification-vertical'.");
     if (records.empty()) records.push_back(rec);
+    if (!o.boundaryPolicy.empty() || o.tileWidth != 1 || o.inversePolicy != "full-zero") {
+        const std::string detail = "boundary policy '" + (o.boundaryPolicy.empty() ? "default" : o.boundaryPolicy) +
+                                   "', tile width " + std::to_string(o.tileWidth) + ", inverse preparation '" +
+                                   o.inversePolicy +
+                                   "': recorded only; the GPU column embed rebuilds each column band from the "
+                                   "retained values in one pass, so these CPU scratch strategies have no "
+                                   "counterpart and do not change the result";
+        for (auto& r : records) r.ledger.push_back({"streaming preparation options", StageState::elided, detail});
+    }
     for (auto& r : records) {
         r.compilerFlags = "nvcc -gencode arch=compute_100a,code=sm_100a -O3";
         r.sourceIdentity = std::string("libskb_cuda ") + skb_version();

@@ -55,3 +55,29 @@ def test_bad_fixture_exits_2(tmp_path):
     assert "wrong magic" in out.stderr
     out = cli("run", "--kernel", "fft", "--spectral-flux-fixture", str(bad))
     assert out.returncode == 2 and "valid only for production-lifetime-flux" in out.stderr
+
+
+@pytest.mark.parametrize("args,message", [
+    (("--kernel", "fft", "--streaming-inverse-policy", "active-reset"), "production-lifetime-flux only"),
+    (("--kernel", "production-lifetime-flux", "--streaming-inverse-policy", "compact-preserved"),
+     "needs a prepared fixture"),
+    (("--kernel", "production-lifetime-flux", "--streaming-inverse-policy", "sideways"), "expected full-zero"),
+    (("--kernel", "production-lifetime-flux", "--boundary-policy", "wvm-packed-split"),
+     "wvm-direct, streaming-pruned-compact-split"),
+    (("--kernel", "spectral-pipeline", "--boundary-policy", "pruned-compact-interleaved"), "plane-major-fused-split"),
+])
+def test_streaming_options_are_checked_like_the_reference(args, message):
+    """--boundary-policy / --streaming-tile-width / --streaming-inverse-policy
+    (the reference's streaming-provider knobs) are accepted, and the values the
+    reference refuses for a kernel are refused with exit 2 before device work."""
+    out = cli("run", *args)
+    assert out.returncode == 2, out.stdout + out.stderr
+    assert message in out.stderr
+
+
+def test_tile_width_other_than_sixteen_is_refused_for_a_prepared_fixture(tmp_path):
+    path = tmp_path / "f.bin"
+    path.write_bytes(b"SKFXP001")
+    out = cli("run", "--kernel", "production-lifetime-flux", "--spectral-flux-fixture", str(path),
+              "--streaming-tile-width", "8")
+    assert out.returncode == 2 and "16-plane tiles" in out.stderr

@@ -129,3 +129,15 @@ def test_authoritative_fixture_run(tmp_path, mode):
     provider = report["providers"][0]
     assert len(provider["correctness"]) == 1 and provider["correctness"][0]["passed"]
     assert "synthetic" in provider["planning"]["configuration"]
+
+
+def test_streaming_options_are_recorded(tmp_path):
+    """The reference's streaming-provider knobs run the flux unchanged and are
+    recorded in the provider's ledger."""
+    report, _ = run(tmp_path, "--kernel", "production-lifetime-flux", "--flux-mode", "fp64-plain", "--nx", "32",
+                    "--ny", "32", "--nz", "9", "--boundary-policy", "streaming-pruned-compact-split",
+                    "--streaming-tile-width", "16")
+    assert report["status"] == "passed"
+    ledger = report["providers"][0]["componentLedger"]
+    entry = next(e for e in ledger if e["stage"] == "streaming preparation options")
+    assert "streaming-pruned-compact-split" in entry["detail"] and "tile width 16" in entry["detail"]

@@ -154,3 +154,27 @@ def test_tf32x3_rejects_split_layout():
     w = skb_cuda.Workload(16, 16, 9, 3)
     with pytest.raises(ValueError):
         provider(w, layout=skb_cuda.SPLIT, precision=skb_cuda.GEMM_TF32X3)
+
+
+def test_tf32x3_expired_wait_is_reported_and_the_context_survives():
+    """The tensor-core GEMM's error path: a bounded device wait on a barrier
+    that nothing signals runs out; the call reports SKB_ERR_RUNTIME instead of
+    hanging, and a new provider on the same context computes correctly."""
+    import ctypes
+
+    shape = (64, 64, 17, 2)
+    w = skb_cuda.Workload(*shape)
+    H = len(orc.retained_modes(w.nx, w.ny))
+    rng = np.random.default_rng(3)
+    phys = rng.uniform(-1, 1, H * w.fields * w.nz) + 1j * rng.uniform(-1, 1, H * w.fields * w.nz)
+    vp = provider(w, precision=skb_cuda.GEMM_TF32X3)
+    skb_cuda.check(skb_cuda.library().skb_vertical_expire_wait_for_test(vp.h, ctypes.c_int(1)))
+    vp.load_physical_input(phys)
+    with pytest.raises(RuntimeError, match="bounded device wait expired"):
+        vp.execute_forward()
+    vp.close()
+    fresh = provider(w, precision=skb_cuda.GEMM_TF32X3)
+    fresh.load_physical_input(phys)
+    fresh.execute_forward()
+    ref = orc.grouped_vertical(orc.Workload(*shape), orc.k2_family(orc.Workload(*shape)), "forward", phys)
+    assert orc.rel_l2_error(fresh.copy_forward_output(), ref) <= 1e-6
