@@ -51,7 +51,8 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
-    p.add_argument("--mode", choices=["split", "fp32", "fp64"], default="split")
+    p.add_argument("--mode", choices=["split", "bf16x3", "fp32", "fp64"], default="split",
+                   help="split: split-TF32x3 tensor-core GEMMs; bf16x3: split-BF16x3 ones")
     p.add_argument("--n", type=int, default=512)
     p.add_argument("--nz", type=int, default=129)
     p.add_argument("--members", type=int, default=8)
@@ -286,7 +287,8 @@ def profile_run(args, dist):
     import skb_cuda as S
 
     S.set_device(dist.local)
-    mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
+    mode = {"split": S.FLUX_SPLIT_TF32X3, "bf16x3": S.FLUX_SPLIT_BF16X3, "fp32": S.FLUX_FP32,
+            "fp64": S.FLUX_FP64_PLAIN}[args.mode]
     families = synthetic_families(args.n, args.nz) if args.families else None
     flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode, families=families)
     x = power_law_inputs(args.n, args.nz, args.members, seed=129 + dist.rank)
@@ -306,10 +308,11 @@ def cuda_arm(args, dist):
     import skb_cuda as S
 
     S.set_device(dist.local)
-    mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
+    mode = {"split": S.FLUX_SPLIT_TF32X3, "bf16x3": S.FLUX_SPLIT_BF16X3, "fp32": S.FLUX_FP32,
+            "fp64": S.FLUX_FP64_PLAIN}[args.mode]
     families = synthetic_families(args.n, args.nz) if args.families else None
     flux = S.Flux(args.n, args.nz, targets=4, members=args.members, mode=mode, families=families)
-    mode_name = {"split": "split-tf32x3"}.get(args.mode, args.mode)
+    mode_name = {"split": "split-tf32x3", "bf16x3": "split-bf16x3"}.get(args.mode, args.mode)
     dtype = flux.device_dtype
     x = power_law_inputs(args.n, args.nz, args.members, seed=129 + dist.rank)
     din = S.DeviceArray.from_numpy(x.astype(dtype))
@@ -419,7 +422,7 @@ def cuda_arm(args, dist):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if mode == S.FLUX_FP64_PLAIN else ("f32" if mode == S.FLUX_FP32 else "tf32x3+f32"),
+        "dtype": {S.FLUX_FP64_PLAIN: "f64", S.FLUX_FP32: "f32", S.FLUX_SPLIT_BF16X3: "bf16x3+f32"}.get(mode, "tf32x3+f32"),
         "data": "synthetic (seeded k^-3 power-law modal spectra, "
                 + ("seeded Gaussian wave-f / wave-g operator families over the K^2 groups)" if families else
                    "K^2 pair-rotation vertical family)"),
@@ -522,17 +525,18 @@ def serve_arm(args, dist):
     import skb_cuda as S
 
     S.set_device(dist.local)
-    mode = {"split": S.FLUX_SPLIT_TF32X3, "fp32": S.FLUX_FP32, "fp64": S.FLUX_FP64_PLAIN}[args.mode]
+    mode = {"split": S.FLUX_SPLIT_TF32X3, "bf16x3": S.FLUX_SPLIT_BF16X3, "fp32": S.FLUX_FP32,
+            "fp64": S.FLUX_FP64_PLAIN}[args.mode]
     r = serving_run(S, mode, args.serve_rate, args.serve_requests, args.serve_batch, args.serve_states, dist)
     if dist.rank != 0:
         return None
-    mode_name = {"split": "split-tf32x3"}.get(args.mode, args.mode)
+    mode_name = {"split": "split-tf32x3", "bf16x3": "split-bf16x3"}.get(args.mode, args.mode)
     return {
         "metric": "serving p99 latency, mixed flux requests (40% 128²×33 f3, 40% 256²×65 f3, 20% 512²×129 f4)",
         "value": r["p99_ms"], "unit": "ms", "n_gpus": dist.world,
         "steps": args.serve_requests, "warmup": len(SERVE_CLASSES), "ms_per_step": r["mean_ms"],
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if mode == S.FLUX_FP64_PLAIN else ("f32" if mode == S.FLUX_FP32 else "tf32x3+f32"),
+        "dtype": {S.FLUX_FP64_PLAIN: "f64", S.FLUX_FP32: "f32", S.FLUX_SPLIT_BF16X3: "bf16x3+f32"}.get(mode, "tf32x3+f32"),
         "data": "synthetic (seeded k^-3 power-law resident states, seeded Poisson arrivals)",
         "config": {"workload": "continuous-batching flux server", "mode": mode_name,
                    "arrival_rate_per_s": args.serve_rate, "requests": args.serve_requests,

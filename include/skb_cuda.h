@@ -505,7 +505,10 @@ SKB_API void* skb_cs_vertical_stream(skb_cs_vertical* p);
  * FP64 complex arrays of one member ([mode][field][j]) or resident states
  * loaded once; results are written to the caller's host array (pinned memory
  * keeps the copy asynchronous).  A member's result does not depend on the
- * other requests in its batch. */
+ * other requests in its batch.  Slot streams carry priorities by class size
+ * (the class with the least work per request highest), so a small request's
+ * kernels are dispatched ahead of the waiting CTAs of a larger class's batch.
+ * slot_bytes is the sum of the slots' own device allocations. */
 typedef struct skb_server_class {
     uint64_t n, nz, targets, max_batch;
     int32_t mode; /* SKB_FLUX_* */

@@ -847,12 +847,12 @@ int skb_vertical_create(const skb_workload* w, const skb_mode_group* groups, uin
         } else if (gemm_precision == SKB_GEMM_FP32) {
             p->gp = GemmPrecision::f32;
             p->p = Precision::f32;
-        } else if (gemm_precision == SKB_GEMM_TF32X3) {
-            require(layout == SKB_LAYOUT_INTERLEAVED, "the split-TF32x3 tensor-core form takes the interleaved layout");
-            p->gp = GemmPrecision::tf32x3;
+        } else if (gemm_precision == SKB_GEMM_TF32X3 || gemm_precision == SKB_GEMM_BF16X3) {
+            require(layout == SKB_LAYOUT_INTERLEAVED, "the split tensor-core forms take the interleaved layout");
+            p->gp = gemm_precision == SKB_GEMM_TF32X3 ? GemmPrecision::tf32x3 : GemmPrecision::bf16x3;
             p->p = Precision::f32;
         } else {
-            throw Error(SKB_ERR_RUNTIME, "unsupported: the split-BF16x3 GEMM form is not built in this library");
+            throw Error(SKB_ERR_INVALID_ARGUMENT, "unknown vertical GEMM precision");
         }
         p->host.p = p->p;
         const auto prepStart = Clock::now();
@@ -930,11 +930,11 @@ int skb_vertical_wvm_create(const skb_workload* w, const skb_mode_group* groups,
         } else if (gemm_precision == SKB_GEMM_FP32) {
             p->gp = GemmPrecision::f32;
             p->p = Precision::f32;
-        } else if (gemm_precision == SKB_GEMM_TF32X3) {
-            p->gp = GemmPrecision::tf32x3;
+        } else if (gemm_precision == SKB_GEMM_TF32X3 || gemm_precision == SKB_GEMM_BF16X3) {
+            p->gp = gemm_precision == SKB_GEMM_TF32X3 ? GemmPrecision::tf32x3 : GemmPrecision::bf16x3;
             p->p = Precision::f32;
         } else {
-            throw Error(SKB_ERR_RUNTIME, "unsupported: the split-BF16x3 GEMM form is not built in this library");
+            throw Error(SKB_ERR_INVALID_ARGUMENT, "unknown vertical GEMM precision");
         }
         p->host.p = p->p;
         const auto prepStart = Clock::now();
@@ -1428,7 +1428,8 @@ int skb_vertical_load_modal_input_split(skb_vertical_provider* p, const double* 
 int skb_vertical_expire_wait_for_test(skb_vertical_provider* p, int enable) {
     return guard([&] {
         require(p != nullptr, "handle must be non-null");
-        require(p->gp == GemmPrecision::tf32x3, "the expired-wait test applies to the tensor-core GEMM form");
+        require(p->gp == GemmPrecision::tf32x3 || p->gp == GemmPrecision::bf16x3,
+                "the expired-wait test applies to the tensor-core GEMM forms");
         for (auto* plan : {p->forward.get(), p->inverse.get()})
             if (plan) plan->set_expire_wait_for_test(enable != 0);
     });

@@ -16,8 +16,6 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
     if (cfg.members == 0) throw Error(-1, "flux requires at least one ensemble member");
     if (3 * cfg.members > static_cast<std::uint64_t>(kMaxViews))
         throw Error(-1, "at most " + std::to_string(kMaxViews / 3) + " ensemble members per flux handle");
-    if (cfg.mode == FluxMode::split_bf16x3)
-        throw Error(-2, "unsupported: the split-BF16x3 flux mode is not built in this library (use split-TF32x3)");
     const auto planStart = Clock::now();
     wOut_ = Workload{cfg.n, cfg.n, cfg.nz, cfg.targets, 1.0, 1.0, true};
     fieldsIn_ = 3 + 3 * cfg.targets;
@@ -57,11 +55,13 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
 
     const auto allocStart = Clock::now();
     const Precision hp = f64() ? Precision::f64 : Precision::f32;
-    const GemmPrecision gp = f64() ? GemmPrecision::f64
+    const bool split = cfg.mode == FluxMode::split_tf32x3 || cfg.mode == FluxMode::split_bf16x3;
+    const GemmPrecision gp = f64()                                ? GemmPrecision::f64
                              : cfg.mode == FluxMode::split_tf32x3 ? GemmPrecision::tf32x3
+                             : cfg.mode == FluxMode::split_bf16x3 ? GemmPrecision::bf16x3
                                                                   : GemmPrecision::f32;
     const size_t es = element_bytes(hp);
-    fused_ = cfg.mode == FluxMode::split_tf32x3 && rows_flux_supported(static_cast<long long>(cfg.n));
+    fused_ = split && rows_flux_supported(static_cast<long long>(cfg.n));
     // Admission by device memory: refuse before allocating what cannot fit.
     const std::uint64_t maxPlanes = fused_ ? 1 : 3 * cfg.members * cfg.nz;
     const std::uint64_t binPlanes = fused_ ? cfg.members * cfg.nz * (fieldsIn_ + cfg.targets) : maxPlanes;
@@ -167,7 +167,8 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
 
 // Tuned launch shapes of the fused path (autotune.hpp):
 //   work-unit size (M-tiles per unit) of each tensor-core GEMM, 4 / 8 / 16 / 32;
-//   z-planes (warps) per CTA of the fused row kernel, 4 / 8 / 16;
+//   the 512-point row kernel's form (one plane per warp, or two planes per
+//   warp with the 16 x 16 FFT) and its z-planes per CTA, 4 / 8 / 16;
 //   kernel form of each 512-point band column stage, direct / warp-per-plane /
 //   persistent direct.
 // With buffers, missing choices are measured on them (tune_pick); without,
@@ -215,7 +216,8 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
         };
     };
     auto gemmKey = [&](const char* dir, const VerticalPlan& g) {
-        return std::string("flux.tc_gemm.unit_tiles ") + dir + shape + " R=" + std::to_string(g.rows_out()) +
+        return std::string("flux.tc_gemm.unit_tiles ") + dir + (g.precision() == GemmPrecision::bf16x3 ? " bf16x3" : "") +
+               shape + " R=" + std::to_string(g.rows_out()) +
                " S=" + std::to_string(g.inner()) + " groups=" + std::to_string(g.groups()) + dev;
     };
     const std::vector<int> tileCandidates{4, 8, 16, 32};
@@ -226,7 +228,18 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
     if (!families_) pick(gemmKey("forward", *forwardGemm_), tileCandidates, unitTiles(*forwardGemm_), [&] {
         forwardGemm_->execute({binsOut_.get(), nullptr}, {modalOut, nullptr}, s, M, &gemmIn, nullptr);
     });
-    pick("flux.rows.planes_per_cta" + shape + dev, {4, 8, 16}, [&](int c) { rowsPlanes_ = c; },
+    if (cfg_.n == 512) {
+        // Row kernel form first (two planes per warp needs 8 or 16 planes per
+        // CTA), then the planes per CTA among those the form takes.
+        pick("flux.rows.pairs" + shape + dev, {0, 1},
+             [&](int c) {
+                 rowsPairs_ = c;
+                 if (c != 0 && rowsPlanes_ < 8) rowsPlanes_ = 8;
+             },
+             [&] { check_cuda(launch_rows_flux(row_args(M), s), "fused row flux kernel"); });
+    }
+    pick("flux.rows.planes_per_cta" + shape + dev, rowsPairs_ != 0 ? std::vector<int>{8, 16} : std::vector<int>{4, 8, 16},
+         [&](int c) { rowsPlanes_ = c; },
          [&] { check_cuda(launch_rows_flux(row_args(M), s), "fused row flux kernel"); });
     if (cfg_.n == 512) {
         // Both forms run in place on the bin arrays; repeated runs leave values
@@ -345,6 +358,7 @@ RowFluxArgs FluxPipeline::row_args(std::uint64_t members) const {
     a.twHalf = horizontal_->twiddlesHalf();
     a.twFull = horizontal_->twiddlesFull();
     a.planes = rowsPlanes_;
+    a.pairs = rowsPairs_;
     return a;
 }
 
@@ -366,15 +380,22 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
     const long long outStored = static_cast<long long>(cfg_.members * T * zStride_);
     const DenseBins binsIn{binsIn_.get(), inStored, keep};
     const DenseBins binsOutArr{binsOut_.get(), outStored, keep};
+    // Tensor-core products per real multiply-add: 3 (TF32 hi/lo) or 6 (BF16 h/m/l).
+    const bool bf16 = cfg_.mode == FluxMode::split_bf16x3;
+    const double splitTerms = bf16 ? 6.0 : 3.0;
+    auto gemmStage = [bf16](bool inverse) {
+        return inverse ? (bf16 ? "gemm_inverse_bf16x3" : "gemm_inverse_tf32x3")
+                       : (bf16 ? "gemm_forward_bf16x3" : "gemm_forward_tf32x3");
+    };
     if (dense_) {
         // GEMM -> retained cells of binsIn -> in-place inverse columns.
         gemm_inverse(modalIn, s, M, true);
-        if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
+        if (rec) rec->end(gemmStage(true), 1, gemmIn, splitTerms * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
         horizontal_->inverse_columns_band(binsIn, static_cast<int>(M * fieldsIn_), static_cast<int>(zStride_), s);
         if (rec) rec->end("columns_inverse_embed", 1, double(inPlanes) * (compactPlane + binsPlane), 0.0);
     } else {
         gemm_inverse(modalIn, s, M, false);
-        if (rec) rec->end("gemm_inverse_tf32x3", 1, gemmIn, 3.0 * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
+        if (rec) rec->end(gemmStage(true), 1, gemmIn, splitTerms * 4.0 * nz * nj_ * double(M) * H * fieldsIn_);
         ViewSet inViews{};
         inViews.count = static_cast<int>(M * fieldsIn_);
         for (std::uint64_t m = 0; m < M; ++m)
@@ -394,7 +415,7 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
         horizontal_->forward_columns_band(binsOutArr, static_cast<int>(M * T), 1.0, static_cast<int>(zStride_), s);
         if (rec) rec->end("columns_forward_gather", 1, double(outPlanes) * (binsPlane + compactPlane), 0.0);
         gemm_forward(modalOut, s, M, true);
-        if (rec) rec->end("gemm_forward_tf32x3", 1, gemmOut, 3.0 * 4.0 * nz * nj_ * double(M) * H * T);
+        if (rec) rec->end(gemmStage(false), 1, gemmOut, splitTerms * 4.0 * nz * nj_ * double(M) * H * T);
         return;
     }
     ViewSet outViews{};
@@ -406,7 +427,7 @@ void FluxPipeline::runFused(const void* modalIn, void* modalOut, cudaStream_t s,
     if (rec) rec->end("columns_forward_gather", 1, double(outPlanes) * (binsPlane + compactPlane), 0.0);
 
     gemm_forward(modalOut, s, M, false);
-    if (rec) rec->end("gemm_forward_tf32x3", 1, gemmOut, 3.0 * 4.0 * nz * nj_ * double(M) * H * T);
+    if (rec) rec->end(gemmStage(false), 1, gemmOut, splitTerms * 4.0 * nz * nj_ * double(M) * H * T);
 }
 
 void FluxPipeline::run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members) {

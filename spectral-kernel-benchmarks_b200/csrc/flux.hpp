@@ -132,6 +132,7 @@ private:
     // Per mode: element offset of (member 0, field 0) in the compact arrays.
     DeviceBuffer cellModalIn_, cellModalOut_, cellPhysIn_, cellPhysOut_;
     int rowsPlanes_ = 8;  // z-planes per CTA of the fused row kernel
+    int rowsPairs_ = 0;   // 512-point rows: two planes per warp (RowFluxArgs::pairs)
     void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graphExec_ = nullptr;

@@ -248,6 +248,237 @@ __global__ void __launch_bounds__(32 * B, 16 / B) rows_flux_kernel(RowFluxArgs a
     }
 }
 
+// ---------------------------------------------------------------------------
+// 512-point rows, two planes per warp.
+//
+// The 256-point complex FFT of the half-length formulation is split 16 x 16:
+// lane t of a half-warp holds elements t + 16 m (m = 0..15) of its plane's
+// sequence; a radix-16 DFT over m in registers, the twiddles W256^(t k2), one
+// 16 x 16 transpose through shared memory, and a second radix-16 DFT in
+// registers leave output k = t + 16 k1 in register k1 — the same lane-owned
+// positions as the input, so U, V, W and the product stay in registers across
+// all transforms as in the warp-per-plane kernel, with one shared-memory
+// exchange per transform instead of two.  Lanes 0-15 own plane 2w of warp w,
+// lanes 16-31 plane 2w + 1.
+
+// Twiddle W16^e with exponent sign SIGN, e in {1, 2, 3, 6, 9} (e = 4 is a
+// multiplication by SIGN*i): cos(2 pi e / 16) + SIGN i sin(2 pi e / 16).
+template <int SIGN, int E>
+__device__ __forceinline__ float2 w16() {
+    constexpr float c1 = 0.923879532511286756128f;  // cos(pi/8)
+    constexpr float s1 = 0.382683432365089771728f;  // sin(pi/8)
+    constexpr float h = 0.707106781186547524401f;   // cos(pi/4)
+    constexpr float sg = SIGN < 0 ? -1.0f : 1.0f;
+    if constexpr (E == 1) return {c1, sg * s1};
+    if constexpr (E == 2) return {h, sg * h};
+    if constexpr (E == 3) return {s1, sg * c1};
+    if constexpr (E == 6) return {-h, sg * h};
+    return {-c1, -sg * s1};  // E == 9
+}
+
+// In-place length-16 DFT over v[0..15] (natural order in and out): 16 = 4 x 4,
+// input m = m2 + 4 m1, output k = k1 + 4 k2.
+template <int SIGN>
+__device__ __forceinline__ void dft16(float2 (&v)[16]) {
+#pragma unroll
+    for (int m2 = 0; m2 < 4; ++m2) dft4<SIGN>(v[m2], v[m2 + 4], v[m2 + 8], v[m2 + 12]);
+    // v[m2 + 4 k1] *= W16^(m2 k1)
+    v[5] = cmul(v[5], w16<SIGN, 1>());
+    v[9] = cmul(v[9], w16<SIGN, 2>());
+    v[13] = cmul(v[13], w16<SIGN, 3>());
+    v[6] = cmul(v[6], w16<SIGN, 2>());
+    v[10] = cmul_si<SIGN>(v[10]);
+    v[14] = cmul(v[14], w16<SIGN, 6>());
+    v[7] = cmul(v[7], w16<SIGN, 3>());
+    v[11] = cmul(v[11], w16<SIGN, 6>());
+    v[15] = cmul(v[15], w16<SIGN, 9>());
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft4<SIGN>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    // v[4 k1 + k2] holds output k1 + 4 k2: transpose the 4 x 4 block.
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = i + 1; j < 4; ++j) {
+            const float2 t = v[4 * i + j];
+            v[4 * i + j] = v[4 * j + i];
+            v[4 * j + i] = t;
+        }
+}
+
+// 256-point FFT of one half-warp's sequence: v[m] = z[t + 16 m] in, Z[t + 16 k]
+// in v[k] out.  xch: this half-warp's 16 x 17 exchange region; tw2[16 k2 + t] =
+// exp(-2 pi i t k2 / 256) (conjugated for SIGN > 0).
+template <int SIGN>
+__device__ __forceinline__ void fft256_pair(float2 (&v)[16], float2* xch, const float2* tw2, int t) {
+    dft16<SIGN>(v);
+#pragma unroll
+    for (int k2 = 1; k2 < 16; ++k2) {
+        const float2 w = tw2[16 * k2 + t];
+        v[k2] = SIGN < 0 ? cmul(v[k2], w) : cmulc(v[k2], w);
+    }
+    __syncwarp();  // the previous transform's reads of xch are done
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) xch[17 * t + k2] = v[k2];
+    __syncwarp();
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) v[n1] = xch[17 * n1 + t];
+    dft16<SIGN>(v);
+}
+
+constexpr int kPairM = 256;       // half-length of the 512-point rows
+constexpr int kPairXch = 16 * 17;  // exchange words per plane
+template <int B>
+constexpr int pair_stage_row() {
+    // kx = 0..M (the pre-processing reads X[M - k]), and a residue mod 16 (in
+    // 8-byte words) that spreads one cp.async instruction's B planes x 32/B
+    // kx over the 16 bank pairs exactly twice.
+    constexpr int want = B == 16 ? 1 : 2;
+    return kPairM + 1 + ((want - (kPairM + 1) % 16) + 16) % 16;
+}
+template <int B>
+constexpr size_t pair_smem_words(int keep) {
+    return 2 * size_t(B) * pair_stage_row<B>() + size_t(B) * kPairXch + size_t(keep) * B + kPairM + kPairM;
+}
+
+template <int B>
+__global__ void __launch_bounds__(16 * B, B == 8 ? 2 : 1) rows_flux_pair_kernel(RowFluxArgs a) {
+    using V = float2;
+    constexpr int M = kPairM;
+    constexpr int NT = 16 * B;
+    constexpr int KP = pair_stage_row<B>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int keep = a.keep;
+    V* stage0 = reinterpret_cast<V*>(smem_raw);
+    V* stage1 = stage0 + B * KP;
+    V* xchAll = stage1 + B * KP;
+    V* outTile = xchAll + B * kPairXch;  // [k][b] at out_slot(k, b)
+    V* tf = outTile + keep * B;          // twFull[0..M)
+    V* tw2 = tf + M;                     // tw2[16 k2 + t] = twHalf[(t k2) mod M]
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int t = lane & 15;
+    const int pl = 2 * warp + (lane >> 4);  // this half-warp's plane within the CTA
+    const int zChunks = (a.nz + B - 1) / B;
+    const int member = blockIdx.x / zChunks;
+    const int z0 = (blockIdx.x % zChunks) * B;
+    const int y = blockIdx.y;
+    const V* twHalf = static_cast<const V*>(a.twHalf);
+    const V* twFull = static_cast<const V*>(a.twFull);
+    const V* in = static_cast<const V*>(a.binsIn.data);
+    V* out = static_cast<V*>(a.binsOut.data);
+    const long long inRow = a.binsIn.planes;
+    const long long outRow = a.binsOut.planes;
+    V* xch = xchAll + pl * kPairXch;
+
+    for (int i = tid; i < M; i += NT) {
+        tf[i] = twFull[i];
+        tw2[i] = twHalf[((i & 15) * (i >> 4)) & (M - 1)];
+    }
+    for (int i = tid; i < 2 * B * (KP - keep); i += NT) {
+        const int row = i / (KP - keep);
+        stage0[row * KP + keep + i % (KP - keep)] = V{0.f, 0.f};
+    }
+
+    // Slot f's bins of this row into a plane-major stage [b][k] (cp.async, as
+    // in the warp-per-plane kernel; planes beyond Nz are zero-filled).
+    constexpr int KSTEP = NT / B;
+    const int cb = tid % B;
+    const int ck = tid / B;
+    const bool cok = z0 + cb < a.nz;
+    auto issue = [&](int f, V* stage) {
+        const long long plane = (static_cast<long long>(member) * a.fieldsIn + f) * a.zStride + z0 + cb;
+        const V* src = in + plane + inRow * (a.binsIn.kxStride * y + ck);
+        V* dst = stage + cb * KP + ck;
+        for (int k = ck; k < keep; k += KSTEP, src += inRow * KSTEP, dst += KSTEP) cp_async8(dst, cok ? src : in, cok ? 8 : 0);
+        cp_async_commit();
+    };
+
+    // c2r of slot f into r[m] = x-pair t + 16 m of this half-warp's plane.
+    auto inverse_row = [&](int f, V (&r)[16]) {
+        cp_async_wait_all();
+        __syncthreads();
+        if (f + 1 < a.fieldsIn) issue(f + 1, ((f + 1) & 1) ? stage1 : stage0);
+        const V* st = ((f & 1) ? stage1 : stage0) + pl * KP;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int k = t + 16 * m;
+            V xk = st[k];
+            V xm = st[M - k];
+            if (m == 0 && t == 0) {  // bins 0 and M are real
+                xk.y = 0.f;
+                xm.y = 0.f;
+            }
+            const V sum = cadd(xk, cconj(xm));
+            const V d = csub(xk, cconj(xm));
+            const V tt = cmulc(d, tf[k]);
+            r[m] = {sum.x - tt.y, sum.y + tt.x};
+        }
+        fft256_pair<+1>(r, xch, tw2, t);
+    };
+
+    issue(0, stage0);
+    V u[16], v[16], w[16];
+    inverse_row(0, u);
+    inverse_row(1, v);
+    inverse_row(2, w);
+    const float scale = a.scale;
+    const int src = ((16 - t) & 15) + (lane & 16);  // lane holding Z[M - k]
+    for (int tg = 0; tg < a.targets; ++tg) {
+        V acc[16], q[16];
+        inverse_row(3 + 3 * tg, q);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) acc[e] = {u[e].x * q[e].x, u[e].y * q[e].y};
+        inverse_row(4 + 3 * tg, q);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) acc[e] = {acc[e].x + v[e].x * q[e].x, acc[e].y + v[e].y * q[e].y};
+        inverse_row(5 + 3 * tg, q);
+#pragma unroll
+        for (int e = 0; e < 16; ++e)
+            acc[e] = {-scale * (acc[e].x + w[e].x * q[e].x), -scale * (acc[e].y + w[e].y * q[e].y)};
+        fft256_pair<-1>(acc, xch, tw2, t);
+        // Real-spectrum split, kx < keep, into [k][b].  Z[M - k] for k = t + 16 k1
+        // is register 15 - k1 of lane 16 - t (t > 0) or register (16 - k1) mod 16
+        // of this lane (t = 0).
+#pragma unroll
+        for (int k1 = 0; k1 < 11; ++k1) {  // k < 176 >= keep
+            const V other = {__shfl_sync(0xFFFFFFFFu, acc[15 - k1].x, src),
+                             __shfl_sync(0xFFFFFFFFu, acc[15 - k1].y, src)};
+            const int k = t + 16 * k1;
+            const V zk = acc[k1];
+            const V zm = cconj(t == 0 ? acc[(16 - k1) & 15] : other);
+            V X;
+            if (k == 0) {
+                X = {zk.x + zk.y, 0.f};
+            } else {
+                const V ev = cscale(cadd(zk, zm), 0.5f);
+                const V d = csub(zk, zm);
+                const V o = {0.5f * d.y, -0.5f * d.x};
+                X = cadd(ev, cmul(tf[k < M ? k : 0], o));
+            }
+            if (k < keep) outTile[out_slot<B>(k, pl)] = X;
+        }
+        __syncthreads();
+        if (cok) {
+            const long long plane = (static_cast<long long>(member) * a.targets + tg) * a.zStride + z0 + cb;
+            V* dst = out + plane + outRow * (a.binsOut.kxStride * y + ck);
+            for (int k = ck; k < keep; k += KSTEP, dst += outRow * KSTEP) *dst = outTile[out_slot<B>(k, cb)];
+        }
+        // The next outTile write happens after the next inverse_row's barrier.
+    }
+}
+
+template <int B>
+cudaError_t launch_pair(const RowFluxArgs& a, cudaStream_t stream) {
+    const int zChunks = (a.nz + B - 1) / B;
+    const dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
+    auto kernel = rows_flux_pair_kernel<B>;
+    const size_t bytes = sizeof(float2) * pair_smem_words<B>(a.keep);
+    const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (err != cudaSuccess) return err;
+    kernel<<<grid, 16 * B, bytes, stream>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 template <int M, int B>
@@ -277,6 +508,10 @@ cudaError_t launch_planes(const RowFluxArgs& a, cudaStream_t stream) {
 cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
     const int M = a.nx / 2;
     if (a.keep < 1 || a.keep > M + 1 || a.fieldsIn != 3 + 3 * a.targets || a.zStride < a.nz) return cudaErrorInvalidValue;
+    if (a.pairs != 0 && M == kPairM && a.keep <= 176) {
+        if (a.planes == 8) return launch_pair<8>(a, stream);
+        if (a.planes == 16) return launch_pair<16>(a, stream);
+    }
     switch (M) {
         case 32: return launch_planes<32>(a, stream);
         case 64: return launch_planes<64>(a, stream);

@@ -278,19 +278,21 @@ VerticalPlan::VerticalPlan(GemmPrecision p, int rowsOut, int inner, const std::v
     memberColumns_ = static_cast<long long>(perMember);
     const std::uint64_t groupsCount = common ? 1 : groups.size();
 
-    if (p == GemmPrecision::tf32x3) {
+    if (p == GemmPrecision::tf32x3 || p == GemmPrecision::bf16x3) {
         if (!tc_gemm_supported(rowsOut, inner))
             throw Error(-2, "unsupported: tensor-core GEMM needs the padded group matrix and two data stages in "
                             "227 KB of shared memory (R=" + std::to_string(rowsOut) + ", S=" + std::to_string(inner) +
                             ")");
         // FP32 matrices (one, if common to all groups) -> the kernel's
-        // operand images, split into TF32 hi/lo and swizzled once here.
+        // operand images, split into TF32 hi/lo or BF16 h/m/l and swizzled
+        // once here.
         std::vector<float> f(natural.begin(), natural.end());
         const DeviceBuffer staged = upload_vector(f);
         const int images = static_cast<int>(groupsCount);
         imageStride_ = common ? 0 : static_cast<long long>(tc_gemm_image_bytes(rowsOut, inner));
         matrices_.allocate(static_cast<size_t>(images) * tc_gemm_image_bytes(rowsOut, inner));
-        check_cuda(tc_gemm_build_images(staged.get<float>(), images, rowsOut, inner, matrices_.get(), nullptr),
+        check_cuda(tc_gemm_build_images(staged.get<float>(), images, rowsOut, inner,
+                                        p == GemmPrecision::bf16x3 ? 1 : 0, matrices_.get(), nullptr),
                    "tensor-core GEMM operand images");
         check_cuda(cudaStreamSynchronize(nullptr), "tensor-core GEMM operand images");
         std::vector<int> gc(groups.size()), gf(groups.size());
@@ -391,7 +393,7 @@ void VerticalPlan::build_units(int tiles) {
 }
 
 void VerticalPlan::set_unit_tiles(int tiles) {
-    if (p_ != GemmPrecision::tf32x3) throw Error(-3, "work-unit size applies to the tensor-core form only");
+    if (!tensor_core()) throw Error(-3, "work-unit size applies to the tensor-core forms only");
     if (tiles != unitTiles_) build_units(tiles);
 }
 
@@ -408,7 +410,7 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
                            const BinBoundary* inBins, const BinBoundary* outBins) const {
     if (members == 0) members = members_;
     if (members > members_) throw Error(-1, "more ensemble members than the plan was built for");
-    if (p_ == GemmPrecision::tf32x3) {
+    if (tensor_core()) {
         if (in.im != nullptr || out.im != nullptr)
             throw Error(-3, "the tensor-core GEMM form takes interleaved complex operands");
         const UnitTable& table = unitTables_[members - 1];
@@ -430,6 +432,7 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
         a.out = static_cast<float2*>(out.re);
         a.error = error_.get<int>();
         a.expireWaitForTest = expireWaitForTest_ ? 1 : 0;
+        a.kind = p_ == GemmPrecision::bf16x3 ? 1 : 0;
         if (inBins != nullptr) a.inBins = *inBins;
         if (outBins != nullptr) a.outBins = *outBins;
         check_cuda(launch_tc_gemm(a, s), "tensor-core grouped vertical GEMM kernel");

@@ -175,6 +175,8 @@ public:
     // nothing signals, so their bounded wait expires (tests the error path).
     void set_expire_wait_for_test(bool on) { expireWaitForTest_ = on; }
     GemmPrecision precision() const { return p_; }
+    // The split TF32x3 and BF16x3 forms run on the tcgen05 tensor cores.
+    bool tensor_core() const { return p_ == GemmPrecision::tf32x3 || p_ == GemmPrecision::bf16x3; }
     std::uint64_t columns() const { return columns_; }
     std::uint64_t matrixBytes() const { return matrices_.bytes(); }
     std::uint64_t persistentBytes() const;

@@ -6,15 +6,6 @@
 
 namespace skb {
 
-namespace {
-
-std::uint64_t free_device_bytes() {
-    size_t freeBytes = 0, totalBytes = 0;
-    check_cuda(cudaMemGetInfo(&freeBytes, &totalBytes), "cudaMemGetInfo");
-    return freeBytes;
-}
-
-}  // namespace
 
 Server::Server(const std::vector<ServerClass>& classes, std::uint64_t hbmBudget, int maxSlotsPerClass) {
     if (classes.empty()) throw Error(-1, "the server needs at least one size class");
@@ -32,10 +23,35 @@ Server::Server(const std::vector<ServerClass>& classes, std::uint64_t hbmBudget,
         cs.f64 = c.mode == FluxMode::fp64_plain;
         classes_.push_back(std::move(cs));
     }
+    // Stream priorities by size class: the class with the least work per
+    // request gets the highest priority, so its kernels' CTAs are dispatched
+    // ahead of the CTAs still waiting in a larger class's launches (running
+    // CTAs are not preempted) and a small request is not held behind a
+    // 512^2 batch.
+    int leastPriority = 0, greatestPriority = 0;
+    check_cuda(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority),
+               "cudaDeviceGetStreamPriorityRange");
+    {
+        std::vector<int> order(classes_.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = static_cast<int>(i);
+        auto work = [&](int i) {
+            const auto& c = classes_[i].config;
+            return static_cast<double>(c.n) * c.n * c.nz * (3 + 4 * c.targets) * (c.mode == FluxMode::fp64_plain ? 2 : 1);
+        };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) < work(b); });
+        // Priorities count down from greatestPriority (numerically the lowest).
+        int level = greatestPriority;
+        for (size_t r = 0; r < order.size(); ++r) {
+            if (r > 0 && work(order[r]) > work(order[r - 1]) && level < leastPriority) ++level;
+            classes_[order[r]].priority = level;
+        }
+    }
     // Slots: one per class first (the minimum service), then more round-robin
-    // while the measured footprint stays inside the budget.
+    // while the footprint stays inside the budget.  A slot's footprint is the
+    // sum of its own device allocations (the flux pipeline's persistent and
+    // scratch buffers, the batch input / output and the FP64 staging), so other
+    // allocations on the device cannot distort the accounting.
     auto makeSlot = [&](int cls) -> std::uint64_t {
-        const auto before = free_device_bytes();
         auto slot = std::make_unique<Slot>();
         slot->cls = cls;
         const auto& c = classes_[cls];
@@ -50,10 +66,11 @@ Server::Server(const std::vector<ServerClass>& classes, std::uint64_t hbmBudget,
         slot->in.allocate(es * c.inElems * fc.members);
         slot->out.allocate(es * c.outElems * fc.members);
         if (!c.f64) slot->stage.allocate(16 * std::max(c.inElems, c.outElems) * fc.members);
-        check_cuda(cudaStreamCreateWithFlags(&slot->stream, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+        check_cuda(cudaStreamCreateWithPriority(&slot->stream, cudaStreamNonBlocking, c.priority),
+                   "cudaStreamCreateWithPriority");
         check_cuda(cudaEventCreateWithFlags(&slot->event, cudaEventDisableTiming), "cudaEventCreateWithFlags");
-        const auto after = free_device_bytes();
-        const std::uint64_t bytes = before > after ? before - after : 0;
+        const std::uint64_t bytes = slot->flux->persistentBytes + slot->flux->scratchBytes + slot->in.bytes() +
+                                    slot->out.bytes() + slot->stage.bytes();
         stats_.slotBytes += bytes;
         slots_.push_back(std::move(slot));
         return bytes;

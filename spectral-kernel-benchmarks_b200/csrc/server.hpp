@@ -92,6 +92,7 @@ private:
     };
     struct ClassState {
         ServerClass config;
+        int priority = 0;  // stream priority of the class's slots (lower value = higher priority)
         std::deque<std::shared_ptr<Request>> queue;
         std::uint64_t inElems = 0, outElems = 0;
         bool f64 = true;

@@ -9,10 +9,16 @@
 // operands are K-major: Bop is the group matrix in its row-major [r][s]
 // layout, Aop is the data row in[c][0..S).
 //
-// Split precision: x = hi + lo with hi = rna_tf32(x), lo = rna_tf32(x - hi);
-// D = Ahi*Blo + Alo*Bhi + Ahi*Bhi accumulated in FP32 in tensor memory, one
-// accumulator per 32-wide K chunk, chunk sums added in FP32 registers.  The
-// dropped lo*lo term is ~2^-22 relative.
+// Split precision, two forms (KIND):
+// * TF32x3: x = hi + lo with hi = rna_tf32(x), lo = rna_tf32(x - hi);
+//   D = Ahi*Blo + Alo*Bhi + Ahi*Bhi (kind::tf32, K = 8 per MMA).  The dropped
+//   lo*lo term is ~2^-22 relative.
+// * BF16x3: x = h + m + l, three round-to-nearest BF16 pieces (8 significant
+//   bits each, so h + m + l carries all 24 bits of x); D = Al*Bh + Ah*Bl +
+//   Am*Bm + Am*Bh + Ah*Bm + Ah*Bh (kind::f16 with BF16 operands, K = 16 per
+//   MMA; the dropped m*l, l*m, l*l terms are <= 2^-24 relative).
+// Both accumulate in FP32 in tensor memory, one accumulator per 32-wide K
+// chunk, chunk sums added in FP32 registers.
 //
 // Work unit: one group and a run of up to 16 M-tiles of its (member,
 // column) list; each CTA (one per SM) walks its share of the units.  The
@@ -25,6 +31,8 @@
 // 16-byte chunk q of row n stored at chunk (q xor n%8).  One elected thread
 // issues the MMAs and commits them to the stage's mbarrier; every wait is
 // bounded and reports through `error` instead of hanging.
+
+#include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cstdint>
@@ -100,6 +108,16 @@ __device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uin
         : "memory");
 }
 
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    const uint32_t mask = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(mask)
+        : "memory");
+}
+
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
@@ -138,9 +156,53 @@ __device__ __forceinline__ uint32_t sw128_offset(int row, int q) {
     return static_cast<uint32_t>((row >> 3) * 1024 + (row & 7) * 128 + ((q ^ (row & 7)) << 4));
 }
 
+// Operand forms of the kernel.
+constexpr int kKindTf32x3 = 0;
+constexpr int kKindBf16x3 = 1;
+
 struct Split4 {
     float4 hi, lo;
 };
+
+// Four values as three BF16 pieces each, packed four to 8 bytes (value e at
+// bytes 2e, 2e+1): h = rn(x), m = rn(x - h), l = rn(x - h - m).  Both
+// differences are exact in FP32 (each piece holds the leading 8 bits of what
+// is left), so h + m + l equals x to within 2^-24 |x|.
+struct Split3 {
+    uint2 h, m, l;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);  // a in the low half
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ Split3 split3(float a, float b, float c, float d) {
+    const float x[4] = {a, b, c, d};
+    float h[4], m[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        h[e] = __bfloat162float(__float2bfloat16_rn(x[e]));
+        const float r = x[e] - h[e];
+        m[e] = __bfloat162float(__float2bfloat16_rn(r));
+        l[e] = r - m[e];
+    }
+    Split3 s;
+    s.h = make_uint2(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]));
+    s.m = make_uint2(pack_bf16x2(m[0], m[1]), pack_bf16x2(m[2], m[3]));
+    s.l = make_uint2(pack_bf16x2(l[0], l[1]), pack_bf16x2(l[2], l[3]));
+    return s;
+}
+
+// BF16x3 operand rows: a 128-byte row of the first region holds the h piece
+// of the chunk's 32 k in bytes 0-63 and the m piece in bytes 64-127; the same
+// row of the second region holds the l piece in bytes 0-63 (64-127 unused).
+// Piece q (8 bytes, 4 values) of a half-row sits in 16-byte chunk q / 2 of that
+// half, at byte 8 (q % 2); chunks are swizzled like every SWIZZLE_128B row.
+__device__ __forceinline__ uint32_t bf16_piece_offset(int row, int half, int q) {
+    return static_cast<uint32_t>((row >> 3) * 1024 + (row & 7) * 128 + (((4 * half + (q >> 1)) ^ (row & 7)) << 4) +
+                                 (q & 1) * 8);
+}
 
 __device__ __forceinline__ Split4 split4(float a, float b, float c, float d) {
     Split4 s;
@@ -203,7 +265,7 @@ __host__ __device__ constexpr int kperm(int q, int e) { return 2 * q + (e & 1) +
 // split, zero-padded to NP x KCH*32, K-major SWIZZLE_128B.  One thread per
 // (group, chunk, row, 16-byte piece).
 __global__ void tc_gemm_image_kernel(const float* __restrict__ natural, int groups, int R, int S, int NP, int KCH,
-                                     unsigned char* __restrict__ images) {
+                                     int kind, unsigned char* __restrict__ images) {
     const long long total = static_cast<long long>(groups) * KCH * NP * 8;
     const long long bytes = image_bytes(NP, KCH);
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
@@ -221,8 +283,20 @@ __global__ void tc_gemm_image_kernel(const float* __restrict__ natural, int grou
             const int s = kc * kChunkK + kperm(q, j);
             v[j] = (n < R && s < S) ? m[static_cast<long long>(n) * S + s] : 0.0f;
         }
-        const Split4 sp = split4(v[0], v[1], v[2], v[3]);
         unsigned char* img = images + g * bytes;
+        if (kind == kKindBf16x3) {
+            // Piece q of each half-row: the same k values (kperm(q, e)) as the
+            // producer warps put in piece q of a data row.
+            const Split3 sp = split3(v[0], v[1], v[2], v[3]);
+            const uint32_t base = kc * NP * 128;
+            *reinterpret_cast<uint2*>(img + base + bf16_piece_offset(n, 0, q)) = sp.h;
+            *reinterpret_cast<uint2*>(img + base + bf16_piece_offset(n, 1, q)) = sp.m;
+            *reinterpret_cast<uint2*>(img + bytes / 2 + base + bf16_piece_offset(n, 0, q)) = sp.l;
+            // The unused second half of the l row stays zero.
+            *reinterpret_cast<uint2*>(img + bytes / 2 + base + bf16_piece_offset(n, 1, q)) = make_uint2(0u, 0u);
+            continue;
+        }
+        const Split4 sp = split4(v[0], v[1], v[2], v[3]);
         const uint32_t off = kc * NP * 128 + sw128_offset(n, q);
         *reinterpret_cast<float4*>(img + off) = sp.hi;
         *reinterpret_cast<float4*>(img + bytes / 2 + off) = sp.lo;
@@ -287,7 +361,7 @@ __device__ __forceinline__ Unit unit_at(const TcGemmArgs& p, int u) {
 //       (the re and im rows of one column) swap halves with a shuffle so each
 //       store instruction writes 16 contiguous bytes of 16 columns.
 // NPH = NP/16: x8 column blocks per epilogue half.
-template <int NPH>
+template <int NPH, int KIND>
 __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArgs p) {
     constexpr int NP = NPH * 16;
     constexpr int HALF = NP / 2;
@@ -447,13 +521,26 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                 const int cc = 4 * j + (lane >> 3);
                 const int cl = warp * 8 + cc;
                 const float sgn = (m & (1u << cc)) ? -1.0f : 1.0f;
-                const Split4 re = split4(v[j][0].x, v[j][0].z, v[j][1].x, v[j][1].z);
-                const Split4 im = split4(sgn * v[j][0].y, sgn * v[j][0].w, sgn * v[j][1].y, sgn * v[j][1].w);
-                const uint32_t o0 = sw128_offset(2 * cl, q), o1 = sw128_offset(2 * cl + 1, q);
-                *reinterpret_cast<float4*>(aHi + o0) = re.hi;
-                *reinterpret_cast<float4*>(aLo + o0) = re.lo;
-                *reinterpret_cast<float4*>(aHi + o1) = im.hi;
-                *reinterpret_cast<float4*>(aLo + o1) = im.lo;
+                if constexpr (KIND == kKindBf16x3) {
+                    // Same values and k order as the TF32 pieces; three BF16
+                    // pieces of 8 bytes each per row (bf16_piece_offset).
+                    const Split3 re = split3(v[j][0].x, v[j][0].z, v[j][1].x, v[j][1].z);
+                    const Split3 im = split3(sgn * v[j][0].y, sgn * v[j][0].w, sgn * v[j][1].y, sgn * v[j][1].w);
+                    *reinterpret_cast<uint2*>(aHi + bf16_piece_offset(2 * cl, 0, q)) = re.h;
+                    *reinterpret_cast<uint2*>(aHi + bf16_piece_offset(2 * cl, 1, q)) = re.m;
+                    *reinterpret_cast<uint2*>(aLo + bf16_piece_offset(2 * cl, 0, q)) = re.l;
+                    *reinterpret_cast<uint2*>(aHi + bf16_piece_offset(2 * cl + 1, 0, q)) = im.h;
+                    *reinterpret_cast<uint2*>(aHi + bf16_piece_offset(2 * cl + 1, 1, q)) = im.m;
+                    *reinterpret_cast<uint2*>(aLo + bf16_piece_offset(2 * cl + 1, 0, q)) = im.l;
+                } else {
+                    const Split4 re = split4(v[j][0].x, v[j][0].z, v[j][1].x, v[j][1].z);
+                    const Split4 im = split4(sgn * v[j][0].y, sgn * v[j][0].w, sgn * v[j][1].y, sgn * v[j][1].w);
+                    const uint32_t o0 = sw128_offset(2 * cl, q), o1 = sw128_offset(2 * cl + 1, q);
+                    *reinterpret_cast<float4*>(aHi + o0) = re.hi;
+                    *reinterpret_cast<float4*>(aLo + o0) = re.lo;
+                    *reinterpret_cast<float4*>(aHi + o1) = im.hi;
+                    *reinterpret_cast<float4*>(aLo + o1) = im.lo;
+                }
             }
             fence_proxy_async();
             mbar_arrive(smem_u32(&st->full[stage]));
@@ -464,7 +551,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
     } else if (warp == kMmaWarp) {
         // --------------------------------------------------------------- MMA
         if (lane == 0) {
-            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(NP >> 3) << 17) |
+            // Instruction descriptor: F32 accumulator, A and B TF32 (2) or
+            // BF16 (1), both K-major, N = NP, M = 128.
+            constexpr uint32_t kOperandFormat = KIND == kKindBf16x3 ? 1u : 2u;
+            const uint32_t idesc = (1u << 4) | (kOperandFormat << 7) | (kOperandFormat << 10) |
+                                   (static_cast<uint32_t>(NP >> 3) << 17) |
                                    (static_cast<uint32_t>(kTileRows >> 4) << 24);
             int it = 0, loads = 0, group = -1;
             // Expired-wait test: before this lane has issued any copy or MMA,
@@ -520,12 +611,27 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                         const uint32_t d = tmem + static_cast<uint32_t>(acc * NP);
                         // k-steps holding any k < S (see kperm).
                         const int left = S - kc * kChunkK;
-                        const int ksteps = left >= 16 ? 4 : (left + 3) / 4;
-                        for (int j = 0; j < ksteps; ++j) {
-                            const uint32_t off = j * 32;
-                            mma_tf32(d, sw128_desc(aH + off), sw128_desc(bL + off), idesc, j > 0 ? 1u : 0u);
-                            mma_tf32(d, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
-                            mma_tf32(d, sw128_desc(aH + off), sw128_desc(bH + off), idesc, 1u);
+                        if constexpr (KIND == kKindBf16x3) {
+                            // k-step j (K = 16) reads pieces 4j..4j+3 of each
+                            // half-row: k = 8j..8j+7 and 16+8j..16+8j+7.
+                            const int ksteps = left > 8 ? 2 : 1;
+                            for (int j = 0; j < ksteps; ++j) {
+                                const uint32_t oh = j * 32, om = 64 + j * 32;
+                                mma_bf16(d, sw128_desc(aL + oh), sw128_desc(bH + oh), idesc, j > 0 ? 1u : 0u);
+                                mma_bf16(d, sw128_desc(aH + oh), sw128_desc(bL + oh), idesc, 1u);
+                                mma_bf16(d, sw128_desc(aH + om), sw128_desc(bH + om), idesc, 1u);
+                                mma_bf16(d, sw128_desc(aH + om), sw128_desc(bH + oh), idesc, 1u);
+                                mma_bf16(d, sw128_desc(aH + oh), sw128_desc(bH + om), idesc, 1u);
+                                mma_bf16(d, sw128_desc(aH + oh), sw128_desc(bH + oh), idesc, 1u);
+                            }
+                        } else {
+                            const int ksteps = left >= 16 ? 4 : (left + 3) / 4;
+                            for (int j = 0; j < ksteps; ++j) {
+                                const uint32_t off = j * 32;
+                                mma_tf32(d, sw128_desc(aH + off), sw128_desc(bL + off), idesc, j > 0 ? 1u : 0u);
+                                mma_tf32(d, sw128_desc(aL + off), sw128_desc(bH + off), idesc, 1u);
+                                mma_tf32(d, sw128_desc(aH + off), sw128_desc(bH + off), idesc, 1u);
+                            }
                         }
                         mma_commit(smem_u32(&st->empty[stage]));
                         mma_commit(smem_u32(&st->accFull[acc]));
@@ -673,13 +779,14 @@ size_t tc_gemm_image_bytes(int R, int S) {
     return static_cast<size_t>(image_bytes((R + 15) / 16 * 16, (S + kChunkK - 1) / kChunkK));
 }
 
-cudaError_t tc_gemm_build_images(const float* natural, int groups, int R, int S, void* images, cudaStream_t stream) {
+cudaError_t tc_gemm_build_images(const float* natural, int groups, int R, int S, int kind, void* images,
+                                 cudaStream_t stream) {
     if (groups <= 0) return cudaSuccess;
     const int NP = (R + 15) / 16 * 16;
     const int KCH = (S + kChunkK - 1) / kChunkK;
     const long long items = static_cast<long long>(groups) * KCH * NP * 8;
     const int blocks = static_cast<int>(std::min<long long>((items + 255) / 256, 148LL * 16));
-    tc_gemm_image_kernel<<<blocks, 256, 0, stream>>>(natural, groups, R, S, NP, KCH,
+    tc_gemm_image_kernel<<<blocks, 256, 0, stream>>>(natural, groups, R, S, NP, KCH, kind,
                                                      static_cast<unsigned char*>(images));
     return cudaGetLastError();
 }
@@ -692,7 +799,8 @@ cudaError_t launch_np(const TcGemmArgs& args, cudaStream_t stream) {
     // At least half an SM's shared memory, so that two CTAs (each holding
     // all 512 TMEM columns) never share an SM.
     const size_t bytes = std::max<size_t>(tc_gemm_smem_bytes(args.R, args.S), 116 * 1024);
-    auto kernel = tc_gemm_pipe_kernel<NPH>;
+    auto kernel = args.kind == kKindBf16x3 ? tc_gemm_pipe_kernel<NPH, kKindBf16x3>
+                                           : tc_gemm_pipe_kernel<NPH, kKindTf32x3>;
     const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (err != cudaSuccess) return err;
     // Persistent: one CTA per SM (or per unit, if fewer).
@@ -709,6 +817,7 @@ cudaError_t launch_np(const TcGemmArgs& args, cudaStream_t stream) {
 
 cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream) {
     if (args.units <= 0) return cudaSuccess;
+    if (args.kind != kKindTf32x3 && args.kind != kKindBf16x3) return cudaErrorInvalidValue;
     if (!tc_gemm_supported(args.R, args.S) || args.NP != (args.R + 15) / 16 * 16) return cudaErrorInvalidValue;
     switch (args.NP / 16) {
         case 1: return launch_np<1>(args, stream);

@@ -93,6 +93,8 @@ struct TcGemmArgs {
     // Test of the expired-wait path: the MMA lane of every CTA first waits on
     // a barrier that nothing arrives on, so that bounded wait runs out.
     int expireWaitForTest;
+    // Operand form: 0 split TF32x3 (kind::tf32), 1 split BF16x3 (kind::f16).
+    int kind;
 };
 bool tc_gemm_supported(int R, int S);
 size_t tc_gemm_smem_bytes(int R, int S);
@@ -100,8 +102,10 @@ size_t tc_gemm_smem_bytes(int R, int S);
 // parts, zero-padded to a multiple of 16 rows and of 32 k, in the swizzled
 // shared-memory layout the kernel's MMAs read.
 size_t tc_gemm_image_bytes(int R, int S);
-// natural [groups][R][S] FP32 (device) -> images[groups] (device).
-cudaError_t tc_gemm_build_images(const float* natural, int groups, int R, int S, void* images, cudaStream_t stream);
+// natural [groups][R][S] FP32 (device) -> images[groups] (device), split
+// into TF32 hi / lo (kind 0) or BF16 h / m / l (kind 1); same size either way.
+cudaError_t tc_gemm_build_images(const float* natural, int groups, int R, int S, int kind, void* images,
+                                 cudaStream_t stream);
 int tc_gemm_unit_tiles();
 cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream);
 

@@ -559,13 +559,14 @@ int gemm_code(const std::string& g) {
     if (g == "fp64") return SKB_GEMM_FP64;
     if (g == "fp32") return SKB_GEMM_FP32;
     if (g == "tf32x3") return SKB_GEMM_TF32X3;
-    throw std::invalid_argument("vertical-gemm-precision must be 'fp64', 'fp32' or 'tf32x3'.");
+    if (g == "bf16x3") return SKB_GEMM_BF16X3;
+    throw std::invalid_argument("vertical-gemm-precision must be 'fp64', 'fp32', 'tf32x3' or 'bf16x3'.");
 }
 
 ProviderRecord run_vertical(const Options& o, const skb_workload& w, Report& report) {
     const int gemm = gemm_code(o.gemm);
     const bool f32 = gemm != SKB_GEMM_FP64;
-    const double tol = gemm == SKB_GEMM_FP64 ? 1e-12 : gemm == SKB_GEMM_TF32X3 ? 1e-6 : 1e-5;
+    const double tol = gemm == SKB_GEMM_FP64 ? 1e-12 : (gemm == SKB_GEMM_TF32X3 || gemm == SKB_GEMM_BF16X3) ? 1e-6 : 1e-5;
     const std::uint64_t s = f32 ? 4 : 8, nz = w.nz, nj = nz < 2 ? 0 : 2 * (nz - 1) / 3;
     const auto modes = retained_modes(w);
     const int family = o.family == "common" ? SKB_FAMILY_COMMON_DCT2 : SKB_FAMILY_K2_ROTATION;
@@ -601,7 +602,9 @@ ProviderRecord run_vertical(const Options& o, const skb_workload& w, Report& rep
     ok(skb_vertical_info(h, &info));
     ProviderRecord rec;
     fill_info(rec, info);
-    rec.algorithmId = gemm == SKB_GEMM_TF32X3 ? "grouped-gemm-tcgen05-tf32x3" : "grouped-gemm-simt-cp-async";
+    rec.algorithmId = gemm == SKB_GEMM_TF32X3   ? "grouped-gemm-tcgen05-tf32x3"
+                      : gemm == SKB_GEMM_BF16X3 ? "grouped-gemm-tcgen05-bf16x3"
+                                                : "grouped-gemm-simt-cp-async";
     rec.nativeRepresentationId = "complex columns [mode][field][z|j] interleaved";
     rec.modeOrderId = "radial-two-thirds-sorted(radius,k,l); K^2 groups contiguous";
     rec.planningConfiguration = std::string(id) + "; " + o.gemm + "; " + std::to_string(groups.size()) + " groups";
@@ -1088,7 +1091,8 @@ int flux_mode(const std::string& m) {
     if (m == "fp64-plain") return SKB_FLUX_FP64_PLAIN;
     if (m == "fp32") return SKB_FLUX_FP32;
     if (m == "split-tf32x3") return SKB_FLUX_SPLIT_TF32X3;
-    throw std::invalid_argument("flux-mode must be 'fp64-plain', 'fp32' or 'split-tf32x3'.");
+    if (m == "split-bf16x3") return SKB_FLUX_SPLIT_BF16X3;
+    throw std::invalid_argument("flux-mode must be 'fp64-plain', 'fp32', 'split-tf32x3' or 'split-bf16x3'.");
 }
 
 // runAuthoritativeProductionLifetimeFluxBenchmark (src/authoritative_spectral_flux.cpp:
@@ -1223,9 +1227,10 @@ ProviderRecord run_flux(const Options& o, const skb_workload& w, Report& report)
     ok(skb_flux_info(h, &info));
     ProviderRecord rec;
     fill_info(rec, info);
-    rec.algorithmId = mode == SKB_FLUX_SPLIT_TF32X3
-                          ? "fused five-launch flux: tcgen05 TF32x3 GEMMs, embed+columns, register-resident rows, "
-                            "columns+retention"
+    const bool split = mode == SKB_FLUX_SPLIT_TF32X3 || mode == SKB_FLUX_SPLIT_BF16X3;
+    rec.algorithmId = split ? std::string("fused five-launch flux: tcgen05 ") +
+                                  (mode == SKB_FLUX_SPLIT_TF32X3 ? "TF32x3" : "BF16x3") +
+                                  " GEMMs, embed+columns, register-resident rows, columns+retention"
                           : "staged flux: grouped GEMM, pruned horizontal, pointwise, pruned horizontal, grouped GEMM";
     rec.nativeRepresentationId = "modal [member][mode][field][j] interleaved";
     rec.modeOrderId = "radial-two-thirds-sorted(radius,k,l); K^2 groups contiguous";
@@ -1283,8 +1288,8 @@ ProviderRecord run_flux(const Options& o, const skb_workload& w, Report& report)
                                      std::uint64_t(stages[i].algorithmic_bytes), {stages[i].ms * 1e-3}));
     rec.ledger = {{"shared U,V,W reconstruction", StageState::executed, "once per composition"},
                   {"derivative reconstruction", StageState::executed, "per target"},
-                  {"pointwise advection", mode == SKB_FLUX_SPLIT_TF32X3 ? StageState::fused : StageState::executed,
-                   mode == SKB_FLUX_SPLIT_TF32X3 ? "inside the row kernel" : "separate kernel"},
+                  {"pointwise advection", split ? StageState::fused : StageState::executed,
+                   split ? "inside the row kernel" : "separate kernel"},
                   {"forward horizontal and retention", StageState::executed, "per target"},
                   {"forward vertical GEMM", StageState::executed, "all targets in one launch"}};
     if (o.autotune)
@@ -1344,7 +1349,7 @@ ProviderRecord run_flux(const Options& o, const skb_workload& w, Report& report)
         ok(skb_stream_synchronize(stream));
         const auto want = widen_complex(dOut64, outN, false, s64);
         const auto got = widen_complex(dOut, outN, true, stream);
-        const double tol = mode == SKB_FLUX_SPLIT_TF32X3 ? 1e-6 : 1e-4;
+        const double tol = split ? 1e-6 : 1e-4;
         rec.correctness.push_back(metric(o.fluxMode + " vs fp64-plain", max_relative_error(got.data(), want.data(), outN),
                                          relative_l2_error(got.data(), want.data(), outN), tol));
     }
@@ -1520,7 +1525,8 @@ void usage(std::ostream& out) {
            "production-lifetime-flux|spectral-pipeline|constant-stratification-vertical] [--profile NAME]\n"
            "              [--providers cuda]\n"
         << "              [--precision fp64|fp32] [--vertical-gemm-family common|k2-grouped]\n"
-        << "              [--vertical-gemm-precision fp64|fp32|tf32x3] [--flux-mode fp64-plain|fp32|split-tf32x3]\n"
+        << "              [--vertical-gemm-precision fp64|fp32|tf32x3|bf16x3]\n"
+        << "              [--flux-mode fp64-plain|fp32|split-tf32x3|split-bf16x3]\n"
         << "              [--members N] [--targets 3|4] [--autotune] [--nx N --ny N --nz N --fields N]\n"
         << "              [--spectral-flux-fixture PREPARED.bin]\n"
         << "              [--boundary-policy NAME] [--streaming-tile-width N] [--streaming-inverse-policy NAME]\n"
@@ -1537,9 +1543,9 @@ void list() {
               << "kernels:\n  fft (alias 2d-rfft)\n  pruned-horizontal\n  vertical-gemm\n  pointwise-advection\n"
               << "  production-lifetime-flux\n  spectral-pipeline\n  constant-stratification-vertical\n"
               << "precisions:\n  fp64\n  fp32\n"
-              << "vertical GEMM precisions:\n  fp64\n  fp32\n  tf32x3\n"
+              << "vertical GEMM precisions:\n  fp64\n  fp32\n  tf32x3\n  bf16x3\n"
               << "vertical GEMM matrix families:\n  common\n  k2-grouped\n"
-              << "flux modes:\n  fp64-plain\n  fp32\n  split-tf32x3\n";
+              << "flux modes:\n  fp64-plain\n  fp32\n  split-tf32x3\n  split-bf16x3\n";
 }
 
 std::string value(int argc, char** argv, int& i) {

@@ -60,11 +60,13 @@ def test_autotune_keeps_parity_and_caches():
     assert orc.rel_l2_error(_run(again, x), want) <= 1e-6
 
 
+@pytest.mark.parametrize("mode", [skb_cuda.FLUX_SPLIT_TF32X3, skb_cuda.FLUX_SPLIT_BF16X3], ids=["tf32x3", "bf16x3"])
 @pytest.mark.parametrize("tiles", [4, 32])
-def test_every_unit_size_is_correct(tiles):
+def test_every_unit_size_is_correct(tiles, mode):
     """A cached choice is applied when a handle is created: force each extreme."""
+    skb_cuda.tune_cache_clear()
     n, nz, members = 64, 17, 3
-    probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    probe = skb_cuda.Flux(n, nz, members=members, mode=mode)
     x = _inputs(probe, 11)
     d_in = skb_cuda.DeviceArray.from_numpy(x)
     d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
@@ -72,7 +74,7 @@ def test_every_unit_size_is_correct(tiles):
     assert len(keys) == 2
     for key in keys:
         skb_cuda.tune_cache_store(key, tiles, 0.0)
-    flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    flux = skb_cuda.Flux(n, nz, members=members, mode=mode)
     assert orc.rel_l2_error(_run(flux, x), _fp64(n, nz, members, x)) <= 1e-6
     skb_cuda.tune_cache_clear()
 
@@ -98,19 +100,25 @@ def test_band_forms_at_512(form):
     skb_cuda.tune_cache_clear()
 
 
-@pytest.mark.parametrize("n,planes", [(64, 4), (64, 16), (512, 4), (512, 16)])
-def test_every_row_kernel_width_is_correct(n, planes):
-    """The fused row kernel with 4, 8 or 16 z-planes per CTA (the tuner's
-    candidates; 8 is covered by every other flux test)."""
+@pytest.mark.parametrize("n,planes,pairs", [(64, 4, 0), (64, 16, 0), (512, 4, 0), (512, 16, 0), (512, 8, 1),
+                                            (512, 16, 1)])
+def test_every_row_kernel_width_is_correct(n, planes, pairs):
+    """The fused row kernel with 4, 8 or 16 z-planes per CTA, and at 512 points
+    the two-planes-per-warp form with 8 or 16 (the tuner's candidates)."""
     skb_cuda.tune_cache_clear()
     nz, members = 17, 2
     probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
     x = _inputs(probe, 31)
     d_in = skb_cuda.DeviceArray.from_numpy(x)
     d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
-    keys = [k for k in probe.autotune(d_in.ptr, d_out.ptr) if k.startswith("flux.rows.planes_per_cta")]
+    chosen = probe.autotune(d_in.ptr, d_out.ptr)
+    keys = [k for k in chosen if k.startswith("flux.rows.planes_per_cta")]
     assert len(keys) == 1
     skb_cuda.tune_cache_store(keys[0], planes, 0.0)
+    pair_keys = [k for k in chosen if k.startswith("flux.rows.pairs")]
+    assert len(pair_keys) == (1 if n == 512 else 0)
+    for key in pair_keys:
+        skb_cuda.tune_cache_store(key, pairs, 0.0)
     flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
     assert orc.rel_l2_error(_run(flux, x), _fp64(n, nz, members, x)) <= 1e-6
     skb_cuda.tune_cache_clear()

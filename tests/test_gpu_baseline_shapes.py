@@ -2,8 +2,8 @@
 
 * The 15 -> 4 flux at 512 x 512, Nz = 129, one member, with the reference's
   modal-input generator (uniform [-0.125, 0.125], real DC): FP64-plain within
-  1e-12 (the reference's own FP64 tolerance) and split TF32x3 within 1e-6 (the
-  split-precision bound), both max-relative and relative-L2.  The same split
+  1e-12 (the reference's own FP64 tolerance) and split TF32x3 / BF16x3 within
+  1e-6 (the split-precision bound), both max-relative and relative-L2.  The same split
   check on the benchmark's own k^-3 power-law inputs.
 * The build-side Sturm-Liouville vertical family (dense, group-dependent
   operators, the realistic case for split-precision error): through the
@@ -65,9 +65,10 @@ def test_flux_fp64_plain_full_size_matches_oracle(reference_case):
     assert max_rel <= 1e-12 and l2 <= 1e-12, (max_rel, l2)
 
 
-def test_flux_split_full_size_matches_oracle(reference_case):
+@pytest.mark.parametrize("mode", [skb_cuda.FLUX_SPLIT_TF32X3, skb_cuda.FLUX_SPLIT_BF16X3], ids=["tf32x3", "bf16x3"])
+def test_flux_split_full_size_matches_oracle(reference_case, mode):
     x, ref = reference_case
-    flux = skb_cuda.Flux(N, NZ, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    flux = skb_cuda.Flux(N, NZ, mode=mode)
     out = flux.execute(x)
     flux.check_device()
     max_rel, l2 = _errors(out, ref)
@@ -91,7 +92,7 @@ def test_flux_split_power_law_inputs_match_oracle(modes512):
 
 
 @pytest.mark.parametrize("precision,tol", [(skb_cuda.GEMM_FP64, 1e-12), (skb_cuda.GEMM_FP32, 1e-6),
-                                           (skb_cuda.GEMM_TF32X3, 1e-6)])
+                                           (skb_cuda.GEMM_TF32X3, 1e-6), (skb_cuda.GEMM_BF16X3, 1e-6)])
 def test_sturm_liouville_grouped_gemm_matches_oracle(precision, tol):
     shape = (256, 256, 65, 3)
     w = skb_cuda.Workload(*shape)
@@ -117,7 +118,8 @@ def test_sturm_liouville_grouped_gemm_matches_oracle(precision, tol):
 def test_sturm_liouville_flux_full_size_matches_oracle(modes512, sl_family):
     x = orc.flux_inputs(modes512, 15, NJ, 131)
     ref = orc.flux(N, NZ, x, family=sl_family, modes=modes512, workers=WORKERS)
-    for mode, tol in ((skb_cuda.FLUX_FP64_PLAIN, 1e-12), (skb_cuda.FLUX_SPLIT_TF32X3, 1e-6)):
+    for mode, tol in ((skb_cuda.FLUX_FP64_PLAIN, 1e-12), (skb_cuda.FLUX_SPLIT_TF32X3, 1e-6),
+                      (skb_cuda.FLUX_SPLIT_BF16X3, 1e-6)):
         flux = skb_cuda.Flux(N, NZ, mode=mode, family=skb_cuda.FAMILY_STURM_LIOUVILLE, family_seed=SL_SEED)
         out = flux.execute(x)
         flux.check_device()
@@ -168,3 +170,27 @@ def test_serving_mix_classes_alone_equals_mixed_and_matches_oracle(reference_cas
         assert max_rel <= tol and l2 <= tol, (classes[c], max_rel, l2)
     for f in alone_cache.values():
         f.close()
+
+
+@pytest.mark.parametrize("planes", [8, 16])
+def test_flux_split_two_planes_per_warp_rows_match_oracle(reference_case, planes):
+    # The 512-point row kernel's two-planes-per-warp form (16 x 16 FFT), forced
+    # through the tuning cache, at the benchmark shape against the oracle.
+    x, ref = reference_case
+    skb_cuda.tune_cache_clear()
+    probe = skb_cuda.Flux(N, NZ, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    d_in = skb_cuda.DeviceArray.from_numpy(x.astype(np.complex64))
+    d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
+    chosen = probe.autotune(d_in.ptr, d_out.ptr)
+    probe.close()
+    for key in chosen:
+        if key.startswith("flux.rows.pairs"):
+            skb_cuda.tune_cache_store(key, 1, 0.0)
+        if key.startswith("flux.rows.planes_per_cta"):
+            skb_cuda.tune_cache_store(key, planes, 0.0)
+    flux = skb_cuda.Flux(N, NZ, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    out = flux.execute(x)
+    flux.check_device()
+    skb_cuda.tune_cache_clear()
+    max_rel, l2 = _errors(out, ref)
+    assert max_rel <= 1e-6 and l2 <= 1e-6, (max_rel, l2)

@@ -95,3 +95,16 @@ def test_flux_tf32x3_full_size_against_fp64_cuda():
     out = fast.execute(x)
     fast.check_device()
     assert orc.rel_l2_error(out, ref) <= 1e-6
+
+
+def test_flux_bf16x3_error_against_oracle():
+    # Split BF16x3 tensor-core GEMMs in the fused flux, two members.
+    n, nz, members = 64, 17, 2
+    modes = orc.retained_modes(n, n)
+    nj = 2 * (nz - 1) // 3
+    xs = [orc.flux_inputs(modes, 15, nj, 151 + m) for m in range(members)]
+    flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_BF16X3)
+    out = flux.execute(np.concatenate(xs)).reshape(members, -1)
+    flux.check_device()
+    for m in range(members):
+        assert orc.rel_l2_error(out[m], orc.flux(n, nz, xs[m])) <= 1e-6

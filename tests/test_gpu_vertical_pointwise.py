@@ -124,10 +124,13 @@ def test_pointwise_large_volume():
 
 # ------------------------------------------------------- tensor-core form
 
+@pytest.mark.parametrize("precision", [skb_cuda.GEMM_TF32X3, skb_cuda.GEMM_BF16X3], ids=["tf32x3", "bf16x3"])
 @pytest.mark.parametrize("shape", [(16, 16, 9, 3), (16, 16, 7, 2), (256, 256, 65, 3), (128, 128, 33, 4),
                                    (512, 512, 129, 15)])
-def test_tf32x3_tensor_core_matches_oracle(shape):
-    # Split TF32x3 on tcgen05, FP32 accumulation: FP32-level error against FP64.
+def test_split_tensor_core_matches_oracle(shape, precision):
+    # Split TF32x3 (kind::tf32) and split BF16x3 (kind::f16, three BF16 pieces,
+    # six products) on tcgen05 with FP32 accumulation: FP32-level error
+    # against FP64.
     w = skb_cuda.Workload(*shape)
     o = orc.Workload(*shape)
     fam = orc.k2_family(o)
@@ -135,7 +138,7 @@ def test_tf32x3_tensor_core_matches_oracle(shape):
     rng = np.random.default_rng(12)
     phys = rng.uniform(-1, 1, H * w.fields * w.nz) + 1j * rng.uniform(-1, 1, H * w.fields * w.nz)
     modal = rng.uniform(-1, 1, H * w.fields * w.nj) + 1j * rng.uniform(-1, 1, H * w.fields * w.nj)
-    vp = provider(w, precision=skb_cuda.GEMM_TF32X3)
+    vp = provider(w, precision=precision)
     vp.load_physical_input(phys)
     vp.execute_forward()
     got = vp.copy_forward_output()
