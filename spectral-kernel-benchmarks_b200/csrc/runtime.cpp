@@ -365,27 +365,85 @@ void VerticalPlan::build_units(int tiles) {
     struct Unit {
         int g, col, count;
     };
+    int device = 0, sms = 0;
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     const int span = tiles * 64;
     std::vector<UnitTable> tables;
     for (std::uint64_t active = 1; active <= members_; ++active) {
-        std::vector<Unit> units;
-        for (std::size_t gi = 0; gi < groupColumnsHost_.size(); ++gi) {
+        // A group's units (runs of <= `tiles` M-tiles of its member columns)
+        // go to one CTA, so the CTA loads the group's operand image once; a
+        // group with more than a CTA's share of the work is cut into pieces of
+        // at most that share.  Pieces are dealt largest first to the CTA with
+        // the least work so far (one tile of work per piece stands for its
+        // image load), and each CTA walks its units as one contiguous range.
+        struct Piece {
+            std::vector<Unit> units;
+            long long work = 0;
+        };
+        const int groups = static_cast<int>(groupColumnsHost_.size());
+        long long totalTiles = 0;
+        int unitCount = 0;
+        for (int gi = 0; gi < groups; ++gi) {
             const int total = static_cast<int>(active) * groupColumnsHost_[gi];
-            for (int c = 0; c < total; c += span)
-                units.push_back({static_cast<int>(gi), c, std::min(span, total - c)});
+            totalTiles += (total + 63) / 64;
+            unitCount += (total + span - 1) / span;
         }
-        std::stable_sort(units.begin(), units.end(), [](const Unit& a, const Unit& b) { return a.count > b.count; });
-        std::vector<int> ug, uc, un;
-        for (const auto& u : units) {
-            ug.push_back(u.g);
-            uc.push_back(u.col);
-            un.push_back(u.count);
+        const int ctas = std::max(1, std::min(unitCount, sms > 0 ? sms : 148));
+        const long long share = std::max<long long>(tiles, (totalTiles + ctas - 1) / ctas);
+        std::vector<Piece> pieces;
+        for (int gi = 0; gi < groups; ++gi) {
+            const int total = static_cast<int>(active) * groupColumnsHost_[gi];
+            Piece cur;
+            for (int col = 0; col < total; col += span) {
+                const Unit u{gi, col, std::min(span, total - col)};
+                const long long t = (u.count + 63) / 64;
+                if (!cur.units.empty() && cur.work + t > share) {
+                    cur.work += 1;
+                    pieces.push_back(std::move(cur));
+                    cur = Piece{};
+                }
+                cur.units.push_back(u);
+                cur.work += t;
+            }
+            if (!cur.units.empty()) {
+                cur.work += 1;
+                pieces.push_back(std::move(cur));
+            }
+        }
+        std::vector<int> order(pieces.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = static_cast<int>(i);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pieces[a].work > pieces[b].work; });
+        std::vector<std::vector<int>> owned(ctas);
+        // Least-loaded CTA by a min-heap of (load, cta).
+        std::vector<std::pair<long long, int>> heap;
+        for (int c = 0; c < ctas; ++c) heap.push_back({0, c});
+        auto greater = [](const std::pair<long long, int>& a, const std::pair<long long, int>& b) { return a > b; };
+        std::make_heap(heap.begin(), heap.end(), greater);
+        for (const int pi : order) {
+            std::pop_heap(heap.begin(), heap.end(), greater);
+            auto& least = heap.back();
+            owned[least.second].push_back(pi);
+            least.first += pieces[pi].work;
+            std::push_heap(heap.begin(), heap.end(), greater);
+        }
+        std::vector<int> ug, uc, un, first{0};
+        for (int c = 0; c < ctas; ++c) {
+            for (const int pi : owned[c])
+                for (const Unit& u : pieces[pi].units) {
+                    ug.push_back(u.g);
+                    uc.push_back(u.col);
+                    un.push_back(u.count);
+                }
+            first.push_back(static_cast<int>(ug.size()));
         }
         UnitTable table;
         table.units = static_cast<int>(ug.size());
+        table.ctas = ctas;
         table.group = upload_vector(ug);
         table.column = upload_vector(uc);
         table.count = upload_vector(un);
+        table.first = upload_vector(first);
         tables.push_back(std::move(table));
     }
     unitTables_ = std::move(tables);
@@ -399,7 +457,7 @@ void VerticalPlan::set_unit_tiles(int tiles) {
 
 std::uint64_t VerticalPlan::persistentBytes() const {
     std::uint64_t units = 0;
-    for (const auto& t : unitTables_) units += t.group.bytes() + t.column.bytes() + t.count.bytes();
+    for (const auto& t : unitTables_) units += t.group.bytes() + t.column.bytes() + t.count.bytes() + t.first.bytes();
     for (const auto& t : tileTables_)
         units += t.group.bytes() + t.column.bytes() + t.count.bytes() + t.per.bytes() + t.first.bytes();
     return matrices_.bytes() + units +
@@ -425,6 +483,8 @@ void VerticalPlan::execute(ComplexOperand in, ComplexOperand out, cudaStream_t s
         a.unitColumn = table.column.get<int>();
         a.unitCount = table.count.get<int>();
         a.units = table.units;
+        a.ctaFirst = table.first.get<int>();
+        a.ctas = table.ctas;
         a.groupColumns = groupColumns_.get<int>();
         a.groupFirst = groupFirst_.get<int>();
         a.memberColumns = memberColumns_;

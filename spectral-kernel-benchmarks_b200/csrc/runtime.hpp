@@ -210,8 +210,8 @@ private:
     long long imageStride_ = 0;  // tensor-core form: bytes between group images (0: one common image)
     // Tensor-core work units, one table per active member count 1..members.
     struct UnitTable {
-        DeviceBuffer group, column, count;
-        int units = 0;
+        DeviceBuffer group, column, count, first;  // first: per-CTA unit ranges (ctas + 1 entries)
+        int units = 0, ctas = 0;
     };
     std::vector<UnitTable> unitTables_;
     std::vector<int> groupColumnsHost_;  // complex columns per member in each group

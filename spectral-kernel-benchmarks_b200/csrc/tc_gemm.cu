@@ -330,6 +330,16 @@ struct Unit {
     int g, vc0, vcN, gcols, tiles;
     long long gfirst;
 };
+
+// The units this CTA walks: [begin, end) with stride `step`.
+struct Walk {
+    int begin, end, step;
+};
+__device__ __forceinline__ Walk unit_walk(const TcGemmArgs& p) {
+    if (p.ctaFirst != nullptr)
+        return {__ldg(p.ctaFirst + blockIdx.x), __ldg(p.ctaFirst + blockIdx.x + 1), 1};
+    return {static_cast<int>(blockIdx.x), p.units, static_cast<int>(gridDim.x)};
+}
 __device__ __forceinline__ Unit unit_at(const TcGemmArgs& p, int u) {
     Unit U;
     U.g = __ldg(p.unitGroup + u);
@@ -342,7 +352,7 @@ __device__ __forceinline__ Unit unit_at(const TcGemmArgs& p, int u) {
 }
 
 // Warp-specialised, persistent split-TF32x3 grouped GEMM.  Each CTA (one per
-// SM) walks the work units blockIdx.x, blockIdx.x + gridDim.x, ...; TMEM, the
+// SM) walks its range of work units (unit_walk); TMEM, the
 // barriers and the stage ring live across units, and every role counts chunks
 // globally so the barrier phases continue from unit to unit.
 //   producer warps 0-7: data chunks (64 columns x 32 k) stream through a
@@ -410,9 +420,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
     if (warp < kProducerWarps) {
         // ---------------------------------------------------------- producer
         // Issue cursor: unit iu, tile itT, chunk itKc of the tile.
-        int iu = blockIdx.x;
+        const Walk W = unit_walk(p);
+        int iu = W.begin;
         Unit IU{};
-        if (iu < p.units) IU = unit_at(p, iu);
+        if (iu < W.end) IU = unit_at(p, iu);
         int itT = 0, itKc = 0, curTile = -1, tileCount = 0;
         long long colBase[8];
         unsigned tileMask = 0;  // bit c: column 8*warp+c of the tile is stored conjugated
@@ -433,7 +444,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         // Copies of the next chunk of the stream into its stage; false at the
         // end of the stream or on an expired wait.
         auto issue_next = [&]() -> bool {
-            if (iu >= p.units || failed) return false;
+            if (iu >= W.end || failed) return false;
             const int stage = issued % kStages;
             const int round = issued / kStages;
             if (round > 0 && !mbar_wait(smem_u32(&st->empty[stage]), (round - 1) & 1, p.error)) {
@@ -453,8 +464,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                 for (int cc = 0; cc < 8; ++cc) colBase[cc] = __shfl_sync(0xFFFFFFFFu, mine.base, cc);
                 if (itT + 1 < IU.tiles) {
                     prefetch_tile(IU, itT + 1);
-                } else if (iu + static_cast<int>(gridDim.x) < p.units) {
-                    prefetch_tile(unit_at(p, iu + gridDim.x), 0);
+                } else if (iu + W.step < W.end) {
+                    prefetch_tile(unit_at(p, iu + W.step), 0);
                 }
             }
             const uint32_t raw = smem_u32(sA + stage * kStageBytes + kTileRows * 128) + lane * 8;
@@ -473,13 +484,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                 if (++itT == IU.tiles) {
                     itT = 0;
                     curTile = -1;
-                    iu += gridDim.x;
-                    if (iu < p.units) IU = unit_at(p, iu);
+                    iu += W.step;
+                    if (iu < W.end) IU = unit_at(p, iu);
                 }
             }
             return true;
         };
-        if (iu < p.units) prefetch_tile(IU, 0);
+        if (iu < W.end) prefetch_tile(IU, 0);
         for (int k = 0; k < kAhead; ++k)
             if (!issue_next()) break;
         while (pending > 0 && !failed) {
@@ -563,7 +574,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
             // the same path as any expired wait (error word, every role stops,
             // copies drained, TMEM freed, SKB_ERR_RUNTIME on the host).
             if (p.expireWaitForTest != 0 && !mbar_wait(smem_u32(&st->never), 0, p.error, kTestWaitLimit)) fail();
-            for (int u = blockIdx.x; u < p.units && !failed; u += gridDim.x) {
+            const Walk W = unit_walk(p);
+            for (int u = W.begin; u < W.end && !failed; u += W.step) {
                 const Unit U = unit_at(p, u);
                 if (U.g != group) {
                     // The resident image may be replaced once every MMA that
@@ -580,11 +592,15 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                     for (uint32_t o = 0; o < imageBytes; o += kBulkPiece)
                         bulk_load(smem_u32(sBhi + o), img + o, min(kBulkPiece, static_cast<uint32_t>(imageBytes - o)),
                                   smem_u32(&st->bFull));
-                    if (u + static_cast<int>(gridDim.x) < p.units) {
-                        const int gn = __ldg(p.unitGroup + u + gridDim.x);
-                        if (gn != U.g)
+                    // L2 prefetch of the next group's image this CTA will load
+                    // (a few units ahead at most).
+                    for (int v = u + W.step, seen = 0; v < W.end && seen < 32; v += W.step, ++seen) {
+                        const int gn = __ldg(p.unitGroup + v);
+                        if (gn != U.g) {
                             bulk_prefetch_l2(p.B + static_cast<long long>(gn) * p.imageStride,
                                              static_cast<uint32_t>(imageBytes));
+                            break;
+                        }
                     }
                     if (!mbar_wait(smem_u32(&st->bFull), loads & 1, p.error)) {
                         fail();
@@ -657,7 +673,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         const uint32_t laneBase = static_cast<uint32_t>(quarter * 32) << 16;
         const uint32_t sumBase = tmem + laneBase + static_cast<uint32_t>(kAccumulators * NP + half * HALF);
         int it = 0;
-        for (int u = blockIdx.x; u < p.units && !failed; u += gridDim.x) {
+        const Walk W = unit_walk(p);
+        for (int u = W.begin; u < W.end && !failed; u += W.step) {
             const Unit U = unit_at(p, u);
             for (int t = 0; t < U.tiles && !failed; ++t) {
                 const int tv0 = U.vc0 + t * 64;
@@ -810,13 +827,15 @@ cudaError_t launch_np(const TcGemmArgs& args, cudaStream_t stream) {
     if (device >= 0 && device < 64 && smCount[device] == 0)
         cudaDeviceGetAttribute(&smCount[device], cudaDevAttrMultiProcessorCount, device);
     const int sms = (device >= 0 && device < 64 && smCount[device] > 0) ? smCount[device] : 148;
-    kernel<<<std::min(args.units, sms), kPipeThreads, bytes, stream>>>(args);
+    const int grid = args.ctaFirst != nullptr ? args.ctas : std::min(args.units, sms);
+    kernel<<<grid, kPipeThreads, bytes, stream>>>(args);
     return cudaGetLastError();
 }
 }  // namespace
 
 cudaError_t launch_tc_gemm(const TcGemmArgs& args, cudaStream_t stream) {
     if (args.units <= 0) return cudaSuccess;
+    if (args.ctaFirst != nullptr && args.ctas <= 0) return cudaErrorInvalidValue;
     if (args.kind != kKindTf32x3 && args.kind != kKindBf16x3) return cudaErrorInvalidValue;
     if (!tc_gemm_supported(args.R, args.S) || args.NP != (args.R + 15) / 16 * 16) return cudaErrorInvalidValue;
     switch (args.NP / 16) {

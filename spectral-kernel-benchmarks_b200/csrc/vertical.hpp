@@ -83,6 +83,12 @@ struct TcGemmArgs {
     const int* unitColumn;  // first virtual column of the unit
     const int* unitCount;   // virtual columns in the unit
     int units;
+    // Per-CTA unit ranges: CTA c walks units ctaFirst[c] .. ctaFirst[c+1]-1 (a
+    // group's units sit in one range, so its operand image is loaded once per
+    // CTA); the launch has `ctas` CTAs.  ctaFirst null: CTA c walks units c,
+    // c + gridDim.x, ... of one grid of min(units, SMs) CTAs.
+    const int* ctaFirst;
+    int ctas;
     const int* groupColumns;  // complex columns per member in each group
     const int* groupFirst;    // first complex column of each group within a member
     long long memberColumns;
