@@ -68,6 +68,7 @@ def parse():
                         "per-stage event timing of one more run as JSON, and exit")
     p.add_argument("--repeat", type=int, default=1)
     p.add_argument("--no-stage-times", action="store_true", help="with --profile-run: skip the extra timed run")
+    p.add_argument("--autotune", action="store_true", help="with --profile-run: apply the autotuner's shapes first")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes instead of the autotuner's choices")
     p.add_argument("--families", action="store_true",
@@ -294,6 +295,7 @@ def profile_run(args, dist):
     x = power_law_inputs(args.n, args.nz, args.members, seed=129 + dist.rank)
     din = S.DeviceArray.from_numpy(x.astype(flux.device_dtype))
     dout = S.DeviceArray(flux.output_elements * np.dtype(flux.device_dtype).itemsize)
+    tuned = flux.autotune(din.ptr, dout.ptr) if args.autotune else {}
     for _ in range(args.repeat):
         flux.execute_device(din.ptr, dout.ptr)
     S.synchronize()
@@ -301,7 +303,8 @@ def profile_run(args, dist):
     if args.no_stage_times or dist.rank != 0:
         return None
     return {"profile_run": {"n": args.n, "nz": args.nz, "members": args.members, "mode": args.mode,
-                            "repeat": args.repeat}, "stages": flux.profile(din.ptr, dout.ptr)}
+                            "repeat": args.repeat, "autotune": {k: v[0] for k, v in tuned.items()}},
+            "stages": flux.profile(din.ptr, dout.ptr)}
 
 
 def cuda_arm(args, dist):

@@ -668,6 +668,94 @@ __global__ void __launch_bounds__(32 * B, 4) columns_forward_band_warp_kernel(in
     }
 }
 
+// 16-plane forms of the two direct band kernels (kBand16).  A CTA of 512
+// threads owns 16 consecutive planes of the flat plane index (slot * zStride
+// + z) and one kx column, so each pass-1 load and pass-3 store instruction of a
+// half-warp moves 128 contiguous bytes of one ky row (the 8-plane forms move
+// 64, which held the stage near 45 % of HBM: a copy with the same addressing
+// and no FFT ran at the same speed, and at 16 planes about 1.6x faster).
+// Chunks over the flat index keep every chunk full of real planes except
+// where it crosses a slot's z padding (planes with z >= Nz are skipped).
+// Pass 1 thread (plane b = t % 16, butterflies j): the two butterflies of a
+// warp are j and j + 2, so with the 2-mod-16 plane region the pass-1 stores
+// and pass-3 loads of a warp fill every bank pair exactly twice.
+// SIGN = +1: inverse (read the band, write every row); SIGN = -1: forward
+// (read every row, write the band times scale).
+__device__ __forceinline__ int band16_butterfly(int t, int q) {
+    const int a = (t >> 5) & 15, c = (t >> 4) & 1;
+    return 4 * (a >> 1) + (a & 1) + 2 * c + 32 * q;
+}
+constexpr size_t kBand16Smem = sizeof(float2) * (16 * kDirectRegion + kDirectTable);
+
+template <int SIGN>
+__global__ void __launch_bounds__(512, 2) columns_band16_kernel(int nz, int zStride, long long flatPlanes, DenseBins bins,
+                                                                const int* __restrict__ bandOf, float scale,
+                                                                const float2* __restrict__ tw) {
+    constexpr int B = 16, N = kDirectN, XP = kDirectRegion;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xs = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float2* tt = xs + B * XP;
+    rr_fill_table<float, N>(tt, tw, tid, 512);
+    const long long p0 = static_cast<long long>(blockIdx.x) * B;
+    const int kx = blockIdx.y;
+    const int b = tid & 15;
+    const long long p = p0 + b;
+    const bool inRange = p < flatPlanes && static_cast<int>(p % zStride) < nz;
+    const int band = __ldg(bandOf + kx);
+    float2* col = static_cast<float2*>(bins.data) + p + bins.planes * kx;
+    const long long rowStride = bins.planes * bins.kxStride;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = band16_butterfly(tid, q);
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int ky = j + 64 * r;
+            const bool load = inRange && (SIGN < 0 || in_band(ky, N, band));
+            v[r] = load ? col[rowStride * ky] : make_float2(0.f, 0.f);
+        }
+        dft8<SIGN>(v);
+        float2* o = xs + b * XP + 8 * j + (j >> 1);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) o[r] = v[r];
+    }
+    __syncthreads();
+    {
+        const long long pw = p0 + warp;  // planes beyond Nz (or the array) stay idle
+        if (pw < flatPlanes && static_cast<int>(pw % zStride) < nz) direct_middle_pass<SIGN>(xs, tt, warp, lane);
+    }
+    __syncthreads();
+    if (!inRange) return;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = ((tid >> 4) & 31) + 32 * q;
+        float2 v[8];
+        direct_last_inputs<SIGN>(xs, tt, b, j, v);
+        dft8<SIGN>(v);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int ky = j + 64 * r;
+            if (SIGN > 0)
+                col[rowStride * ky] = v[r];
+            else if (in_band(ky, N, band))
+                col[rowStride * ky] = make_float2(scale * v[r].x, scale * v[r].y);
+        }
+    }
+}
+
+template <int SIGN>
+cudaError_t launch_band16(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, float scale,
+                          const void* tw, cudaStream_t s) {
+    auto kernel = columns_band16_kernel<SIGN>;
+    cudaError_t err = prepare(kernel, kBand16Smem);
+    if (err != cudaSuccess) return err;
+    const long long flat = static_cast<long long>(slots) * zStride;
+    const dim3 grid(unsigned((flat + 15) / 16), unsigned(columns));
+    kernel<<<grid, 512, kBand16Smem, s>>>(nz, zStride, flat, bins, band, scale, static_cast<const float2*>(tw));
+    return cudaGetLastError();
+}
+
 template <int SIGN>
 cudaError_t launch_band_persist(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band,
                                 float scale, const void* tw, cudaStream_t s) {
@@ -702,6 +790,7 @@ cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBin
     const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
     if (N == kDirectN && form == kBandPersist)
         return launch_band_persist<+1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
+    if (N == kDirectN && form == kBand16) return launch_band16<+1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
     if (N == kDirectN && form != kBandWarp) {
         auto kernel = form == kBandDirect4 ? columns_inverse_band_kernel<4> : columns_inverse_band_kernel<3>;
         cudaError_t err = prepare(kernel, kDirectSmem);
@@ -725,6 +814,8 @@ cudaError_t forward_band_n(int nz, int zStride, int slots, int columns, DenseBin
     const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
     if (N == kDirectN && form == kBandPersist)
         return launch_band_persist<-1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
+    if (N == kDirectN && form == kBand16)
+        return launch_band16<-1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
     if (N == kDirectN && form != kBandWarp) {
         auto kernel = form == kBandDirect4 ? columns_forward_band_kernel<4> : columns_forward_band_kernel<3>;
         cudaError_t err = prepare(kernel, kDirectSmem);

@@ -172,10 +172,15 @@ def test_serving_mix_classes_alone_equals_mixed_and_matches_oracle(reference_cas
         f.close()
 
 
-@pytest.mark.parametrize("planes", [8, 16])
-def test_flux_split_two_planes_per_warp_rows_match_oracle(reference_case, planes):
-    # The 512-point row kernel's two-planes-per-warp form (16 x 16 FFT), forced
-    # through the tuning cache, at the benchmark shape against the oracle.
+@pytest.mark.parametrize("forced", [{"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 8},
+                                    {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 16},
+                                    {"flux.columns_band.form": 4}],
+                         ids=["pair-rows-8", "pair-rows-16", "band16-columns"])
+def test_flux_split_forced_kernel_forms_match_oracle(reference_case, forced):
+    # Kernel forms the tuner may pick, forced through the tuning cache, at the
+    # benchmark shape against the oracle: the 512-point row kernel's
+    # two-planes-per-warp form (16 x 16 FFT) at both CTA widths, and the
+    # 16-plane band column kernels (whose plane chunks cross slot padding).
     x, ref = reference_case
     skb_cuda.tune_cache_clear()
     probe = skb_cuda.Flux(N, NZ, mode=skb_cuda.FLUX_SPLIT_TF32X3)
@@ -184,10 +189,9 @@ def test_flux_split_two_planes_per_warp_rows_match_oracle(reference_case, planes
     chosen = probe.autotune(d_in.ptr, d_out.ptr)
     probe.close()
     for key in chosen:
-        if key.startswith("flux.rows.pairs"):
-            skb_cuda.tune_cache_store(key, 1, 0.0)
-        if key.startswith("flux.rows.planes_per_cta"):
-            skb_cuda.tune_cache_store(key, planes, 0.0)
+        for prefix, value in forced.items():
+            if key.startswith(prefix + " "):
+                skb_cuda.tune_cache_store(key, value, 0.0)
     flux = skb_cuda.Flux(N, NZ, mode=skb_cuda.FLUX_SPLIT_TF32X3)
     out = flux.execute(x)
     flux.check_device()
