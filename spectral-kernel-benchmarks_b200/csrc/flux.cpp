@@ -231,7 +231,9 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
     if (cfg_.n == 512) {
         // Row kernel form first (two planes per warp needs 8 or 16 planes per
         // CTA), then the planes per CTA among those the form takes.
-        pick("flux.rows.pairs" + shape + dev, {0, 1},
+        // pairs 2: the 8-plane form compiled for three CTAs per SM (168
+        // registers, a few spilled) instead of two.
+        pick("flux.rows.pairs" + shape + dev, {0, 1, 2},
              [&](int c) {
                  rowsPairs_ = c;
                  if (c != 0 && rowsPlanes_ < 8) rowsPlanes_ = 8;

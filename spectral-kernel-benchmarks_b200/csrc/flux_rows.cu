@@ -340,8 +340,11 @@ constexpr size_t pair_smem_words(int keep) {
     return 2 * size_t(B) * pair_stage_row<B>() + size_t(B) * kPairXch + size_t(keep) * B + kPairM + kPairM;
 }
 
-template <int B>
-__global__ void __launch_bounds__(16 * B, B == 8 ? 2 : 1) rows_flux_pair_kernel(RowFluxArgs a) {
+// MINB: resident CTAs per SM the register allocation must allow (2 for B = 8,
+// 1 for B = 16: about 240 registers; 3 for the B = 8 form that trades spills
+// to L1-cached local memory for occupancy).
+template <int B, int MINB>
+__global__ void __launch_bounds__(16 * B, MINB) rows_flux_pair_kernel(RowFluxArgs a) {
     using V = float2;
     constexpr int M = kPairM;
     constexpr int NT = 16 * B;
@@ -467,11 +470,11 @@ __global__ void __launch_bounds__(16 * B, B == 8 ? 2 : 1) rows_flux_pair_kernel(
     }
 }
 
-template <int B>
+template <int B, int MINB>
 cudaError_t launch_pair(const RowFluxArgs& a, cudaStream_t stream) {
     const int zChunks = (a.nz + B - 1) / B;
     const dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
-    auto kernel = rows_flux_pair_kernel<B>;
+    auto kernel = rows_flux_pair_kernel<B, MINB>;
     const size_t bytes = sizeof(float2) * pair_smem_words<B>(a.keep);
     const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (err != cudaSuccess) return err;
@@ -509,8 +512,8 @@ cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
     const int M = a.nx / 2;
     if (a.keep < 1 || a.keep > M + 1 || a.fieldsIn != 3 + 3 * a.targets || a.zStride < a.nz) return cudaErrorInvalidValue;
     if (a.pairs != 0 && M == kPairM && a.keep <= 176) {
-        if (a.planes == 8) return launch_pair<8>(a, stream);
-        if (a.planes == 16) return launch_pair<16>(a, stream);
+        if (a.planes == 8) return a.pairs == 2 ? launch_pair<8, 3>(a, stream) : launch_pair<8, 2>(a, stream);
+        if (a.planes == 16) return launch_pair<16, 1>(a, stream);
     }
     switch (M) {
         case 32: return launch_planes<32>(a, stream);

@@ -19,6 +19,7 @@ struct RowFluxArgs {
     int planes = 8;       // z-planes per CTA: 4, 8 or 16 (an autotuner choice)
     // Nx = 512 only: two planes per warp (16 lanes each, 16 x-pairs per lane)
     // with a radix-16 x radix-16 FFT; needs planes 8 or 16 (autotuner choice).
+    // 2: the 8-plane form compiled for three resident CTAs per SM.
     int pairs = 0;
 };
 

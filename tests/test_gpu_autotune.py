@@ -101,7 +101,7 @@ def test_band_forms_at_512(form):
 
 
 @pytest.mark.parametrize("n,planes,pairs", [(64, 4, 0), (64, 16, 0), (512, 4, 0), (512, 16, 0), (512, 8, 1),
-                                            (512, 16, 1)])
+                                            (512, 16, 1), (512, 8, 2)])
 def test_every_row_kernel_width_is_correct(n, planes, pairs):
     """The fused row kernel with 4, 8 or 16 z-planes per CTA, and at 512 points
     the two-planes-per-warp form with 8 or 16 (the tuner's candidates)."""
