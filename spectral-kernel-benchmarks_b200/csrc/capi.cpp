@@ -631,9 +631,7 @@ int skb_pruned_info(const skb_pruned_provider* p, skb_provider_info* info) {
         info->row_transforms_per_direction = p->w.ny * p->w.planes();
         info->column_transforms_per_direction = info->active_kx * p->w.planes();
         info->omitted_column_transforms_per_direction = (info->full_kx - info->active_kx) * p->w.planes();
-        // A row and a column launch per L2-resident group of fields.
-        const int batch = p->plan->field_batch(static_cast<int>(p->w.fields));
-        info->launches_per_execution = 2 * ((p->w.fields + batch - 1) / batch);
+        info->launches_per_execution = 2;
         info->precision = p->p == Precision::f64 ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
         fill_identity(info, "skb-cuda hand-written sm_100a pruned row/active-column FFT with fused retention");
     });

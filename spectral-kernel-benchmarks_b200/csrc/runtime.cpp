@@ -204,48 +204,17 @@ void HorizontalPlan::inverse_rows(void* real, std::uint64_t planes, cudaStream_t
                "row c2r kernel");
 }
 
-// Fields per pass of the pruned transforms: as for the dense ones
-// (dense_batch), the row and column passes run over groups of fields whose
-// intermediate bins fit in a quarter of L2, all groups reusing the same scratch
-// so its lines stay in L2 and the second pass reads them there.
-int HorizontalPlan::field_batch(int fields) const {
-    constexpr double kL2Share = 126.0 * 1024 * 1024 / 4;
-    const double perField = 2.0 * element_bytes(p_) * static_cast<double>(w_.ny) * keep_ * w_.nz;
-    const int batch = std::max(1, static_cast<int>(kL2Share / perField));
-    return fields <= 2 * batch ? fields : batch;
-}
-
-namespace {
-ViewSet view_slice(const ViewSet& views, int first, int count) {
-    ViewSet out{};
-    out.count = count;
-    for (int i = 0; i < count; ++i) out.v[i] = views.v[first + i];
-    return out;
-}
-}  // namespace
-
 void HorizontalPlan::forward(const void* real, std::uint64_t planes, const ViewSet& views, double scale,
                              cudaStream_t s) const {
     if (planes != static_cast<std::uint64_t>(views.count) * w_.nz)
         throw Error(-1, "field views must cover every real plane");
-    const int batch = field_batch(views.count);
-    const size_t realField = element_bytes(p_) * w_.nx * w_.ny * w_.nz;
-    for (int f0 = 0; f0 < views.count; f0 += batch) {
-        const int n = std::min(batch, views.count - f0);
-        forward_rows(static_cast<const unsigned char*>(real) + realField * f0, static_cast<std::uint64_t>(n) * w_.nz,
-                     s);
-        forward_columns(view_slice(views, f0, n), scale, s);
-    }
+    forward_rows(real, planes, s);
+    forward_columns(views, scale, s);
 }
 
 void HorizontalPlan::inverse(const ViewSet& views, void* real, cudaStream_t s) const {
-    const int batch = field_batch(views.count);
-    const size_t realField = element_bytes(p_) * w_.nx * w_.ny * w_.nz;
-    for (int f0 = 0; f0 < views.count; f0 += batch) {
-        const int n = std::min(batch, views.count - f0);
-        inverse_columns(view_slice(views, f0, n), s);
-        inverse_rows(static_cast<unsigned char*>(real) + realField * f0, static_cast<std::uint64_t>(n) * w_.nz, s);
-    }
+    inverse_columns(views, s);
+    inverse_rows(real, static_cast<std::uint64_t>(views.count) * w_.nz, s);
 }
 
 // Planes per pass of the dense 2-D transforms: the row and column passes run

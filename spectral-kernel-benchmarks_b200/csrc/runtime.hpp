@@ -100,8 +100,6 @@ public:
     ModeTables tables() const;
     // Planes per batch of the dense forward / inverse (L2-resident intermediate).
     std::uint64_t dense_batch(std::uint64_t planes) const;
-    // Fields per batch of the pruned forward / inverse (L2-resident bins).
-    int field_batch(int fields) const;
     DenseBins scratch(std::uint64_t planes) const {
         return {bins_.get(), static_cast<long long>(planes), static_cast<long long>(keep_)};
     }
