@@ -410,9 +410,7 @@ int skb_fft_info(const skb_fft_provider* p, skb_provider_info* info) {
         info->full_kx = p->w.nxHalf();
         info->row_transforms_per_direction = p->w.ny * p->w.planes();
         info->column_transforms_per_direction = p->w.nxHalf() * p->w.planes();
-        // A row and a column launch per L2-resident batch of planes.
-        const std::uint64_t batch = p->plan->dense_batch(p->w.planes());
-        info->launches_per_execution = 2 * ((p->w.planes() + batch - 1) / batch);
+        info->launches_per_execution = 2;
         info->precision = p->p == Precision::f64 ? SKB_PRECISION_FP64 : SKB_PRECISION_FP32;
         info->destroys_native_input = 0;
         fill_identity(info, "skb-cuda hand-written sm_100a row/column shared-memory FFT");

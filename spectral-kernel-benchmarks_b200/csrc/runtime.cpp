@@ -217,58 +217,28 @@ void HorizontalPlan::inverse(const ViewSet& views, void* real, cudaStream_t s) c
     inverse_rows(real, static_cast<std::uint64_t>(views.count) * w_.nz, s);
 }
 
-// Planes per pass of the dense 2-D transforms: the row and column passes run
-// over batches of planes whose intermediate spectrum (Ny x keep complex values
-// per plane) fits in a quarter of the 126 MB L2, so the second pass reads the
-// first pass's output from L2.  The forward runs in place on the output, so
-// each batch's row-pass lines are overwritten by its column pass while still
-// in L2 and reach HBM once, with their final values; the inverse reuses one
-// batch-sized scratch, whose lines stay in L2 from batch to batch.  Batches
-// are a multiple of 16 planes (whole 128-byte rows of planes for the column
-// kernels); workloads up to two batches run as one pass.
-std::uint64_t HorizontalPlan::dense_batch(std::uint64_t planes) const {
-    constexpr double kL2Share = 126.0 * 1024 * 1024 / 4;
-    const double perPlane = 2.0 * element_bytes(p_) * static_cast<double>(w_.ny) * keep_;
-    std::uint64_t batch = static_cast<std::uint64_t>(kL2Share / perPlane) / 16 * 16;
-    if (batch < 16) batch = 16;
-    return planes <= 2 * batch ? planes : batch;
-}
-
 void HorizontalPlan::forward_dense(const void* real, void* wvm, std::uint64_t planes, cudaStream_t s) const {
     if (keep_ != static_cast<int>(w_.nxHalf())) throw Error(-3, "dense transform requested from a pruned plan");
-    const std::uint64_t batch = dense_batch(planes);
-    const size_t es = element_bytes(p_);
-    for (std::uint64_t p0 = 0; p0 < planes; p0 += batch) {
-        const std::uint64_t n = std::min(batch, planes - p0);
-        const DenseBins out{static_cast<unsigned char*>(wvm) + 2 * es * p0, static_cast<long long>(planes),
-                            static_cast<long long>(w_.nxHalf())};
-        const void* in = static_cast<const unsigned char*>(real) + es * p0 * w_.nx * w_.ny;
-        check_cuda(launch_rows_forward(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny), static_cast<long long>(n),
-                                       keep_, in, out, twHalf_.get(), twFull_.get(), s),
-                   "row r2c kernel");
-        check_cuda(launch_columns_dense(p_, -1, static_cast<int>(w_.ny), keep_, static_cast<long long>(n), out, out,
-                                        twCol_.get(), s),
-                   "column c2c kernel");
-    }
+    const DenseBins out{wvm, static_cast<long long>(planes), static_cast<long long>(w_.nxHalf())};
+    check_cuda(launch_rows_forward(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny),
+                                   static_cast<long long>(planes), keep_, real, out, twHalf_.get(), twFull_.get(), s),
+               "row r2c kernel");
+    check_cuda(launch_columns_dense(p_, -1, static_cast<int>(w_.ny), keep_, static_cast<long long>(planes), out, out,
+                                    twCol_.get(), s),
+               "column c2c kernel");
 }
 
 void HorizontalPlan::inverse_dense(const void* wvm, void* real, std::uint64_t planes, cudaStream_t s) const {
     if (keep_ != static_cast<int>(w_.nxHalf())) throw Error(-3, "dense transform requested from a pruned plan");
     if (planes > maxPlanes_) throw Error(-1, "plane count exceeds the plan's scratch");
-    const std::uint64_t batch = dense_batch(planes);
-    const size_t es = element_bytes(p_);
-    for (std::uint64_t p0 = 0; p0 < planes; p0 += batch) {
-        const std::uint64_t n = std::min(batch, planes - p0);
-        const DenseBins in{const_cast<unsigned char*>(static_cast<const unsigned char*>(wvm)) + 2 * es * p0,
-                           static_cast<long long>(planes), static_cast<long long>(w_.nxHalf())};
-        void* out = static_cast<unsigned char*>(real) + es * p0 * w_.nx * w_.ny;
-        check_cuda(launch_columns_dense(p_, +1, static_cast<int>(w_.ny), keep_, static_cast<long long>(n), in,
-                                        scratch(n), twCol_.get(), s),
-                   "column c2c kernel");
-        check_cuda(launch_rows_inverse(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny), static_cast<long long>(n),
-                                       keep_, scratch(n), out, twHalf_.get(), twFull_.get(), s),
-                   "row c2r kernel");
-    }
+    const DenseBins in{const_cast<void*>(wvm), static_cast<long long>(planes), static_cast<long long>(w_.nxHalf())};
+    check_cuda(launch_columns_dense(p_, +1, static_cast<int>(w_.ny), keep_, static_cast<long long>(planes), in,
+                                    scratch(planes), twCol_.get(), s),
+               "column c2c kernel");
+    check_cuda(launch_rows_inverse(p_, static_cast<int>(w_.nx), static_cast<int>(w_.ny),
+                                   static_cast<long long>(planes), keep_, scratch(planes), real, twHalf_.get(),
+                                   twFull_.get(), s),
+               "row c2r kernel");
 }
 
 void HorizontalPlan::gather_dense(const void* wvm, std::uint64_t planes, const ViewSet& views, double scale,

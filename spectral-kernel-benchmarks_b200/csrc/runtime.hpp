@@ -98,8 +98,6 @@ public:
     int keep() const { return keep_; }
     std::uint64_t modes() const { return modeCount_; }
     ModeTables tables() const;
-    // Planes per batch of the dense forward / inverse (L2-resident intermediate).
-    std::uint64_t dense_batch(std::uint64_t planes) const;
     DenseBins scratch(std::uint64_t planes) const {
         return {bins_.get(), static_cast<long long>(planes), static_cast<long long>(keep_)};
     }
