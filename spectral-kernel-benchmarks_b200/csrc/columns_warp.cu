@@ -668,38 +668,80 @@ __global__ void __launch_bounds__(32 * B, 4) columns_forward_band_warp_kernel(in
     }
 }
 
-// 16-plane forms of the two direct band kernels (kBand16).  A CTA of 512
-// threads owns 16 consecutive planes of the flat plane index (slot * zStride
-// + z) and one kx column, so each pass-1 load and pass-3 store instruction of a
-// half-warp moves 128 contiguous bytes of one ky row (the 8-plane forms move
+// 16- and 32-plane forms of the two direct band kernels (kBand16, kBand32).
+// A CTA of 32 B threads owns B consecutive planes of the flat plane index
+// (slot * zStride + z) and one kx column, so each pass-1 load and pass-3 store
+// instruction moves 8 B contiguous bytes of one ky row (the 8-plane forms move
 // 64, which held the stage near 45 % of HBM: a copy with the same addressing
 // and no FFT ran at the same speed, and at 16 planes about 1.6x faster).
-// Chunks over the flat index keep every chunk full of real planes except
-// where it crosses a slot's z padding (planes with z >= Nz are skipped).
-// Pass 1 thread (plane b = t % 16, butterflies j): the two butterflies of a
-// warp are j and j + 2, so with the 2-mod-16 plane region the pass-1 stores
-// and pass-3 loads of a warp fill every bank pair exactly twice.
+// Chunks over the flat index keep every chunk full of real planes except where
+// it crosses a slot's z padding (planes with z >= Nz are skipped).
+// Pass-1 thread (plane b = t % B, butterflies j).  B = 16: the two butterflies
+// of a warp are j and j + 2, and with the 2-mod-16 plane region the pass-1
+// stores and pass-3 loads of a warp fill every bank pair exactly twice.
+// B = 32: a warp is 32 planes of one butterfly, and a plane region of 1 mod 16
+// does the same.
 // SIGN = +1: inverse (read the band, write every row); SIGN = -1: forward
 // (read every row, write the band times scale).
-__device__ __forceinline__ int band16_butterfly(int t, int q) {
-    const int a = (t >> 5) & 15, c = (t >> 4) & 1;
-    return 4 * (a >> 1) + (a & 1) + 2 * c + 32 * q;
+template <int B>
+__device__ __forceinline__ int band_wide_butterfly(int t, int q) {
+    if constexpr (B == 16) {
+        const int a = (t >> 5) & 15, c = (t >> 4) & 1;
+        return 4 * (a >> 1) + (a & 1) + 2 * c + 32 * q;
+    } else {
+        return (t >> 5) + 32 * q;
+    }
 }
-constexpr size_t kBand16Smem = sizeof(float2) * (16 * kDirectRegion + kDirectTable);
+template <int B>
+constexpr int band_wide_region() {
+    return B == 16 ? kDirectRegion : 577;  // 577 % 16 == 1, > 511 + 8 * 7
+}
+template <int B>
+constexpr size_t band_wide_smem() {
+    return sizeof(float2) * (size_t(B) * band_wide_region<B>() + kDirectTable);
+}
 
-template <int SIGN>
-__global__ void __launch_bounds__(512, 2) columns_band16_kernel(int nz, int zStride, long long flatPlanes, DenseBins bins,
-                                                                const int* __restrict__ bandOf, float scale,
-                                                                const float2* __restrict__ tw) {
-    constexpr int B = 16, N = kDirectN, XP = kDirectRegion;
+// The direct kernels' middle pass with an explicit plane region.
+template <int SIGN, int XP>
+__device__ __forceinline__ void wide_middle_pass(float2* xs, const float2* tt, int warp, int lane) {
+    float2* x = xs + warp * XP;
+    float2 v[2][8];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = lane + 32 * q;
+        const float2* in = x + j + (j >> 4);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[q][r] = in[68 * r];
+        const float2* t2 = tt + (j % 8);
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[q][r] = cmul(v[q][r], twiddle_plain<SIGN>(t2, 8 * (r - 1)));
+        dft8<SIGN>(v[q]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = lane + 32 * q;
+        float2* o = x + 72 * (j / 8) + (j % 8);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) o[8 * r] = v[q][r];
+    }
+}
+
+template <int B, int SIGN>
+__global__ void __launch_bounds__(32 * B, 32 / B) columns_band_wide_kernel(int nz, int zStride, long long flatPlanes,
+                                                                          DenseBins bins,
+                                                                          const int* __restrict__ bandOf, float scale,
+                                                                          const float2* __restrict__ tw) {
+    constexpr int N = kDirectN, XP = band_wide_region<B>();
+    constexpr int NT = 32 * B;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* xs = reinterpret_cast<float2*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     float2* tt = xs + B * XP;
-    rr_fill_table<float, N>(tt, tw, tid, 512);
+    rr_fill_table<float, N>(tt, tw, tid, NT);
     const long long p0 = static_cast<long long>(blockIdx.x) * B;
     const int kx = blockIdx.y;
-    const int b = tid & 15;
+    const int b = tid % B;
     const long long p = p0 + b;
     const bool inRange = p < flatPlanes && static_cast<int>(p % zStride) < nz;
     const int band = __ldg(bandOf + kx);
@@ -707,7 +749,7 @@ __global__ void __launch_bounds__(512, 2) columns_band16_kernel(int nz, int zStr
     const long long rowStride = bins.planes * bins.kxStride;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-        const int j = band16_butterfly(tid, q);
+        const int j = band_wide_butterfly<B>(tid, q);
         float2 v[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
@@ -723,15 +765,19 @@ __global__ void __launch_bounds__(512, 2) columns_band16_kernel(int nz, int zStr
     __syncthreads();
     {
         const long long pw = p0 + warp;  // planes beyond Nz (or the array) stay idle
-        if (pw < flatPlanes && static_cast<int>(pw % zStride) < nz) direct_middle_pass<SIGN>(xs, tt, warp, lane);
+        if (pw < flatPlanes && static_cast<int>(pw % zStride) < nz) wide_middle_pass<SIGN, XP>(xs, tt, warp, lane);
     }
     __syncthreads();
     if (!inRange) return;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-        const int j = ((tid >> 4) & 31) + 32 * q;
+        const int j = (tid / B) + 32 * q;
+        const float2* in = xs + b * XP + j;  // pass-3 inputs: elements j + 64 r at j + 72 r
         float2 v[8];
-        direct_last_inputs<SIGN>(xs, tt, b, j, v);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = in[72 * r];
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], twiddle_plain<SIGN>(tt + 56 + j, 64 * (r - 1)));
         dft8<SIGN>(v);
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
@@ -744,15 +790,16 @@ __global__ void __launch_bounds__(512, 2) columns_band16_kernel(int nz, int zStr
     }
 }
 
-template <int SIGN>
-cudaError_t launch_band16(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, float scale,
-                          const void* tw, cudaStream_t s) {
-    auto kernel = columns_band16_kernel<SIGN>;
-    cudaError_t err = prepare(kernel, kBand16Smem);
+template <int B, int SIGN>
+cudaError_t launch_band_wide(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, float scale,
+                             const void* tw, cudaStream_t s) {
+    auto kernel = columns_band_wide_kernel<B, SIGN>;
+    cudaError_t err = prepare(kernel, band_wide_smem<B>());
     if (err != cudaSuccess) return err;
     const long long flat = static_cast<long long>(slots) * zStride;
-    const dim3 grid(unsigned((flat + 15) / 16), unsigned(columns));
-    kernel<<<grid, 512, kBand16Smem, s>>>(nz, zStride, flat, bins, band, scale, static_cast<const float2*>(tw));
+    const dim3 grid(unsigned((flat + B - 1) / B), unsigned(columns));
+    kernel<<<grid, 32 * B, band_wide_smem<B>(), s>>>(nz, zStride, flat, bins, band, scale,
+                                                     static_cast<const float2*>(tw));
     return cudaGetLastError();
 }
 
@@ -790,7 +837,10 @@ cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBin
     const dim3 grid(unsigned(zChunks * slots), unsigned(columns));
     if (N == kDirectN && form == kBandPersist)
         return launch_band_persist<+1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
-    if (N == kDirectN && form == kBand16) return launch_band16<+1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
+    if (N == kDirectN && form == kBand16)
+        return launch_band_wide<16, +1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
+    if (N == kDirectN && form == kBand32)
+        return launch_band_wide<32, +1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
     if (N == kDirectN && form != kBandWarp) {
         auto kernel = form == kBandDirect4 ? columns_inverse_band_kernel<4> : columns_inverse_band_kernel<3>;
         cudaError_t err = prepare(kernel, kDirectSmem);
@@ -815,7 +865,9 @@ cudaError_t forward_band_n(int nz, int zStride, int slots, int columns, DenseBin
     if (N == kDirectN && form == kBandPersist)
         return launch_band_persist<-1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
     if (N == kDirectN && form == kBand16)
-        return launch_band16<-1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
+        return launch_band_wide<16, -1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
+    if (N == kDirectN && form == kBand32)
+        return launch_band_wide<32, -1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
     if (N == kDirectN && form != kBandWarp) {
         auto kernel = form == kBandDirect4 ? columns_forward_band_kernel<4> : columns_forward_band_kernel<3>;
         cudaError_t err = prepare(kernel, kDirectSmem);

@@ -36,6 +36,8 @@ constexpr int kBandDirect4 = 3;
 // kBand16: the direct kernel with 16 planes per CTA over the flat plane index
 // (128-byte global accesses per ky row; Ny = 512).
 constexpr int kBand16 = 4;
+// kBand32: the same with 32 planes per CTA (256-byte accesses, one CTA per SM).
+constexpr int kBand32 = 5;
 cudaError_t launch_columns_inverse_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
                                         const int* band, const void* tw, int form, cudaStream_t s);
 cudaError_t launch_columns_forward_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,

@@ -402,11 +402,14 @@ __global__ void __launch_bounds__(16 * B, MINB) rows_flux_pair_kernel(RowFluxArg
         __syncthreads();
         if (f + 1 < a.fieldsIn) issue(f + 1, ((f + 1) & 1) ? stage1 : stage0);
         const V* st = ((f & 1) ? stage1 : stage0) + pl * KP;
+        // keep <= 176 (checked at launch): bins k >= 176 (m >= 11) and
+        // M - k >= 177 (m <= 4) lie beyond the 2/3 band and are zero, so those
+        // shared-memory reads are left out.
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int k = t + 16 * m;
-            V xk = st[k];
-            V xm = st[M - k];
+            V xk = m < 11 ? st[k] : V{0.f, 0.f};
+            V xm = m > 4 ? st[M - k] : V{0.f, 0.f};
             if (m == 0 && t == 0) {  // bins 0 and M are real
                 xk.y = 0.f;
                 xm.y = 0.f;

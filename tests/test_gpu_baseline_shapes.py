@@ -175,8 +175,9 @@ def test_serving_mix_classes_alone_equals_mixed_and_matches_oracle(reference_cas
 @pytest.mark.parametrize("forced", [{"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 8},
                                     {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 16},
                                     {"flux.rows.pairs": 2, "flux.rows.planes_per_cta": 8},
-                                    {"flux.columns_band.form": 4}],
-                         ids=["pair-rows-8", "pair-rows-16", "pair-rows-8-3cta", "band16-columns"])
+                                    {"flux.columns_band.form": 4}, {"flux.columns_band.form": 5}],
+                         ids=["pair-rows-8", "pair-rows-16", "pair-rows-8-3cta", "band16-columns",
+                              "band32-columns"])
 def test_flux_split_forced_kernel_forms_match_oracle(reference_case, forced):
     # Kernel forms the tuner may pick, forced through the tuning cache, at the
     # benchmark shape against the oracle: the 512-point row kernel's
