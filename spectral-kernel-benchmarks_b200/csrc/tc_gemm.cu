@@ -44,7 +44,7 @@ namespace {
 
 constexpr int kTileRows = 128;    // M
 constexpr int kChunkK = 32;       // tf32 elements per 128-byte row
-constexpr int kTmemCols = 512;  // two chunk accumulators + the running sum, NP columns each
+constexpr int kTmemCols = 512;  // two chunk accumulators of NP columns each (power of two)
 constexpr int kStageBytes = 2 * kTileRows * 128;  // hi + lo
 constexpr long long kWaitLimit = 1LL << 22;
 constexpr long long kTestWaitLimit = 1LL << 14;  // the expired-wait test's wait (expireWaitForTest)
@@ -129,13 +129,6 @@ __device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, uint32_t (&v)[8]) {
                  : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_st_x8(uint32_t taddr, const uint32_t (&v)[8]) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ float tf32_rna(float x) {
     uint32_t r;
@@ -234,11 +227,26 @@ __device__ __forceinline__ void cp_async_value(uint32_t dst, const void* src, in
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 
-// Warp roles of the pipelined kernel.
+// Warp roles of the pipelined kernel, one role per warpgroup (4 warps) so
+// that each role can set its own register count: warpgroups 0-1 are the
+// producers, warpgroup 2 holds the MMA warp (its other three warps have no
+// work), warpgroups 3-5 are the epilogue.
 constexpr int kProducerWarps = 8;
 constexpr int kMmaWarp = kProducerWarps;
-constexpr int kEpilogueWarps = 8;
-constexpr int kPipeThreads = (kProducerWarps + 1 + kEpilogueWarps) * 32;
+constexpr int kEpilogueFirst = kMmaWarp + 4;
+constexpr int kEpilogueGroups = 3;  // epilogue warps per TMEM lane quarter
+constexpr int kEpilogueWarps = 4 * kEpilogueGroups;
+constexpr int kPipeThreads = (kEpilogueFirst + kEpilogueWarps) * 32;
+// Registers per thread: the launch gives every thread kLaunchRegs (65,536
+// per SM over 768 threads, in steps of 8); the MMA warpgroup hands most of
+// its share to the epilogue, which keeps a tile's running sums in registers.
+constexpr int kLaunchRegs = 65536 / kPipeThreads / 8 * 8;
+constexpr int kProducerRegs = 56;
+constexpr int kMmaGroupRegs = 32;
+constexpr int kEpilogueRegs = 112;
+static_assert(kProducerWarps * 32 * kProducerRegs + 128 * kMmaGroupRegs + kEpilogueWarps * 32 * kEpilogueRegs <=
+                  kPipeThreads * kLaunchRegs,
+              "register split exceeds the launch's registers");
 constexpr int kStages = 3;
 constexpr int kAccumulators = 2;
 constexpr int kAhead = 2;               // data chunks each producer thread has in flight
@@ -247,6 +255,7 @@ constexpr uint32_t kBulkPiece = 32768;  // bytes per bulk copy of a group image
 struct PipeState {
     uint64_t full[kStages], empty[kStages], accFull[kAccumulators], accEmpty[kAccumulators], done, unitDone, bFull;
     uint64_t never;  // no thread or copy ever arrives on it (expired-wait test)
+    long long colBase[kProducerWarps][8];  // each producer warp's 8 input columns of the current tile
     uint32_t tmem;
 };
 
@@ -365,16 +374,16 @@ __device__ __forceinline__ Unit unit_at(const TcGemmArgs& p, int u) {
 //       all K chunks) into shared memory and prefetches the next unit's into
 //       L2; per chunk, 3 MMAs per k-step into one of two ping-pong TMEM chunk
 //       accumulators; commits empty[stage] and accFull.
-//   epilogue warps 9-16: add each chunk accumulator into an FP32 running sum
-//       kept in TMEM (tcgen05.ld / tcgen05.st), release it (accEmpty), and
+//   warps 9-11: no work (they only lend their registers to the epilogue).
+//   epilogue warps 12-23: read each chunk accumulator (tcgen05.ld), release
+//       it (accEmpty) and add it into an FP32 running sum held in registers;
 //       after the tile's last chunk write the tile's outputs: lane pairs
 //       (the re and im rows of one column) swap halves with a shuffle so each
 //       store instruction writes 16 contiguous bytes of 16 columns.
-// NPH = NP/16: x8 column blocks per epilogue half.
+// NPH = NP/16.
 template <int NPH, int KIND>
 __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArgs p) {
     constexpr int NP = NPH * 16;
-    constexpr int HALF = NP / 2;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -418,6 +427,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
     };
 
     if (warp < kProducerWarps) {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kProducerRegs));
         // ---------------------------------------------------------- producer
         // Issue cursor: unit iu, tile itT, chunk itKc of the tile.
         const Walk W = unit_walk(p);
@@ -425,7 +435,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         Unit IU{};
         if (iu < W.end) IU = unit_at(p, iu);
         int itT = 0, itKc = 0, curTile = -1, tileCount = 0;
-        long long colBase[8];
+        long long* colBase = st->colBase[warp];
         unsigned tileMask = 0;  // bit c: column 8*warp+c of the tile is stored conjugated
         int issued = 0, converted = 0, pending = 0;
         unsigned fifo = 0;  // conjugation masks of the chunks in flight, oldest in the low byte
@@ -460,8 +470,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                 ColumnRef mine{0, -1, false};
                 if (lane < 8 && cl < tileCount) mine = column_ref(p, p.inBins, tv0 + cl, IU.gcols, IU.gfirst, S);
                 tileMask = __ballot_sync(0xFFFFFFFFu, lane < 8 && mine.conj) & 0xFFu;
-#pragma unroll
-                for (int cc = 0; cc < 8; ++cc) colBase[cc] = __shfl_sync(0xFFFFFFFFu, mine.base, cc);
+                if (lane < 8) colBase[lane] = mine.base;
+                __syncwarp();
                 if (itT + 1 < IU.tiles) {
                     prefetch_tile(IU, itT + 1);
                 } else if (iu + W.step < W.end) {
@@ -559,9 +569,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         }
         // No copy may still be writing this CTA's shared memory at exit.
         asm volatile("cp.async.wait_group 0;" ::: "memory");
-    } else if (warp == kMmaWarp) {
+    } else if (warp < kEpilogueFirst) {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kMmaGroupRegs));
         // --------------------------------------------------------------- MMA
-        if (lane == 0) {
+        if (warp == kMmaWarp && lane == 0) {
             // Instruction descriptor: F32 accumulator, A and B TF32 (2) or
             // BF16 (1), both K-major, N = NP, M = 128.
             constexpr uint32_t kOperandFormat = KIND == kKindBf16x3 ? 1u : 2u;
@@ -660,30 +671,35 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
         }
         __syncwarp();
     } else {
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kEpilogueRegs));
         // ---------------------------------------------------------- epilogue
-        // Running chunk sums live in a third TMEM region (columns 2*NP ..),
-        // read-added-stored eight columns at a time.  The final chunk's sum
-        // goes straight to global memory.  TMEM lane 32*quarter + lane is
-        // tile row 2*column + part: this lane holds the real (part 0) or
-        // imaginary (part 1) row of column 16*quarter + lane/2.
+        // Twelve warps, three per TMEM lane quarter: warp (quarter, group)
+        // owns the 8-column accumulator blocks [group * GB, group * GB + GB)
+        // of its 32 TMEM lanes.  The tile's chunk accumulators are added, in
+        // chunk order and in FP32, into a running sum held in registers (no
+        // TMEM round trip per chunk); each accumulator is released as soon as
+        // it has been read, and after the tile's last chunk the sum goes to
+        // global memory.  TMEM lane 32*quarter + lane is tile row
+        // 2*column + part: this lane holds the real (part 0) or imaginary
+        // (part 1) row of column 16*quarter + lane/2.
+        constexpr int NB = NP / 8;
+        constexpr int GB = (NB + kEpilogueGroups - 1) / kEpilogueGroups;
+        // Blocks whose TMEM loads are issued before one wait (fewer at the
+        // widest tiles, where the sums leave no room for three).
+        constexpr int kG = GB <= 6 ? 3 : 1;
         const int quarter = warp & 3;  // TMEM lanes this warp may access
-        const int half = (warp - kMmaWarp - 1) >> 2;
+        const int group = (warp - kEpilogueFirst) >> 2;
+        const int blk0 = group * GB;
+        const int nblk = max(0, min(NB, blk0 + GB) - blk0);
         const int part = lane & 1;
         const int cl = quarter * 16 + (lane >> 1);
         const uint32_t laneBase = static_cast<uint32_t>(quarter * 32) << 16;
-        const uint32_t sumBase = tmem + laneBase + static_cast<uint32_t>(kAccumulators * NP + half * HALF);
+        float sum[GB][8];
         int it = 0;
         const Walk W = unit_walk(p);
         for (int u = W.begin; u < W.end && !failed; u += W.step) {
             const Unit U = unit_at(p, u);
             for (int t = 0; t < U.tiles && !failed; ++t) {
-                const int tv0 = U.vc0 + t * 64;
-                const bool valid = cl < min(64, U.vc0 + U.vcN - tv0);
-                const ColumnRef ref =
-                    valid ? column_ref(p, p.outBins, tv0 + cl, U.gcols, U.gfirst, R) : ColumnRef{0, -1, false};
-                const float sg = ref.conj ? -1.0f : 1.0f;
-                // 16-byte stores need even element offsets (true for bin cells).
-                const bool wide = ((ref.base | (ref.partner < 0 ? 0 : ref.partner)) & 1) == 0;
                 for (int kc = 0; kc < KCH; ++kc, ++it) {
                     const int acc = it % kAccumulators;
                     if (!mbar_wait(smem_u32(&st->accFull[acc]), (it / kAccumulators) & 1, p.error)) {
@@ -691,84 +707,78 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_gemm_pipe_kernel(TcGemmArg
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t accBase = tmem + laneBase + static_cast<uint32_t>(acc * NP + half * HALF);
-                    const bool first = kc == 0, last = kc == KCH - 1;
-                    // Blocks of 8 accumulator columns are handled kG at a
-                    // time: their TMEM loads are issued together and waited
-                    // for once.
-                    constexpr int kBlocks = HALF / 8, kG = 3;
-#pragma unroll 1
-                    for (int b0 = 0; b0 < kBlocks; b0 += kG) {
-                        uint32_t a[kG][8], b[kG][8];
+                    const uint32_t accBase = tmem + laneBase + static_cast<uint32_t>(acc * NP + blk0 * 8);
+                    const bool first = kc == 0;
+#pragma unroll
+                    for (int b0 = 0; b0 < GB; b0 += kG) {
+                        uint32_t a[kG][8];
 #pragma unroll
                         for (int i = 0; i < kG; ++i)
-                            if (b0 + i < kBlocks) {
-                                tmem_ld_x8(accBase + (b0 + i) * 8, a[i]);
-                                if (!first) tmem_ld_x8(sumBase + (b0 + i) * 8, b[i]);
-                            }
+                            if (b0 + i < GB && b0 + i < nblk) tmem_ld_x8(accBase + (b0 + i) * 8, a[i]);
                         tmem_wait_ld();
 #pragma unroll
                         for (int i = 0; i < kG; ++i) {
-                            if (b0 + i >= kBlocks) break;
-                            const int blk = b0 + i;
-                            float x8[8];
+                            if (b0 + i >= GB) break;
 #pragma unroll
                             for (int j = 0; j < 8; ++j)
-                                x8[j] = first ? __uint_as_float(a[i][j])
-                                              : __uint_as_float(b[i][j]) + __uint_as_float(a[i][j]);
-                            if (!last) {
-                                uint32_t o[8];
+                                sum[b0 + i][j] = first ? __uint_as_float(a[i][j]) : sum[b0 + i][j] + __uint_as_float(a[i][j]);
+                        }
+                    }
+                    // The accumulator may be overwritten once all its loads have completed.
+                    tc_fence_before();
+                    mbar_arrive(smem_u32(&st->accEmpty[acc]));
+                    if (kc != KCH - 1) continue;
+                    // The output column is looked up only now, so that no
+                    // register holds it while the chunks are summed.
+                    const int tv0 = U.vc0 + t * 64;
+                    const bool valid = cl < min(64, U.vc0 + U.vcN - tv0);
+                    const ColumnRef ref =
+                        valid ? column_ref(p, p.outBins, tv0 + cl, U.gcols, U.gfirst, R) : ColumnRef{0, -1, false};
+                    const float sg = ref.conj ? -1.0f : 1.0f;
+                    // 16-byte stores need even element offsets (true for bin cells).
+                    const bool wide = ((ref.base | (ref.partner < 0 ? 0 : ref.partner)) & 1) == 0;
 #pragma unroll
-                                for (int j = 0; j < 8; ++j) o[j] = __float_as_uint(x8[j]);
-                                tmem_st_x8(sumBase + blk * 8, o);
+                    for (int i = 0; i < GB; ++i) {
+                        if (i >= nblk) break;
+                        const float* x8 = sum[i];
+                        // Rows n0 .. n0+7 of this column.  The even lane stores
+                        // outputs n0+{0,1} and n0+{4,5}, the odd lane n0+{2,3}
+                        // and n0+{6,7}, after trading the other part with its
+                        // partner, so each store instruction fills whole
+                        // 32-byte sectors of 16 columns.
+                        const int n0 = (blk0 + i) * 8;
+                        float o[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int e = (k & 1) + 4 * (k >> 1);
+                            o[k] = __shfl_xor_sync(0xFFFFFFFFu, part ? x8[e] : x8[e + 2], 1);
+                        }
+                        if (!valid) continue;
+#pragma unroll
+                        for (int h2 = 0; h2 < 2; ++h2) {
+                            const int e = 4 * h2;
+                            const int n = n0 + e + 2 * part;
+                            const float re0 = part ? o[2 * h2] : x8[e];
+                            const float im0 = sg * (part ? x8[e + 2] : o[2 * h2]);
+                            const float re1 = part ? o[2 * h2 + 1] : x8[e + 1];
+                            const float im1 = sg * (part ? x8[e + 3] : o[2 * h2 + 1]);
+                            if (wide && n + 1 < R) {
+                                *reinterpret_cast<float4*>(p.out + ref.base + n) = make_float4(re0, im0, re1, im1);
+                                if (ref.partner >= 0)
+                                    *reinterpret_cast<float4*>(p.out + ref.partner + n) =
+                                        make_float4(re0, -im0, re1, -im1);
                             } else {
-                                // Rows n0 .. n0+7 of this column.  The even lane
-                                // stores outputs n0+{0,1} and n0+{4,5}, the odd
-                                // lane n0+{2,3} and n0+{6,7}, after trading the
-                                // other part with its partner, so each store
-                                // instruction fills whole 32-byte sectors of 16
-                                // columns.
-                                const int n0 = half * HALF + blk * 8;
-                                float o[4];
-#pragma unroll
-                                for (int k = 0; k < 4; ++k) {
-                                    const int e = (k & 1) + 4 * (k >> 1);
-                                    o[k] = __shfl_xor_sync(0xFFFFFFFFu, part ? x8[e] : x8[e + 2], 1);
+                                if (n < R) {
+                                    p.out[ref.base + n] = make_float2(re0, im0);
+                                    if (ref.partner >= 0) p.out[ref.partner + n] = make_float2(re0, -im0);
                                 }
-                                if (valid) {
-#pragma unroll
-                                    for (int h2 = 0; h2 < 2; ++h2) {
-                                        const int e = 4 * h2;
-                                        const int n = n0 + e + 2 * part;
-                                        const float re0 = part ? o[2 * h2] : x8[e];
-                                        const float im0 = sg * (part ? x8[e + 2] : o[2 * h2]);
-                                        const float re1 = part ? o[2 * h2 + 1] : x8[e + 1];
-                                        const float im1 = sg * (part ? x8[e + 3] : o[2 * h2 + 1]);
-                                        if (wide && n + 1 < R) {
-                                            *reinterpret_cast<float4*>(p.out + ref.base + n) =
-                                                make_float4(re0, im0, re1, im1);
-                                            if (ref.partner >= 0)
-                                                *reinterpret_cast<float4*>(p.out + ref.partner + n) =
-                                                    make_float4(re0, -im0, re1, -im1);
-                                        } else {
-                                            if (n < R) {
-                                                p.out[ref.base + n] = make_float2(re0, im0);
-                                                if (ref.partner >= 0) p.out[ref.partner + n] = make_float2(re0, -im0);
-                                            }
-                                            if (n + 1 < R) {
-                                                p.out[ref.base + n + 1] = make_float2(re1, im1);
-                                                if (ref.partner >= 0)
-                                                    p.out[ref.partner + n + 1] = make_float2(re1, -im1);
-                                            }
-                                        }
-                                    }
+                                if (n + 1 < R) {
+                                    p.out[ref.base + n + 1] = make_float2(re1, im1);
+                                    if (ref.partner >= 0) p.out[ref.partner + n + 1] = make_float2(re1, -im1);
                                 }
                             }
                         }
                     }
-                    if (!last) tmem_wait_st();
-                    tc_fence_before();
-                    mbar_arrive(smem_u32(&st->accEmpty[acc]));
                 }
             }
         }
@@ -789,7 +799,7 @@ size_t tc_gemm_smem_bytes(int R, int S) {
 
 bool tc_gemm_supported(int R, int S) {
     const int NP = (R + 15) / 16 * 16;
-    return NP >= 16 && NP <= 160 && (kAccumulators + 1) * NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
+    return NP >= 16 && NP <= 160 && kAccumulators * NP <= kTmemCols && tc_gemm_smem_bytes(R, S) <= 227 * 1024;
 }
 
 size_t tc_gemm_image_bytes(int R, int S) {
