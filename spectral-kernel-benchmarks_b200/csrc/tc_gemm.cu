@@ -828,6 +828,18 @@ cudaError_t launch_np(const TcGemmArgs& args, cudaStream_t stream) {
     const size_t bytes = std::max<size_t>(tc_gemm_smem_bytes(args.R, args.S), 116 * 1024);
     auto kernel = args.kind == kKindBf16x3 ? tc_gemm_pipe_kernel<NPH, kKindBf16x3>
                                            : tc_gemm_pipe_kernel<NPH, kKindTf32x3>;
+    // The warpgroups' setmaxnreg split assumes the kernel was built with
+    // exactly kLaunchRegs registers per thread; with fewer, the epilogue's
+    // increase could never be granted, so such a build is refused.
+    static int launchRegs[2] = {0, 0};
+    int& regs = launchRegs[args.kind == kKindBf16x3 ? 1 : 0];
+    if (regs == 0) {
+        cudaFuncAttributes attr{};
+        const cudaError_t aerr = cudaFuncGetAttributes(&attr, kernel);
+        if (aerr != cudaSuccess) return aerr;
+        regs = attr.numRegs;
+    }
+    if (regs != kLaunchRegs) return cudaErrorInvalidDeviceFunction;
     const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (err != cudaSuccess) return err;
     // Persistent: one CTA per SM (or per unit, if fewer).
