@@ -126,6 +126,8 @@ FluxPipeline::FluxPipeline(const FluxConfig& cfg) : cfg_(cfg) {
         const std::uint64_t keep = static_cast<std::uint64_t>(horizontal_->keep());
         binsIn_.allocate(2 * es * cfg.n * keep * cfg.members * fieldsIn_ * zStride_);
         binsOut_.allocate(2 * es * cfg.n * keep * cfg.members * cfg.targets * zStride_);
+        rowsError_.allocate(sizeof(int));
+        check_cuda(cudaMemset(rowsError_.get(), 0, sizeof(int)), "cudaMemset");
         if (dense_) {
             const long long inStored = static_cast<long long>(cfg.members * fieldsIn_ * zStride_);
             const long long outStored = static_cast<long long>(cfg.members * cfg.targets * zStride_);
@@ -238,6 +240,12 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
                  rowsPairs_ = c;
                  if (c != 0 && rowsPlanes_ < 8) rowsPlanes_ = 8;
              },
+             [&] { check_cuda(launch_rows_flux(row_args(M), s), "fused row flux kernel"); });
+    }
+    if (cfg_.n == 512 && rowsPairs_ != 0) {
+        // Two-planes-per-warp forms: stage fills by per-thread cp.async (0) or
+        // by one TMA tensor copy per slot (1).
+        pick("flux.rows.tma" + shape + dev, {0, 1}, [&](int c) { rowsTma_ = c; },
              [&] { check_cuda(launch_rows_flux(row_args(M), s), "fused row flux kernel"); });
     }
     pick("flux.rows.planes_per_cta" + shape + dev, rowsPairs_ != 0 ? std::vector<int>{8, 16} : std::vector<int>{4, 8, 16},
@@ -361,6 +369,8 @@ RowFluxArgs FluxPipeline::row_args(std::uint64_t members) const {
     a.twFull = horizontal_->twiddlesFull();
     a.planes = rowsPlanes_;
     a.pairs = rowsPairs_;
+    a.tma = rowsTma_;
+    a.error = static_cast<int*>(rowsError_.get());
     return a;
 }
 
@@ -571,6 +581,11 @@ void FluxPipeline::gemm_forward(void* modalOut, cudaStream_t s, std::uint64_t M,
 
 void FluxPipeline::check_device_errors() const {
     for (const VerticalPlan* g : gemm_plans()) g->check_device_error();
+    if (rowsError_.bytes() != 0) {
+        int flag = 0;
+        check_cuda(cudaMemcpy(&flag, rowsError_.get(), sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
+        if (flag != 0) throw Error(-2, "fused row kernel: a bounded wait for a stage copy expired");
+    }
 }
 
 void FluxPipeline::capture(const void* modalIn, void* modalOut, cudaStream_t s) {

@@ -133,6 +133,8 @@ private:
     DeviceBuffer cellModalIn_, cellModalOut_, cellPhysIn_, cellPhysOut_;
     int rowsPlanes_ = 8;  // z-planes per CTA of the fused row kernel
     int rowsPairs_ = 0;   // 512-point rows: two planes per warp (RowFluxArgs::pairs)
+    int rowsTma_ = 0;     // two-planes-per-warp rows: stages filled by TMA tensor copies (RowFluxArgs::tma)
+    DeviceBuffer rowsError_;  // set by the fused row kernel when a bounded wait expires
     void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graphExec_ = nullptr;

@@ -27,6 +27,7 @@
 
 #include "async_copy.cuh"
 #include "fft_device.cuh"
+#include "tensor_map.hpp"
 
 namespace skb {
 namespace {
@@ -340,20 +341,70 @@ constexpr size_t pair_smem_words(int keep) {
     return 2 * size_t(B) * pair_stage_row<B>() + size_t(B) * kPairXch + size_t(keep) * B + kPairM + kPairM;
 }
 
+// TMA form of the stage: rows kx = 0..kTmaRows-1 (the pre-processing reads no
+// bin beyond kx = 176, see inverse_row), each row the B planes' values
+// (64 or 128 bytes) in the SWIZZLE_64B / SWIZZLE_128B pattern the tensor
+// copy writes; rows keep..kTmaRows-1 are zero.  Stages start on 1024-byte
+// boundaries (the swizzle pattern's period).
+constexpr int kTmaRows = 177;
+template <int B>
+constexpr size_t tma_stage_bytes() {
+    return (size_t(kTmaRows) * B * 8 + 1023) / 1024 * 1024;
+}
+template <int B>
+constexpr size_t pair_tma_smem_bytes(int keep) {
+    return 1024 + 2 * tma_stage_bytes<B>() +
+           sizeof(float2) * (size_t(B) * kPairXch + size_t(keep) * B + kPairM + kPairM);
+}
+// Byte offset of (kx k, plane b) in a swizzled TMA stage.
+template <int B>
+__device__ __forceinline__ unsigned tma_stage_offset(int k, int b) {
+    const unsigned off = static_cast<unsigned>((k * B + b) * 8);
+    return off ^ (((off >> 7) & (B == 8 ? 3u : 7u)) << 4);
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+// A bounded wait on an mbarrier phase (false once the limit is reached).
+__device__ __forceinline__ bool stage_wait(unsigned bar, unsigned parity) {
+    for (long long i = 0; i < (1LL << 22); ++i) {
+        unsigned ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
 // MINB: resident CTAs per SM the register allocation must allow (2 for B = 8,
 // 1 for B = 16: about 240 registers; 3 for the B = 8 form that trades spills
 // to L1-cached local memory for occupancy).
-template <int B, int MINB>
-__global__ void __launch_bounds__(16 * B, MINB) rows_flux_pair_kernel(RowFluxArgs a) {
+// TMA: each slot's stage is filled by one tensor copy (thread 0, onto an
+// mbarrier; `tmIn` maps the input bins as [cell][plane]) instead of 8-byte
+// cp.async by every thread.  Thread 0's bounded wait on the copy is folded
+// into the slot's CTA barrier (__syncthreads_and), so an expired wait makes
+// every thread leave together after setting the error word.
+template <int B, int MINB, bool TMA>
+__global__ void __launch_bounds__(16 * B, MINB)
+    rows_flux_pair_kernel(RowFluxArgs a, const __grid_constant__ CUtensorMap tmIn) {
     using V = float2;
     constexpr int M = kPairM;
     constexpr int NT = 16 * B;
     constexpr int KP = pair_stage_row<B>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long stageFull[2];
     const int keep = a.keep;
-    V* stage0 = reinterpret_cast<V*>(smem_raw);
-    V* stage1 = stage0 + B * KP;
-    V* xchAll = stage1 + B * KP;
+    unsigned char* tmaBase =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    V* stage0 = TMA ? reinterpret_cast<V*>(tmaBase) : reinterpret_cast<V*>(smem_raw);
+    V* stage1 = TMA ? reinterpret_cast<V*>(tmaBase + tma_stage_bytes<B>()) : stage0 + B * KP;
+    V* xchAll = TMA ? reinterpret_cast<V*>(tmaBase + 2 * tma_stage_bytes<B>()) : stage1 + B * KP;
     V* outTile = xchAll + B * kPairXch;  // [k][b] at out_slot(k, b)
     V* tf = outTile + keep * B;          // twFull[0..M)
     V* tw2 = tf + M;                     // tw2[16 k2 + t] = twHalf[(t k2) mod M]
@@ -377,39 +428,96 @@ __global__ void __launch_bounds__(16 * B, MINB) rows_flux_pair_kernel(RowFluxArg
         tf[i] = twFull[i];
         tw2[i] = twHalf[((i & 15) * (i >> 4)) & (M - 1)];
     }
-    for (int i = tid; i < 2 * B * (KP - keep); i += NT) {
-        const int row = i / (KP - keep);
-        stage0[row * KP + keep + i % (KP - keep)] = V{0.f, 0.f};
+    if constexpr (TMA) {
+        // Rows keep..kTmaRows-1 of both stages are zero (the tensor copies
+        // write rows 0..keep-1 only; the swizzle stays inside a row).
+        for (int i = tid; i < 2 * (kTmaRows - keep) * B; i += NT) {
+            const int st = i / ((kTmaRows - keep) * B);
+            const int j = i % ((kTmaRows - keep) * B);
+            reinterpret_cast<V*>(tmaBase + st * tma_stage_bytes<B>())[keep * B + j] = V{0.f, 0.f};
+        }
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&stageFull[0])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&stageFull[1])) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+    } else {
+        for (int i = tid; i < 2 * B * (KP - keep); i += NT) {
+            const int row = i / (KP - keep);
+            stage0[row * KP + keep + i % (KP - keep)] = V{0.f, 0.f};
+        }
     }
 
     // Slot f's bins of this row into a plane-major stage [b][k] (cp.async, as
-    // in the warp-per-plane kernel; planes beyond Nz are zero-filled).
+    // in the warp-per-plane kernel; planes beyond Nz are zero-filled), or, in
+    // the TMA form, into a swizzled [k][b] stage by one tensor copy (planes
+    // beyond Nz then hold the next slot's or padding values; those planes'
+    // results are never stored).
     constexpr int KSTEP = NT / B;
     const int cb = tid % B;
     const int ck = tid / B;
     const bool cok = z0 + cb < a.nz;
+    const int tmaLo = static_cast<int>(tma_stage_offset<B>(t, pl));
+    const int tmaHi = static_cast<int>(tma_stage_offset<B>(M - t, pl));
     auto issue = [&](int f, V* stage) {
-        const long long plane = (static_cast<long long>(member) * a.fieldsIn + f) * a.zStride + z0 + cb;
-        const V* src = in + plane + inRow * (a.binsIn.kxStride * y + ck);
-        V* dst = stage + cb * KP + ck;
-        for (int k = ck; k < keep; k += KSTEP, src += inRow * KSTEP, dst += KSTEP) cp_async8(dst, cok ? src : in, cok ? 8 : 0);
-        cp_async_commit();
+        if constexpr (TMA) {
+            if (tid == 0) {
+                const int x = (member * a.fieldsIn + f) * a.zStride + z0;
+                const int yc = static_cast<int>(a.binsIn.kxStride * y);
+                const unsigned bar = smem_addr(&stageFull[f & 1]);
+                // The stage's earlier shared-memory reads precede the copy's writes.
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                             "r"(static_cast<unsigned>(keep * B * 8))
+                             : "memory");
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                    "%3}], [%4];" ::"r"(smem_addr(stage)),
+                    "l"(reinterpret_cast<unsigned long long>(&tmIn)), "r"(x), "r"(yc), "r"(bar)
+                    : "memory");
+            }
+        } else {
+            const long long plane = (static_cast<long long>(member) * a.fieldsIn + f) * a.zStride + z0 + cb;
+            const V* src = in + plane + inRow * (a.binsIn.kxStride * y + ck);
+            V* dst = stage + cb * KP + ck;
+            for (int k = ck; k < keep; k += KSTEP, src += inRow * KSTEP, dst += KSTEP) cp_async8(dst, cok ? src : in, cok ? 8 : 0);
+            cp_async_commit();
+        }
     };
 
-    // c2r of slot f into r[m] = x-pair t + 16 m of this half-warp's plane.
-    auto inverse_row = [&](int f, V (&r)[16]) {
-        cp_async_wait_all();
-        __syncthreads();
+    // c2r of slot f into r[m] = x-pair t + 16 m of this half-warp's plane;
+    // false if the TMA form's wait for the slot's copy expired.
+    auto inverse_row = [&](int f, V (&r)[16]) -> bool {
+        if constexpr (TMA) {
+            const bool ok = tid != 0 || stage_wait(smem_addr(&stageFull[f & 1]), (f >> 1) & 1);
+            if (!__syncthreads_and(ok)) {
+                if (tid == 0 && a.error != nullptr) atomicExch(a.error, 1);
+                return false;
+            }
+        } else {
+            cp_async_wait_all();
+            __syncthreads();
+        }
         if (f + 1 < a.fieldsIn) issue(f + 1, ((f + 1) & 1) ? stage1 : stage0);
         const V* st = ((f & 1) ? stage1 : stage0) + pl * KP;
+        const unsigned char* stb = reinterpret_cast<const unsigned char*>((f & 1) ? stage1 : stage0);
+        // TMA form: bins k = t + 16 m and M - k sit at this lane's swizzled
+        // offsets of m = 0 plus or minus m rows of 16 (16 * B * 8 bytes, a
+        // multiple of the swizzle period, so the pattern repeats).
+        auto bin = [&](int m, bool mirror) -> V {
+            if constexpr (TMA)
+                return *reinterpret_cast<const V*>(stb + (mirror ? tmaHi - m * 128 * B : tmaLo + m * 128 * B));
+            else
+                return st[mirror ? M - t - 16 * m : t + 16 * m];
+        };
         // keep <= 176 (checked at launch): bins k >= 176 (m >= 11) and
         // M - k >= 177 (m <= 4) lie beyond the 2/3 band and are zero, so those
         // shared-memory reads are left out.
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int k = t + 16 * m;
-            V xk = m < 11 ? st[k] : V{0.f, 0.f};
-            V xm = m > 4 ? st[M - k] : V{0.f, 0.f};
+            V xk = m < 11 ? bin(m, false) : V{0.f, 0.f};
+            V xm = m > 4 ? bin(m, true) : V{0.f, 0.f};
             if (m == 0 && t == 0) {  // bins 0 and M are real
                 xk.y = 0.f;
                 xm.y = 0.f;
@@ -420,24 +528,24 @@ __global__ void __launch_bounds__(16 * B, MINB) rows_flux_pair_kernel(RowFluxArg
             r[m] = {sum.x - tt.y, sum.y + tt.x};
         }
         fft256_pair<+1>(r, xch, tw2, t);
+        return true;
     };
 
+    if constexpr (TMA) __syncthreads();  // barrier init and zero rows before the first copy and reads
     issue(0, stage0);
     V u[16], v[16], w[16];
-    inverse_row(0, u);
-    inverse_row(1, v);
-    inverse_row(2, w);
+    if (!inverse_row(0, u) || !inverse_row(1, v) || !inverse_row(2, w)) return;
     const float scale = a.scale;
     const int src = ((16 - t) & 15) + (lane & 16);  // lane holding Z[M - k]
     for (int tg = 0; tg < a.targets; ++tg) {
         V acc[16], q[16];
-        inverse_row(3 + 3 * tg, q);
+        if (!inverse_row(3 + 3 * tg, q)) return;
 #pragma unroll
         for (int e = 0; e < 16; ++e) acc[e] = {u[e].x * q[e].x, u[e].y * q[e].y};
-        inverse_row(4 + 3 * tg, q);
+        if (!inverse_row(4 + 3 * tg, q)) return;
 #pragma unroll
         for (int e = 0; e < 16; ++e) acc[e] = {acc[e].x + v[e].x * q[e].x, acc[e].y + v[e].y * q[e].y};
-        inverse_row(5 + 3 * tg, q);
+        if (!inverse_row(5 + 3 * tg, q)) return;
 #pragma unroll
         for (int e = 0; e < 16; ++e)
             acc[e] = {-scale * (acc[e].x + w[e].x * q[e].x), -scale * (acc[e].y + w[e].y * q[e].y)};
@@ -473,16 +581,34 @@ __global__ void __launch_bounds__(16 * B, MINB) rows_flux_pair_kernel(RowFluxArg
     }
 }
 
-template <int B, int MINB>
+template <int B, int MINB, bool TMA>
 cudaError_t launch_pair(const RowFluxArgs& a, cudaStream_t stream) {
     const int zChunks = (a.nz + B - 1) / B;
     const dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
-    auto kernel = rows_flux_pair_kernel<B, MINB>;
-    const size_t bytes = sizeof(float2) * pair_smem_words<B>(a.keep);
+    auto kernel = rows_flux_pair_kernel<B, MINB, TMA>;
+    CUtensorMap map{};
+    size_t bytes = sizeof(float2) * pair_smem_words<B>(a.keep);
+    if constexpr (TMA) {
+        // The input bins as [cell][plane]: a cell's planes are contiguous and
+        // cells (ky * kxStride + kx) lie `planes` values apart.
+        const cudaError_t merr =
+            encode_complex_map_2d(&map, a.binsIn.data, static_cast<unsigned long long>(a.binsIn.planes),
+                                  static_cast<unsigned long long>(a.ny) * a.binsIn.kxStride,
+                                  static_cast<unsigned long long>(a.binsIn.planes) * 8, B, a.keep);
+        if (merr != cudaSuccess) return merr;
+        bytes = pair_tma_smem_bytes<B>(a.keep);
+    }
     const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (err != cudaSuccess) return err;
-    kernel<<<grid, 16 * B, bytes, stream>>>(a);
+    kernel<<<grid, 16 * B, bytes, stream>>>(a, map);
     return cudaGetLastError();
+}
+
+template <bool TMA>
+cudaError_t launch_pair_form(const RowFluxArgs& a, cudaStream_t stream) {
+    if (a.planes == 8) return a.pairs == 2 ? launch_pair<8, 3, TMA>(a, stream) : launch_pair<8, 2, TMA>(a, stream);
+    if (a.planes == 16) return launch_pair<16, 1, TMA>(a, stream);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace
@@ -514,9 +640,11 @@ cudaError_t launch_planes(const RowFluxArgs& a, cudaStream_t stream) {
 cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
     const int M = a.nx / 2;
     if (a.keep < 1 || a.keep > M + 1 || a.fieldsIn != 3 + 3 * a.targets || a.zStride < a.nz) return cudaErrorInvalidValue;
-    if (a.pairs != 0 && M == kPairM && a.keep <= 176) {
-        if (a.planes == 8) return a.pairs == 2 ? launch_pair<8, 3>(a, stream) : launch_pair<8, 2>(a, stream);
-        if (a.planes == 16) return launch_pair<16, 1>(a, stream);
+    if (a.pairs != 0 && M == kPairM && a.keep <= 176 && (a.planes == 8 || a.planes == 16)) {
+        // The TMA form needs the error word (its copy waits are bounded) and
+        // 16-byte aligned cells.
+        const bool tma = a.tma != 0 && a.error != nullptr && a.binsIn.planes % 2 == 0 && a.zStride % 2 == 0;
+        return tma ? launch_pair_form<true>(a, stream) : launch_pair_form<false>(a, stream);
     }
     switch (M) {
         case 32: return launch_planes<32>(a, stream);

@@ -21,6 +21,11 @@ struct RowFluxArgs {
     // with a radix-16 x radix-16 FFT; needs planes 8 or 16 (autotuner choice).
     // 2: the 8-plane form compiled for three resident CTAs per SM.
     int pairs = 0;
+    // Two-planes-per-warp forms only: 1 fills each slot's stage with one TMA
+    // tensor copy instead of per-thread cp.async (an autotuner choice; needs
+    // `error`).
+    int tma = 0;
+    int* error = nullptr;  // device word set to 1 when a bounded wait expires
 };
 
 bool rows_flux_supported(long long nx);

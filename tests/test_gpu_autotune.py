@@ -100,11 +100,13 @@ def test_band_forms_at_512(form):
     skb_cuda.tune_cache_clear()
 
 
-@pytest.mark.parametrize("n,planes,pairs", [(64, 4, 0), (64, 16, 0), (512, 4, 0), (512, 16, 0), (512, 8, 1),
-                                            (512, 16, 1), (512, 8, 2)])
-def test_every_row_kernel_width_is_correct(n, planes, pairs):
+@pytest.mark.parametrize("n,planes,pairs,tma", [(64, 4, 0, 0), (64, 16, 0, 0), (512, 4, 0, 0), (512, 16, 0, 0),
+                                                (512, 8, 1, 0), (512, 16, 1, 0), (512, 8, 2, 0), (512, 8, 1, 1),
+                                                (512, 16, 1, 1), (512, 8, 2, 1)])
+def test_every_row_kernel_width_is_correct(n, planes, pairs, tma):
     """The fused row kernel with 4, 8 or 16 z-planes per CTA, and at 512 points
-    the two-planes-per-warp form with 8 or 16 (the tuner's candidates)."""
+    the two-planes-per-warp form with 8 or 16, its stages filled by cp.async
+    or by TMA tensor copies (the tuner's candidates)."""
     skb_cuda.tune_cache_clear()
     nz, members = 17, 2
     probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
@@ -119,6 +121,8 @@ def test_every_row_kernel_width_is_correct(n, planes, pairs):
     assert len(pair_keys) == (1 if n == 512 else 0)
     for key in pair_keys:
         skb_cuda.tune_cache_store(key, pairs, 0.0)
+        skb_cuda.tune_cache_store(key.replace("flux.rows.pairs", "flux.rows.tma", 1), tma, 0.0)
     flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
     assert orc.rel_l2_error(_run(flux, x), _fp64(n, nz, members, x)) <= 1e-6
+    flux.check_device()
     skb_cuda.tune_cache_clear()

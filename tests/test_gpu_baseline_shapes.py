@@ -172,17 +172,23 @@ def test_serving_mix_classes_alone_equals_mixed_and_matches_oracle(reference_cas
         f.close()
 
 
-@pytest.mark.parametrize("forced", [{"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 8},
-                                    {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 16},
-                                    {"flux.rows.pairs": 2, "flux.rows.planes_per_cta": 8},
+@pytest.mark.parametrize("forced", [{"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 8, "flux.rows.tma": 0},
+                                    {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 16, "flux.rows.tma": 0},
+                                    {"flux.rows.pairs": 2, "flux.rows.planes_per_cta": 8, "flux.rows.tma": 0},
+                                    {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 8, "flux.rows.tma": 1},
+                                    {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 16, "flux.rows.tma": 1},
+                                    {"flux.rows.pairs": 2, "flux.rows.planes_per_cta": 8, "flux.rows.tma": 1},
                                     {"flux.columns_band.form": 4}, {"flux.columns_band.form": 5}],
-                         ids=["pair-rows-8", "pair-rows-16", "pair-rows-8-3cta", "band16-columns",
-                              "band32-columns"])
+                         ids=["pair-rows-8", "pair-rows-16", "pair-rows-8-3cta", "pair-rows-8-tma",
+                              "pair-rows-16-tma", "pair-rows-8-3cta-tma", "band16-columns", "band32-columns"])
 def test_flux_split_forced_kernel_forms_match_oracle(reference_case, forced):
     # Kernel forms the tuner may pick, forced through the tuning cache, at the
     # benchmark shape against the oracle: the 512-point row kernel's
-    # two-planes-per-warp form (16 x 16 FFT) at both CTA widths, and the
-    # 16-plane band column kernels (whose plane chunks cross slot padding).
+    # two-planes-per-warp form (16 x 16 FFT) at both CTA widths, with
+    # cp.async or TMA stage fills (the 16-plane TMA box of the last plane
+    # chunk reaches past the slot's padding and, for the last slot, past the
+    # array: those planes are zero-filled and never stored), and the 16- and
+    # 32-plane band column kernels (whose plane chunks cross slot padding).
     x, ref = reference_case
     skb_cuda.tune_cache_clear()
     probe = skb_cuda.Flux(N, NZ, mode=skb_cuda.FLUX_SPLIT_TF32X3)
@@ -190,7 +196,11 @@ def test_flux_split_forced_kernel_forms_match_oracle(reference_case, forced):
     d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
     chosen = probe.autotune(d_in.ptr, d_out.ptr)
     probe.close()
-    for key in chosen:
+    keys = list(chosen)
+    # The TMA choice is only tuned when the tuner picked a paired form; its
+    # key shares the pairs key's shape and device suffix.
+    keys += [k.replace("flux.rows.pairs", "flux.rows.tma", 1) for k in chosen if k.startswith("flux.rows.pairs ")]
+    for key in set(keys):
         for prefix, value in forced.items():
             if key.startswith(prefix + " "):
                 skb_cuda.tune_cache_store(key, value, 0.0)
