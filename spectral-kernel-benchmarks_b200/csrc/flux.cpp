@@ -248,7 +248,7 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
         pick("flux.rows.tma" + shape + dev, {0, 1}, [&](int c) { rowsTma_ = c; },
              [&] { check_cuda(launch_rows_flux(row_args(M), s), "fused row flux kernel"); });
     }
-    pick("flux.rows.planes_per_cta" + shape + dev, rowsPairs_ != 0 ? std::vector<int>{8, 16} : std::vector<int>{4, 8, 16},
+    pick("flux.rows.planes_per_cta" + shape + dev, rowsPairs_ != 0 ? std::vector<int>{8, 16, 24} : std::vector<int>{4, 8, 16},
          [&](int c) { rowsPlanes_ = c; },
          [&] { check_cuda(launch_rows_flux(row_args(M), s), "fused row flux kernel"); });
     if (cfg_.n == 512) {

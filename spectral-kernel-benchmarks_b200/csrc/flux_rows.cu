@@ -48,9 +48,18 @@ constexpr int stage_row() {
 // Output tile [k][b], row stride B, plane b of row k at b ^ swz(k): a warp's
 // 16 consecutive kx of one plane and a copy-out instruction's B planes x 32/B
 // consecutive kx both touch every bank pair equally often.
+// B = 24 (no XOR swizzle stays inside a 24-plane row): rows of 25 slots,
+// whose odd stride spreads 16 consecutive kx of one plane over all bank pairs.
+template <int B>
+constexpr int out_row() {
+    return B == 24 ? 25 : B;
+}
 template <int B>
 __device__ __forceinline__ int out_slot(int k, int b) {
-    return k * B + (b ^ ((k / (16 / B)) & (B - 1)));
+    if constexpr (B == 24)
+        return k * out_row<B>() + b;
+    else
+        return k * B + (b ^ ((k / (16 / B)) & (B - 1)));
 }
 // Entries of the lane-ordered FFT twiddle table (512-point rows only).
 template <int M>
@@ -333,12 +342,13 @@ constexpr int pair_stage_row() {
     // kx = 0..M (the pre-processing reads X[M - k]), and a residue mod 16 (in
     // 8-byte words) that spreads one cp.async instruction's B planes x 32/B
     // kx over the 16 bank pairs exactly twice.
-    constexpr int want = B == 16 ? 1 : 2;
+    // (B = 24: an odd stride, at most three accesses per bank pair.)
+    constexpr int want = B == 16 || B == 24 ? 1 : 2;
     return kPairM + 1 + ((want - (kPairM + 1) % 16) + 16) % 16;
 }
 template <int B>
 constexpr size_t pair_smem_words(int keep) {
-    return 2 * size_t(B) * pair_stage_row<B>() + size_t(B) * kPairXch + size_t(keep) * B + kPairM + kPairM;
+    return 2 * size_t(B) * pair_stage_row<B>() + size_t(B) * kPairXch + size_t(keep) * out_row<B>() + kPairM + kPairM;
 }
 
 // TMA form of the stage: rows kx = 0..kTmaRows-1 (the pre-processing reads no
@@ -354,7 +364,7 @@ constexpr size_t tma_stage_bytes() {
 template <int B>
 constexpr size_t pair_tma_smem_bytes(int keep) {
     return 1024 + 2 * tma_stage_bytes<B>() +
-           sizeof(float2) * (size_t(B) * kPairXch + size_t(keep) * B + kPairM + kPairM);
+           sizeof(float2) * (size_t(B) * kPairXch + size_t(keep) * out_row<B>() + kPairM + kPairM);
 }
 // Byte offset of (kx k, plane b) in a swizzled TMA stage.
 template <int B>
@@ -406,7 +416,7 @@ __global__ void __launch_bounds__(16 * B, MINB)
     V* stage1 = TMA ? reinterpret_cast<V*>(tmaBase + tma_stage_bytes<B>()) : stage0 + B * KP;
     V* xchAll = TMA ? reinterpret_cast<V*>(tmaBase + 2 * tma_stage_bytes<B>()) : stage1 + B * KP;
     V* outTile = xchAll + B * kPairXch;  // [k][b] at out_slot(k, b)
-    V* tf = outTile + keep * B;          // twFull[0..M)
+    V* tf = outTile + keep * out_row<B>();  // twFull[0..M)
     V* tw2 = tf + M;                     // tw2[16 k2 + t] = twHalf[(t k2) mod M]
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -608,6 +618,9 @@ template <bool TMA>
 cudaError_t launch_pair_form(const RowFluxArgs& a, cudaStream_t stream) {
     if (a.planes == 8) return a.pairs == 2 ? launch_pair<8, 3, TMA>(a, stream) : launch_pair<8, 2, TMA>(a, stream);
     if (a.planes == 16) return launch_pair<16, 1, TMA>(a, stream);
+    // 24 planes (12 warps, one CTA per SM, 192-byte pieces): cp.async only,
+    // no TMA swizzle pattern fits a 192-byte row.
+    if (a.planes == 24) return launch_pair<24, 1, false>(a, stream);
     return cudaErrorInvalidValue;
 }
 
@@ -640,7 +653,7 @@ cudaError_t launch_planes(const RowFluxArgs& a, cudaStream_t stream) {
 cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
     const int M = a.nx / 2;
     if (a.keep < 1 || a.keep > M + 1 || a.fieldsIn != 3 + 3 * a.targets || a.zStride < a.nz) return cudaErrorInvalidValue;
-    if (a.pairs != 0 && M == kPairM && a.keep <= 176 && (a.planes == 8 || a.planes == 16)) {
+    if (a.pairs != 0 && M == kPairM && a.keep <= 176 && (a.planes == 8 || a.planes == 16 || a.planes == 24)) {
         // The TMA form needs the error word (its copy waits are bounded) and
         // 16-byte aligned cells.
         const bool tma = a.tma != 0 && a.error != nullptr && a.binsIn.planes % 2 == 0 && a.zStride % 2 == 0;

@@ -16,7 +16,7 @@ struct RowFluxArgs {
     DenseBins binsOut;    // target bins, plane (member*targets + t)*zStride + z
     const void* twHalf;   // exp(-2 pi i k/(nx/2)), float2
     const void* twFull;   // exp(-2 pi i k/nx), float2
-    int planes = 8;       // z-planes per CTA: 4, 8 or 16 (an autotuner choice)
+    int planes = 8;       // z-planes per CTA: 4, 8 or 16, and 24 for the two-planes-per-warp form (an autotuner choice)
     // Nx = 512 only: two planes per warp (16 lanes each, 16 x-pairs per lane)
     // with a radix-16 x radix-16 FFT; needs planes 8 or 16 (autotuner choice).
     // 2: the 8-plane form compiled for three resident CTAs per SM.
