@@ -790,6 +790,108 @@ __global__ void __launch_bounds__(32 * B, 32 / B) columns_band_wide_kernel(int n
     }
 }
 
+// Pipelined 16-plane forms (kBand16Pipe*): one CTA per SM walks `perCta` kx
+// columns of its 16 planes (every gridDim.y-th column), with the pass-1 loads
+// of the next column issued into registers right after the current column's
+// pass 1, so they are in flight during its middle pass and pass 3.  Two
+// shared-memory regions alternate between columns; the passes are those of
+// columns_band_wide_kernel.
+constexpr size_t band_pipe_smem() {
+    return sizeof(float2) * (2 * size_t(16) * band_wide_region<16>() + kDirectTable);
+}
+template <int SIGN>
+__global__ void __launch_bounds__(512, 1) columns_band_pipe_kernel(int nz, int zStride, long long flatPlanes,
+                                                                   int columns, DenseBins bins,
+                                                                   const int* __restrict__ bandOf, float scale,
+                                                                   const float2* __restrict__ tw) {
+    constexpr int B = 16;
+    constexpr int N = kDirectN, XP = band_wide_region<B>();
+    constexpr int NT = 32 * B;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* xsAll = reinterpret_cast<float2*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float2* tt = xsAll + 2 * B * XP;
+    rr_fill_table<float, N>(tt, tw, tid, NT);
+    const long long p0 = static_cast<long long>(blockIdx.x) * B;
+    const int b = tid % B;
+    const long long p = p0 + b;
+    const bool inRange = p < flatPlanes && static_cast<int>(p % zStride) < nz;
+    const long long pw = p0 + warp;
+    const bool warpActive = pw < flatPlanes && static_cast<int>(pw % zStride) < nz;
+    const long long rowStride = bins.planes * bins.kxStride;
+    float2* base = static_cast<float2*>(bins.data) + p;
+    // Pass-1 inputs of column kx into v (the loads are only issued here).
+    auto load = [&](int kx, float2 (&v)[2][8]) {
+        const int band = __ldg(bandOf + kx);
+        const float2* col = base + bins.planes * kx;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = band_wide_butterfly<B>(tid, q);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int ky = j + 64 * r;
+                const bool ld = inRange && (SIGN < 0 || in_band(ky, N, band));
+                v[q][r] = ld ? col[rowStride * ky] : make_float2(0.f, 0.f);
+            }
+        }
+    };
+    float2 v[2][8];
+    int kx = blockIdx.y;
+    if (kx < columns) load(kx, v);
+    for (int i = 0; kx < columns; ++i, kx += gridDim.y) {
+        float2* xs = xsAll + (i & 1) * B * XP;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = band_wide_butterfly<B>(tid, q);
+            dft8<SIGN>(v[q]);
+            float2* o = xs + b * XP + 8 * j + (j >> 1);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) o[r] = v[q][r];
+        }
+        const int next = kx + static_cast<int>(gridDim.y);
+        if (next < columns) load(next, v);
+        __syncthreads();
+        if (warpActive) wide_middle_pass<SIGN, XP>(xs, tt, warp, lane);
+        __syncthreads();
+        if (inRange) {
+            const int band = __ldg(bandOf + kx);
+            float2* col = base + bins.planes * kx;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int j = (tid / B) + 32 * q;
+                const float2* in = xs + b * XP + j;
+                float2 w[8];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) w[r] = in[72 * r];
+#pragma unroll
+                for (int r = 1; r < 8; ++r) w[r] = cmul(w[r], twiddle_plain<SIGN>(tt + 56 + j, 64 * (r - 1)));
+                dft8<SIGN>(w);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const int ky = j + 64 * r;
+                    if (SIGN > 0)
+                        col[rowStride * ky] = w[r];
+                    else if (in_band(ky, N, band))
+                        col[rowStride * ky] = make_float2(scale * w[r].x, scale * w[r].y);
+                }
+            }
+        }
+    }
+}
+
+template <int SIGN>
+cudaError_t launch_band_pipe(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band,
+                             float scale, const void* tw, int perCta, cudaStream_t s) {
+    auto kernel = columns_band_pipe_kernel<SIGN>;
+    cudaError_t err = prepare(kernel, band_pipe_smem());
+    if (err != cudaSuccess) return err;
+    const long long flat = static_cast<long long>(slots) * zStride;
+    const dim3 grid(unsigned((flat + 15) / 16), unsigned((columns + perCta - 1) / perCta));
+    kernel<<<grid, 512, band_pipe_smem(), s>>>(nz, zStride, flat, columns, bins, band, scale,
+                                               static_cast<const float2*>(tw));
+    return cudaGetLastError();
+}
+
 template <int B, int SIGN>
 cudaError_t launch_band_wide(int nz, int zStride, int slots, int columns, DenseBins bins, const int* band, float scale,
                              const void* tw, cudaStream_t s) {
@@ -841,6 +943,8 @@ cudaError_t inverse_band_n(int nz, int zStride, int slots, int columns, DenseBin
         return launch_band_wide<16, +1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
     if (N == kDirectN && form == kBand32)
         return launch_band_wide<32, +1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, s);
+    if (N == kDirectN && band_pipe_columns(form) > 0)
+        return launch_band_pipe<+1>(nz, zStride, slots, columns, bins, band, 1.0f, tw, band_pipe_columns(form), s);
     if (N == kDirectN && form != kBandWarp) {
         auto kernel = form == kBandDirect4 ? columns_inverse_band_kernel<4> : columns_inverse_band_kernel<3>;
         cudaError_t err = prepare(kernel, kDirectSmem);
@@ -868,6 +972,8 @@ cudaError_t forward_band_n(int nz, int zStride, int slots, int columns, DenseBin
         return launch_band_wide<16, -1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
     if (N == kDirectN && form == kBand32)
         return launch_band_wide<32, -1>(nz, zStride, slots, columns, bins, band, float(scale), tw, s);
+    if (N == kDirectN && band_pipe_columns(form) > 0)
+        return launch_band_pipe<-1>(nz, zStride, slots, columns, bins, band, float(scale), tw, band_pipe_columns(form), s);
     if (N == kDirectN && form != kBandWarp) {
         auto kernel = form == kBandDirect4 ? columns_forward_band_kernel<4> : columns_forward_band_kernel<3>;
         cudaError_t err = prepare(kernel, kDirectSmem);

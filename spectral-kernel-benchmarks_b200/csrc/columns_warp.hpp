@@ -38,6 +38,15 @@ constexpr int kBandDirect4 = 3;
 constexpr int kBand16 = 4;
 // kBand32: the same with 32 planes per CTA (256-byte accesses, one CTA per SM).
 constexpr int kBand32 = 5;
+// kBand16Pipe16/32/64: the 16-plane form with one CTA per SM walking 16, 32
+// or 64 kx columns, the next column's loads in flight during the current
+// one's passes.
+constexpr int kBand16Pipe16 = 6;
+constexpr int kBand16Pipe32 = 7;
+constexpr int kBand16Pipe64 = 8;
+constexpr int band_pipe_columns(int form) {
+    return form == kBand16Pipe16 ? 16 : form == kBand16Pipe32 ? 32 : form == kBand16Pipe64 ? 64 : 0;
+}
 cudaError_t launch_columns_inverse_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,
                                         const int* band, const void* tw, int form, cudaStream_t s);
 cudaError_t launch_columns_forward_band(int ny, int nz, int zStride, int slots, int columns, DenseBins bins,

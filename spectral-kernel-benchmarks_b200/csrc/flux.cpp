@@ -254,7 +254,8 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
     if (cfg_.n == 512) {
         // Both forms run in place on the bin arrays; repeated runs leave values
         // the final execution below overwrites.
-        const std::vector<int> forms{kBandDefault, kBandWarp, kBandPersist, kBandDirect4, kBand16, kBand32};
+        const std::vector<int> forms{kBandDefault,  kBandWarp,     kBandPersist,  kBandDirect4, kBand16,
+                                     kBand32,       kBand16Pipe16, kBand16Pipe32, kBand16Pipe64};
         pick("flux.columns_band.form inverse" + shape + dev, forms,
              [&](int c) { horizontal_->set_band_forms(c, horizontal_->band_form_forward()); },
              [&] { horizontal_->inverse_columns_band(binsIn, static_cast<int>(M * fieldsIn_), static_cast<int>(zStride_), s); });

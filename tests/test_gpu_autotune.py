@@ -79,11 +79,12 @@ def test_every_unit_size_is_correct(tiles, mode):
     skb_cuda.tune_cache_clear()
 
 
-@pytest.mark.parametrize("form", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("form", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 def test_band_forms_at_512(form):
     """Every 512-point band-column kernel form (direct, warp-per-plane,
     persistent direct, direct at four CTAs per SM, direct with 16 or 32 planes
-    per CTA) the tuner chooses between gives the split flux within 1e-6 of FP64."""
+    per CTA, and the 16-plane form walking 16, 32 or 64 columns per CTA) the
+    tuner chooses between gives the split flux within 1e-6 of FP64."""
     skb_cuda.tune_cache_clear()
     n, nz, members = 512, 9, 1
     probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)

@@ -179,10 +179,11 @@ def test_serving_mix_classes_alone_equals_mixed_and_matches_oracle(reference_cas
                                     {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 16, "flux.rows.tma": 1},
                                     {"flux.rows.pairs": 2, "flux.rows.planes_per_cta": 8, "flux.rows.tma": 1},
                                     {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 24, "flux.rows.tma": 0},
-                                    {"flux.columns_band.form": 4}, {"flux.columns_band.form": 5}],
+                                    {"flux.columns_band.form": 4}, {"flux.columns_band.form": 5},
+                                    {"flux.columns_band.form": 7}],
                          ids=["pair-rows-8", "pair-rows-16", "pair-rows-8-3cta", "pair-rows-8-tma",
                               "pair-rows-16-tma", "pair-rows-8-3cta-tma", "pair-rows-24", "band16-columns",
-                              "band32-columns"])
+                              "band32-columns", "band16-pipelined-columns"])
 def test_flux_split_forced_kernel_forms_match_oracle(reference_case, forced):
     # Kernel forms the tuner may pick, forced through the tuning cache, at the
     # benchmark shape against the oracle: the 512-point row kernel's
