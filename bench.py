@@ -138,10 +138,16 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a while to print its first sample: wait for it
+            # (at most 3 s), then keep only the samples of the timed region.
+            t0 = time.time()
+            while not self.lines and self.proc.poll() is None and time.time() - t0 < 3.0:
+                time.sleep(0.005)
+            self.lines.clear()
         except (OSError, ValueError):
             self.proc = None
         return self
