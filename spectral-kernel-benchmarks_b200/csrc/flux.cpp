@@ -244,8 +244,8 @@ std::vector<TuneEntry> FluxPipeline::apply_tuned(const void* modalIn, void* moda
     }
     if (cfg_.n == 512 && rowsPairs_ != 0) {
         // Two-planes-per-warp forms: stage fills by per-thread cp.async (0) or
-        // by one TMA tensor copy per slot (1).
-        pick("flux.rows.tma" + shape + dev, {0, 1}, [&](int c) { rowsTma_ = c; },
+        // by one TMA tensor copy per slot, one (1) or two (2) slots ahead.
+        pick("flux.rows.tma" + shape + dev, {0, 1, 2}, [&](int c) { rowsTma_ = c; },
              [&] { check_cuda(launch_rows_flux(row_args(M), s), "fused row flux kernel"); });
     }
     pick("flux.rows.planes_per_cta" + shape + dev, rowsPairs_ != 0 ? std::vector<int>{8, 16, 24} : std::vector<int>{4, 8, 16},

@@ -361,9 +361,9 @@ template <int B>
 constexpr size_t tma_stage_bytes() {
     return (size_t(kTmaRows) * B * 8 + 1023) / 1024 * 1024;
 }
-template <int B>
+template <int B, int NS>
 constexpr size_t pair_tma_smem_bytes(int keep) {
-    return 1024 + 2 * tma_stage_bytes<B>() +
+    return 1024 + NS * tma_stage_bytes<B>() +
            sizeof(float2) * (size_t(B) * kPairXch + size_t(keep) * out_row<B>() + kPairM + kPairM);
 }
 // Byte offset of (kx k, plane b) in a swizzled TMA stage.
@@ -395,26 +395,34 @@ __device__ __forceinline__ bool stage_wait(unsigned bar, unsigned parity) {
 // MINB: resident CTAs per SM the register allocation must allow (2 for B = 8,
 // 1 for B = 16: about 240 registers; 3 for the B = 8 form that trades spills
 // to L1-cached local memory for occupancy).
-// TMA: each slot's stage is filled by one tensor copy (thread 0, onto an
-// mbarrier; `tmIn` maps the input bins as [cell][plane]) instead of 8-byte
-// cp.async by every thread.  Thread 0's bounded wait on the copy is folded
-// into the slot's CTA barrier (__syncthreads_and), so an expired wait makes
-// every thread leave together after setting the error word.
-template <int B, int MINB, bool TMA>
+// TMA (NS = 2 or 3 stages; 0: cp.async): each slot's stage is filled by one
+// tensor copy (thread 0, onto an mbarrier; `tmIn` maps the input bins as
+// [cell][plane]) instead of 8-byte cp.async by every thread, NS - 1 slots
+// ahead of the one being transformed.  Thread 0's bounded wait on the copy is
+// folded into the slot's CTA barrier (__syncthreads_and), so an expired wait
+// makes every thread leave together after setting the error word.
+template <int B, int MINB, int NS>
 __global__ void __launch_bounds__(16 * B, MINB)
     rows_flux_pair_kernel(RowFluxArgs a, const __grid_constant__ CUtensorMap tmIn) {
     using V = float2;
+    constexpr bool TMA = NS != 0;
+    constexpr int NST = TMA ? NS : 2;  // stages
     constexpr int M = kPairM;
     constexpr int NT = 16 * B;
     constexpr int KP = pair_stage_row<B>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(8) unsigned long long stageFull[2];
+    __shared__ __align__(8) unsigned long long stageFull[NST];
     const int keep = a.keep;
     unsigned char* tmaBase =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    V* stage0 = TMA ? reinterpret_cast<V*>(tmaBase) : reinterpret_cast<V*>(smem_raw);
-    V* stage1 = TMA ? reinterpret_cast<V*>(tmaBase + tma_stage_bytes<B>()) : stage0 + B * KP;
-    V* xchAll = TMA ? reinterpret_cast<V*>(tmaBase + 2 * tma_stage_bytes<B>()) : stage1 + B * KP;
+    auto stage_of = [&](int f) -> V* {
+        if constexpr (TMA)
+            return reinterpret_cast<V*>(tmaBase + (f % NST) * tma_stage_bytes<B>());
+        else
+            return reinterpret_cast<V*>(smem_raw) + (f & 1) * B * KP;
+    };
+    V* stage0 = stage_of(0);
+    V* xchAll = TMA ? reinterpret_cast<V*>(tmaBase + NST * tma_stage_bytes<B>()) : stage0 + 2 * B * KP;
     V* outTile = xchAll + B * kPairXch;  // [k][b] at out_slot(k, b)
     V* tf = outTile + keep * out_row<B>();  // twFull[0..M)
     V* tw2 = tf + M;                     // tw2[16 k2 + t] = twHalf[(t k2) mod M]
@@ -439,16 +447,16 @@ __global__ void __launch_bounds__(16 * B, MINB)
         tw2[i] = twHalf[((i & 15) * (i >> 4)) & (M - 1)];
     }
     if constexpr (TMA) {
-        // Rows keep..kTmaRows-1 of both stages are zero (the tensor copies
+        // Rows keep..kTmaRows-1 of every stage are zero (the tensor copies
         // write rows 0..keep-1 only; the swizzle stays inside a row).
-        for (int i = tid; i < 2 * (kTmaRows - keep) * B; i += NT) {
+        for (int i = tid; i < NST * (kTmaRows - keep) * B; i += NT) {
             const int st = i / ((kTmaRows - keep) * B);
             const int j = i % ((kTmaRows - keep) * B);
             reinterpret_cast<V*>(tmaBase + st * tma_stage_bytes<B>())[keep * B + j] = V{0.f, 0.f};
         }
         if (tid == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&stageFull[0])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&stageFull[1])) : "memory");
+            for (int i = 0; i < NST; ++i)
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&stageFull[i])) : "memory");
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
     } else {
@@ -469,12 +477,13 @@ __global__ void __launch_bounds__(16 * B, MINB)
     const bool cok = z0 + cb < a.nz;
     const int tmaLo = static_cast<int>(tma_stage_offset<B>(t, pl));
     const int tmaHi = static_cast<int>(tma_stage_offset<B>(M - t, pl));
-    auto issue = [&](int f, V* stage) {
+    auto issue = [&](int f) {
+        V* stage = stage_of(f);
         if constexpr (TMA) {
             if (tid == 0) {
                 const int x = (member * a.fieldsIn + f) * a.zStride + z0;
                 const int yc = static_cast<int>(a.binsIn.kxStride * y);
-                const unsigned bar = smem_addr(&stageFull[f & 1]);
+                const unsigned bar = smem_addr(&stageFull[f % NST]);
                 // The stage's earlier shared-memory reads precede the copy's writes.
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
@@ -499,7 +508,7 @@ __global__ void __launch_bounds__(16 * B, MINB)
     // false if the TMA form's wait for the slot's copy expired.
     auto inverse_row = [&](int f, V (&r)[16]) -> bool {
         if constexpr (TMA) {
-            const bool ok = tid != 0 || stage_wait(smem_addr(&stageFull[f & 1]), (f >> 1) & 1);
+            const bool ok = tid != 0 || stage_wait(smem_addr(&stageFull[f % NST]), (f / NST) & 1);
             if (!__syncthreads_and(ok)) {
                 if (tid == 0 && a.error != nullptr) atomicExch(a.error, 1);
                 return false;
@@ -508,9 +517,11 @@ __global__ void __launch_bounds__(16 * B, MINB)
             cp_async_wait_all();
             __syncthreads();
         }
-        if (f + 1 < a.fieldsIn) issue(f + 1, ((f + 1) & 1) ? stage1 : stage0);
-        const V* st = ((f & 1) ? stage1 : stage0) + pl * KP;
-        const unsigned char* stb = reinterpret_cast<const unsigned char*>((f & 1) ? stage1 : stage0);
+        // The stage refilled here was last read in the previous slot, before
+        // this barrier.
+        if (f + NST - 1 < a.fieldsIn) issue(f + NST - 1);
+        const V* st = stage_of(f) + pl * KP;
+        const unsigned char* stb = reinterpret_cast<const unsigned char*>(stage_of(f));
         // TMA form: bins k = t + 16 m and M - k sit at this lane's swizzled
         // offsets of m = 0 plus or minus m rows of 16 (16 * B * 8 bytes, a
         // multiple of the swizzle period, so the pattern repeats).
@@ -542,7 +553,7 @@ __global__ void __launch_bounds__(16 * B, MINB)
     };
 
     if constexpr (TMA) __syncthreads();  // barrier init and zero rows before the first copy and reads
-    issue(0, stage0);
+    for (int f = 0; f < NST - 1 && f < a.fieldsIn; ++f) issue(f);
     V u[16], v[16], w[16];
     if (!inverse_row(0, u) || !inverse_row(1, v) || !inverse_row(2, w)) return;
     const float scale = a.scale;
@@ -591,11 +602,12 @@ __global__ void __launch_bounds__(16 * B, MINB)
     }
 }
 
-template <int B, int MINB, bool TMA>
+template <int B, int MINB, int NS>
 cudaError_t launch_pair(const RowFluxArgs& a, cudaStream_t stream) {
+    constexpr bool TMA = NS != 0;
     const int zChunks = (a.nz + B - 1) / B;
     const dim3 grid(unsigned(zChunks * a.members), unsigned(a.ny));
-    auto kernel = rows_flux_pair_kernel<B, MINB, TMA>;
+    auto kernel = rows_flux_pair_kernel<B, MINB, NS>;
     CUtensorMap map{};
     size_t bytes = sizeof(float2) * pair_smem_words<B>(a.keep);
     if constexpr (TMA) {
@@ -606,7 +618,7 @@ cudaError_t launch_pair(const RowFluxArgs& a, cudaStream_t stream) {
                                   static_cast<unsigned long long>(a.ny) * a.binsIn.kxStride,
                                   static_cast<unsigned long long>(a.binsIn.planes) * 8, B, a.keep);
         if (merr != cudaSuccess) return merr;
-        bytes = pair_tma_smem_bytes<B>(a.keep);
+        bytes = pair_tma_smem_bytes<B, NS>(a.keep);
     }
     const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (err != cudaSuccess) return err;
@@ -614,13 +626,13 @@ cudaError_t launch_pair(const RowFluxArgs& a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-template <bool TMA>
+template <int NS>
 cudaError_t launch_pair_form(const RowFluxArgs& a, cudaStream_t stream) {
-    if (a.planes == 8) return a.pairs == 2 ? launch_pair<8, 3, TMA>(a, stream) : launch_pair<8, 2, TMA>(a, stream);
-    if (a.planes == 16) return launch_pair<16, 1, TMA>(a, stream);
+    if (a.planes == 8) return a.pairs == 2 ? launch_pair<8, 3, NS>(a, stream) : launch_pair<8, 2, NS>(a, stream);
+    if (a.planes == 16) return launch_pair<16, 1, NS>(a, stream);
     // 24 planes (12 warps, one CTA per SM, 192-byte pieces): cp.async only,
     // no TMA swizzle pattern fits a 192-byte row.
-    if (a.planes == 24) return launch_pair<24, 1, false>(a, stream);
+    if (a.planes == 24) return launch_pair<24, 1, 0>(a, stream);
     return cudaErrorInvalidValue;
 }
 
@@ -657,7 +669,8 @@ cudaError_t launch_rows_flux(const RowFluxArgs& a, cudaStream_t stream) {
         // The TMA form needs the error word (its copy waits are bounded) and
         // 16-byte aligned cells.
         const bool tma = a.tma != 0 && a.error != nullptr && a.binsIn.planes % 2 == 0 && a.zStride % 2 == 0;
-        return tma ? launch_pair_form<true>(a, stream) : launch_pair_form<false>(a, stream);
+        if (!tma) return launch_pair_form<0>(a, stream);
+        return a.tma == 2 ? launch_pair_form<3>(a, stream) : launch_pair_form<2>(a, stream);
     }
     switch (M) {
         case 32: return launch_planes<32>(a, stream);

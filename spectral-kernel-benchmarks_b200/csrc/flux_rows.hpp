@@ -22,7 +22,8 @@ struct RowFluxArgs {
     // 2: the 8-plane form compiled for three resident CTAs per SM.
     int pairs = 0;
     // Two-planes-per-warp forms only: 1 fills each slot's stage with one TMA
-    // tensor copy instead of per-thread cp.async (an autotuner choice; needs
+    // tensor copy instead of per-thread cp.async, one slot ahead; 2 does so
+    // two slots ahead through three stages (an autotuner choice; needs
     // `error`).
     int tma = 0;
     int* error = nullptr;  // device word set to 1 when a bounded wait expires

@@ -103,11 +103,13 @@ def test_band_forms_at_512(form):
 
 @pytest.mark.parametrize("n,planes,pairs,tma", [(64, 4, 0, 0), (64, 16, 0, 0), (512, 4, 0, 0), (512, 16, 0, 0),
                                                 (512, 8, 1, 0), (512, 16, 1, 0), (512, 8, 2, 0), (512, 8, 1, 1),
-                                                (512, 16, 1, 1), (512, 8, 2, 1), (512, 24, 1, 0)])
+                                                (512, 16, 1, 1), (512, 8, 2, 1), (512, 24, 1, 0),
+                                                (512, 8, 2, 2), (512, 16, 1, 2)])
 def test_every_row_kernel_width_is_correct(n, planes, pairs, tma):
     """The fused row kernel with 4, 8 or 16 z-planes per CTA, and at 512 points
     the two-planes-per-warp form with 8, 16 or 24, its stages filled by
-    cp.async or by TMA tensor copies (the tuner's candidates)."""
+    cp.async or by TMA tensor copies one or two slots ahead (the tuner's
+    candidates)."""
     skb_cuda.tune_cache_clear()
     nz, members = 17, 2
     probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)

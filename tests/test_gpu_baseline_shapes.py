@@ -179,17 +179,18 @@ def test_serving_mix_classes_alone_equals_mixed_and_matches_oracle(reference_cas
                                     {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 16, "flux.rows.tma": 1},
                                     {"flux.rows.pairs": 2, "flux.rows.planes_per_cta": 8, "flux.rows.tma": 1},
                                     {"flux.rows.pairs": 1, "flux.rows.planes_per_cta": 24, "flux.rows.tma": 0},
+                                    {"flux.rows.pairs": 2, "flux.rows.planes_per_cta": 8, "flux.rows.tma": 2},
                                     {"flux.columns_band.form": 4}, {"flux.columns_band.form": 5},
                                     {"flux.columns_band.form": 7}],
                          ids=["pair-rows-8", "pair-rows-16", "pair-rows-8-3cta", "pair-rows-8-tma",
-                              "pair-rows-16-tma", "pair-rows-8-3cta-tma", "pair-rows-24", "band16-columns",
+                              "pair-rows-16-tma", "pair-rows-8-3cta-tma", "pair-rows-24", "pair-rows-8-3cta-tma3", "band16-columns",
                               "band32-columns", "band16-pipelined-columns"])
 def test_flux_split_forced_kernel_forms_match_oracle(reference_case, forced):
     # Kernel forms the tuner may pick, forced through the tuning cache, at the
     # benchmark shape against the oracle: the 512-point row kernel's
     # two-planes-per-warp form (16 x 16 FFT) at 8, 16 and 24 planes per CTA
     # (the last 24-plane chunk runs past Nz = 129 and the slot padding), with
-    # cp.async or TMA stage fills (the 16-plane TMA box of the last plane
+    # cp.async or TMA stage fills, one or two slots ahead (the 16-plane TMA box of the last plane
     # chunk reaches past the slot's padding and, for the last slot, past the
     # array: those planes are zero-filled and never stored), and the 16- and
     # 32-plane band column kernels (whose plane chunks cross slot padding).
