@@ -419,6 +419,24 @@ def cuda_arm(args, dist):
     per_launch_ms = dominant["ms"] / max(1, dominant["launches"])
     per_launch_bytes = dominant["bytes"] / max(1, dominant["launches"])
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    # The compute side of the same kernel: measured SIMT FMA peaks, and for the
+    # fused row kernel its nominal flops per launch, 19 real transforms of
+    # 2.5 N log2 N and 4 targets x 6 flops per point, per (row, plane, member).
+    simt = None
+    try:
+        f32, f64 = S.simt_peaks()
+        simt = {"fp32_tflops": f32, "fp64_tflops": f64,
+                "how": "independent FMA chains at full occupancy, best of 3 (skb_measure_simt_peaks)"}
+    except (RuntimeError, ValueError, MemoryError):
+        pass
+    compute = None
+    if simt and dominant["name"] == "rows_flux_fused":
+        per_row = (19 * 2.5 * args.n * np.log2(args.n) + 4 * 6 * args.n)
+        flops = per_row * args.n * args.nz * args.members
+        tf = flops / (per_launch_ms * 1e-3) / 1e12
+        peak_c = simt["fp64_tflops"] if mode == S.FLUX_FP64_PLAIN else simt["fp32_tflops"]
+        compute = {"flops_per_launch": flops, "achieved_tflops": tf, "peak_tflops": peak_c,
+                   "frac": tf / peak_c if peak_c else None, "peak_kind": "measured (SIMT FMA)"}
     total_ms = sum(s["ms"] for s in stages)
     line = {
         "metric": METRIC,
@@ -450,7 +468,9 @@ def cuda_arm(args, dist):
         "roofline": {"bound": "hbm", "kernel": dominant["name"], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": ncu_traffic(dominant["name"]),
-                     "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": per_launch_ms},
+                     "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": per_launch_ms,
+                     "compute": compute},
+        "simt_peaks": simt,
         "stages": [{"name": s["name"], "ms": round(s["ms"], 4), "share": round(s["ms"] / total_ms, 4),
                     "launches": s["launches"], "GBps": (s["bytes"] / (s["ms"] * 1e-3) / 1e9) if s["ms"] else None}
                    for s in stages],

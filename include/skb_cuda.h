@@ -139,6 +139,12 @@ SKB_API int skb_device_count(int* count);
 SKB_API int skb_set_device(int device);
 /* Synchronise the current device (host-side barrier for timing). */
 SKB_API int skb_device_synchronize(void);
+/* Measured FP32 and FP64 SIMT FMA throughput of the current device in
+ * TFLOP/s (2 flops per FMA; independent FMA chains at full occupancy, best
+ * of three runs of a few ms each).  No counterpart in the reference: it gives
+ * the FFT, pointwise and FP64-plain kernels' rooflines a measured compute
+ * peak.  Allocates a small device buffer for the kernels' results. */
+SKB_API int skb_measure_simt_peaks(double* fp32_tflops, double* fp64_tflops);
 
 /* ------------------------------------------------- model (host, no GPU)  */
 /* retainedHorizontalModes, src/model.cpp:129-167. */

@@ -13,6 +13,7 @@
 #include "autotune.hpp"
 #include "flux.hpp"
 #include "noalloc.hpp"
+#include "peaks.hpp"
 #include "pipeline.hpp"
 #include "server.hpp"
 #include "pointwise.hpp"
@@ -295,6 +296,13 @@ int skb_set_device(int device) {
 
 int skb_device_synchronize(void) {
     return guard([&] { check_cuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize"); });
+}
+
+int skb_measure_simt_peaks(double* fp32_tflops, double* fp64_tflops) {
+    return guard([&] {
+        require(fp32_tflops != nullptr && fp64_tflops != nullptr, "outputs must be non-null");
+        check_cuda(measure_simt_peaks(fp32_tflops, fp64_tflops), "SIMT peak measurement");
+    });
 }
 
 // ------------------------------------------------------------------- model

@@ -185,6 +185,14 @@ def synchronize():
     check(library().skb_device_synchronize())
 
 
+def simt_peaks():
+    """Measured FP32 and FP64 SIMT FMA throughput of the current device,
+    (fp32_tflops, fp64_tflops)."""
+    f32, f64 = ctypes.c_double(), ctypes.c_double()
+    check(library().skb_measure_simt_peaks(ctypes.byref(f32), ctypes.byref(f64)))
+    return f32.value, f64.value
+
+
 # ------------------------------------------------------------------ model
 
 def retained_modes(w: Workload):
