@@ -497,6 +497,17 @@ def serving_run(S, mode, rate, requests, batch, states_per_class, dist, classes_
     two modes see the same requests at the same times."""
     mix = classes_mix or SERVE_CLASSES
     classes = [(n, nz, t, batch, mode) for n, nz, t, _ in mix]
+    # The slots' pipelines take their launch shapes from the project tuning
+    # cache: tune each class once, at the slots' batch size, before serving.
+    for n, nz, t, _ in mix:
+        f = S.Flux(n, nz, targets=t, members=batch, mode=mode)
+        dtype = f.device_dtype
+        din = S.DeviceArray.from_numpy(power_law_inputs(n, nz, batch, targets=t, seed=31).astype(dtype))
+        dout = S.DeviceArray(f.output_elements * np.dtype(dtype).itemsize)
+        f.autotune(din.ptr, dout.ptr)
+        f.close()
+        din.free()
+        dout.free()
     server = S.Server(classes, hbm_budget_bytes=64 << 30, max_slots_per_class=2)
     states = []
     for c, (n, nz, t, _) in enumerate(mix):
