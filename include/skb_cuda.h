@@ -409,6 +409,15 @@ SKB_API int skb_flux_profile(skb_flux* p, const void* modal_input, void* modal_o
  * this handle expired since creation (the kernel then skipped its work and
  * released its tensor memory instead of hanging). */
 SKB_API int skb_flux_check_device(skb_flux* p);
+/* Test of the fused row kernel's failure path (no counterpart in the
+ * reference).  With enable != 0, later launches of the row kernel's TMA forms
+ * (the autotuner's flux.rows.tma = 1 or 2) make thread 0 of every CTA wait,
+ * once its first stage copy has landed, on a barrier nothing signals.  The
+ * wait is bounded (a short limit), so it runs out: every thread of the CTA
+ * leaves, the kernel's error word is set, and skb_flux_check_device reports
+ * SKB_ERR_RUNTIME.  Other row-kernel forms ignore the flag.  Executions that
+ * are not already captured in a graph pick it up. */
+SKB_API int skb_flux_rows_expire_wait_for_test(skb_flux* p, int enable);
 /* Capture execute_device on these buffers into a CUDA graph and replay it. */
 SKB_API int skb_flux_capture_graph(skb_flux* p, const void* modal_input, void* modal_output);
 SKB_API int skb_flux_replay_graph(skb_flux* p, void* stream);

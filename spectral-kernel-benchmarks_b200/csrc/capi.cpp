@@ -1764,6 +1764,13 @@ int skb_flux_check_device(skb_flux* p) {
     });
 }
 
+int skb_flux_rows_expire_wait_for_test(skb_flux* p, int enable) {
+    return guard([&] {
+        require(p != nullptr, "handle must be non-null");
+        p->pipeline->set_rows_expire_wait_for_test(enable != 0);
+    });
+}
+
 int skb_flux_capture_graph(skb_flux* p, const void* in, void* out) {
     return guard([&] {
         require(p && in && out, "handle and buffers must be non-null");

@@ -372,6 +372,7 @@ RowFluxArgs FluxPipeline::row_args(std::uint64_t members) const {
     a.pairs = rowsPairs_;
     a.tma = rowsTma_;
     a.error = static_cast<int*>(rowsError_.get());
+    a.expireWaitForTest = rowsExpireWaitForTest_ ? 1 : 0;
     return a;
 }
 

@@ -77,6 +77,8 @@ public:
     double tunedSeconds = 0.0;
     // Raises if a bounded device wait inside a tensor-core kernel expired.
     void check_device_errors() const;
+    // Failure-path test of the row kernel's TMA forms (RowFluxArgs::expireWaitForTest).
+    void set_rows_expire_wait_for_test(bool enable) { rowsExpireWaitForTest_ = enable; }
     void replay(cudaStream_t s);
 
     std::uint64_t modes() const { return modes_; }
@@ -134,6 +136,7 @@ private:
     int rowsPlanes_ = 8;  // z-planes per CTA of the fused row kernel
     int rowsPairs_ = 0;   // 512-point rows: two planes per warp (RowFluxArgs::pairs)
     int rowsTma_ = 0;     // two-planes-per-warp rows: stages filled by TMA tensor copies (RowFluxArgs::tma)
+    bool rowsExpireWaitForTest_ = false;  // RowFluxArgs::expireWaitForTest
     DeviceBuffer rowsError_;  // set by the fused row kernel when a bounded wait expires
     void run(const void* modalIn, void* modalOut, cudaStream_t s, Recorder* rec, std::uint64_t members);
     cudaGraph_t graph_ = nullptr;

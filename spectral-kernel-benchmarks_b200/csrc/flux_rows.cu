@@ -377,8 +377,8 @@ __device__ __forceinline__ unsigned smem_addr(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
 // A bounded wait on an mbarrier phase (false once the limit is reached).
-__device__ __forceinline__ bool stage_wait(unsigned bar, unsigned parity) {
-    for (long long i = 0; i < (1LL << 22); ++i) {
+__device__ __forceinline__ bool stage_wait(unsigned bar, unsigned parity, long long limit = 1LL << 22) {
+    for (long long i = 0; i < limit; ++i) {
         unsigned ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -412,6 +412,7 @@ __global__ void __launch_bounds__(16 * B, MINB)
     constexpr int KP = pair_stage_row<B>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long stageFull[NST];
+    __shared__ __align__(8) unsigned long long never;  // nothing arrives on it (expired-wait test)
     const int keep = a.keep;
     unsigned char* tmaBase =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -457,6 +458,7 @@ __global__ void __launch_bounds__(16 * B, MINB)
         if (tid == 0) {
             for (int i = 0; i < NST; ++i)
                 asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&stageFull[i])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&never)) : "memory");
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
     } else {
@@ -508,7 +510,12 @@ __global__ void __launch_bounds__(16 * B, MINB)
     // false if the TMA form's wait for the slot's copy expired.
     auto inverse_row = [&](int f, V (&r)[16]) -> bool {
         if constexpr (TMA) {
-            const bool ok = tid != 0 || stage_wait(smem_addr(&stageFull[f % NST]), (f / NST) & 1);
+            bool ok = tid != 0 || stage_wait(smem_addr(&stageFull[f % NST]), (f / NST) & 1);
+            // Expired-wait test: once slot 0's copy has landed (no copy is then
+            // in flight), a short bounded wait on a barrier nothing signals
+            // runs out and takes the path of any expired wait.
+            if (tid == 0 && ok && f == 0 && a.expireWaitForTest != 0)
+                ok = stage_wait(smem_addr(&never), 0, 1LL << 14);
             if (!__syncthreads_and(ok)) {
                 if (tid == 0 && a.error != nullptr) atomicExch(a.error, 1);
                 return false;

@@ -27,6 +27,9 @@ struct RowFluxArgs {
     // `error`).
     int tma = 0;
     int* error = nullptr;  // device word set to 1 when a bounded wait expires
+    // Test of the failure path (TMA forms): thread 0 of every CTA also waits,
+    // briefly and bounded, on a barrier nothing signals, after slot 0's copy.
+    int expireWaitForTest = 0;
 };
 
 bool rows_flux_supported(long long nx);

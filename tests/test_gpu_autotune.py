@@ -129,3 +129,35 @@ def test_every_row_kernel_width_is_correct(n, planes, pairs, tma):
     assert orc.rel_l2_error(_run(flux, x), _fp64(n, nz, members, x)) <= 1e-6
     flux.check_device()
     skb_cuda.tune_cache_clear()
+
+
+def test_row_kernel_expired_wait_is_reported_and_the_context_survives():
+    """The fused row kernel's TMA forms bound the wait for each stage copy:
+    with the test flag, thread 0 also waits on a barrier nothing signals, the
+    wait runs out, the flux reports SKB_ERR_RUNTIME instead of hanging, and a
+    new handle on the same context computes correctly."""
+    import ctypes
+
+    skb_cuda.tune_cache_clear()
+    n, nz, members = 512, 9, 1
+    probe = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    x = _inputs(probe, 41)
+    d_in = skb_cuda.DeviceArray.from_numpy(x)
+    d_out = skb_cuda.DeviceArray(probe.output_elements * 8)
+    chosen = probe.autotune(d_in.ptr, d_out.ptr)
+    probe.close()
+    pair_keys = [k for k in chosen if k.startswith("flux.rows.pairs ")]
+    assert len(pair_keys) == 1
+    skb_cuda.tune_cache_store(pair_keys[0], 2, 0.0)
+    skb_cuda.tune_cache_store(pair_keys[0].replace("flux.rows.pairs", "flux.rows.tma", 1), 1, 0.0)
+    skb_cuda.tune_cache_store(pair_keys[0].replace("flux.rows.pairs", "flux.rows.planes_per_cta", 1), 8, 0.0)
+    flux = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    skb_cuda.check(skb_cuda.library().skb_flux_rows_expire_wait_for_test(flux.h, ctypes.c_int(1)))
+    _run(flux, x)
+    with pytest.raises(RuntimeError, match="bounded wait"):
+        flux.check_device()
+    flux.close()
+    fresh = skb_cuda.Flux(n, nz, members=members, mode=skb_cuda.FLUX_SPLIT_TF32X3)
+    assert orc.rel_l2_error(_run(fresh, x), _fp64(n, nz, members, x)) <= 1e-6
+    fresh.check_device()
+    skb_cuda.tune_cache_clear()
