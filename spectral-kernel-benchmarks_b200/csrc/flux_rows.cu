@@ -361,10 +361,17 @@ template <int B>
 constexpr size_t tma_stage_bytes() {
     return (size_t(kTmaRows) * B * 8 + 1023) / 1024 * 1024;
 }
-template <int B, int NS>
+// W_SMEM: the third velocity row W is kept in a lane-private shared region
+// (16 values per thread) instead of registers.
+template <int B, int MINB, int NS>
+constexpr bool pair_w_in_smem() {
+    return B == 8 && MINB == 3 && NS == 2;
+}
+template <int B, int NS, bool WSM = false>
 constexpr size_t pair_tma_smem_bytes(int keep) {
     return 1024 + NS * tma_stage_bytes<B>() +
-           sizeof(float2) * (size_t(B) * kPairXch + size_t(keep) * out_row<B>() + kPairM + kPairM);
+           sizeof(float2) * (size_t(B) * kPairXch + size_t(keep) * out_row<B>() + kPairM + kPairM +
+                             (WSM ? size_t(16) * 16 * B : 0));
 }
 // Byte offset of (kx k, plane b) in a swizzled TMA stage.
 template <int B>
@@ -427,6 +434,11 @@ __global__ void __launch_bounds__(16 * B, MINB)
     V* outTile = xchAll + B * kPairXch;  // [k][b] at out_slot(k, b)
     V* tf = outTile + keep * out_row<B>();  // twFull[0..M)
     V* tw2 = tf + M;                     // tw2[16 k2 + t] = twHalf[(t k2) mod M]
+    // Three-CTA two-stage TMA form: W (16 values per thread) lives here, at
+    // wsm[16 * e ... ] + tid, which takes the register peak of u, v, w, the
+    // product and the current derivative under the 168-register bound.
+    constexpr bool WSM = pair_w_in_smem<B, MINB, NS>();
+    V* wsm = tw2 + M;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int t = lane & 15;
@@ -563,6 +575,10 @@ __global__ void __launch_bounds__(16 * B, MINB)
     for (int f = 0; f < NST - 1 && f < a.fieldsIn; ++f) issue(f);
     V u[16], v[16], w[16];
     if (!inverse_row(0, u) || !inverse_row(1, v) || !inverse_row(2, w)) return;
+    if constexpr (WSM) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) wsm[e * NT + tid] = w[e];
+    }
     const float scale = a.scale;
     const int src = ((16 - t) & 15) + (lane & 16);  // lane holding Z[M - k]
     for (int tg = 0; tg < a.targets; ++tg) {
@@ -575,8 +591,10 @@ __global__ void __launch_bounds__(16 * B, MINB)
         for (int e = 0; e < 16; ++e) acc[e] = {acc[e].x + v[e].x * q[e].x, acc[e].y + v[e].y * q[e].y};
         if (!inverse_row(5 + 3 * tg, q)) return;
 #pragma unroll
-        for (int e = 0; e < 16; ++e)
-            acc[e] = {-scale * (acc[e].x + w[e].x * q[e].x), -scale * (acc[e].y + w[e].y * q[e].y)};
+        for (int e = 0; e < 16; ++e) {
+            const V we = WSM ? wsm[e * NT + tid] : w[e];
+            acc[e] = {-scale * (acc[e].x + we.x * q[e].x), -scale * (acc[e].y + we.y * q[e].y)};
+        }
         fft256_pair<-1>(acc, xch, tw2, t);
         // Real-spectrum split, kx < keep, into [k][b].  Z[M - k] for k = t + 16 k1
         // is register 15 - k1 of lane 16 - t (t > 0) or register (16 - k1) mod 16
@@ -625,7 +643,7 @@ cudaError_t launch_pair(const RowFluxArgs& a, cudaStream_t stream) {
                                   static_cast<unsigned long long>(a.ny) * a.binsIn.kxStride,
                                   static_cast<unsigned long long>(a.binsIn.planes) * 8, B, a.keep);
         if (merr != cudaSuccess) return merr;
-        bytes = pair_tma_smem_bytes<B, NS>(a.keep);
+        bytes = pair_tma_smem_bytes<B, NS, pair_w_in_smem<B, MINB, NS>()>(a.keep);
     }
     const cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
     if (err != cudaSuccess) return err;
