@@ -1590,7 +1590,7 @@ int run(int argc, char** argv) {
     if (!o.fluxFixture.empty() && o.kernel != "production-lifetime-flux")
         throw std::invalid_argument("--spectral-flux-fixture is valid only for production-lifetime-flux.");
     if (o.providers != "cuda" && o.providers != "both")
-        throw std::invalid_argument("providers must be 'cuda' (this build provides no other).");
+        throw std::invalid_argument("providers must be 'cuda' (this binary provides no other).");
     const auto prof = profile_named(o.profile);
     skb_workload w = prof.w;
     if (o.nx) w.nx = o.nx;

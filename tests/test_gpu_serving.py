@@ -1,4 +1,4 @@
-"""GPU tests of the continuous-batching request loop (serving).
+"""GPU tests of the continuous-batching request loop (serving, the mixed-size request benchmark).
 
 The contract under test: requests of mixed grid sizes arrive while others run,
 join the next batch of their class, and each result equals the same request
